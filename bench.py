@@ -1,0 +1,371 @@
+"""Benchmark of the differentiable render path on one B200 (render-only kernel benchmark
+configuration): 1,000,000 Gaussians, one 1920x1080 view, 16x16 tiles, plain FP32 forward
+and backward with an upstream dL/dpixel drawn N(0,1) per channel.
+
+One step = projection + binning (scan, key emission, radix sort, tile ranges) +
+compositing forward + compositing backward + projection backward for that view. The metric
+is megapixels per second of forward+backward (W*H per step). Inputs are larger than L2 (the
+parameter planes alone are 240 MB), so no L2 flush is needed between steps.
+
+Usage:
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+Under torchrun every rank runs an independent replica of the workload (the path does not
+shard across views in this configuration); the slowest rank's time is reported.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WIDTH, HEIGHT = 1920, 1080
+METRIC = "train iters/s and Mpix/s fwd+bwd at 1 B200 vs plain GPU & CPU, at matched PSNR"
+UNIT = "Mpix/s"
+WORKLOAD = "render fwd+bwd, 1M Gaussians, 1920x1080, 16x16 tiles, SH degree 3, dL/dpix ~ N(0,1)"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--n", type=int, default=1_000_000)
+    ap.add_argument("--cpu-steps", type=int, default=3, help="steps of the CPU baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-small", action="store_true",
+                    help="a reduced case for ncu captures (fewer Gaussians, one step)")
+    return ap.parse_args()
+
+
+def dist_info():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = max(mx, float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+# Algorithmic work per unit (fixed constants): bytes for the HBM-bound stages.
+PROJ_FWD_BYTES = 236 + 64          # parameters read + projection record written, per Gaussian
+PROJ_BWD_BYTES = 236 + 36 + 236    # parameters + screen gradients read, parameter gradients written
+SORT_BYTES_PER_KEY_PASS = 24       # one read and one write of a (u64 key, u32 value) pair
+EMIT_BYTES_PER_ENTRY = 12          # key + value written
+RASTER_FWD_BYTES_PER_PIXEL = 20    # image (12) + final T (4) + n_contrib (4) written
+RASTER_BWD_BYTES_PER_PIXEL = 20    # dL/dpix (12) + final T (4) + n_contrib (4) read
+RASTER_BYTES_PER_ENTRY = 52        # sorted index (4) + record gather (48)
+RASTER_FWD_FLOP_PER_PAIR = 20
+RASTER_BWD_FLOP_PER_PAIR = 50
+
+
+def run_ours(args, rank, world, local):
+    import torch
+    from splatrs_b200 import gpu as G
+    from splatrs_b200 import scenes
+    from splatrs_b200._lib import Camera, ProjOpts
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    n = args.n
+    s = scenes.config1(n=n)
+    cam = Camera.from_record(s["cam"])
+    opts = ProjOpts.make(sh_degree=3)
+    bg = s["background"]
+    stream = torch.cuda.current_stream(dev)
+    ctx = G.Context(local, stream)
+
+    params = torch.from_numpy(s["params"]).to(dev)
+    planes = G.params_to_planes(ctx, params)
+    dimage = torch.from_numpy(s["dimage"]).to(dev)
+    pgrad = torch.zeros((3, n, 4), dtype=torch.float32, device=dev)
+    del params
+
+    # Stage-level step with events between stages.
+    def full_step(ev=None):
+        def mark(i):
+            if ev is not None:
+                ev[i].record(stream)
+        mark(0)
+        proj = G.project_all(ctx, planes, n, n, cam, opts)
+        mark(1)
+        b = G.bin(ctx, proj)
+        mark(2)
+        out = G.rasterize_forward(ctx, proj, b, bg)
+        mark(3)
+        ctx.zero(pgrad)
+        G.rasterize_backward(ctx, proj, b, bg, out, dimage, pgrad=pgrad, cap=n)
+        mark(4)
+        G.project_backward_all(ctx, planes, n, n, cam, opts, proj, pgrad)
+        mark(5)
+        return proj, b, out
+
+    # Counters from one untimed step: entries, pairs.
+    proj, b, out = full_step()
+    pairs_fwd = int(out.pairs.item())
+    pp = torch.zeros(1, dtype=torch.int64, device=dev)
+    ctx.zero(pgrad)
+    G.rasterize_backward(ctx, proj, b, bg, out, dimage, pgrad=pgrad, cap=n, pairs=pp)
+    pairs_bwd = int(pp.item())
+    entries = b.num_entries
+    visible = int((proj.num_tiles > 0).sum().item())
+    torch.cuda.synchronize(dev)
+
+    for _ in range(args.warmup):
+        full_step()
+    torch.cuda.synchronize(dev)
+
+    import torch.distributed as dist
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    sampler = ClockSampler(local)
+    sampler.start()
+    launches0 = ctx.launches
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(6)] for _ in range(args.steps)]
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for k in range(args.steps):
+        full_step(ev[k])
+    t1.record(stream)
+    torch.cuda.synchronize(dev)
+    launches = ctx.launches - launches0
+    clocks = sampler.stop()
+    elapsed_ms = t0.elapsed_time(t1)
+    if world > 1:
+        tt = torch.tensor([elapsed_ms], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        elapsed_ms = float(tt.item())
+        dist.barrier()
+    stage_ms = {nm: 0.0 for nm in ["project_fwd", "bin", "raster_fwd", "raster_bwd", "project_bwd"]}
+    for k in range(args.steps):
+        e = ev[k]
+        stage_ms["project_fwd"] += e[0].elapsed_time(e[1])
+        stage_ms["bin"] += e[1].elapsed_time(e[2])
+        stage_ms["raster_fwd"] += e[2].elapsed_time(e[3])
+        stage_ms["raster_bwd"] += e[3].elapsed_time(e[4])
+        stage_ms["project_bwd"] += e[4].elapsed_time(e[5])
+    for k in stage_ms:
+        stage_ms[k] /= args.steps
+    ms_per_step = elapsed_ms / args.steps
+    mpix = WIDTH * HEIGHT / 1e6
+    value = mpix * world / (ms_per_step / 1e3)
+
+    # End to end through the host-buffer C ABI call (splat_renderer_render_backward): the
+    # model is resident (uploaded once, as a loaded model is); each step uploads dL/dpix
+    # from pinned memory and downloads the image and the 59 parameter gradients.
+    r = G.Renderer(ctx)
+    r.set_model(s["params"], 3)
+    dimage_h = torch.from_numpy(s["dimage"]).pin_memory().numpy()
+    img_h = torch.empty(WIDTH * HEIGHT * 3, dtype=torch.float32).pin_memory().numpy()
+    grads_h = torch.empty((n, 59), dtype=torch.float32).pin_memory().numpy()
+    for _ in range(max(1, args.warmup)):
+        r.render_backward(cam, opts, bg, dimage_h, img_h, grads_h)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    e_steps = max(3, args.steps // 2)
+    tw = time.perf_counter()
+    for _ in range(e_steps):
+        r.render_backward(cam, opts, bg, dimage_h, img_h, grads_h)
+    e2e_ms = (time.perf_counter() - tw) * 1e3 / e_steps
+    if world > 1:
+        tt = torch.tensor([e2e_ms], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_ms = float(tt.item())
+    r.close()
+    e2e = {"value": round(mpix * world / (e2e_ms / 1e3), 3), "unit": UNIT,
+           "h2d_bytes_per_step": int(dimage_h.nbytes), "d2h_bytes_per_step": int(img_h.nbytes + grads_h.nbytes),
+           "ms_per_step": round(e2e_ms, 3), "api": "splat_renderer_render_backward"}
+
+    # Roofline of the dominant kernel.
+    hbm_peak, peak_kind = measured_peaks()
+    dom = max(stage_ms, key=stage_ms.get)
+    sort_passes = None
+    if dom in ("raster_fwd", "raster_bwd"):
+        byts = (RASTER_FWD_BYTES_PER_PIXEL if dom == "raster_fwd" else RASTER_BWD_BYTES_PER_PIXEL) * WIDTH * HEIGHT \
+               + RASTER_BYTES_PER_ENTRY * entries
+    elif dom == "project_fwd":
+        byts = PROJ_FWD_BYTES * n
+    elif dom == "project_bwd":
+        byts = PROJ_BWD_BYTES * n
+    else:
+        byts = (EMIT_BYTES_PER_ENTRY + SORT_BYTES_PER_KEY_PASS) * entries
+    achieved = byts / (stage_ms[dom] / 1e3) / 1e9
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
+                "frac": round(achieved / hbm_peak, 4), "traffic": None, "peak_source": peak_kind,
+                "algorithmic_bytes_per_launch": int(byts)}
+    flops = {"raster_fwd": RASTER_FWD_FLOP_PER_PAIR * pairs_fwd, "raster_bwd": RASTER_BWD_FLOP_PER_PAIR * pairs_bwd}
+    compute = {k: {"pairs": p, "flop": flops[k], "ms": round(stage_ms[k], 4),
+                   "tflops": round(flops[k] / (stage_ms[k] / 1e3) / 1e12, 3),
+                   "ns_per_pair": round(stage_ms[k] * 1e6 / max(p, 1), 4)}
+               for k, p in (("raster_fwd", pairs_fwd), ("raster_bwd", pairs_bwd))}
+    hbm_stages = {
+        "project_fwd": PROJ_FWD_BYTES * n, "project_bwd": PROJ_BWD_BYTES * n,
+    }
+    stage_hbm = {k: {"ms": round(stage_ms[k], 4), "gbs": round(v / (stage_ms[k] / 1e3) / 1e9, 1),
+                     "frac": round(v / (stage_ms[k] / 1e3) / 1e9 / hbm_peak, 4)} for k, v in hbm_stages.items()}
+
+    line = {
+        "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded; config-1 distributions)",
+        "config": {"workload": WORKLOAD, "gaussians": n, "width": WIDTH, "height": HEIGHT, "tile": 16,
+                   "l2": "inputs larger than L2 (240 MB parameter planes), no flush", "parallelism": f"replicas x{world}"},
+        "iters_per_s": round(1e3 / ms_per_step, 3),
+        "stages_ms": {k: round(v, 4) for k, v in stage_ms.items()},
+        "entries": entries, "visible": visible, "sort_keys_per_s": round(entries / (stage_ms["bin"] / 1e3), 1),
+        "pairs": {"fwd": pairs_fwd, "bwd": pairs_bwd},
+        "e2e": e2e, "gpu_launches": int(launches), "roofline": roofline, "compute": compute, "hbm_stages": stage_hbm,
+        "clocks": clocks,
+    }
+    ctx.close()
+    return line
+
+
+def cpu_reference_steps(args, steps):
+    """The CPU oracle (the reference's hot path restated in C++, all host threads) on the
+    same workload: `steps` full forward+backward passes of the 1920x1080 view."""
+    from oracle import oracle as O
+    from splatrs_b200 import scenes
+    s = scenes.config1(n=args.n)
+    p, cam, dimage = s["params"], s["cam"], s["dimage"]
+    bg = np.zeros(3, np.float32)
+
+    def one():
+        projs = O.project_all(p, cam, sh_degree=3)
+        b = O.bin(projs, WIDTH, HEIGHT)
+        img, ft, nc, _ = O.rasterize_forward(projs, b, WIDTH, HEIGHT, bg)
+        g, a, _ = O.rasterize_backward(projs, b, WIDTH, HEIGHT, bg, ft, nc, dimage)
+        O.project_backward_all(p, cam, g, sh_degree=3)
+
+    one()  # warm caches and thread pool
+    t = time.perf_counter()
+    for _ in range(steps):
+        one()
+    dt = (time.perf_counter() - t) / steps
+    return dt, O.threads()
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_info()
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    if args.profile_small:
+        args.n = 200_000
+        args.steps = 1
+        args.warmup = 1
+        args.no_cpu_baseline = True
+
+    if args.impl == "reference":
+        if rank == 0:
+            steps = max(1, args.steps if args.steps <= 5 else 3)
+            dt, cores = cpu_reference_steps(args, steps)
+            v = WIDTH * HEIGHT / 1e6 / dt
+            line = {"impl": "reference", "metric": METRIC, "value": round(v, 4), "unit": UNIT, "n_gpus": world,
+                    "steps": steps, "warmup": 1, "ms_per_step": round(dt * 1e3, 2), "higher_is_better": True,
+                    "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                    "data": "synthetic (seeded; config-1 distributions)",
+                    "config": {"workload": WORKLOAD, "gaussians": args.n, "width": WIDTH, "height": HEIGHT},
+                    "cpu_baseline": {"value": round(v, 4), "unit": UNIT, "cores": cores, "kind": "port",
+                                     "sample": f"{steps} full fwd+bwd steps of the workload"},
+                    "e2e": {"value": round(v, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            print(json.dumps(line), flush=True)
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+
+    line = run_ours(args, rank, world, local)
+    if rank == 0:
+        if not args.no_cpu_baseline and world == 1:
+            dt, cores = cpu_reference_steps(args, args.cpu_steps)
+            line["cpu_baseline"] = {"value": round(WIDTH * HEIGHT / 1e6 / dt, 4), "unit": UNIT, "cores": cores,
+                                    "kind": "port", "sample": f"{args.cpu_steps} full fwd+bwd steps of the workload"}
+        elif world > 1:
+            line["cpu_baseline"] = None
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,241 @@
+/*
+ * splat_gpu.h: the C ABI of the B200 (sm_100a) render-and-train path for 3D Gaussian
+ * splatting.
+ *
+ * The reference implementation (harryprayiv/splatrs) is a pure-Rust CPU crate with no FFI
+ * today (`#![forbid(unsafe_code)]`, src/lib.rs:13). These entry points are what its
+ * functions would bind to, one per reference function, named in each comment. Plain C
+ * types only: pointers, sizes, POD structs. No C++ or torch types cross this boundary.
+ *
+ * Conventions
+ *  - Every entry point returns an int status (SPLAT_OK on success) and never aborts. The
+ *    message of the last failure on a context is available from splat_last_error().
+ *  - Pointers whose name ends in `_dev` are device pointers (cudaMalloc'd or any device
+ *    allocation on the context's device); `_host` pointers are host memory (pinned or
+ *    pageable). The stage functions are asynchronous on the context's stream unless their
+ *    comment says they synchronise (they do only to read a count back, as the reference's
+ *    `Vec` sizes require).
+ *  - A context is used from one host thread at a time. Separate contexts may run
+ *    concurrently on separate streams.
+ *
+ * Device layouts
+ *  - Parameter planes (`planes_dev`): SPLAT_PLANES planes of float4, plane p at
+ *    planes_dev + 4*p*cap floats, element i of plane p holds:
+ *        plane 0: mean.x mean.y mean.z opacity(logit)
+ *        plane 1: quat w x y z (unnormalised)
+ *        plane 2: log_scale x y z, 0
+ *        plane 3+q (q = 0..11): sh coefficients j = 4q..4q+3 where j = 3*k + channel
+ *    Gradients and Adam moments use the same layout. Each warp-wide load of a plane is one
+ *    contiguous 512-byte transaction.
+ *  - Reference Gaussian record (`aos59`): 59 floats = mean[3] log_scale[3] quat[4]
+ *    opacity sh[16][3] (reference src/model.rs:16-28), the layout the .ply codec and a
+ *    Rust `&[Gaussian]` hand over.
+ *  - Projection record (`proj_dev`): 16 floats per Gaussian (see SPLAT_PROJ_FLOATS),
+ *    produced by splat_project_fwd or splat_proj_from_reference and consumed by the
+ *    binning, compositing and projection-backward stages.
+ *  - Reference projection record (`proj15`): 15 floats = mean2d[2] conic[3] depth radius
+ *    opacity color[3] tile_min[2] tile_max[2] with the integers stored as exact floats
+ *    (reference src/project.rs:47-64).
+ *  - Screen-space gradients (`pgrad_dev`): 3 planes of float4 with stride cap:
+ *        (d mean2d.x, d mean2d.y, d conic.A, d conic.B), (d conic.C, d opacity, d r, d g),
+ *        (d b, |d mean2d.x| sum, |d mean2d.y| sum, 0)
+ *    i.e. ProjGrad plus the AbsGS accumulators (reference src/project.rs:84-93,
+ *    src/rasterize.rs:339-341).
+ *  - Images are row-major H x W x 3 float (reference src/rasterize.rs:43-50).
+ */
+#ifndef SPLAT_GPU_H
+#define SPLAT_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SPLAT_API __attribute__((visibility("default")))
+
+/* Status codes. */
+#define SPLAT_OK 0
+#define SPLAT_ERR_INVALID 1   /* bad argument; the reference panics or returns Error::Invalid */
+#define SPLAT_ERR_CAPACITY 2  /* a fixed-capacity buffer is too small; retry with a larger one */
+#define SPLAT_ERR_CUDA 3      /* a CUDA runtime call failed */
+#define SPLAT_ERR_TIMEOUT 4   /* a bounded device wait ran out */
+
+#define SPLAT_PLANES 15
+#define SPLAT_PROJ_FLOATS 16
+#define SPLAT_TILE 16
+
+/* Pinhole camera with COLMAP conventions (reference src/camera.rs:13-32). */
+typedef struct splat_camera {
+  uint32_t width, height;
+  float fx, fy, cx, cy;
+  float rot[9];   /* world-to-camera rotation, row major */
+  float trans[3]; /* world-to-camera translation */
+} splat_camera;
+
+/* Projection options (reference src/project.rs:22-43). */
+typedef struct splat_proj_opts {
+  float near_plane; /* 0.2 */
+  float eps2d;      /* 0.3 */
+  int32_t antialias;
+  int32_t sh_degree;
+} splat_proj_opts;
+
+/* Per-group learning rates (reference src/adam.rs:11-24). */
+typedef struct splat_lr {
+  float mean, log_scale, quat, opacity, sh_dc, sh_rest;
+} splat_lr;
+
+/* Densification thresholds (reference src/densify.rs:69-103). */
+typedef struct splat_densify_config {
+  float grad_threshold;      /* 0.0002 */
+  float percent_dense;       /* 0.01 */
+  float min_opacity;         /* 0.005 */
+  int32_t prune_big_world;   /* 0 */
+  float max_world_size_frac; /* 0.1 */
+  int64_t max_screen_size;   /* < 0 means None */
+  int32_t split_children;    /* 2 */
+} splat_densify_config;
+
+/* Training hyperparameters (reference src/train.rs:20-109). */
+typedef struct splat_train_config {
+  uint32_t iterations;
+  float position_lr_init, position_lr_final;
+  uint32_t position_lr_max_steps;
+  float feature_lr, opacity_lr, scaling_lr, rotation_lr, lambda_dssim;
+  int32_t densify;
+  uint32_t densify_from_iter, densify_until_iter, densification_interval, opacity_reset_interval;
+  float densify_grad_threshold, percent_dense, min_opacity;
+  int64_t max_screen_size; /* < 0 means None */
+  int32_t absgrad, antialias, white_background, sh_degree;
+  uint32_t sh_degree_interval;
+  float near_plane;
+  uint64_t seed;
+} splat_train_config;
+
+typedef struct splat_ctx splat_ctx;
+
+/* ----------------------------------------------------------------------------------------
+ * Context: device, stream, scratch arena, error message.
+ * -------------------------------------------------------------------------------------- */
+/* `stream` is a cudaStream_t (NULL for the legacy default stream). */
+SPLAT_API int splat_ctx_create(int device, void* stream, splat_ctx** out);
+SPLAT_API int splat_ctx_destroy(splat_ctx* ctx);
+SPLAT_API int splat_ctx_set_stream(splat_ctx* ctx, void* stream);
+SPLAT_API int splat_ctx_synchronize(splat_ctx* ctx);
+SPLAT_API const char* splat_last_error(const splat_ctx* ctx);
+SPLAT_API const char* splat_status_string(int status);
+SPLAT_API int splat_version(void);
+/* Kernels launched through this context since creation (all stage entry points count). */
+SPLAT_API uint64_t splat_ctx_launch_count(const splat_ctx* ctx);
+
+/* ----------------------------------------------------------------------------------------
+ * Parameter layout conversion (reference Gaussian records <-> planes).
+ * -------------------------------------------------------------------------------------- */
+SPLAT_API int splat_params_from_aos(splat_ctx* ctx, const float* aos59_dev, int64_t n, float* planes_dev,
+                                    int64_t cap);
+SPLAT_API int splat_params_to_aos(splat_ctx* ctx, const float* planes_dev, int64_t n, int64_t cap,
+                                  float* aos59_dev);
+
+/* ----------------------------------------------------------------------------------------
+ * Projection: project_all (reference src/project.rs:320-330, project_one :277-317,
+ * core :137-269). Writes n projection records and n per-Gaussian tile counts
+ * (Proj::num_tiles, :73-79). `depth_range_dev` (2 x uint32) receives the min and max
+ * float bits of the visible depths; it is reset by this call.
+ * -------------------------------------------------------------------------------------- */
+SPLAT_API int splat_project_fwd(splat_ctx* ctx, const float* planes_dev, int64_t n, int64_t cap,
+                                const splat_camera* cam, const splat_proj_opts* opts, float* proj_dev,
+                                uint32_t* num_tiles_dev, uint32_t* depth_range_dev);
+
+/* Build projection records from reference-layout Proj records (proj15, device), e.g. to
+ * bin and composite projections made elsewhere. Also writes tile counts and depth range. */
+SPLAT_API int splat_proj_from_reference(splat_ctx* ctx, const float* proj15_dev, int64_t n, uint32_t width,
+                                        uint32_t height, float* proj_dev, uint32_t* num_tiles_dev,
+                                        uint32_t* depth_range_dev);
+
+/* Reference-layout Proj records (proj15, device) from projection records. */
+SPLAT_API int splat_proj_to_reference(splat_ctx* ctx, const float* proj_dev, int64_t n, float* proj15_dev);
+
+/* ----------------------------------------------------------------------------------------
+ * Binning: bin (reference src/rasterize.rs:60-128), in two calls.
+ * splat_bin_count: exclusive scan of the tile counts into entry_offset_dev (n + 1 values,
+ * Binning::entry_offset) and the number of entries. Synchronises to return the count and
+ * the depth range used by splat_bin_sort.
+ * splat_bin_sort: emits one (tile | depth) key per (Gaussian, tile) in Gaussian order,
+ * radix-sorts them stably (ties keep entry order, as the reference's (key, entry) sort
+ * does) and writes, for every sorted entry, its Gaussian index (gauss_dev), its 64-bit
+ * reference key (keys_dev, optional: may be NULL) and the [start, end) range of every
+ * tile (tile_range_dev, 2 x uint32 per tile, Binning::tile_range).
+ * -------------------------------------------------------------------------------------- */
+SPLAT_API int splat_bin_count(splat_ctx* ctx, const uint32_t* num_tiles_dev, int64_t n,
+                              uint32_t* entry_offset_dev, int64_t* num_entries);
+SPLAT_API int splat_bin_sort(splat_ctx* ctx, const float* proj_dev, const uint32_t* entry_offset_dev, int64_t n,
+                             int64_t num_entries, const uint32_t* depth_range_dev, uint32_t width, uint32_t height,
+                             uint32_t* gauss_dev, uint64_t* keys_dev, uint32_t* tile_range_dev);
+
+/* ----------------------------------------------------------------------------------------
+ * Compositing forward: rasterize_forward (reference src/rasterize.rs:305-337,
+ * forward_tile :249-302). Writes image (H*W*3), final transmittance (H*W) and n_contrib
+ * (H*W). `pairs_dev` (optional, 1 x uint64, accumulated) counts evaluated (entry, pixel)
+ * pairs.
+ * -------------------------------------------------------------------------------------- */
+SPLAT_API int splat_rasterize_fwd(splat_ctx* ctx, const float* proj_dev, const uint32_t* gauss_dev,
+                                  const uint32_t* tile_range_dev, uint32_t width, uint32_t height,
+                                  const float background[3], float* image_dev, float* final_t_dev,
+                                  uint32_t* n_contrib_dev, uint64_t* pairs_dev);
+
+/* Compositing backward: rasterize_backward (reference src/rasterize.rs:459-505,
+ * backward_tile :354-455). Accumulates into pgrad_dev (3 planes, stride cap), which the
+ * caller zeroes (splat_zero) before the first view whose gradients it wants. */
+SPLAT_API int splat_rasterize_bwd(splat_ctx* ctx, const float* proj_dev, const uint32_t* gauss_dev,
+                                  const uint32_t* tile_range_dev, uint32_t width, uint32_t height,
+                                  const float background[3], const float* final_t_dev,
+                                  const uint32_t* n_contrib_dev, const float* dimage_dev, float* pgrad_dev,
+                                  int64_t cap, uint64_t* pairs_dev);
+
+/* ----------------------------------------------------------------------------------------
+ * Projection backward: project_backward_all (reference src/project.rs:477-493,
+ * project_backward_one :335-474). Writes the 59 parameter gradients into grad_planes_dev
+ * (parameter-plane layout). If `stats_dev` is not NULL it also performs
+ * DensifyStats::accumulate (reference src/densify.rs:36-60) for this view: stats_dev holds
+ * grad_accum (float, cap), denom (uint32, cap) and max_radii (uint32, cap), in that order;
+ * `absgrad` selects the AbsGS accumulators.
+ * -------------------------------------------------------------------------------------- */
+SPLAT_API int splat_project_bwd(splat_ctx* ctx, const float* planes_dev, int64_t n, int64_t cap,
+                                const splat_camera* cam, const splat_proj_opts* opts, const float* proj_dev,
+                                const float* pgrad_dev, float* grad_planes_dev, void* stats_dev, int32_t absgrad);
+
+/* Fill `bytes` bytes of device memory with zeros on the context stream. */
+SPLAT_API int splat_zero(splat_ctx* ctx, void* dev, size_t bytes);
+
+/* ----------------------------------------------------------------------------------------
+ * Renderer: a model resident in device memory, driven with HOST buffers. All calls
+ * synchronise before returning.
+ *   splat_renderer_set_model: upload n reference Gaussian records (aos59, host) and the
+ *     model's active SH degree (Model::sh_degree, reference src/model.rs:54-61).
+ *   splat_renderer_render: render::render (reference src/render.rs:14-23) into a host
+ *     H*W*3 image (the model's SH degree overrides opts->sh_degree, as project_all does,
+ *     src/project.rs:321-324).
+ *   splat_renderer_render_backward: the differentiable chain of examples/profile.rs:34-52:
+ *     project_all -> bin -> rasterize_forward (image to image_host if not NULL) ->
+ *     rasterize_backward with dimage_host (H*W*3) -> project_backward_all, writing the
+ *     parameter gradients as n reference records (grads_aos59_host, may be NULL).
+ * -------------------------------------------------------------------------------------- */
+typedef struct splat_renderer splat_renderer;
+SPLAT_API int splat_renderer_create(splat_ctx* ctx, splat_renderer** out);
+SPLAT_API int splat_renderer_destroy(splat_renderer* r);
+SPLAT_API int splat_renderer_set_model(splat_renderer* r, const float* aos59_host, int64_t n, int32_t sh_degree);
+SPLAT_API int splat_renderer_render(splat_renderer* r, const splat_camera* cam, const splat_proj_opts* opts,
+                                    const float background[3], float* image_host);
+SPLAT_API int splat_renderer_render_backward(splat_renderer* r, const splat_camera* cam, const splat_proj_opts* opts,
+                                             const float background[3], const float* dimage_host, float* image_host,
+                                             float* grads_aos59_host);
+/* Tile entries of the last rendered view (Binning::sorted.len()). */
+SPLAT_API int64_t splat_renderer_last_entries(const splat_renderer* r);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SPLAT_GPU_H */

@@ -1,0 +1,184 @@
+"""ctypes binding of libsplatrs_b200.so, the C ABI declared in include/splat_gpu.h.
+
+The library is built in-tree (splatrs_b200/build.py). There is no fallback: if the
+library is missing or fails to load, every entry point raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libsplatrs_b200.so")
+
+SPLAT_OK = 0
+SPLAT_ERR_INVALID = 1
+SPLAT_ERR_CAPACITY = 2
+SPLAT_ERR_CUDA = 3
+SPLAT_ERR_TIMEOUT = 4
+PLANES = 15
+PROJ_FLOATS = 16
+
+
+class SplatError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"[{status}] {msg}")
+        self.status = status
+
+
+class Camera(C.Structure):
+    """splat_camera (reference src/camera.rs:13-32)."""
+    _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("fx", C.c_float), ("fy", C.c_float),
+                ("cx", C.c_float), ("cy", C.c_float), ("rot", C.c_float * 9), ("trans", C.c_float * 3)]
+
+    @classmethod
+    def from_record(cls, rec):
+        """From the 18-value record width, height, fx, fy, cx, cy, rot[9], trans[3]."""
+        r = [float(x) for x in rec]
+        c = cls()
+        c.width, c.height = int(r[0]), int(r[1])
+        c.fx, c.fy, c.cx, c.cy = r[2], r[3], r[4], r[5]
+        for i in range(9):
+            c.rot[i] = r[6 + i]
+        for i in range(3):
+            c.trans[i] = r[15 + i]
+        return c
+
+
+class ProjOpts(C.Structure):
+    """splat_proj_opts (reference src/project.rs:22-43)."""
+    _fields_ = [("near_plane", C.c_float), ("eps2d", C.c_float), ("antialias", C.c_int32), ("sh_degree", C.c_int32)]
+
+    @classmethod
+    def make(cls, near=0.2, eps2d=0.3, antialias=False, sh_degree=3):
+        return cls(near, eps2d, int(bool(antialias)), int(sh_degree))
+
+
+class LearningRates(C.Structure):
+    """splat_lr (reference src/adam.rs:11-24)."""
+    _fields_ = [(n, C.c_float) for n in ("mean", "log_scale", "quat", "opacity", "sh_dc", "sh_rest")]
+
+
+class DensifyConfig(C.Structure):
+    """splat_densify_config (reference src/densify.rs:69-103)."""
+    _fields_ = [("grad_threshold", C.c_float), ("percent_dense", C.c_float), ("min_opacity", C.c_float),
+                ("prune_big_world", C.c_int32), ("max_world_size_frac", C.c_float), ("max_screen_size", C.c_int64),
+                ("split_children", C.c_int32)]
+
+    @classmethod
+    def make(cls, grad_threshold=0.0002, percent_dense=0.01, min_opacity=0.005, prune_big_world=False,
+             max_world_size_frac=0.1, max_screen_size=None, split_children=2):
+        return cls(grad_threshold, percent_dense, min_opacity, int(bool(prune_big_world)), max_world_size_frac,
+                   -1 if max_screen_size is None else int(max_screen_size), int(split_children))
+
+
+class TrainConfig(C.Structure):
+    """splat_train_config (reference src/train.rs:20-109)."""
+    _fields_ = [("iterations", C.c_uint32), ("position_lr_init", C.c_float), ("position_lr_final", C.c_float),
+                ("position_lr_max_steps", C.c_uint32), ("feature_lr", C.c_float), ("opacity_lr", C.c_float),
+                ("scaling_lr", C.c_float), ("rotation_lr", C.c_float), ("lambda_dssim", C.c_float),
+                ("densify", C.c_int32), ("densify_from_iter", C.c_uint32), ("densify_until_iter", C.c_uint32),
+                ("densification_interval", C.c_uint32), ("opacity_reset_interval", C.c_uint32),
+                ("densify_grad_threshold", C.c_float), ("percent_dense", C.c_float), ("min_opacity", C.c_float),
+                ("max_screen_size", C.c_int64), ("absgrad", C.c_int32), ("antialias", C.c_int32),
+                ("white_background", C.c_int32), ("sh_degree", C.c_int32), ("sh_degree_interval", C.c_uint32),
+                ("near_plane", C.c_float), ("seed", C.c_uint64)]
+
+    DEFAULTS = dict(iterations=30000, position_lr_init=0.00016, position_lr_final=0.0000016,
+                    position_lr_max_steps=30000, feature_lr=0.0025, opacity_lr=0.025, scaling_lr=0.005,
+                    rotation_lr=0.001, lambda_dssim=0.2, densify=1, densify_from_iter=500, densify_until_iter=15000,
+                    densification_interval=100, opacity_reset_interval=3000, densify_grad_threshold=0.0002,
+                    percent_dense=0.01, min_opacity=0.005, max_screen_size=-1, absgrad=0, antialias=0,
+                    white_background=0, sh_degree=3, sh_degree_interval=1000, near_plane=0.2, seed=0)
+
+    @classmethod
+    def make(cls, **kw):
+        d = dict(cls.DEFAULTS)
+        if "near" in kw:
+            kw["near_plane"] = kw.pop("near")
+        for k, v in kw.items():
+            if k not in d:
+                raise KeyError(k)
+            d[k] = -1 if (k == "max_screen_size" and v is None) else v
+        c = cls()
+        for k, v in d.items():
+            setattr(c, k, int(v) if isinstance(getattr(c, k), int) else float(v))
+        return c
+
+
+_lib = None
+
+
+def _declare(L):
+    vp, i64, u32, i32, sz = C.c_void_p, C.c_int64, C.c_uint32, C.c_int32, C.c_size_t
+    P = C.POINTER
+    sig = {
+        "splat_version": ([], C.c_int),
+        "splat_status_string": ([C.c_int], C.c_char_p),
+        "splat_ctx_create": ([C.c_int, vp, P(vp)], C.c_int),
+        "splat_ctx_destroy": ([vp], C.c_int),
+        "splat_ctx_set_stream": ([vp, vp], C.c_int),
+        "splat_ctx_synchronize": ([vp], C.c_int),
+        "splat_last_error": ([vp], C.c_char_p),
+        "splat_ctx_launch_count": ([vp], C.c_uint64),
+        "splat_zero": ([vp, vp, sz], C.c_int),
+        "splat_params_from_aos": ([vp, vp, i64, vp, i64], C.c_int),
+        "splat_params_to_aos": ([vp, vp, i64, i64, vp], C.c_int),
+        "splat_project_fwd": ([vp, vp, i64, i64, P(Camera), P(ProjOpts), vp, vp, vp], C.c_int),
+        "splat_proj_from_reference": ([vp, vp, i64, u32, u32, vp, vp, vp], C.c_int),
+        "splat_proj_to_reference": ([vp, vp, i64, vp], C.c_int),
+        "splat_bin_count": ([vp, vp, i64, vp, P(i64)], C.c_int),
+        "splat_bin_sort": ([vp, vp, vp, i64, i64, vp, u32, u32, vp, vp, vp], C.c_int),
+        "splat_rasterize_fwd": ([vp, vp, vp, vp, u32, u32, P(C.c_float), vp, vp, vp, vp], C.c_int),
+        "splat_rasterize_bwd": ([vp, vp, vp, vp, u32, u32, P(C.c_float), vp, vp, vp, vp, i64, vp], C.c_int),
+        "splat_project_bwd": ([vp, vp, i64, i64, P(Camera), P(ProjOpts), vp, vp, vp, vp, i32], C.c_int),
+    }
+    sig.update({
+        "splat_renderer_create": ([vp, P(vp)], C.c_int),
+        "splat_renderer_destroy": ([vp], C.c_int),
+        "splat_renderer_set_model": ([vp, vp, i64, i32], C.c_int),
+        "splat_renderer_render": ([vp, P(Camera), P(ProjOpts), P(C.c_float), vp], C.c_int),
+        "splat_renderer_render_backward": ([vp, P(Camera), P(ProjOpts), P(C.c_float), vp, vp, vp], C.c_int),
+        "splat_renderer_last_entries": ([vp], i64),
+    })
+    optional = {
+        "splat_loss_fwd_bwd": ([vp, vp, vp, i32, u32, u32, C.c_float, vp, vp], C.c_int),
+        "splat_psnr": ([vp, vp, vp, i32, i64, vp], C.c_int),
+        "splat_adam_step": ([vp, vp, vp, vp, vp, i64, i64, C.c_uint64, P(LearningRates)], C.c_int),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = res
+    for name, (args, res) in optional.items():
+        if hasattr(L, name):
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = res
+
+
+def exported_symbols():
+    """Names this binding expects the library to export."""
+    import re
+    hdr = os.path.join(os.path.dirname(HERE), "include", "splat_gpu.h")
+    with open(hdr) as f:
+        return sorted(set(re.findall(r"SPLAT_API\s+[\w\s\*]+?\b(splat_\w+)\s*\(", f.read())))
+
+
+def lib():
+    """Load the in-tree library; raises if it is missing (there is no CPU fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m splatrs_b200.build` "
+                               "(or __graft_entry__.build()); the CUDA path has no fallback")
+        L = C.CDLL(LIB_PATH)
+        _declare(L)
+        _lib = L
+    return _lib
+
+
+def check(status: int, ctx=None):
+    if status != SPLAT_OK:
+        msg = lib().splat_last_error(ctx).decode() if ctx else lib().splat_status_string(status).decode()
+        raise SplatError(status, msg)

@@ -1,0 +1,308 @@
+// The C ABI (include/splat_gpu.h): argument checks, context and scratch management, and
+// dispatch to the stage launchers. No entry point aborts; failures return a status and
+// leave a message on the context.
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <new>
+
+#include "common.cuh"
+#include "kernels.cuh"
+#include "renderer.cuh"
+
+namespace splat {
+
+Status arena_reserve(Ctx* c, size_t bytes, void** out) {
+  Arena& a = c->arena;
+  bytes = (bytes + 255) & ~(size_t)255;
+  if (bytes == 0) bytes = 256;
+  if (a.chunks.empty() || a.used + bytes > a.chunks.back().size) {
+    size_t want = std::max(bytes, a.chunks.empty() ? (size_t)(64u << 20) : a.chunks.back().size * 2);
+    void* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, want);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      return Status::make(SPLAT_ERR_CUDA, std::string("scratch allocation of ") + std::to_string(want) +
+                                              " bytes failed: " + cudaGetErrorString(e));
+    }
+    a.chunks.push_back(ArenaChunk{p, want});
+    a.used = 0;
+  }
+  *out = static_cast<char*>(a.chunks.back().ptr) + a.used;
+  a.used += bytes;
+  return Status::ok();
+}
+
+void arena_reset(Ctx* c) {
+  Arena& a = c->arena;
+  if (a.chunks.size() > 1) {
+    size_t total = 0;
+    for (auto& ch : a.chunks) total += ch.size;
+    cudaStreamSynchronize(c->stream);
+    for (auto& ch : a.chunks) cudaFree(ch.ptr);
+    a.chunks.clear();
+    void* p = nullptr;
+    if (cudaMalloc(&p, total) == cudaSuccess)
+      a.chunks.push_back(ArenaChunk{p, total});
+    else
+      cudaGetLastError();
+  }
+  a.used = 0;
+}
+
+void arena_free(Ctx* c) {
+  for (auto& ch : c->arena.chunks) cudaFree(ch.ptr);
+  c->arena.chunks.clear();
+  c->arena.used = 0;
+}
+
+}  // namespace splat
+
+using namespace splat;
+
+struct splat_ctx {
+  Ctx c;
+};
+
+namespace splat {
+Ctx* splat_ctx_impl(splat_ctx* ctx) { return &ctx->c; }
+}  // namespace splat
+
+namespace {
+int fail(splat_ctx* ctx, const Status& s) {
+  if (ctx) ctx->c.last_error = s.msg;
+  return s.code;
+}
+int invalid(splat_ctx* ctx, const char* msg) { return fail(ctx, Status::make(SPLAT_ERR_INVALID, msg)); }
+
+// Every entry point runs on the context's device with a fresh scratch arena.
+struct Enter {
+  splat_ctx* ctx;
+  int prev = -1;
+  explicit Enter(splat_ctx* x) : ctx(x) {
+    if (cudaGetDevice(&prev) != cudaSuccess) {
+      cudaGetLastError();
+      prev = -1;
+    }
+    if (prev != x->c.device) cudaSetDevice(x->c.device);
+    arena_reset(&x->c);
+  }
+  ~Enter() {
+    if (prev >= 0 && prev != ctx->c.device) cudaSetDevice(prev);
+  }
+};
+
+int finish(splat_ctx* ctx, const Status& s) { return s.good() ? SPLAT_OK : fail(ctx, s); }
+
+bool cam_ok(const splat_camera* cam) {
+  return cam && cam->width > 0 && cam->height > 0 && cam->width <= 65535 && cam->height <= 65535;
+}
+bool opts_ok(const splat_proj_opts* o) { return o && o->sh_degree >= 0 && o->sh_degree <= 3; }
+}  // namespace
+
+extern "C" {
+
+SPLAT_API int splat_version(void) { return 1; }
+
+SPLAT_API const char* splat_status_string(int status) {
+  switch (status) {
+    case SPLAT_OK: return "ok";
+    case SPLAT_ERR_INVALID: return "invalid argument";
+    case SPLAT_ERR_CAPACITY: return "capacity exceeded";
+    case SPLAT_ERR_CUDA: return "CUDA error";
+    case SPLAT_ERR_TIMEOUT: return "device wait timed out";
+    default: return "unknown status";
+  }
+}
+
+SPLAT_API int splat_ctx_create(int device, void* stream, splat_ctx** out) {
+  if (!out) return SPLAT_ERR_INVALID;
+  *out = nullptr;
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0 || device >= count) {
+    cudaGetLastError();
+    return SPLAT_ERR_CUDA;
+  }
+  splat_ctx* ctx = new (std::nothrow) splat_ctx();
+  if (!ctx) return SPLAT_ERR_INVALID;
+  ctx->c.device = device;
+  ctx->c.stream = reinterpret_cast<cudaStream_t>(stream);
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaSetDevice(device);
+  cudaDeviceGetAttribute(&ctx->c.sm_count, cudaDevAttrMultiProcessorCount, device);
+  if (cudaMallocHost(&ctx->c.host_small, 4096) != cudaSuccess) {
+    cudaGetLastError();
+    cudaSetDevice(prev);
+    delete ctx;
+    return SPLAT_ERR_CUDA;
+  }
+  cudaSetDevice(prev);
+  *out = ctx;
+  return SPLAT_OK;
+}
+
+SPLAT_API int splat_ctx_destroy(splat_ctx* ctx) {
+  if (!ctx) return SPLAT_OK;
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaSetDevice(ctx->c.device);
+  cudaStreamSynchronize(ctx->c.stream);
+  arena_free(&ctx->c);
+  if (ctx->c.host_small) cudaFreeHost(ctx->c.host_small);
+  cudaSetDevice(prev);
+  delete ctx;
+  return SPLAT_OK;
+}
+
+SPLAT_API int splat_ctx_set_stream(splat_ctx* ctx, void* stream) {
+  if (!ctx) return SPLAT_ERR_INVALID;
+  ctx->c.stream = reinterpret_cast<cudaStream_t>(stream);
+  return SPLAT_OK;
+}
+
+SPLAT_API int splat_ctx_synchronize(splat_ctx* ctx) {
+  if (!ctx) return SPLAT_ERR_INVALID;
+  Enter e(ctx);
+  return finish(ctx, cuda_status(cudaStreamSynchronize(ctx->c.stream), "cudaStreamSynchronize"));
+}
+
+SPLAT_API const char* splat_last_error(const splat_ctx* ctx) { return ctx ? ctx->c.last_error.c_str() : "no context"; }
+
+SPLAT_API uint64_t splat_ctx_launch_count(const splat_ctx* ctx) { return ctx ? ctx->c.launches.count : 0; }
+
+SPLAT_API int splat_zero(splat_ctx* ctx, void* dev, size_t bytes) {
+  if (!ctx || (!dev && bytes)) return invalid(ctx, "splat_zero: null pointer");
+  Enter e(ctx);
+  return finish(ctx, cuda_status(cudaMemsetAsync(dev, 0, bytes, ctx->c.stream), "cudaMemsetAsync"));
+}
+
+SPLAT_API int splat_params_from_aos(splat_ctx* ctx, const float* aos59_dev, int64_t n, float* planes_dev, int64_t cap) {
+  if (!ctx) return SPLAT_ERR_INVALID;
+  if (n < 0 || cap < n || (n && (!aos59_dev || !planes_dev))) return invalid(ctx, "splat_params_from_aos: bad sizes");
+  Enter e(ctx);
+  return finish(ctx, launch_params_from_aos(&ctx->c, aos59_dev, n, planes_dev, cap));
+}
+
+SPLAT_API int splat_params_to_aos(splat_ctx* ctx, const float* planes_dev, int64_t n, int64_t cap, float* aos59_dev) {
+  if (!ctx) return SPLAT_ERR_INVALID;
+  if (n < 0 || cap < n || (n && (!aos59_dev || !planes_dev))) return invalid(ctx, "splat_params_to_aos: bad sizes");
+  Enter e(ctx);
+  return finish(ctx, launch_params_to_aos(&ctx->c, planes_dev, n, cap, aos59_dev));
+}
+
+SPLAT_API int splat_project_fwd(splat_ctx* ctx, const float* planes_dev, int64_t n, int64_t cap,
+                                const splat_camera* cam, const splat_proj_opts* opts, float* proj_dev,
+                                uint32_t* num_tiles_dev, uint32_t* depth_range_dev) {
+  if (!ctx) return SPLAT_ERR_INVALID;
+  if (!cam_ok(cam)) return invalid(ctx, "splat_project_fwd: camera size must be in 1..65535");
+  if (!opts_ok(opts)) return invalid(ctx, "splat_project_fwd: sh_degree must be in 0..3");
+  if (n < 0 || cap < n || !depth_range_dev || (n && (!planes_dev || !proj_dev || !num_tiles_dev)))
+    return invalid(ctx, "splat_project_fwd: bad buffers");
+  Enter e(ctx);
+  return finish(ctx, launch_project_fwd(&ctx->c, planes_dev, n, cap, *cam, *opts, proj_dev, num_tiles_dev,
+                                        depth_range_dev));
+}
+
+SPLAT_API int splat_proj_from_reference(splat_ctx* ctx, const float* proj15_dev, int64_t n, uint32_t width,
+                                        uint32_t height, float* proj_dev, uint32_t* num_tiles_dev,
+                                        uint32_t* depth_range_dev) {
+  if (!ctx) return SPLAT_ERR_INVALID;
+  if (width == 0 || height == 0 || width > 65535 || height > 65535)
+    return invalid(ctx, "splat_proj_from_reference: image size must be in 1..65535");
+  if (n < 0 || !depth_range_dev || (n && (!proj15_dev || !proj_dev || !num_tiles_dev)))
+    return invalid(ctx, "splat_proj_from_reference: bad buffers");
+  Enter e(ctx);
+  return finish(ctx, launch_proj_from_reference(&ctx->c, proj15_dev, n, width, height, proj_dev, num_tiles_dev,
+                                                depth_range_dev));
+}
+
+SPLAT_API int splat_proj_to_reference(splat_ctx* ctx, const float* proj_dev, int64_t n, float* proj15_dev) {
+  if (!ctx) return SPLAT_ERR_INVALID;
+  if (n < 0 || (n && (!proj_dev || !proj15_dev))) return invalid(ctx, "splat_proj_to_reference: bad buffers");
+  Enter e(ctx);
+  return finish(ctx, launch_proj_to_reference(&ctx->c, proj_dev, n, proj15_dev));
+}
+
+SPLAT_API int splat_bin_count(splat_ctx* ctx, const uint32_t* num_tiles_dev, int64_t n, uint32_t* entry_offset_dev,
+                              int64_t* num_entries) {
+  if (!ctx) return SPLAT_ERR_INVALID;
+  if (n < 0 || !entry_offset_dev || !num_entries || (n && !num_tiles_dev))
+    return invalid(ctx, "splat_bin_count: bad buffers");
+  Enter e(ctx);
+  uint64_t* total = nullptr;
+  Status s = arena_reserve(&ctx->c, 8, (void**)&total);
+  if (s.good()) s = launch_scan_u32(&ctx->c, num_tiles_dev, n, entry_offset_dev, 1, total);
+  uint64_t* h = reinterpret_cast<uint64_t*>(ctx->c.host_small);
+  if (s.good()) s = cuda_status(cudaMemcpyAsync(h, total, 8, cudaMemcpyDeviceToHost, ctx->c.stream), "read entry count");
+  if (s.good()) s = cuda_status(cudaStreamSynchronize(ctx->c.stream), "cudaStreamSynchronize");
+  if (!s.good()) return fail(ctx, s);
+  if (h[0] >= 0xffffffffull) return fail(ctx, Status::make(SPLAT_ERR_CAPACITY, "too many tile entries for 32-bit offsets"));
+  *num_entries = (int64_t)h[0];
+  return SPLAT_OK;
+}
+
+SPLAT_API int splat_bin_sort(splat_ctx* ctx, const float* proj_dev, const uint32_t* entry_offset_dev, int64_t n,
+                             int64_t num_entries, const uint32_t* depth_range_dev, uint32_t width, uint32_t height,
+                             uint32_t* gauss_dev, uint64_t* keys_dev, uint32_t* tile_range_dev) {
+  if (!ctx) return SPLAT_ERR_INVALID;
+  if (width == 0 || height == 0 || width > 65535 || height > 65535)
+    return invalid(ctx, "splat_bin_sort: image size must be in 1..65535");
+  if (n < 0 || num_entries < 0 || !tile_range_dev || !depth_range_dev ||
+      (num_entries && (!proj_dev || !entry_offset_dev || !gauss_dev)))
+    return invalid(ctx, "splat_bin_sort: bad buffers");
+  Enter e(ctx);
+  uint32_t* h = reinterpret_cast<uint32_t*>(ctx->c.host_small);
+  Status s = cuda_status(cudaMemcpyAsync(h, depth_range_dev, 8, cudaMemcpyDeviceToHost, ctx->c.stream), "read depth range");
+  if (s.good()) s = cuda_status(cudaStreamSynchronize(ctx->c.stream), "cudaStreamSynchronize");
+  if (!s.good()) return fail(ctx, s);
+  const uint32_t dmin = h[0], dmax = h[1];
+  if (num_entries > 0 && dmin > dmax) return invalid(ctx, "splat_bin_sort: depth range is empty but entries exist");
+  return finish(ctx, launch_bin_sort(&ctx->c, proj_dev, entry_offset_dev, n, num_entries, depth_range_dev, dmin,
+                                     num_entries > 0 ? dmax : dmin, width, height, gauss_dev, keys_dev,
+                                     tile_range_dev));
+}
+
+SPLAT_API int splat_rasterize_fwd(splat_ctx* ctx, const float* proj_dev, const uint32_t* gauss_dev,
+                                  const uint32_t* tile_range_dev, uint32_t width, uint32_t height,
+                                  const float background[3], float* image_dev, float* final_t_dev,
+                                  uint32_t* n_contrib_dev, uint64_t* pairs_dev) {
+  if (!ctx) return SPLAT_ERR_INVALID;
+  if (width == 0 || height == 0 || width > 65535 || height > 65535)
+    return invalid(ctx, "splat_rasterize_fwd: image size must be in 1..65535");
+  if (!background || !tile_range_dev || !image_dev || !final_t_dev || !n_contrib_dev)
+    return invalid(ctx, "splat_rasterize_fwd: bad buffers");
+  Enter e(ctx);
+  return finish(ctx, launch_raster_fwd(&ctx->c, proj_dev, gauss_dev, tile_range_dev, width, height, background,
+                                       image_dev, final_t_dev, n_contrib_dev, pairs_dev));
+}
+
+SPLAT_API int splat_rasterize_bwd(splat_ctx* ctx, const float* proj_dev, const uint32_t* gauss_dev,
+                                  const uint32_t* tile_range_dev, uint32_t width, uint32_t height,
+                                  const float background[3], const float* final_t_dev,
+                                  const uint32_t* n_contrib_dev, const float* dimage_dev, float* pgrad_dev,
+                                  int64_t cap, uint64_t* pairs_dev) {
+  if (!ctx) return SPLAT_ERR_INVALID;
+  if (width == 0 || height == 0 || width > 65535 || height > 65535)
+    return invalid(ctx, "splat_rasterize_bwd: image size must be in 1..65535");
+  if (!background || !tile_range_dev || !final_t_dev || !n_contrib_dev || !dimage_dev || !pgrad_dev || cap < 0)
+    return invalid(ctx, "splat_rasterize_bwd: bad buffers");
+  Enter e(ctx);
+  return finish(ctx, launch_raster_bwd(&ctx->c, proj_dev, gauss_dev, tile_range_dev, width, height, background,
+                                       final_t_dev, n_contrib_dev, dimage_dev, pgrad_dev, cap, pairs_dev));
+}
+
+SPLAT_API int splat_project_bwd(splat_ctx* ctx, const float* planes_dev, int64_t n, int64_t cap,
+                                const splat_camera* cam, const splat_proj_opts* opts, const float* proj_dev,
+                                const float* pgrad_dev, float* grad_planes_dev, void* stats_dev, int32_t absgrad) {
+  if (!ctx) return SPLAT_ERR_INVALID;
+  if (!cam_ok(cam)) return invalid(ctx, "splat_project_bwd: camera size must be in 1..65535");
+  if (!opts_ok(opts)) return invalid(ctx, "splat_project_bwd: sh_degree must be in 0..3");
+  if (n < 0 || cap < n || (n && (!planes_dev || !proj_dev || !pgrad_dev || !grad_planes_dev)))
+    return invalid(ctx, "splat_project_bwd: bad buffers");
+  Enter e(ctx);
+  return finish(ctx, launch_project_bwd(&ctx->c, planes_dev, n, cap, *cam, *opts, proj_dev, pgrad_dev,
+                                        grad_planes_dev, stats_dev, absgrad));
+}
+
+}  // extern "C"

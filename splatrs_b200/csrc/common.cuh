@@ -1,0 +1,119 @@
+// Shared definitions for the sm_100a kernels and their host launchers.
+//
+// Every translation unit is compiled with --fmad=false: a*b+c is two roundings, as in the
+// reference's Rust, so decisions taken on float values (the alpha and transmittance
+// thresholds, tile rectangles, radii) come out exactly as the reference computes them.
+// Kernels that only accumulate gradients opt in to fused multiply-adds explicitly.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/splat_gpu.h"
+#include "crmath.h"
+
+namespace splat {
+
+constexpr int kPlanes = SPLAT_PLANES;
+constexpr int kProjFloats = SPLAT_PROJ_FLOATS;
+constexpr uint32_t kTile = SPLAT_TILE;
+
+// Error carried from a launcher to the C ABI.
+struct Status {
+  int code = SPLAT_OK;
+  std::string msg;
+  static Status ok() { return Status(); }
+  static Status make(int c, std::string m) {
+    Status s;
+    s.code = c;
+    s.msg = std::move(m);
+    return s;
+  }
+  bool good() const { return code == SPLAT_OK; }
+};
+
+inline Status cuda_status(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return Status::ok();
+  return Status::make(SPLAT_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define SPLAT_TRY(expr)            \
+  do {                             \
+    ::splat::Status _s = (expr);   \
+    if (!_s.good()) return _s;     \
+  } while (0)
+
+#define SPLAT_CUDA(expr) SPLAT_TRY(::splat::cuda_status((expr), #expr))
+#define SPLAT_LAUNCHED(what) SPLAT_TRY(::splat::cuda_status(cudaGetLastError(), what))
+
+// Scratch memory handed out by the context: a list of device chunks. Reserving never
+// moves memory already handed out; chunks are merged at the next reset.
+struct ArenaChunk {
+  void* ptr;
+  size_t size;
+};
+struct Arena {
+  std::vector<ArenaChunk> chunks;
+  size_t used = 0;  // bytes used in the last chunk
+};
+
+// Launch bookkeeping shared by all launchers.
+struct LaunchCounter {
+  uint64_t count = 0;
+};
+
+struct Ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  Arena arena;
+  LaunchCounter launches;
+  std::string last_error;
+  int sm_count = 148;
+  // Pinned host staging for small read-backs.
+  void* host_small = nullptr;
+};
+
+// Reserve `bytes` of scratch (256-byte aligned) from the context arena. The arena is
+// reset at the start of every public entry point; reserving more than is available
+// reallocates it (after synchronising the stream, so no kernel still uses the old one).
+Status arena_reserve(Ctx* c, size_t bytes, void** out);
+void arena_reset(Ctx* c);
+void arena_free(Ctx* c);
+
+inline uint32_t ceil_div(uint64_t a, uint64_t b) { return (uint32_t)((a + b - 1) / b); }
+
+// Float <-> bits.
+__host__ __device__ __forceinline__ uint32_t fbits(float f) {
+#if defined(__CUDA_ARCH__)
+  return __float_as_uint(f);
+#else
+  uint32_t b;
+  __builtin_memcpy(&b, &f, 4);
+  return b;
+#endif
+}
+__host__ __device__ __forceinline__ float bitsf(uint32_t b) {
+#if defined(__CUDA_ARCH__)
+  return __uint_as_float(b);
+#else
+  float f;
+  __builtin_memcpy(&f, &b, 4);
+  return f;
+#endif
+}
+
+// Rust's saturating `as u32` for floats (NaN and negatives to 0).
+__host__ __device__ __forceinline__ uint32_t sat_u32(float v) {
+  if (!(v > 0.0f)) return 0u;
+  if (v >= 4294967295.0f) return 0xffffffffu;
+  return (uint32_t)v;
+}
+
+// Compositing constants (reference src/rasterize.rs:53-57).
+#define SPLAT_ALPHA_MIN (1.0f / 255.0f)
+#define SPLAT_ALPHA_MAX 0.99f
+#define SPLAT_T_MIN 1e-4f
+
+}  // namespace splat

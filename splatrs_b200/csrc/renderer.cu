@@ -1,0 +1,240 @@
+// splat_renderer: a model resident in device memory plus the per-view buffers of the
+// render path, driven with host buffers. It is the drop-in for render::render
+// (reference src/render.rs:14-23) and for the differentiable chain of
+// examples/profile.rs:34-52 (project_all -> bin -> rasterize_forward -> rasterize_backward
+// -> project_backward_all).
+#include <algorithm>
+#include <cstring>
+#include <new>
+
+#include "common.cuh"
+#include "kernels.cuh"
+#include "renderer.cuh"
+
+namespace splat {
+
+Status DevBuf::ensure(size_t want) {
+  if (want <= bytes) return Status::ok();
+  const size_t grow = std::max(want, bytes + bytes / 2);
+  if (ptr) cudaFree(ptr);
+  ptr = nullptr;
+  bytes = 0;
+  cudaError_t e = cudaMalloc(&ptr, grow);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return Status::make(SPLAT_ERR_CUDA, std::string("device allocation of ") + std::to_string(grow) +
+                                            " bytes failed: " + cudaGetErrorString(e));
+  }
+  bytes = grow;
+  return Status::ok();
+}
+
+void DevBuf::release() {
+  if (ptr) cudaFree(ptr);
+  ptr = nullptr;
+  bytes = 0;
+}
+
+Status ViewBuffers::ensure(int64_t n, uint32_t width, uint32_t height) {
+  const size_t npix = (size_t)width * height;
+  const uint32_t tiles = ((width + kTile - 1) / kTile) * ((height + kTile - 1) / kTile);
+  SPLAT_TRY(proj.ensure((size_t)std::max<int64_t>(n, 1) * kProjFloats * 4));
+  SPLAT_TRY(num_tiles.ensure((size_t)std::max<int64_t>(n, 1) * 4));
+  SPLAT_TRY(entry_offset.ensure((size_t)(n + 1) * 4));
+  SPLAT_TRY(depth_range.ensure(8));
+  SPLAT_TRY(tile_range.ensure((size_t)tiles * 8));
+  SPLAT_TRY(image.ensure(npix * 12));
+  SPLAT_TRY(final_t.ensure(npix * 4));
+  SPLAT_TRY(n_contrib.ensure(npix * 4));
+  SPLAT_TRY(dimage.ensure(npix * 12));
+  SPLAT_TRY(pairs.ensure(16));
+  return Status::ok();
+}
+
+void ViewBuffers::release() {
+  for (DevBuf* b : {&proj, &num_tiles, &entry_offset, &depth_range, &tile_range, &gauss, &image, &final_t, &n_contrib,
+                    &dimage, &pairs})
+    b->release();
+}
+
+// Projection, binning and forward compositing of one view into `v`.
+Status render_view(Ctx* c, const float* planes, int64_t n, int64_t cap, const splat_camera& cam,
+                   const splat_proj_opts& opts, const float bg[3], ViewBuffers& v, int64_t* entries_out) {
+  SPLAT_TRY(v.ensure(n, cam.width, cam.height));
+  float* proj = v.proj.as<float>();
+  uint32_t* nt = v.num_tiles.as<uint32_t>();
+  uint32_t* dr = v.depth_range.as<uint32_t>();
+  SPLAT_TRY(launch_project_fwd(c, planes, n, cap, cam, opts, proj, nt, dr));
+  uint64_t* total = nullptr;
+  SPLAT_TRY(arena_reserve(c, 8, (void**)&total));
+  SPLAT_TRY(launch_scan_u32(c, nt, n, v.entry_offset.as<uint32_t>(), 1, total));
+  // One read-back per view: the entry count and the depth range size the sort.
+  uint64_t* h = reinterpret_cast<uint64_t*>(c->host_small);
+  SPLAT_CUDA(cudaMemcpyAsync(h, total, 8, cudaMemcpyDeviceToHost, c->stream));
+  SPLAT_CUDA(cudaMemcpyAsync(h + 1, dr, 8, cudaMemcpyDeviceToHost, c->stream));
+  SPLAT_CUDA(cudaStreamSynchronize(c->stream));
+  const uint64_t E = h[0];
+  if (E >= 0xffffffffull) return Status::make(SPLAT_ERR_CAPACITY, "too many tile entries for 32-bit offsets");
+  const uint32_t* drh = reinterpret_cast<const uint32_t*>(h + 1);
+  SPLAT_TRY(v.gauss.ensure((size_t)std::max<uint64_t>(E, 1) * 4));
+  SPLAT_TRY(launch_bin_sort(c, proj, v.entry_offset.as<uint32_t>(), n, (int64_t)E, dr, drh[0],
+                            E > 0 ? drh[1] : drh[0], cam.width, cam.height, v.gauss.as<uint32_t>(), nullptr,
+                            v.tile_range.as<uint32_t>()));
+  SPLAT_TRY(launch_raster_fwd(c, proj, v.gauss.as<uint32_t>(), v.tile_range.as<uint32_t>(), cam.width, cam.height, bg,
+                              v.image.as<float>(), v.final_t.as<float>(), v.n_contrib.as<uint32_t>(), nullptr));
+  if (entries_out) *entries_out = (int64_t)E;
+  return Status::ok();
+}
+
+}  // namespace splat
+
+using namespace splat;
+
+struct splat_renderer {
+  splat_ctx* ctx;
+  Ctx* c;
+  int64_t n = 0, cap = 0;
+  int32_t sh_degree = 3;
+  DevBuf planes, aos, pgrad, grad_planes, grad_aos;
+  ViewBuffers v;
+  int64_t last_entries = 0;
+};
+
+namespace {
+int rfail(splat_renderer* r, const Status& s) {
+  r->c->last_error = s.msg;
+  return s.code;
+}
+struct REnter {
+  splat_renderer* r;
+  int prev = -1;
+  explicit REnter(splat_renderer* x) : r(x) {
+    if (cudaGetDevice(&prev) != cudaSuccess) {
+      cudaGetLastError();
+      prev = -1;
+    }
+    if (prev != x->c->device) cudaSetDevice(x->c->device);
+    arena_reset(x->c);
+  }
+  ~REnter() {
+    if (prev >= 0 && prev != r->c->device) cudaSetDevice(prev);
+  }
+};
+bool cam_ok(const splat_camera* cam) {
+  return cam && cam->width > 0 && cam->height > 0 && cam->width <= 65535 && cam->height <= 65535;
+}
+}  // namespace
+
+extern "C" {
+
+SPLAT_API int splat_renderer_create(splat_ctx* ctx, splat_renderer** out) {
+  if (!ctx || !out) return SPLAT_ERR_INVALID;
+  splat_renderer* r = new (std::nothrow) splat_renderer();
+  if (!r) return SPLAT_ERR_INVALID;
+  r->ctx = ctx;
+  r->c = splat_ctx_impl(ctx);
+  *out = r;
+  return SPLAT_OK;
+}
+
+SPLAT_API int splat_renderer_destroy(splat_renderer* r) {
+  if (!r) return SPLAT_OK;
+  {
+    REnter e(r);
+    cudaStreamSynchronize(r->c->stream);
+    for (DevBuf* b : {&r->planes, &r->aos, &r->pgrad, &r->grad_planes, &r->grad_aos}) b->release();
+    r->v.release();
+  }
+  delete r;
+  return SPLAT_OK;
+}
+
+SPLAT_API int splat_renderer_set_model(splat_renderer* r, const float* aos59_host, int64_t n, int32_t sh_degree) {
+  if (!r) return SPLAT_ERR_INVALID;
+  if (n < 0 || (n && !aos59_host) || sh_degree < 0 || sh_degree > 3) {
+    r->c->last_error = "splat_renderer_set_model: bad arguments";
+    return SPLAT_ERR_INVALID;
+  }
+  REnter e(r);
+  Ctx* c = r->c;
+  const int64_t cap = std::max<int64_t>(n, 1);
+  Status s = r->planes.ensure((size_t)cap * kPlanes * 16);
+  if (s.good()) s = r->aos.ensure((size_t)cap * 59 * 4);
+  if (s.good() && n) s = cuda_status(cudaMemcpyAsync(r->aos.ptr, aos59_host, (size_t)n * 59 * 4, cudaMemcpyHostToDevice,
+                                                     c->stream), "upload model");
+  if (s.good()) s = launch_params_from_aos(c, r->aos.as<float>(), n, r->planes.as<float>(), cap);
+  if (s.good()) s = cuda_status(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
+  if (!s.good()) return rfail(r, s);
+  r->n = n;
+  r->cap = cap;
+  r->sh_degree = sh_degree;
+  return SPLAT_OK;
+}
+
+SPLAT_API int splat_renderer_render(splat_renderer* r, const splat_camera* cam, const splat_proj_opts* opts,
+                                    const float background[3], float* image_host) {
+  if (!r) return SPLAT_ERR_INVALID;
+  if (!cam_ok(cam) || !opts || !background) {
+    r->c->last_error = "splat_renderer_render: bad arguments";
+    return SPLAT_ERR_INVALID;
+  }
+  REnter e(r);
+  Ctx* c = r->c;
+  splat_proj_opts o = *opts;
+  o.sh_degree = r->sh_degree;  // project_all uses the model's active degree (project.rs:321-324)
+  Status s = render_view(c, r->planes.as<float>(), r->n, r->cap, *cam, o, background, r->v, &r->last_entries);
+  const size_t npix = (size_t)cam->width * cam->height;
+  if (s.good() && image_host)
+    s = cuda_status(cudaMemcpyAsync(image_host, r->v.image.ptr, npix * 12, cudaMemcpyDeviceToHost, c->stream),
+                    "download image");
+  if (s.good()) s = cuda_status(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
+  return s.good() ? SPLAT_OK : rfail(r, s);
+}
+
+SPLAT_API int splat_renderer_render_backward(splat_renderer* r, const splat_camera* cam, const splat_proj_opts* opts,
+                                             const float background[3], const float* dimage_host, float* image_host,
+                                             float* grads_aos59_host) {
+  if (!r) return SPLAT_ERR_INVALID;
+  if (!cam_ok(cam) || !opts || !background || !dimage_host) {
+    r->c->last_error = "splat_renderer_render_backward: bad arguments";
+    return SPLAT_ERR_INVALID;
+  }
+  REnter e(r);
+  Ctx* c = r->c;
+  splat_proj_opts o = *opts;
+  o.sh_degree = r->sh_degree;
+  const size_t npix = (size_t)cam->width * cam->height;
+  Status s = r->v.ensure(r->n, cam->width, cam->height);
+  // The upload of dL/dimage overlaps nothing here but is issued first so the copy engine
+  // runs while the projection kernels start.
+  if (s.good()) s = cuda_status(cudaMemcpyAsync(r->v.dimage.ptr, dimage_host, npix * 12, cudaMemcpyHostToDevice,
+                                                c->stream), "upload dimage");
+  if (s.good()) s = render_view(c, r->planes.as<float>(), r->n, r->cap, *cam, o, background, r->v, &r->last_entries);
+  if (s.good() && image_host)
+    s = cuda_status(cudaMemcpyAsync(image_host, r->v.image.ptr, npix * 12, cudaMemcpyDeviceToHost, c->stream),
+                    "download image");
+  if (s.good()) s = r->pgrad.ensure((size_t)r->cap * 3 * 16);
+  if (s.good()) s = r->grad_planes.ensure((size_t)r->cap * kPlanes * 16);
+  if (s.good()) s = r->grad_aos.ensure((size_t)r->cap * 59 * 4);
+  if (s.good()) s = cuda_status(cudaMemsetAsync(r->pgrad.ptr, 0, (size_t)r->cap * 3 * 16, c->stream), "zero pgrad");
+  if (s.good())
+    s = launch_raster_bwd(c, r->v.proj.as<float>(), r->v.gauss.as<uint32_t>(), r->v.tile_range.as<uint32_t>(),
+                          cam->width, cam->height, background, r->v.final_t.as<float>(), r->v.n_contrib.as<uint32_t>(),
+                          r->v.dimage.as<float>(), r->pgrad.as<float>(), r->cap, nullptr);
+  if (s.good())
+    s = launch_project_bwd(c, r->planes.as<float>(), r->n, r->cap, *cam, o, r->v.proj.as<float>(), r->pgrad.as<float>(),
+                           r->grad_planes.as<float>(), nullptr, 0);
+  if (s.good() && grads_aos59_host) {
+    s = launch_params_to_aos(c, r->grad_planes.as<float>(), r->n, r->cap, r->grad_aos.as<float>());
+    if (s.good() && r->n)
+      s = cuda_status(cudaMemcpyAsync(grads_aos59_host, r->grad_aos.ptr, (size_t)r->n * 59 * 4, cudaMemcpyDeviceToHost,
+                                      c->stream),
+                      "download gradients");
+  }
+  if (s.good()) s = cuda_status(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
+  return s.good() ? SPLAT_OK : rfail(r, s);
+}
+
+SPLAT_API int64_t splat_renderer_last_entries(const splat_renderer* r) { return r ? r->last_entries : -1; }
+
+}  // extern "C"

@@ -1,0 +1,374 @@
+// Binning (reference src/rasterize.rs:60-128) on the device:
+//   scan of per-Gaussian tile counts -> entry offsets (Binning::entry_offset),
+//   warp-cooperative emission of one (tile | depth) key per entry in Gaussian order,
+//   stable LSD radix sort of the keys carrying the Gaussian index,
+//   per-tile [start, end) ranges.
+//
+// Keys are compacted before sorting: the reference key is (tile << 32) | depth_bits with
+// depth_bits the f32 bits of a positive depth. Subtracting the smallest visible depth bits
+// and packing the tile above the remaining significant bits keeps the order of every pair
+// of keys, so the sort runs over ceil((tile bits + depth bits) / 8) passes instead of 8.
+// The sort is stable, and entries enter it in entry order, which reproduces the
+// reference's tie-break on the entry index.
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace splat {
+
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 16;
+constexpr int kScanTile = kScanThreads * kScanItems;  // 4096 values per block
+
+// ---------------------------------------------------------------------------------------
+// Exclusive scan of uint32 counts into uint32 offsets (with the total written at [n]).
+// Three kernels: per-block sums, a single-block scan of the sums, per-block scan + add.
+// Totals are carried in 64 bits; a total that does not fit in 32 bits raises a flag.
+// ---------------------------------------------------------------------------------------
+__device__ __forceinline__ uint64_t block_sum_u64(uint64_t v, uint64_t* sh) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if (lane == 0) sh[warp] = v;
+  __syncthreads();
+  uint64_t t = 0;
+  if (threadIdx.x < 32) {
+    t = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : 0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+  }
+  __syncthreads();
+  return t;  // valid in thread 0
+}
+
+// Block-wide exclusive scan of one uint64 per thread; returns the exclusive prefix, and
+// the block total through *total.
+__device__ __forceinline__ uint64_t block_exclusive_u64(uint64_t v, uint64_t* sh, uint64_t* total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  uint64_t incl = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    uint64_t y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  if (lane == 31) sh[warp] = incl;
+  __syncthreads();
+  if (warp == 0) {
+    uint64_t w = lane < nw ? sh[lane] : 0;
+    uint64_t wi = w;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      uint64_t y = __shfl_up_sync(0xffffffffu, wi, o);
+      if (lane >= o) wi += y;
+    }
+    if (lane < nw) sh[lane] = wi - w;
+    if (lane == nw - 1) sh[32] = wi;
+  }
+  __syncthreads();
+  uint64_t r = sh[warp] + incl - v;
+  *total = sh[32];
+  __syncthreads();
+  return r;
+}
+
+__global__ void __launch_bounds__(kScanThreads) scan_reduce_kernel(const uint32_t* __restrict__ in, int64_t n,
+                                                                   uint64_t* __restrict__ partial) {
+  __shared__ uint64_t sh[33];
+  const int64_t base = (int64_t)blockIdx.x * kScanTile;
+  uint64_t s = 0;
+#pragma unroll
+  for (int j = 0; j < kScanItems; j++) {
+    const int64_t idx = base + (int64_t)j * kScanThreads + threadIdx.x;
+    if (idx < n) s += in[idx];
+  }
+  s = block_sum_u64(s, sh);
+  if (threadIdx.x == 0) partial[blockIdx.x] = s;
+}
+
+// Single block: exclusive scan of `m` partials in place; total to *total.
+__global__ void __launch_bounds__(1024) scan_partials_kernel(uint64_t* __restrict__ partial, int64_t m,
+                                                             uint64_t* __restrict__ total) {
+  __shared__ uint64_t sh[33];
+  uint64_t carry = 0;
+  for (int64_t base = 0; base < m; base += blockDim.x) {
+    const int64_t idx = base + threadIdx.x;
+    const uint64_t v = idx < m ? partial[idx] : 0;
+    uint64_t tot;
+    const uint64_t ex = block_exclusive_u64(v, sh, &tot);
+    if (idx < m) partial[idx] = carry + ex;
+    carry += tot;
+  }
+  if (threadIdx.x == 0) *total = carry;
+}
+
+// Writes out[i] = exclusive prefix (uint32) for i < n, and out[n] = total when `write_total`.
+__global__ void __launch_bounds__(kScanThreads) scan_apply_kernel(const uint32_t* __restrict__ in, int64_t n,
+                                                                  const uint64_t* __restrict__ partial,
+                                                                  const uint64_t* __restrict__ total,
+                                                                  uint32_t* __restrict__ out, int write_total) {
+  __shared__ uint64_t sh[33];
+  const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
+  uint32_t v[kScanItems];
+  uint64_t s = 0;
+#pragma unroll
+  for (int j = 0; j < kScanItems; j++) {
+    const int64_t idx = base + j;
+    v[j] = idx < n ? in[idx] : 0u;
+    s += v[j];
+  }
+  uint64_t tot;
+  uint64_t run = partial[blockIdx.x] + block_exclusive_u64(s, sh, &tot);
+#pragma unroll
+  for (int j = 0; j < kScanItems; j++) {
+    const int64_t idx = base + j;
+    if (idx < n) out[idx] = (uint32_t)run;
+    run += v[j];
+  }
+  if (write_total && blockIdx.x == 0 && threadIdx.x == 0) out[n] = (uint32_t)*total;
+}
+
+Status launch_scan_u32(Ctx* c, const uint32_t* in, int64_t n, uint32_t* out, int write_total, uint64_t* total_dev) {
+  const uint32_t blocks = ceil_div((uint64_t)std::max<int64_t>(n, 1), kScanTile);
+  uint64_t* partial = nullptr;
+  SPLAT_TRY(arena_reserve(c, (size_t)blocks * 8, (void**)&partial));
+  scan_reduce_kernel<<<blocks, kScanThreads, 0, c->stream>>>(in, n, partial);
+  scan_partials_kernel<<<1, 1024, 0, c->stream>>>(partial, blocks, total_dev);
+  scan_apply_kernel<<<blocks, kScanThreads, 0, c->stream>>>(in, n, partial, total_dev, out, write_total);
+  c->launches.count += 3;
+  SPLAT_LAUNCHED("scan kernels");
+  return Status::ok();
+}
+
+// ---------------------------------------------------------------------------------------
+// Key emission (rasterize.rs:76-104): the entries of Gaussian g occupy
+// [entry_offset[g], entry_offset[g+1]) and enumerate its tile rectangle row by row.
+// Each warp takes 32 consecutive Gaussians and writes their entries contiguously.
+// ---------------------------------------------------------------------------------------
+template <typename K>
+__global__ void __launch_bounds__(256) emit_keys_kernel(const float4* __restrict__ rec,
+                                                        const uint32_t* __restrict__ entry_offset, int64_t n,
+                                                        uint32_t tiles_x, const uint32_t* __restrict__ depth_range,
+                                                        int dbits, K* __restrict__ keys, uint32_t* __restrict__ vals) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warp_id = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t g = warp_id * 32 + lane;
+  const int64_t first = warp_id * 32;
+  if (first >= n) return;
+  uint32_t cnt = 0, tx0 = 0, ty0 = 0, w = 1, dkey = 0;
+  if (g < n) {
+    const uint32_t o0 = entry_offset[g], o1 = entry_offset[g + 1];
+    cnt = o1 - o0;
+    if (cnt) {
+      const float4 r3 = rec[4 * g + 3];
+      const uint32_t tmin = fbits(r3.z), tmax = fbits(r3.w);
+      tx0 = tmin & 0xffffu;
+      ty0 = tmin >> 16;
+      w = (tmax & 0xffffu) - tx0;
+      dkey = fbits(r3.x) - depth_range[0];
+    }
+  }
+  const uint32_t start = entry_offset[first];
+  // Inclusive warp scan of the counts.
+  uint32_t incl = cnt;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+  for (uint32_t j0 = 0; j0 < total; j0 += 32) {
+    const uint32_t j = j0 + lane;
+    // Owner lane: first lane whose inclusive count exceeds j (binary search over lanes).
+    int lo = 0;
+#pragma unroll
+    for (int step = 16; step > 0; step >>= 1) {
+      const uint32_t v = __shfl_sync(0xffffffffu, incl, lo + step - 1);
+      if (v <= j) lo += step;
+    }
+    const uint32_t o_incl = __shfl_sync(0xffffffffu, incl, lo);
+    const uint32_t o_cnt = __shfl_sync(0xffffffffu, cnt, lo);
+    const uint32_t o_tx0 = __shfl_sync(0xffffffffu, tx0, lo);
+    const uint32_t o_ty0 = __shfl_sync(0xffffffffu, ty0, lo);
+    const uint32_t o_w = __shfl_sync(0xffffffffu, w, lo);
+    const uint32_t o_dkey = __shfl_sync(0xffffffffu, dkey, lo);
+    if (j < total) {
+      const uint32_t local = j - (o_incl - o_cnt);
+      const uint32_t ty = o_ty0 + local / o_w;
+      const uint32_t tx = o_tx0 + local % o_w;
+      const uint64_t tile = (uint64_t)ty * tiles_x + tx;
+      keys[start + j] = (K)((tile << dbits) | (uint64_t)o_dkey);
+      vals[start + j] = (uint32_t)(first + lo);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// Stable LSD radix sort, 8-bit digits, reduce-then-scan per pass.
+// A block sorts 4096 keys: 8 warps, each owning 512 consecutive keys that it ranks in
+// 16 rounds of 32 (position order), with match-any peer groups and per-warp digit
+// counters; a per-digit prefix over the warps then gives block-local stable ranks.
+// ---------------------------------------------------------------------------------------
+constexpr int kSortThreads = 256;
+constexpr int kSortWarps = kSortThreads / 32;
+constexpr int kSortRounds = 16;
+constexpr int kSortTile = kSortThreads * kSortRounds;  // 4096
+
+template <typename K>
+__global__ void __launch_bounds__(kSortThreads) radix_upsweep_kernel(const K* __restrict__ keys, int64_t n, int shift,
+                                                                     uint32_t* __restrict__ hist, uint32_t nblocks) {
+  __shared__ uint32_t cnt[256];
+  cnt[threadIdx.x] = 0;
+  __syncthreads();
+  const int64_t base = (int64_t)blockIdx.x * kSortTile;
+#pragma unroll 4
+  for (int r = 0; r < kSortRounds; r++) {
+    const int64_t idx = base + (int64_t)r * kSortThreads + threadIdx.x;
+    if (idx < n) {
+      const uint32_t d = (uint32_t)(keys[idx] >> shift) & 0xffu;
+      // Aggregate equal digits within the warp before the shared-memory atomic.
+      const uint32_t peers = __match_any_sync(__activemask(), d);
+      if ((threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&cnt[d], (uint32_t)__popc(peers));
+    }
+  }
+  __syncthreads();
+  hist[(int64_t)threadIdx.x * nblocks + blockIdx.x] = cnt[threadIdx.x];
+}
+
+template <typename K>
+__global__ void __launch_bounds__(kSortThreads) radix_downsweep_kernel(const K* __restrict__ keys_in,
+                                                                       const uint32_t* __restrict__ vals_in, int64_t n,
+                                                                       int shift, const uint32_t* __restrict__ offsets,
+                                                                       uint32_t nblocks, K* __restrict__ keys_out,
+                                                                       uint32_t* __restrict__ vals_out) {
+  __shared__ uint32_t wcnt[kSortWarps][256];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int d = lane; d < 256; d += 32) wcnt[warp][d] = 0;
+  __syncwarp();
+  const int64_t wbase = (int64_t)blockIdx.x * kSortTile + (int64_t)warp * (32 * kSortRounds);
+  K k[kSortRounds];
+  uint32_t v[kSortRounds];
+  uint32_t rank[kSortRounds];
+  const uint32_t lt = (1u << lane) - 1u;
+#pragma unroll
+  for (int r = 0; r < kSortRounds; r++) {
+    const int64_t idx = wbase + r * 32 + lane;
+    const bool valid = idx < n;
+    k[r] = valid ? keys_in[idx] : (K)0;
+    v[r] = valid ? vals_in[idx] : 0u;
+    const uint32_t d = valid ? ((uint32_t)(k[r] >> shift) & 0xffu) : 256u;
+    const uint32_t peers = __match_any_sync(0xffffffffu, d);
+    const uint32_t before = valid ? wcnt[warp][d] : 0u;
+    rank[r] = before + __popc(peers & lt);
+    __syncwarp();
+    if (valid && lane == __ffs(peers) - 1) wcnt[warp][d] = before + __popc(peers);
+    __syncwarp();
+  }
+  __syncthreads();
+  // Per-digit exclusive prefix over the warps (thread d owns digit d).
+  {
+    const int d = threadIdx.x;
+    uint32_t run = 0;
+#pragma unroll
+    for (int w = 0; w < kSortWarps; w++) {
+      const uint32_t c = wcnt[w][d];
+      wcnt[w][d] = run;
+      run += c;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int r = 0; r < kSortRounds; r++) {
+    const int64_t idx = wbase + r * 32 + lane;
+    if (idx < n) {
+      const uint32_t d = (uint32_t)(k[r] >> shift) & 0xffu;
+      const uint32_t pos = offsets[(int64_t)d * nblocks + blockIdx.x] + wcnt[warp][d] + rank[r];
+      keys_out[pos] = k[r];
+      vals_out[pos] = v[r];
+    }
+  }
+}
+
+// Tile ranges (rasterize.rs:108-119) and, optionally, the reference 64-bit keys.
+template <typename K>
+__global__ void tile_ranges_kernel(const K* __restrict__ keys, int64_t n, int dbits,
+                                   const uint32_t* __restrict__ depth_range, uint32_t* __restrict__ ranges,
+                                   uint64_t* __restrict__ ref_keys) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint64_t k = (uint64_t)keys[i];
+  const uint64_t tile = k >> dbits;
+  if (i == 0 || ((uint64_t)keys[i - 1] >> dbits) != tile) ranges[2 * tile] = (uint32_t)i;
+  if (i == n - 1 || ((uint64_t)keys[i + 1] >> dbits) != tile) ranges[2 * tile + 1] = (uint32_t)(i + 1);
+  if (ref_keys) {
+    const uint64_t mask = dbits >= 64 ? ~0ull : ((1ull << dbits) - 1ull);
+    const uint32_t depth_bits = (uint32_t)(k & mask) + depth_range[0];
+    ref_keys[i] = (tile << 32) | depth_bits;
+  }
+}
+
+template <typename K>
+static Status sort_and_range(Ctx* c, const float* proj, const uint32_t* entry_offset, int64_t n, int64_t E,
+                             const uint32_t* depth_range, int dbits, int total_bits, uint32_t tiles_x,
+                             uint32_t num_tiles, uint32_t* gauss_out, uint64_t* keys_out, uint32_t* ranges) {
+  const int passes = (total_bits + 7) / 8;
+  K *ka = nullptr, *kb = nullptr;
+  uint32_t* vb = nullptr;
+  SPLAT_TRY(arena_reserve(c, (size_t)E * sizeof(K), (void**)&ka));
+  SPLAT_TRY(arena_reserve(c, (size_t)E * sizeof(K), (void**)&kb));
+  SPLAT_TRY(arena_reserve(c, (size_t)E * 4, (void**)&vb));
+  // Ping-pong so that the last pass writes the caller's buffer.
+  uint32_t* va = (passes % 2 == 0) ? gauss_out : vb;
+  uint32_t* vo = (passes % 2 == 0) ? vb : gauss_out;
+  const uint32_t warps = ceil_div(n, 32);
+  emit_keys_kernel<K><<<ceil_div((uint64_t)warps * 32, 256), 256, 0, c->stream>>>(
+      reinterpret_cast<const float4*>(proj), entry_offset, n, tiles_x, depth_range, dbits, ka, va);
+  c->launches.count++;
+  SPLAT_LAUNCHED("emit_keys_kernel");
+  const uint32_t nblocks = ceil_div(E, kSortTile);
+  uint32_t* hist = nullptr;
+  uint32_t* offs = nullptr;
+  uint64_t* tot = nullptr;
+  SPLAT_TRY(arena_reserve(c, (size_t)nblocks * 256 * 4, (void**)&hist));
+  SPLAT_TRY(arena_reserve(c, (size_t)nblocks * 256 * 4, (void**)&offs));
+  SPLAT_TRY(arena_reserve(c, 8, (void**)&tot));
+  K* kin = ka;
+  K* kout = kb;
+  uint32_t* vin = va;
+  uint32_t* vout = vo;
+  for (int p = 0; p < passes; p++) {
+    const int shift = 8 * p;
+    radix_upsweep_kernel<K><<<nblocks, kSortThreads, 0, c->stream>>>(kin, E, shift, hist, nblocks);
+    SPLAT_TRY(launch_scan_u32(c, hist, (int64_t)nblocks * 256, offs, 0, tot));
+    radix_downsweep_kernel<K><<<nblocks, kSortThreads, 0, c->stream>>>(kin, vin, E, shift, offs, nblocks, kout, vout);
+    c->launches.count += 2;
+    SPLAT_LAUNCHED("radix sort pass");
+    std::swap(kin, kout);
+    std::swap(vin, vout);
+  }
+  SPLAT_CUDA(cudaMemsetAsync(ranges, 0, (size_t)num_tiles * 8, c->stream));
+  tile_ranges_kernel<K><<<ceil_div(E, 256), 256, 0, c->stream>>>(kin, E, dbits, depth_range, ranges, keys_out);
+  c->launches.count++;
+  SPLAT_LAUNCHED("tile_ranges_kernel");
+  return Status::ok();
+}
+
+Status launch_bin_sort(Ctx* c, const float* proj, const uint32_t* entry_offset, int64_t n, int64_t E,
+                       const uint32_t* depth_range_dev, uint32_t depth_min, uint32_t depth_max, uint32_t width,
+                       uint32_t height, uint32_t* gauss_out, uint64_t* keys_out, uint32_t* ranges) {
+  const uint32_t tiles_x = (width + kTile - 1) / kTile, tiles_y = (height + kTile - 1) / kTile;
+  const uint32_t num_tiles = tiles_x * tiles_y;
+  if (E == 0) {
+    SPLAT_CUDA(cudaMemsetAsync(ranges, 0, (size_t)num_tiles * 8, c->stream));
+    return Status::ok();
+  }
+  const uint32_t span = depth_max - depth_min;
+  const int dbits = span == 0 ? 0 : 32 - __builtin_clz(span);
+  const int tbits = num_tiles <= 1 ? 0 : 32 - __builtin_clz(num_tiles - 1);
+  const int total = dbits + tbits;
+  if (total <= 32)
+    return sort_and_range<uint32_t>(c, proj, entry_offset, n, E, depth_range_dev, dbits, total, tiles_x, num_tiles,
+                                    gauss_out, keys_out, ranges);
+  return sort_and_range<uint64_t>(c, proj, entry_offset, n, E, depth_range_dev, dbits, total, tiles_x, num_tiles,
+                                  gauss_out, keys_out, ranges);
+}
+
+}  // namespace splat

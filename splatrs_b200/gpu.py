@@ -1,0 +1,289 @@
+"""Python mirror of the reference's hot-path API over the C ABI, on device tensors.
+
+Function names and argument meaning follow the reference (harryprayiv/splatrs, src/):
+``project_all`` (src/project.rs:320), ``bin`` (src/rasterize.rs:60), ``rasterize_forward``
+(:305), ``rasterize_backward`` (:459), ``project_backward_all`` (src/project.rs:477). Device
+memory comes from torch tensors (plumbing only); every computation runs in the sm_100a
+kernels of libsplatrs_b200.so. There is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import torch
+
+from . import _lib as L
+from ._lib import Camera, ProjOpts, check
+
+PLANES = L.PLANES
+PROJ_FLOATS = L.PROJ_FLOATS
+
+
+def _ptr(t):
+    return C.c_void_p(t.data_ptr()) if t is not None else None
+
+
+class Context:
+    """A splat_ctx: device, stream and scratch arena."""
+
+    def __init__(self, device: int = 0, stream=None):
+        self.device = device
+        self.lib = L.lib()
+        h = C.c_void_p()
+        s = stream.cuda_stream if stream is not None else torch.cuda.current_stream(device).cuda_stream
+        st = self.lib.splat_ctx_create(device, C.c_void_p(s), C.byref(h))
+        if st != L.SPLAT_OK:
+            raise L.SplatError(st, "splat_ctx_create failed")
+        self.h = h
+
+    def set_stream(self, stream):
+        check(self.lib.splat_ctx_set_stream(self.h, C.c_void_p(stream.cuda_stream)), self.h)
+
+    def synchronize(self):
+        check(self.lib.splat_ctx_synchronize(self.h), self.h)
+
+    @property
+    def launches(self) -> int:
+        return int(self.lib.splat_ctx_launch_count(self.h))
+
+    def zero(self, t: torch.Tensor):
+        check(self.lib.splat_zero(self.h, _ptr(t), t.numel() * t.element_size()), self.h)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.splat_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def empty_planes(cap: int, device="cuda") -> torch.Tensor:
+    return torch.zeros(PLANES * cap * 4, dtype=torch.float32, device=device)
+
+
+def params_to_planes(ctx: Context, aos59: torch.Tensor, cap: int | None = None) -> torch.Tensor:
+    """Reference Gaussian records (n, 59) on the device -> parameter planes."""
+    aos59 = aos59.contiguous().to(torch.float32)
+    n = aos59.shape[0]
+    cap = n if cap is None else cap
+    planes = empty_planes(cap, aos59.device)
+    check(ctx.lib.splat_params_from_aos(ctx.h, _ptr(aos59), n, _ptr(planes), cap), ctx.h)
+    return planes
+
+
+def planes_to_params(ctx: Context, planes: torch.Tensor, n: int, cap: int) -> torch.Tensor:
+    out = torch.empty((n, 59), dtype=torch.float32, device=planes.device)
+    check(ctx.lib.splat_params_to_aos(ctx.h, _ptr(planes), n, cap, _ptr(out)), ctx.h)
+    return out
+
+
+@dataclass
+class Projection:
+    """Projection records for one camera (the device form of Vec<Proj>)."""
+    rec: torch.Tensor          # (n, 16) float32
+    num_tiles: torch.Tensor    # (n,) int32 (uint32 values)
+    depth_range: torch.Tensor  # (2,) int32 (uint32 bits)
+    n: int
+    width: int
+    height: int
+
+    def to_reference(self, ctx: Context) -> torch.Tensor:
+        """Reference-layout Proj records (n, 15)."""
+        out = torch.empty((self.n, 15), dtype=torch.float32, device=self.rec.device)
+        check(ctx.lib.splat_proj_to_reference(ctx.h, _ptr(self.rec), self.n, _ptr(out)), ctx.h)
+        return out
+
+
+def project_all(ctx: Context, planes: torch.Tensor, n: int, cap: int, cam: Camera, opts: ProjOpts) -> Projection:
+    """project_all (src/project.rs:320-330)."""
+    dev = planes.device
+    rec = torch.empty((n, PROJ_FLOATS), dtype=torch.float32, device=dev)
+    nt = torch.empty(n, dtype=torch.int32, device=dev)
+    dr = torch.empty(2, dtype=torch.int32, device=dev)
+    check(ctx.lib.splat_project_fwd(ctx.h, _ptr(planes), n, cap, C.byref(cam), C.byref(opts), _ptr(rec), _ptr(nt),
+                                    _ptr(dr)), ctx.h)
+    return Projection(rec, nt, dr, n, cam.width, cam.height)
+
+
+def proj_from_reference(ctx: Context, proj15: torch.Tensor, width: int, height: int) -> Projection:
+    """Projection records from reference-layout Proj records (n, 15) on the device."""
+    proj15 = proj15.contiguous().to(torch.float32)
+    n = proj15.shape[0]
+    dev = proj15.device
+    rec = torch.empty((n, PROJ_FLOATS), dtype=torch.float32, device=dev)
+    nt = torch.empty(n, dtype=torch.int32, device=dev)
+    dr = torch.empty(2, dtype=torch.int32, device=dev)
+    check(ctx.lib.splat_proj_from_reference(ctx.h, _ptr(proj15), n, width, height, _ptr(rec), _ptr(nt), _ptr(dr)),
+          ctx.h)
+    return Projection(rec, nt, dr, n, width, height)
+
+
+@dataclass
+class Binning:
+    """Binning (src/rasterize.rs:26-39) on the device: sorted Gaussian indices per entry."""
+    entry_offset: torch.Tensor  # (n + 1,)
+    gauss: torch.Tensor         # (E,) Gaussian index of each sorted entry
+    keys: torch.Tensor | None   # (E,) int64 (uint64 reference keys) if requested
+    tile_range: torch.Tensor    # (tiles, 2)
+    num_entries: int
+    tiles_x: int
+    tiles_y: int
+
+
+def bin(ctx: Context, proj: Projection, want_keys: bool = False) -> Binning:
+    """bin (src/rasterize.rs:60-128)."""
+    dev = proj.rec.device
+    off = torch.empty(proj.n + 1, dtype=torch.int32, device=dev)
+    e = C.c_int64()
+    check(ctx.lib.splat_bin_count(ctx.h, _ptr(proj.num_tiles), proj.n, _ptr(off), C.byref(e)), ctx.h)
+    E = int(e.value)
+    tx = (proj.width + 15) // 16
+    ty = (proj.height + 15) // 16
+    gauss = torch.empty(max(E, 1), dtype=torch.int32, device=dev)
+    keys = torch.empty(max(E, 1), dtype=torch.int64, device=dev) if want_keys else None
+    tr = torch.empty((tx * ty, 2), dtype=torch.int32, device=dev)
+    check(ctx.lib.splat_bin_sort(ctx.h, _ptr(proj.rec), _ptr(off), proj.n, E, _ptr(proj.depth_range), proj.width,
+                                 proj.height, _ptr(gauss), _ptr(keys), _ptr(tr)), ctx.h)
+    return Binning(off, gauss[:E], keys[:E] if keys is not None else None, tr, E, tx, ty)
+
+
+def _bg(background):
+    arr = (C.c_float * 3)(*[float(x) for x in background])
+    return C.cast(arr, C.POINTER(C.c_float)), arr
+
+
+@dataclass
+class RasterOutput:
+    """RasterOutput (src/rasterize.rs:43-50) on the device."""
+    image: torch.Tensor    # (H*W*3,)
+    final_t: torch.Tensor  # (H*W,)
+    n_contrib: torch.Tensor  # (H*W,) int32
+    pairs: torch.Tensor    # (1,) int64, evaluated (entry, pixel) pairs
+
+
+def rasterize_forward(ctx: Context, proj: Projection, b: Binning, background) -> RasterOutput:
+    """rasterize_forward (src/rasterize.rs:305-337)."""
+    dev = proj.rec.device
+    npix = proj.width * proj.height
+    image = torch.empty(npix * 3, dtype=torch.float32, device=dev)
+    ft = torch.empty(npix, dtype=torch.float32, device=dev)
+    nc = torch.empty(npix, dtype=torch.int32, device=dev)
+    pairs = torch.zeros(1, dtype=torch.int64, device=dev)
+    bgp, keep = _bg(background)
+    check(ctx.lib.splat_rasterize_fwd(ctx.h, _ptr(proj.rec), _ptr(b.gauss), _ptr(b.tile_range), proj.width,
+                                      proj.height, bgp, _ptr(image), _ptr(ft), _ptr(nc), _ptr(pairs)), ctx.h)
+    return RasterOutput(image, ft, nc, pairs)
+
+
+def rasterize_backward(ctx: Context, proj: Projection, b: Binning, background, out: RasterOutput,
+                       dimage: torch.Tensor, pgrad: torch.Tensor | None = None, cap: int | None = None,
+                       pairs: torch.Tensor | None = None) -> torch.Tensor:
+    """rasterize_backward (src/rasterize.rs:459-505). Returns the screen-space gradient
+    planes (3, cap, 4): ProjGrad plus the AbsGS accumulators."""
+    dev = proj.rec.device
+    cap = proj.n if cap is None else cap
+    if pgrad is None:
+        pgrad = torch.zeros((3, cap, 4), dtype=torch.float32, device=dev)
+    bgp, keep = _bg(background)
+    check(ctx.lib.splat_rasterize_bwd(ctx.h, _ptr(proj.rec), _ptr(b.gauss), _ptr(b.tile_range), proj.width,
+                                      proj.height, bgp, _ptr(out.final_t), _ptr(out.n_contrib),
+                                      _ptr(dimage.contiguous()), _ptr(pgrad), cap, _ptr(pairs)), ctx.h)
+    return pgrad
+
+
+def pgrad_to_reference(pgrad: torch.Tensor, n: int):
+    """Screen-space gradient planes -> (ProjGrad (n, 9), abs (n, 2)) in the reference layout."""
+    g0, g1, g2 = pgrad[0, :n], pgrad[1, :n], pgrad[2, :n]
+    grads = torch.stack([g0[:, 0], g0[:, 1], g0[:, 2], g0[:, 3], g1[:, 0], g1[:, 1], g1[:, 2], g1[:, 3], g2[:, 0]], 1)
+    absg = g2[:, 1:3]
+    return grads, absg
+
+
+def pgrad_from_reference(grads9: torch.Tensor, abs2: torch.Tensor | None = None, cap: int | None = None):
+    n = grads9.shape[0]
+    cap = n if cap is None else cap
+    p = torch.zeros((3, cap, 4), dtype=torch.float32, device=grads9.device)
+    p[0, :n] = grads9[:, 0:4]
+    p[1, :n] = grads9[:, 4:8]
+    p[2, :n, 0] = grads9[:, 8]
+    if abs2 is not None:
+        p[2, :n, 1:3] = abs2
+    return p
+
+
+def project_backward_all(ctx: Context, planes: torch.Tensor, n: int, cap: int, cam: Camera, opts: ProjOpts,
+                         proj: Projection, pgrad: torch.Tensor, stats: torch.Tensor | None = None,
+                         absgrad: bool = False) -> torch.Tensor:
+    """project_backward_all (src/project.rs:477-493); returns gradient planes.
+
+    With ``stats`` (3 * cap 32-bit words: grad_accum f32, denom u32, max_radii u32) it also
+    performs DensifyStats::accumulate (src/densify.rs:36-60)."""
+    out = torch.empty(PLANES * cap * 4, dtype=torch.float32, device=planes.device)
+    check(ctx.lib.splat_project_bwd(ctx.h, _ptr(planes), n, cap, C.byref(cam), C.byref(opts), _ptr(proj.rec),
+                                    _ptr(pgrad), _ptr(out), _ptr(stats), int(bool(absgrad))), ctx.h)
+    return out
+
+
+class Renderer:
+    """splat_renderer: a device-resident model driven with host (numpy) buffers.
+
+    ``render`` is render::render (src/render.rs:14-23); ``render_backward`` runs the chain
+    of examples/profile.rs:34-52 and returns the parameter gradients as reference records."""
+
+    def __init__(self, ctx: Context):
+        self.ctx = ctx
+        self.lib = ctx.lib
+        h = C.c_void_p()
+        check(self.lib.splat_renderer_create(ctx.h, C.byref(h)), ctx.h)
+        self.h = h
+        self.n = 0
+
+    def set_model(self, aos59, sh_degree: int):
+        import numpy as np
+        a = np.ascontiguousarray(aos59, np.float32).reshape(-1, 59)
+        self.n = a.shape[0]
+        check(self.lib.splat_renderer_set_model(self.h, a.ctypes.data_as(C.c_void_p), self.n, sh_degree), self.ctx.h)
+
+    def render(self, cam: Camera, opts: ProjOpts, background, image_out=None):
+        import numpy as np
+        if image_out is None:
+            image_out = np.empty(cam.width * cam.height * 3, np.float32)
+        bgp, keep = _bg(background)
+        check(self.lib.splat_renderer_render(self.h, C.byref(cam), C.byref(opts), bgp,
+                                             image_out.ctypes.data_as(C.c_void_p)), self.ctx.h)
+        return image_out
+
+    def render_backward(self, cam: Camera, opts: ProjOpts, background, dimage, image_out=None, grads_out=None,
+                        want_image=True, want_grads=True):
+        import numpy as np
+        if want_image and image_out is None:
+            image_out = np.empty(cam.width * cam.height * 3, np.float32)
+        if want_grads and grads_out is None:
+            grads_out = np.empty((self.n, 59), np.float32)
+        d = np.ascontiguousarray(dimage, np.float32)
+        bgp, keep = _bg(background)
+        check(self.lib.splat_renderer_render_backward(
+            self.h, C.byref(cam), C.byref(opts), bgp, d.ctypes.data_as(C.c_void_p),
+            image_out.ctypes.data_as(C.c_void_p) if want_image else None,
+            grads_out.ctypes.data_as(C.c_void_p) if want_grads else None), self.ctx.h)
+        return image_out, grads_out
+
+    @property
+    def last_entries(self) -> int:
+        return int(self.lib.splat_renderer_last_entries(self.h))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.splat_renderer_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,88 @@
+"""Seeded synthetic scenes with the shapes and value distributions of the benchmark
+configurations. No public dataset is involved: every scene is drawn from numpy generators
+with fixed seeds, and the same arrays feed the CUDA path and the CPU oracle.
+
+Parameter records use the reference layout (59 floats per Gaussian: mean[3] log_scale[3]
+quat[4] opacity sh[16][3], reference src/model.rs:16-28); cameras are 18-value records
+(width, height, fx, fy, cx, cy, rot[9] row major, trans[3]) built like Camera::look_at
+(reference src/camera.rs:66-93).
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+SH_C0 = 0.28209479177387814
+
+
+def look_at(width, height, fx, fy, eye, target, up=(0.0, -1.0, 0.0)):
+    """Camera::look_at (src/camera.rs:66-93): +z forward, x right, y down."""
+    eye = np.asarray(eye, np.float64)
+    fwd = np.asarray(target, np.float64) - eye
+    fwd /= np.linalg.norm(fwd)
+    right = np.cross(fwd, np.asarray(up, np.float64))
+    right /= np.linalg.norm(right)
+    down = np.cross(fwd, right)
+    rot = np.stack([right, down, fwd]).astype(np.float32)
+    trans = -(rot.astype(np.float64) @ eye)
+    rec = np.zeros(18, np.float32)
+    rec[0:6] = [width, height, fx, fy, width / 2.0, height / 2.0]
+    rec[6:15] = rot.ravel()
+    rec[15:18] = trans
+    return rec
+
+
+def random_gaussians(rng, n, mean_lo, mean_hi, log_scale_mu, log_scale_sigma, opacity_sigma, dc_mu=0.5,
+                     dc_sigma=0.2, rest_sigma=0.05):
+    """Gaussians with means uniform in a box, normal log-scales and opacity logits,
+    quaternions normalise(N(0,1)^4), SH degree 3 with normal DC and higher bands."""
+    g = np.zeros((n, 59), np.float32)
+    g[:, 0:3] = rng.uniform(mean_lo, mean_hi, (n, 3))
+    g[:, 3:6] = rng.normal(log_scale_mu, log_scale_sigma, (n, 3))
+    q = rng.normal(0.0, 1.0, (n, 4))
+    g[:, 6:10] = q / np.linalg.norm(q, axis=1, keepdims=True)
+    g[:, 10] = rng.normal(0.0, opacity_sigma, n)
+    sh = rng.normal(0.0, rest_sigma, (n, 16, 3))
+    sh[:, 0, :] = rng.normal(dc_mu, dc_sigma, (n, 3))
+    g[:, 11:] = sh.reshape(n, 48)
+    return g
+
+
+def fibonacci_sphere(n, radius):
+    """n points spread over a sphere (golden-angle spiral), none at the poles."""
+    pts = []
+    ga = math.pi * (3.0 - math.sqrt(5.0))
+    for i in range(n):
+        y = 1.0 - 2.0 * (i + 0.5) / n
+        r = math.sqrt(max(0.0, 1.0 - y * y))
+        th = ga * i
+        pts.append((radius * r * math.cos(th), radius * y, radius * r * math.sin(th)))
+    return np.array(pts)
+
+
+def config0(seed_gt=0, seed_init=1, n_gt=10000, n_cams=16, size=256, f=300.0, n_init=5000):
+    """Plain method on a small scene: 10k ground-truth Gaussians in [-1,1]^3, log-scales
+    N(-4,0.3), opacity logits N(0,1), SH degree 3 (DC N(0.5,0.2), rest N(0,0.05)); 16
+    cameras on a radius-4 sphere looking at the origin at 256x256, f=300, c=128; 5k
+    initial points = ground-truth means + N(0,0.02)."""
+    rng = np.random.default_rng(seed_gt)
+    gt = random_gaussians(rng, n_gt, -1.0, 1.0, -4.0, 0.3, 1.0)
+    cams = np.stack([look_at(size, size, f, f, eye, (0, 0, 0)) for eye in fibonacci_sphere(n_cams, 4.0)])
+    rng1 = np.random.default_rng(seed_init)
+    pick = rng1.choice(n_gt, size=n_init, replace=False)
+    pts = (gt[pick, 0:3] + rng1.normal(0.0, 0.02, (n_init, 3))).astype(np.float32)
+    rgb = np.round(np.clip(gt[pick, 11:14] * SH_C0 + 0.5, 0.0, 1.0) * 255.0).astype(np.uint8)
+    return dict(gt=gt, cams=cams, init_points=pts, init_rgb=rgb, sh_degree=3, background=(0.0, 0.0, 0.0))
+
+
+def config1(seed=0, n=1_000_000, width=1920, height=1080, f=1500.0, distance=12.0):
+    """Render-only kernel benchmark: 1M Gaussians with means uniform in a 10x10x10 box
+    centred at the origin, camera at distance 12 looking at the centre, f=1500, 1920x1080,
+    log-scales N(-4.5,0.5), opacity logits N(0,1.5), SH degree 3 as in config 0, and an
+    upstream dL/dpixel drawn N(0,1) per channel."""
+    rng = np.random.default_rng(seed)
+    g = random_gaussians(rng, n, -5.0, 5.0, -4.5, 0.5, 1.5)
+    cam = look_at(width, height, f, f, (0.0, 0.0, -distance), (0.0, 0.0, 0.0))
+    dimage = rng.normal(0.0, 1.0, width * height * 3).astype(np.float32)
+    return dict(params=g, cam=cam, dimage=dimage, sh_degree=3, background=(0.0, 0.0, 0.0))
