@@ -107,6 +107,17 @@ class ClockSampler:
         return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def max_over_ranks(value: float, world: int, device=None) -> float:
+    """The slowest rank's value (every rank calls this in the same order)."""
+    if world <= 1:
+        return float(value)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def measured_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -160,7 +171,7 @@ def run_ours(args, rank, world, local):
         mark(1)
         b = G.bin(ctx, proj)
         mark(2)
-        out = G.rasterize_forward(ctx, proj, b, bg)
+        out = G.rasterize_forward(ctx, proj, b, bg, count_pairs=ev is None)
         mark(3)
         ctx.zero(pgrad)
         G.rasterize_backward(ctx, proj, b, bg, out, dimage, pgrad=pgrad, cap=n)
@@ -201,11 +212,8 @@ def run_ours(args, rank, world, local):
     torch.cuda.synchronize(dev)
     launches = ctx.launches - launches0
     clocks = sampler.stop()
-    elapsed_ms = t0.elapsed_time(t1)
+    elapsed_ms = max_over_ranks(t0.elapsed_time(t1), world, dev)
     if world > 1:
-        tt = torch.tensor([elapsed_ms], device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        elapsed_ms = float(tt.item())
         dist.barrier()
     stage_ms = {nm: 0.0 for nm in ["project_fwd", "bin", "raster_fwd", "raster_bwd", "project_bwd"]}
     for k in range(args.steps):
@@ -238,11 +246,7 @@ def run_ours(args, rank, world, local):
     tw = time.perf_counter()
     for _ in range(e_steps):
         r.render_backward(cam, opts, bg, dimage_h, img_h, grads_h)
-    e2e_ms = (time.perf_counter() - tw) * 1e3 / e_steps
-    if world > 1:
-        tt = torch.tensor([e2e_ms], device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_ms = float(tt.item())
+    e2e_ms = max_over_ranks((time.perf_counter() - tw) * 1e3 / e_steps, world, dev)
     r.close()
     e2e = {"value": round(mpix * world / (e2e_ms / 1e3), 3), "unit": UNIT,
            "h2d_bytes_per_step": int(dimage_h.nbytes), "d2h_bytes_per_step": int(img_h.nbytes + grads_h.nbytes),

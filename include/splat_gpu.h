@@ -16,7 +16,8 @@
  *    comment says they synchronise (they do only to read a count back, as the reference's
  *    `Vec` sizes require).
  *  - A context is used from one host thread at a time. Separate contexts may run
- *    concurrently on separate streams.
+ *    concurrently on separate streams. Renderers and trainers borrow their context and
+ *    must be destroyed before it.
  *
  * Device layouts
  *  - Parameter planes (`planes_dev`): SPLAT_PLANES planes of float4, plane p at
@@ -206,6 +207,11 @@ SPLAT_API int splat_project_bwd(splat_ctx* ctx, const float* planes_dev, int64_t
                                 const splat_camera* cam, const splat_proj_opts* opts, const float* proj_dev,
                                 const float* pgrad_dev, float* grad_planes_dev, void* stats_dev, int32_t absgrad);
 
+/* Diagnostic: the largest relative error of the fast exp used for the backward pass's
+ * screening against the correctly rounded exp, over every float x with |x| in [lo, hi]
+ * (negative != 0 selects -|x|). Synchronises. */
+SPLAT_API int splat_diag_fast_exp_error(splat_ctx* ctx, float lo, float hi, int32_t negative, float* max_rel_error);
+
 /* Fill `bytes` bytes of device memory with zeros on the context stream. */
 SPLAT_API int splat_zero(splat_ctx* ctx, void* dev, size_t bytes);
 
@@ -233,6 +239,83 @@ SPLAT_API int splat_renderer_render_backward(splat_renderer* r, const splat_came
                                              float* grads_aos59_host);
 /* Tile entries of the last rendered view (Binning::sorted.len()). */
 SPLAT_API int64_t splat_renderer_last_entries(const splat_renderer* r);
+
+/* ----------------------------------------------------------------------------------------
+ * Loss: photometric_loss (reference src/loss.rs:137-171, ssim_with_grad :75-134) with the
+ * prediction pred_dev (H*W*3 float) against target_dev, either 8-bit pixels converted as
+ * View::to_real does (target_is_u8 = 1, reference src/dataset.rs:23-25) or floats. Writes
+ * d loss / d pred to grad_dev and (loss, mean SSIM, PSNR) to out3_dev (3 floats; PSNR as
+ * in loss.rs:175-190).
+ * -------------------------------------------------------------------------------------- */
+SPLAT_API int splat_loss_fwd_bwd(splat_ctx* ctx, const float* pred_dev, const void* target_dev, int32_t target_is_u8,
+                                 uint32_t width, uint32_t height, float lambda_dssim, float* grad_dev,
+                                 float* out3_dev);
+
+/* Adam::step (reference src/adam.rs:77-161) on parameter planes: params, first and second
+ * moments updated in place from the gradient planes. `step` is the step count after the
+ * increment (1 for the first step); beta1 0.9, beta2 0.999, eps 1e-15. */
+SPLAT_API int splat_adam_step(splat_ctx* ctx, float* planes_dev, const float* grad_planes_dev, float* m_dev,
+                              float* v_dev, int64_t n, int64_t cap, uint64_t step, const splat_lr* lr);
+
+/* What one densification step did (reference src/densify.rs:107-114) and the new count. */
+typedef struct splat_densify_report {
+  uint64_t cloned, split, pruned, new_count;
+} splat_densify_report;
+
+/* densify_and_prune (reference src/densify.rs:125-221): clone, split and prune n Gaussians
+ * (params, Adam moments, statistics as written by splat_project_bwd) into the output
+ * planes (capacity cap_out), in the reference's order: surviving originals, surviving
+ * clones, surviving split children. Split offsets are drawn from the SplitMix64 generator
+ * whose state is *rng_state (advanced in place), per split parent, per child, x then y
+ * then z, with Box-Muller normals. If the survivors exceed cap_out the call returns
+ * SPLAT_ERR_CAPACITY with report->new_count set, writes nothing and leaves *rng_state
+ * unchanged. Synchronises once to read the counts. */
+SPLAT_API int splat_densify(splat_ctx* ctx, const float* planes_dev, const float* m_dev, const float* v_dev, int64_t n,
+                            int64_t cap, const void* stats_dev, const splat_densify_config* cfg, float extent,
+                            uint64_t* rng_state, float* planes_out_dev, float* m_out_dev, float* v_out_dev,
+                            int64_t cap_out, splat_densify_report* report);
+
+/* reset_opacity (reference src/densify.rs:224-230): opacity logits clamped to
+ * inverse_sigmoid(max_alpha) and the opacity moments zeroed. */
+SPLAT_API int splat_reset_opacity(splat_ctx* ctx, float* planes_dev, float* m_dev, float* v_dev, int64_t n,
+                                  float max_alpha);
+
+/* ----------------------------------------------------------------------------------------
+ * Trainer: train::train (reference src/train.rs:161-306) one iteration per call, with the
+ * model, Adam state, statistics and the training views (8-bit pixels) resident in device
+ * memory. The view order and split offsets come from a SplitMix64 generator seeded with
+ * cfg->seed (the reference uses ChaCha8; the schedule is otherwise the reference's).
+ * -------------------------------------------------------------------------------------- */
+typedef struct splat_trainer splat_trainer;
+
+/* Progress of one iteration (reference src/train.rs:142-157, DensifyReport). */
+typedef struct splat_step_info {
+  double loss;
+  double psnr; /* of this iteration's render against its view */
+  uint32_t view;
+  int32_t densified;
+  int32_t reset;
+  uint64_t num_gaussians;
+  uint64_t cloned, split, pruned;
+  uint64_t entries;
+} splat_step_info;
+
+/* Fails with SPLAT_ERR_INVALID for zero iterations or sh_degree > 3 (train.rs:169-183). */
+SPLAT_API int splat_trainer_create(splat_ctx* ctx, const splat_train_config* cfg, float extent, splat_trainer** out);
+SPLAT_API int splat_trainer_destroy(splat_trainer* t);
+/* Initial model as n reference records (e.g. from Model::from_points). */
+SPLAT_API int splat_trainer_set_model(splat_trainer* t, const float* aos59_host, int64_t n);
+/* One training view: camera and H*W*3 8-bit pixels (View, reference src/dataset.rs:14-26). */
+SPLAT_API int splat_trainer_add_view(splat_trainer* t, const splat_camera* cam, const uint8_t* rgb_host);
+/* Reset generator, optimiser state and statistics; SH degree 0 (train.rs:184-189). */
+SPLAT_API int splat_trainer_start(splat_trainer* t);
+SPLAT_API int splat_trainer_step(splat_trainer* t, splat_step_info* info);
+SPLAT_API int64_t splat_trainer_count(const splat_trainer* t);
+SPLAT_API int32_t splat_trainer_sh_degree(const splat_trainer* t);
+SPLAT_API uint32_t splat_trainer_iteration(const splat_trainer* t);
+SPLAT_API int splat_trainer_get_model(splat_trainer* t, float* aos59_host);
+/* render::render of the current model at the active SH degree and the config's background. */
+SPLAT_API int splat_trainer_render(splat_trainer* t, const splat_camera* cam, float* image_host);
 
 #ifdef __cplusplus
 }

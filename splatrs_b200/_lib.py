@@ -106,6 +106,21 @@ class TrainConfig(C.Structure):
         return c
 
 
+class DensifyReport(C.Structure):
+    """splat_densify_report (reference src/densify.rs:107-114, plus the new count)."""
+    _fields_ = [("cloned", C.c_uint64), ("split", C.c_uint64), ("pruned", C.c_uint64), ("new_count", C.c_uint64)]
+
+
+class StepInfo(C.Structure):
+    """splat_step_info (reference src/train.rs:142-157)."""
+    _fields_ = [("loss", C.c_double), ("psnr", C.c_double), ("view", C.c_uint32), ("densified", C.c_int32),
+                ("reset", C.c_int32), ("num_gaussians", C.c_uint64), ("cloned", C.c_uint64), ("split", C.c_uint64),
+                ("pruned", C.c_uint64), ("entries", C.c_uint64)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
 _lib = None
 
 
@@ -122,6 +137,7 @@ def _declare(L):
         "splat_last_error": ([vp], C.c_char_p),
         "splat_ctx_launch_count": ([vp], C.c_uint64),
         "splat_zero": ([vp, vp, sz], C.c_int),
+        "splat_diag_fast_exp_error": ([vp, C.c_float, C.c_float, i32, P(C.c_float)], C.c_int),
         "splat_params_from_aos": ([vp, vp, i64, vp, i64], C.c_int),
         "splat_params_to_aos": ([vp, vp, i64, i64, vp], C.c_int),
         "splat_project_fwd": ([vp, vp, i64, i64, P(Camera), P(ProjOpts), vp, vp, vp], C.c_int),
@@ -141,11 +157,25 @@ def _declare(L):
         "splat_renderer_render_backward": ([vp, P(Camera), P(ProjOpts), P(C.c_float), vp, vp, vp], C.c_int),
         "splat_renderer_last_entries": ([vp], i64),
     })
-    optional = {
+    sig.update({
         "splat_loss_fwd_bwd": ([vp, vp, vp, i32, u32, u32, C.c_float, vp, vp], C.c_int),
-        "splat_psnr": ([vp, vp, vp, i32, i64, vp], C.c_int),
         "splat_adam_step": ([vp, vp, vp, vp, vp, i64, i64, C.c_uint64, P(LearningRates)], C.c_int),
-    }
+        "splat_densify": ([vp, vp, vp, vp, i64, i64, vp, P(DensifyConfig), C.c_float, P(C.c_uint64), vp, vp, vp, i64,
+                           P(DensifyReport)], C.c_int),
+        "splat_reset_opacity": ([vp, vp, vp, vp, i64, C.c_float], C.c_int),
+        "splat_trainer_create": ([vp, P(TrainConfig), C.c_float, P(vp)], C.c_int),
+        "splat_trainer_destroy": ([vp], C.c_int),
+        "splat_trainer_set_model": ([vp, vp, i64], C.c_int),
+        "splat_trainer_add_view": ([vp, P(Camera), vp], C.c_int),
+        "splat_trainer_start": ([vp], C.c_int),
+        "splat_trainer_step": ([vp, P(StepInfo)], C.c_int),
+        "splat_trainer_count": ([vp], i64),
+        "splat_trainer_sh_degree": ([vp], i32),
+        "splat_trainer_iteration": ([vp], u32),
+        "splat_trainer_get_model": ([vp, vp], C.c_int),
+        "splat_trainer_render": ([vp, P(Camera), vp], C.c_int),
+    })
+    optional = {}
     for name, (args, res) in sig.items():
         f = getattr(L, name)
         f.argtypes = args

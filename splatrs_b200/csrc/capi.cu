@@ -2,9 +2,11 @@
 // dispatch to the stage launchers. No entry point aborts; failures return a status and
 // leave a message on the context.
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <new>
+#include <vector>
 
 #include "common.cuh"
 #include "kernels.cuh"
@@ -171,6 +173,13 @@ SPLAT_API const char* splat_last_error(const splat_ctx* ctx) { return ctx ? ctx-
 
 SPLAT_API uint64_t splat_ctx_launch_count(const splat_ctx* ctx) { return ctx ? ctx->c.launches.count : 0; }
 
+SPLAT_API int splat_diag_fast_exp_error(splat_ctx* ctx, float lo, float hi, int32_t negative, float* max_rel_error) {
+  if (!ctx) return SPLAT_ERR_INVALID;
+  if (!max_rel_error || !(lo >= 0.0f) || !(hi >= lo) || !(hi < 1e30f)) return invalid(ctx, "splat_diag_fast_exp_error: bad range");
+  Enter e(ctx);
+  return finish(ctx, launch_diag_fast_exp(&ctx->c, lo, hi, negative, max_rel_error));
+}
+
 SPLAT_API int splat_zero(splat_ctx* ctx, void* dev, size_t bytes) {
   if (!ctx || (!dev && bytes)) return invalid(ctx, "splat_zero: null pointer");
   Enter e(ctx);
@@ -303,6 +312,99 @@ SPLAT_API int splat_project_bwd(splat_ctx* ctx, const float* planes_dev, int64_t
   Enter e(ctx);
   return finish(ctx, launch_project_bwd(&ctx->c, planes_dev, n, cap, *cam, *opts, proj_dev, pgrad_dev,
                                         grad_planes_dev, stats_dev, absgrad));
+}
+
+}  // extern "C"
+
+namespace {
+struct SplitMix64State {
+  uint64_t s;
+  uint64_t next() {
+    uint64_t z = (s += 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+  }
+  double uniform() { return (double)(next() >> 11) * (1.0 / 9007199254740992.0); }
+  double normal() {  // Box-Muller with u1 kept away from zero (densify.rs:116-121)
+    const double u1 = std::max(uniform(), 1e-12);
+    const double u2 = uniform();
+    return std::sqrt(-2.0 * std::log(u1)) * std::cos(2.0 * 3.14159265358979323846 * u2);
+  }
+};
+}  // namespace
+
+extern "C" {
+
+SPLAT_API int splat_loss_fwd_bwd(splat_ctx* ctx, const float* pred_dev, const void* target_dev, int32_t target_is_u8,
+                                 uint32_t width, uint32_t height, float lambda_dssim, float* grad_dev,
+                                 float* out3_dev) {
+  if (!ctx) return SPLAT_ERR_INVALID;
+  if (!pred_dev || !target_dev || !grad_dev || !out3_dev || width == 0 || height == 0)
+    return invalid(ctx, "splat_loss_fwd_bwd: bad arguments");
+  Enter e(ctx);
+  return finish(ctx, launch_loss(&ctx->c, pred_dev, target_dev, target_is_u8 ? 1 : 0, width, height, lambda_dssim,
+                                 grad_dev, out3_dev));
+}
+
+SPLAT_API int splat_adam_step(splat_ctx* ctx, float* planes_dev, const float* grad_planes_dev, float* m_dev,
+                              float* v_dev, int64_t n, int64_t cap, uint64_t step, const splat_lr* lr) {
+  if (!ctx) return SPLAT_ERR_INVALID;
+  if (!lr || n < 0 || cap < n || step == 0 || (n && (!planes_dev || !grad_planes_dev || !m_dev || !v_dev)))
+    return invalid(ctx, "splat_adam_step: bad arguments");
+  Enter e(ctx);
+  return finish(ctx, launch_adam(&ctx->c, planes_dev, grad_planes_dev, m_dev, v_dev, n, cap, step, *lr));
+}
+
+SPLAT_API int splat_densify(splat_ctx* ctx, const float* planes_dev, const float* m_dev, const float* v_dev, int64_t n,
+                            int64_t cap, const void* stats_dev, const splat_densify_config* cfg, float extent,
+                            uint64_t* rng_state, float* planes_out_dev, float* m_out_dev, float* v_out_dev,
+                            int64_t cap_out, splat_densify_report* report) {
+  if (!ctx) return SPLAT_ERR_INVALID;
+  if (!cfg || !rng_state || !report || n < 0 || cap < n || cfg->split_children < 1 || cfg->split_children > 16 ||
+      (n && (!planes_dev || !m_dev || !v_dev || !stats_dev || !planes_out_dev || !m_out_dev || !v_out_dev)))
+    return invalid(ctx, "splat_densify: bad arguments");
+  Enter e(ctx);
+  Ctx* c = &ctx->c;
+  DensifyParams dp;
+  dp.cfg = *cfg;
+  dp.extent = extent;
+  dp.shrink = logf(0.8f * (float)cfg->split_children);
+  const float* accum = static_cast<const float*>(stats_dev);
+  const uint32_t* denom = reinterpret_cast<const uint32_t*>(accum + cap);
+  const uint32_t* maxr = denom + cap;
+  DensifyPlan plan;
+  Status s = densify_plan(c, planes_dev, n, cap, accum, denom, maxr, dp, &plan);
+  if (!s.good()) return fail(ctx, s);
+  report->cloned = plan.cloned;
+  report->split = plan.split;
+  report->pruned = plan.pruned;
+  report->new_count = plan.new_count();
+  if ((int64_t)plan.new_count() > cap_out)
+    return fail(ctx, Status::make(SPLAT_ERR_CAPACITY, "splat_densify: output capacity too small"));
+  SplitMix64State rng{*rng_state};
+  const size_t nn = (size_t)plan.split * cfg->split_children * 3;
+  std::vector<double> normals(nn);
+  for (size_t q = 0; q < nn; q++) normals[q] = rng.normal();
+  double* nd = nullptr;
+  s = arena_reserve(c, std::max<size_t>(nn, 1) * 8, (void**)&nd);
+  if (s.good() && nn) s = cuda_status(cudaMemcpyAsync(nd, normals.data(), nn * 8, cudaMemcpyHostToDevice, c->stream),
+                                      "upload normals");
+  if (s.good()) s = densify_apply(c, planes_dev, m_dev, v_dev, n, cap, plan, nd, planes_out_dev, m_out_dev, v_out_dev,
+                                  cap_out);
+  if (s.good()) s = cuda_status(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
+  if (!s.good()) return fail(ctx, s);
+  *rng_state = rng.s;
+  return SPLAT_OK;
+}
+
+SPLAT_API int splat_reset_opacity(splat_ctx* ctx, float* planes_dev, float* m_dev, float* v_dev, int64_t n,
+                                  float max_alpha) {
+  if (!ctx) return SPLAT_ERR_INVALID;
+  if (n < 0 || (n && (!planes_dev || !m_dev || !v_dev))) return invalid(ctx, "splat_reset_opacity: bad arguments");
+  Enter e(ctx);
+  const float limit = logf(max_alpha / (1.0f - max_alpha));  // inverse_sigmoid (math.rs:454)
+  return finish(ctx, launch_reset_opacity(&ctx->c, planes_dev, m_dev, v_dev, n, limit));
 }
 
 }  // extern "C"

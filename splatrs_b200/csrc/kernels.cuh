@@ -29,4 +29,41 @@ Status launch_raster_bwd(Ctx* c, const float* proj, const uint32_t* gauss, const
                          uint32_t height, const float bg[3], const float* final_t, const uint32_t* n_contrib,
                          const float* dimage, float* pgrad, int64_t cap, uint64_t* pairs);
 
+Status launch_diag_fast_exp(Ctx* c, float magnitude_lo, float magnitude_hi, int negative, float* out_host);
+
+Status launch_loss(Ctx* c, const float* pred, const void* target, int target_u8, uint32_t width, uint32_t height,
+                   float lambda, float* grad, float* out3);
+
+Status launch_adam(Ctx* c, float* params, const float* grads, float* m, float* v, int64_t n, int64_t cap,
+                   uint64_t step, const splat_lr& lr);
+Status launch_reset_opacity(Ctx* c, float* params, float* m, float* v, int64_t n, float limit);
+
+struct DensifyArgs {
+  float grad_threshold, size_limit, min_opacity, big_world_limit, shrink;
+  int prune_big_world;
+  int64_t max_screen_size;
+  int children;
+};
+struct DensifyParams {
+  splat_densify_config cfg;
+  float extent;
+  float shrink;  // ln(0.8 * children), densify.rs:169
+};
+// Decisions of one densification step; the arrays live in the context arena until the
+// next entry point.
+struct DensifyPlan {
+  uint64_t kept_orig = 0, cloned = 0, kept_clones = 0, split = 0, kept_children = 0, pruned = 0;
+  uint32_t *flags = nullptr, *off_orig = nullptr, *off_clone = nullptr, *off_split = nullptr, *off_child = nullptr;
+  DensifyArgs args;
+  uint64_t new_count() const { return kept_orig + kept_clones + kept_children; }
+};
+// Marks, scans and reads the counts back (synchronises).
+Status densify_plan(Ctx* c, const float* params, int64_t n, int64_t cap, const float* accum, const uint32_t* denom,
+                    const uint32_t* maxr, const DensifyParams& dp, DensifyPlan* plan);
+// Writes the new parameters and Adam state (out of place). `normals_dev` holds
+// 3 * children samples per split parent, in the reference's draw order.
+Status densify_apply(Ctx* c, const float* params, const float* m, const float* v, int64_t n, int64_t cap,
+                     const DensifyPlan& plan, const double* normals_dev, float* po, float* mo, float* vo,
+                     int64_t cap_out);
+
 }  // namespace splat

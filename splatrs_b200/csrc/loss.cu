@@ -1,0 +1,265 @@
+// Photometric loss (1 - lambda) L1 + lambda (1 - SSIM) with its gradient (reference
+// src/loss.rs:14-190), as two tiled kernels.
+//
+//   ssim_fwd: per 32x32 output tile and channel, the 11-tap separable zero-padded blur of
+//     x, y, x^2, y^2 and xy from a shared-memory tile with a 5-pixel halo; per-pixel SSIM
+//     and its partial derivatives w.r.t. mu_x, E[x^2], E[xy] (written to scratch); block
+//     sums of SSIM, |x - y| and the clamped squared error for PSNR (loss.rs:175-190).
+//   ssim_bwd: the same blur of the three partial maps (the blur is self-adjoint,
+//     loss.rs:124-127) and the gradient of the whole loss w.r.t. the prediction.
+// The target can be the view's 8-bit pixels, converted exactly as View::to_real does
+// (reference src/dataset.rs:23-25), or floats. Blur sums run over the window in the
+// reference's order and skip out-of-image taps, so the blurred maps, the partial maps and
+// the gradient are bit-identical to the reference's; only the three scalar sums depend on
+// summation order (accumulated in double here).
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace splat {
+
+constexpr int kLT = 32;            // output tile edge
+constexpr int kHalo = 5;           // SSIM_WINDOW / 2
+constexpr int kLE = kLT + 2 * kHalo;
+constexpr int kLossThreads = 256;
+
+struct LossKernel {
+  float w[11];
+};
+
+__device__ __forceinline__ float load_target(const void* target, int target_u8, size_t idx) {
+  if (target_u8) return (float)static_cast<const uint8_t*>(target)[idx] / 255.0f;
+  return static_cast<const float*>(target)[idx];
+}
+
+// Sums: [0] SSIM, [1] |x - y|, [2] squared clamped error (PSNR).
+__global__ void __launch_bounds__(kLossThreads) ssim_fwd_kernel(const float* __restrict__ pred,
+                                                                const void* __restrict__ target, int target_u8,
+                                                                uint32_t width, uint32_t height, LossKernel K,
+                                                                float* __restrict__ dmaps, double* __restrict__ sums) {
+  __shared__ float sx[kLE][kLE], sy[kLE][kLE];
+  __shared__ float h[5][kLE][kLT];
+  __shared__ double red[3][kLossThreads / 32];
+  const int ox0 = blockIdx.x * kLT, oy0 = blockIdx.y * kLT;
+  const int tid = threadIdx.x;
+  const float c1 = 0.01f * 0.01f, c2 = 0.03f * 0.03f;
+  double s_ssim = 0.0, s_l1 = 0.0, s_se = 0.0;
+  for (int ch = 0; ch < 3; ch++) {
+    for (int i = tid; i < kLE * kLE; i += kLossThreads) {
+      const int r = i / kLE, c = i % kLE;
+      const int gy = oy0 - kHalo + r, gx = ox0 - kHalo + c;
+      float vx = 0.0f, vy = 0.0f;
+      if (gx >= 0 && gx < (int)width && gy >= 0 && gy < (int)height) {
+        const size_t idx = ((size_t)gy * width + gx) * 3 + ch;
+        vx = pred[idx];
+        vy = load_target(target, target_u8, idx);
+      }
+      sx[r][c] = vx;
+      sy[r][c] = vy;
+    }
+    __syncthreads();
+    // Horizontal pass (loss.rs:42-56) for every halo row and every output column.
+    for (int i = tid; i < kLE * kLT; i += kLossThreads) {
+      const int r = i / kLT, c = i % kLT;
+      const int gx = ox0 + c;
+      float a0 = 0.0f, a1 = 0.0f, a2 = 0.0f, a3 = 0.0f, a4 = 0.0f;
+#pragma unroll
+      for (int k = 0; k < 11; k++) {
+        const int xs = gx + k - kHalo;
+        if (xs >= 0 && xs < (int)width) {
+          const float vx = sx[r][c + k], vy = sy[r][c + k];
+          a0 += K.w[k] * vx;
+          a1 += K.w[k] * vy;
+          a2 += K.w[k] * (vx * vx);
+          a3 += K.w[k] * (vy * vy);
+          a4 += K.w[k] * (vx * vy);
+        }
+      }
+      h[0][r][c] = a0;
+      h[1][r][c] = a1;
+      h[2][r][c] = a2;
+      h[3][r][c] = a3;
+      h[4][r][c] = a4;
+    }
+    __syncthreads();
+    // Vertical pass (loss.rs:58-70) and per-pixel SSIM (loss.rs:101-119).
+    for (int i = tid; i < kLT * kLT; i += kLossThreads) {
+      const int r = i / kLT, c = i % kLT;
+      const int gy = oy0 + r, gx = ox0 + c;
+      if (gx >= (int)width || gy >= (int)height) continue;
+      float mx = 0.0f, my = 0.0f, exx = 0.0f, eyy = 0.0f, exy = 0.0f;
+#pragma unroll
+      for (int k = 0; k < 11; k++) {
+        const int ys = gy + k - kHalo;
+        if (ys >= 0 && ys < (int)height) {
+          const float kv = K.w[k];
+          mx += kv * h[0][r + k][c];
+          my += kv * h[1][r + k][c];
+          exx += kv * h[2][r + k][c];
+          eyy += kv * h[3][r + k][c];
+          exy += kv * h[4][r + k][c];
+        }
+      }
+      const float sx2 = exx - mx * mx;
+      const float sy2 = eyy - my * my;
+      const float sxy = exy - mx * my;
+      const float n1 = 2.0f * mx * my + c1;
+      const float n2 = 2.0f * sxy + c2;
+      const float d1 = mx * mx + my * my + c1;
+      const float d2 = sx2 + sy2 + c2;
+      const float num = n1 * n2;
+      const float den = d1 * d2;
+      const float s = num / den;
+      const float dn_dmx = 2.0f * my * n2 - 2.0f * my * n1;
+      const float dd_dmx = 2.0f * mx * d2 - 2.0f * mx * d1;
+      const size_t idx = ((size_t)gy * width + gx) * 3 + ch;
+      const size_t npix3 = (size_t)width * height * 3;
+      dmaps[idx] = (dn_dmx * den - num * dd_dmx) / (den * den);
+      dmaps[npix3 + idx] = -num * d1 / (den * den);
+      dmaps[2 * npix3 + idx] = 2.0f * n1 / den;
+      const float x = sx[r + kHalo][c + kHalo], y = sy[r + kHalo][c + kHalo];
+      s_ssim += (double)s;
+      s_l1 += (double)fabsf(x - y);
+      const double e = (double)fminf(fmaxf(x, 0.0f), 1.0f) - (double)fminf(fmaxf(y, 0.0f), 1.0f);
+      s_se += e * e;
+    }
+    __syncthreads();
+  }
+  const int lane = tid & 31, warp = tid >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    s_ssim += __shfl_xor_sync(0xffffffffu, s_ssim, o);
+    s_l1 += __shfl_xor_sync(0xffffffffu, s_l1, o);
+    s_se += __shfl_xor_sync(0xffffffffu, s_se, o);
+  }
+  if (lane == 0) {
+    red[0][warp] = s_ssim;
+    red[1][warp] = s_l1;
+    red[2][warp] = s_se;
+  }
+  __syncthreads();
+  if (tid < 3) {
+    double t = 0.0;
+    for (int w = 0; w < kLossThreads / 32; w++) t += red[tid][w];
+    atomicAdd(&sums[tid], t);
+  }
+}
+
+// Gradient of the loss w.r.t. the prediction (loss.rs:124-133, :155-169).
+__global__ void __launch_bounds__(kLossThreads) ssim_bwd_kernel(const float* __restrict__ pred,
+                                                                const void* __restrict__ target, int target_u8,
+                                                                uint32_t width, uint32_t height, LossKernel K,
+                                                                const float* __restrict__ dmaps, float lambda,
+                                                                float* __restrict__ grad) {
+  __shared__ float sm[3][kLE][kLE];
+  __shared__ float h[3][kLE][kLT];
+  const int ox0 = blockIdx.x * kLT, oy0 = blockIdx.y * kLT;
+  const int tid = threadIdx.x;
+  const size_t npix3 = (size_t)width * height * 3;
+  const float inv_n = 1.0f / (float)npix3;
+  const float w1 = (1.0f - lambda) * inv_n;
+  for (int ch = 0; ch < 3; ch++) {
+    for (int i = tid; i < kLE * kLE; i += kLossThreads) {
+      const int r = i / kLE, c = i % kLE;
+      const int gy = oy0 - kHalo + r, gx = ox0 - kHalo + c;
+      float a = 0.0f, b = 0.0f, e = 0.0f;
+      if (gx >= 0 && gx < (int)width && gy >= 0 && gy < (int)height) {
+        const size_t idx = ((size_t)gy * width + gx) * 3 + ch;
+        a = dmaps[idx];
+        b = dmaps[npix3 + idx];
+        e = dmaps[2 * npix3 + idx];
+      }
+      sm[0][r][c] = a;
+      sm[1][r][c] = b;
+      sm[2][r][c] = e;
+    }
+    __syncthreads();
+    for (int i = tid; i < kLE * kLT; i += kLossThreads) {
+      const int r = i / kLT, c = i % kLT;
+      const int gx = ox0 + c;
+      float a0 = 0.0f, a1 = 0.0f, a2 = 0.0f;
+#pragma unroll
+      for (int k = 0; k < 11; k++) {
+        const int xs = gx + k - kHalo;
+        if (xs >= 0 && xs < (int)width) {
+          a0 += K.w[k] * sm[0][r][c + k];
+          a1 += K.w[k] * sm[1][r][c + k];
+          a2 += K.w[k] * sm[2][r][c + k];
+        }
+      }
+      h[0][r][c] = a0;
+      h[1][r][c] = a1;
+      h[2][r][c] = a2;
+    }
+    __syncthreads();
+    for (int i = tid; i < kLT * kLT; i += kLossThreads) {
+      const int r = i / kLT, c = i % kLT;
+      const int gy = oy0 + r, gx = ox0 + c;
+      if (gx >= (int)width || gy >= (int)height) continue;
+      float bmu = 0.0f, bexx = 0.0f, bexy = 0.0f;
+#pragma unroll
+      for (int k = 0; k < 11; k++) {
+        const int ys = gy + k - kHalo;
+        if (ys >= 0 && ys < (int)height) {
+          const float kv = K.w[k];
+          bmu += kv * h[0][r + k][c];
+          bexx += kv * h[1][r + k][c];
+          bexy += kv * h[2][r + k][c];
+        }
+      }
+      const size_t idx = ((size_t)gy * width + gx) * 3 + ch;
+      const float x = pred[idx];
+      const float y = load_target(target, target_u8, idx);
+      const float dssim = (bmu + 2.0f * x * bexx + y * bexy) * inv_n;
+      const float d = x - y;
+      const float sign = d > 0.0f ? 1.0f : (d < 0.0f ? -1.0f : 0.0f);
+      grad[idx] = w1 * sign - lambda * dssim;
+    }
+    __syncthreads();
+  }
+}
+
+// loss = (1 - lambda) * l1 + lambda * (1 - ssim) (loss.rs:147-154) and PSNR (loss.rs:175-190).
+__global__ void loss_finalize_kernel(const double* __restrict__ sums, uint64_t n, float lambda, float* __restrict__ out) {
+  const float inv_n = 1.0f / (float)n;
+  const float l1 = (float)sums[1] * inv_n;
+  const float ssim = (float)(sums[0] / (double)n);
+  out[0] = (1.0f - lambda) * l1 + lambda * (1.0f - ssim);
+  out[1] = ssim;
+  const double mse = sums[2] / (double)(n > 0 ? n : 1);
+  out[2] = mse <= 0.0 ? INFINITY : (float)(-10.0 * log10(mse));
+}
+
+LossKernel make_loss_kernel() {
+  // gaussian_kernel (loss.rs:14-27), in f32 with the host libm, as the reference does.
+  LossKernel k;
+  const float sigma = 1.5f;
+  float sum = 0.0f;
+  for (int i = 0; i < 11; i++) {
+    const float x = (float)i - 5.0f;
+    k.w[i] = expf(-(x * x) / (2.0f * sigma * sigma));
+    sum += k.w[i];
+  }
+  for (int i = 0; i < 11; i++) k.w[i] /= sum;
+  return k;
+}
+
+Status launch_loss(Ctx* c, const float* pred, const void* target, int target_u8, uint32_t width, uint32_t height,
+                   float lambda, float* grad, float* out3) {
+  const size_t npix3 = (size_t)width * height * 3;
+  float* dmaps = nullptr;
+  double* sums = nullptr;
+  SPLAT_TRY(arena_reserve(c, npix3 * 3 * 4, (void**)&dmaps));
+  SPLAT_TRY(arena_reserve(c, 3 * 8, (void**)&sums));
+  SPLAT_CUDA(cudaMemsetAsync(sums, 0, 3 * 8, c->stream));
+  const LossKernel K = make_loss_kernel();
+  const dim3 grid(ceil_div(width, kLT), ceil_div(height, kLT));
+  ssim_fwd_kernel<<<grid, kLossThreads, 0, c->stream>>>(pred, target, target_u8, width, height, K, dmaps, sums);
+  ssim_bwd_kernel<<<grid, kLossThreads, 0, c->stream>>>(pred, target, target_u8, width, height, K, dmaps, lambda,
+                                                         grad);
+  loss_finalize_kernel<<<1, 1, 0, c->stream>>>(sums, npix3, lambda, out3);
+  c->launches.count += 3;
+  SPLAT_LAUNCHED("loss kernels");
+  return Status::ok();
+}
+
+}  // namespace splat

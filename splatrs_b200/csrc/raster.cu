@@ -59,6 +59,67 @@ __device__ __forceinline__ bool evaluate(float px, float py, float mx, float my,
   return true;
 }
 
+// evaluate for the backward pass. The decisions must be the forward's, which were taken on
+// the correctly rounded exp; the value may carry a few ulps. A fast exp (MUFU ex2) decides
+// whenever the product opacity * gauss lies outside a relative band of kExpBand around the
+// two thresholds (1/255 and 0.99); inside the band the correctly rounded exp is evaluated
+// and decides. kExpBand bounds the fast exp's relative error on the argument range
+// [-ln(255), 0] with a wide margin (the bound is checked on the device by
+// splat_diag_fast_exp_error). *unclamped is the reference's `opacity * gauss < 0.99`.
+constexpr float kExpBand = 3e-5f;
+
+__device__ __forceinline__ bool evaluate_bwd(float px, float py, float mx, float my, float A, float B, float C,
+                                             float opacity, float sigma_max, float* gauss_out, float* alpha_out,
+                                             bool* unclamped) {
+  const float dx = px - mx;
+  const float dy = py - my;
+  const float sigma = 0.5f * (A * dx * dx + C * dy * dy) + B * dx * dy;
+  if (sigma < 0.0f || sigma > sigma_max) return false;
+  float gauss = __expf(-sigma);
+  float og = opacity * gauss;
+  const bool near_min = og < SPLAT_ALPHA_MIN * (1.0f + kExpBand) && og > SPLAT_ALPHA_MIN * (1.0f - kExpBand);
+  const bool near_max = og < SPLAT_ALPHA_MAX * (1.0f + kExpBand) && og > SPLAT_ALPHA_MAX * (1.0f - kExpBand);
+  if (near_min || near_max) {
+    gauss = crm::expf_cr(-sigma);
+    og = opacity * gauss;
+  }
+  if (og < SPLAT_ALPHA_MIN) return false;
+  *gauss_out = gauss;
+  *alpha_out = fminf(og, SPLAT_ALPHA_MAX);
+  *unclamped = og < SPLAT_ALPHA_MAX;
+  return true;
+}
+
+// Largest relative error of the fast exp against the correctly rounded one over every
+// float in [lo, hi] (a diagnostic of the bound kExpBand relies on).
+__global__ void diag_fast_exp_kernel(uint32_t lo_bits, uint32_t count, int negative, unsigned int* max_rel_bits) {
+  float worst = 0.0f;
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x) {
+    const uint32_t b = lo_bits + k;
+    const float x = negative ? -__uint_as_float(b) : __uint_as_float(b);
+    const float e = crm::expf_cr(x);
+    const float f = __expf(x);
+    if (e > 0.0f) worst = fmaxf(worst, fabsf(f - e) / e);
+  }
+  for (int o = 16; o > 0; o >>= 1) worst = fmaxf(worst, __shfl_xor_sync(0xffffffffu, worst, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(max_rel_bits, __float_as_uint(worst));
+}
+
+Status launch_diag_fast_exp(Ctx* c, float magnitude_lo, float magnitude_hi, int negative, float* out_host) {
+  unsigned int* d = nullptr;
+  SPLAT_TRY(arena_reserve(c, 4, (void**)&d));
+  SPLAT_CUDA(cudaMemsetAsync(d, 0, 4, c->stream));
+  const uint32_t lo = fbits(magnitude_lo), hi = fbits(magnitude_hi);
+  diag_fast_exp_kernel<<<c->sm_count * 8, 256, 0, c->stream>>>(lo, hi - lo + 1, negative, d);
+  c->launches.count++;
+  SPLAT_LAUNCHED("diag_fast_exp_kernel");
+  unsigned int h = 0;
+  SPLAT_CUDA(cudaMemcpyAsync(&h, d, 4, cudaMemcpyDeviceToHost, c->stream));
+  SPLAT_CUDA(cudaStreamSynchronize(c->stream));
+  *out_host = bitsf(h);
+  return Status::ok();
+}
+
 // forward_tile (rasterize.rs:249-302) for one tile per block.
 __global__ void __launch_bounds__(kRasterThreads) raster_fwd_kernel(
     const float4* __restrict__ rec, const uint32_t* __restrict__ gauss, const uint2* __restrict__ ranges,
@@ -190,41 +251,45 @@ __global__ void __launch_bounds__(kRasterThreads) raster_bwd_kernel(
         npairs++;
         const float4 e0 = s0[kk], e1 = s1[kk];
         float gval, alpha;
-        if (evaluate(px, py, e0.x, e0.y, e0.z, e0.w, e1.x, e1.y, e1.z, &gval, &alpha)) {
+        bool unclamped;
+        if (evaluate_bwd(px, py, e0.x, e0.y, e0.z, e0.w, e1.x, e1.y, e1.z, &gval, &alpha, &unclamped)) {
           active = true;
+          // Values only from here on: the arithmetic is fused and the divisions are
+          // reciprocals; every decision was taken above exactly as in the forward pass.
           const float col_r = e1.w, col_g = e2.x, col_b = e2.y;
-          T = T / (1.0f - alpha);
+          const float inv = __frcp_rn(1.0f - alpha);
+          T = T * inv;
           const float t = T;
-          float dalpha = 0.0f;
-          acc_r = last_alpha * lc_r + (1.0f - last_alpha) * acc_r;
-          dalpha += (col_r - acc_r) * d0;
-          c[6] = alpha * t * d0;
-          acc_g = last_alpha * lc_g + (1.0f - last_alpha) * acc_g;
-          dalpha += (col_g - acc_g) * d1;
-          c[7] = alpha * t * d1;
-          acc_b = last_alpha * lc_b + (1.0f - last_alpha) * acc_b;
-          dalpha += (col_b - acc_b) * d2;
-          c[8] = alpha * t * d2;
-          dalpha *= t;
+          const float keep = 1.0f - last_alpha;
+          acc_r = __fmaf_rn(last_alpha, lc_r, keep * acc_r);
+          acc_g = __fmaf_rn(last_alpha, lc_g, keep * acc_g);
+          acc_b = __fmaf_rn(last_alpha, lc_b, keep * acc_b);
+          float dalpha = (col_r - acc_r) * d0;
+          dalpha = __fmaf_rn(col_g - acc_g, d1, dalpha);
+          dalpha = __fmaf_rn(col_b - acc_b, d2, dalpha);
+          const float at = alpha * t;
+          c[6] = at * d0;
+          c[7] = at * d1;
+          c[8] = at * d2;
           lc_r = col_r;
           lc_g = col_g;
           lc_b = col_b;
           last_alpha = alpha;
-          dalpha += -t_fin / (1.0f - alpha) * bg_dot;
-          const float opacity = e1.y;
-          if (opacity * gval < SPLAT_ALPHA_MAX) {
+          dalpha = __fmaf_rn(dalpha, t, -t_fin * inv * bg_dot);
+          if (unclamped) {
+            const float opacity = e1.y;
             c[5] = gval * dalpha;
-            const float dgauss = opacity * dalpha;
-            const float dsigma = -dgauss * gval;
+            const float dsigma = -(opacity * dalpha) * gval;
             const float dx = px - e0.x;
             const float dy = py - e0.y;
-            const float ddx = dsigma * (e0.z * dx + e0.w * dy);
-            const float ddy = dsigma * (e0.w * dx + e1.x * dy);
+            const float ddx = dsigma * __fmaf_rn(e0.z, dx, e0.w * dy);
+            const float ddy = dsigma * __fmaf_rn(e0.w, dx, e1.x * dy);
             c[0] = -ddx;
             c[1] = -ddy;
-            c[2] = dsigma * 0.5f * dx * dx;
+            const float hs = 0.5f * dsigma;
+            c[2] = hs * dx * dx;
             c[3] = dsigma * dx * dy;
-            c[4] = dsigma * 0.5f * dy * dy;
+            c[4] = hs * dy * dy;
             c[9] = fabsf(ddx);
             c[10] = fabsf(ddy);
           }

@@ -9,12 +9,13 @@ kernels of libsplatrs_b200.so. There is no CPU fallback.
 from __future__ import annotations
 
 import ctypes as C
+import weakref
 from dataclasses import dataclass
 
 import torch
 
 from . import _lib as L
-from ._lib import Camera, ProjOpts, check
+from ._lib import Camera, DensifyConfig, DensifyReport, LearningRates, ProjOpts, StepInfo, TrainConfig, check
 
 PLANES = L.PLANES
 PROJ_FLOATS = L.PROJ_FLOATS
@@ -36,6 +37,11 @@ class Context:
         if st != L.SPLAT_OK:
             raise L.SplatError(st, "splat_ctx_create failed")
         self.h = h
+        self._dependents = weakref.WeakSet()
+
+    def _adopt(self, obj):
+        """Renderers and trainers must be destroyed before their context."""
+        self._dependents.add(obj)
 
     def set_stream(self, stream):
         check(self.lib.splat_ctx_set_stream(self.h, C.c_void_p(stream.cuda_stream)), self.h)
@@ -52,6 +58,8 @@ class Context:
 
     def close(self):
         if getattr(self, "h", None):
+            for d in list(getattr(self, "_dependents", ())):
+                d.close()
             self.lib.splat_ctx_destroy(self.h)
             self.h = None
 
@@ -166,14 +174,18 @@ class RasterOutput:
     pairs: torch.Tensor    # (1,) int64, evaluated (entry, pixel) pairs
 
 
-def rasterize_forward(ctx: Context, proj: Projection, b: Binning, background) -> RasterOutput:
-    """rasterize_forward (src/rasterize.rs:305-337)."""
+def rasterize_forward(ctx: Context, proj: Projection, b: Binning, background, count_pairs: bool = True,
+                      out: RasterOutput | None = None) -> RasterOutput:
+    """rasterize_forward (src/rasterize.rs:305-337). `out` reuses buffers of a previous call."""
     dev = proj.rec.device
     npix = proj.width * proj.height
-    image = torch.empty(npix * 3, dtype=torch.float32, device=dev)
-    ft = torch.empty(npix, dtype=torch.float32, device=dev)
-    nc = torch.empty(npix, dtype=torch.int32, device=dev)
-    pairs = torch.zeros(1, dtype=torch.int64, device=dev)
+    if out is not None:
+        image, ft, nc = out.image, out.final_t, out.n_contrib
+    else:
+        image = torch.empty(npix * 3, dtype=torch.float32, device=dev)
+        ft = torch.empty(npix, dtype=torch.float32, device=dev)
+        nc = torch.empty(npix, dtype=torch.int32, device=dev)
+    pairs = torch.zeros(1, dtype=torch.int64, device=dev) if count_pairs else None
     bgp, keep = _bg(background)
     check(ctx.lib.splat_rasterize_fwd(ctx.h, _ptr(proj.rec), _ptr(b.gauss), _ptr(b.tile_range), proj.width,
                                       proj.height, bgp, _ptr(image), _ptr(ft), _ptr(nc), _ptr(pairs)), ctx.h)
@@ -242,6 +254,7 @@ class Renderer:
         check(self.lib.splat_renderer_create(ctx.h, C.byref(h)), ctx.h)
         self.h = h
         self.n = 0
+        ctx._adopt(self)
 
     def set_model(self, aos59, sh_degree: int):
         import numpy as np
@@ -280,6 +293,104 @@ class Renderer:
     def close(self):
         if getattr(self, "h", None):
             self.lib.splat_renderer_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def photometric_loss(ctx: Context, pred: torch.Tensor, target: torch.Tensor, width: int, height: int,
+                     lambda_dssim: float):
+    """photometric_loss (src/loss.rs:137-171): returns (loss, mean ssim, psnr) as a device
+    tensor of 3 floats and the gradient w.r.t. pred. `target` may be uint8 (converted as
+    View::to_real, src/dataset.rs:23-25) or float32."""
+    pred = pred.contiguous()
+    target = target.contiguous()
+    is_u8 = target.dtype == torch.uint8
+    grad = torch.empty_like(pred)
+    out = torch.empty(3, dtype=torch.float32, device=pred.device)
+    check(ctx.lib.splat_loss_fwd_bwd(ctx.h, _ptr(pred), _ptr(target), int(is_u8), width, height, float(lambda_dssim),
+                                     _ptr(grad), _ptr(out)), ctx.h)
+    return out, grad
+
+
+def adam_step(ctx: Context, planes, grads, m, v, n: int, cap: int, step: int, lr: LearningRates):
+    """Adam::step (src/adam.rs:77-161) in place; `step` is the count after the increment."""
+    check(ctx.lib.splat_adam_step(ctx.h, _ptr(planes), _ptr(grads), _ptr(m), _ptr(v), n, cap, step, C.byref(lr)),
+          ctx.h)
+
+
+def densify_and_prune(ctx: Context, planes, m, v, n: int, cap: int, stats, cfg: DensifyConfig, extent: float,
+                      rng_state: int, cap_out: int | None = None):
+    """densify_and_prune (src/densify.rs:125-221). Returns (planes, m, v, report, rng_state)."""
+    cap_out = cap_out if cap_out is not None else max(1, n * (2 + cfg.split_children))
+    po = torch.zeros(PLANES * cap_out * 4, dtype=torch.float32, device=planes.device)
+    mo = torch.zeros_like(po)
+    vo = torch.zeros_like(po)
+    st = C.c_uint64(rng_state)
+    rep = DensifyReport()
+    check(ctx.lib.splat_densify(ctx.h, _ptr(planes), _ptr(m), _ptr(v), n, cap, _ptr(stats), C.byref(cfg),
+                                float(extent), C.byref(st), _ptr(po), _ptr(mo), _ptr(vo), cap_out, C.byref(rep)), ctx.h)
+    return po, mo, vo, rep, int(st.value), cap_out
+
+
+def reset_opacity(ctx: Context, planes, m, v, n: int, max_alpha: float = 0.01):
+    """reset_opacity (src/densify.rs:224-230) in place."""
+    check(ctx.lib.splat_reset_opacity(ctx.h, _ptr(planes), _ptr(m), _ptr(v), n, float(max_alpha)), ctx.h)
+
+
+class Trainer:
+    """train::train (src/train.rs:161-306) on the device, one iteration per step()."""
+
+    def __init__(self, ctx: Context, init_params, extent: float, views, **cfg):
+        import numpy as np
+        self.ctx = ctx
+        self.lib = ctx.lib
+        self.cfg = TrainConfig.make(**cfg)
+        h = C.c_void_p()
+        check(self.lib.splat_trainer_create(ctx.h, C.byref(self.cfg), float(extent), C.byref(h)), ctx.h)
+        self.h = h
+        ctx._adopt(self)
+        p = np.ascontiguousarray(init_params, np.float32).reshape(-1, 59)
+        check(self.lib.splat_trainer_set_model(self.h, p.ctypes.data_as(C.c_void_p), p.shape[0]), ctx.h)
+        for cam, rgb in views:
+            c = cam if isinstance(cam, Camera) else Camera.from_record(cam)
+            r = np.ascontiguousarray(rgb, np.uint8)
+            check(self.lib.splat_trainer_add_view(self.h, C.byref(c), r.ctypes.data_as(C.c_void_p)), ctx.h)
+        check(self.lib.splat_trainer_start(self.h), ctx.h)
+
+    def step(self) -> dict:
+        info = StepInfo()
+        check(self.lib.splat_trainer_step(self.h, C.byref(info)), self.ctx.h)
+        return info.as_dict()
+
+    @property
+    def count(self) -> int:
+        return int(self.lib.splat_trainer_count(self.h))
+
+    @property
+    def sh_degree(self) -> int:
+        return int(self.lib.splat_trainer_sh_degree(self.h))
+
+    def model(self):
+        import numpy as np
+        out = np.empty((self.count, 59), np.float32)
+        check(self.lib.splat_trainer_get_model(self.h, out.ctypes.data_as(C.c_void_p)), self.ctx.h)
+        return out
+
+    def render(self, cam):
+        import numpy as np
+        c = cam if isinstance(cam, Camera) else Camera.from_record(cam)
+        out = np.empty(c.width * c.height * 3, np.float32)
+        check(self.lib.splat_trainer_render(self.h, C.byref(c), out.ctypes.data_as(C.c_void_p)), self.ctx.h)
+        return out
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.splat_trainer_destroy(self.h)
             self.h = None
 
     def __del__(self):

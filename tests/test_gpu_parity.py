@@ -260,7 +260,7 @@ def test_project_backward_densify_stats(ctx):
         oden = np.zeros(n, np.uint32)
         omr = np.zeros(n, np.uint32)
         for _ in range(2):
-            O.densify_accumulate(p, w, a2 if absgrad else None, cam[0], cam[1], oacc, oden, omr)
+            O.densify_accumulate(p, w, a2 if absgrad else None, int(cam[0]), int(cam[1]), oacc, oden, omr)
         assert (bits(acc) == bits(oacc)).all() and (den == oden).all() and (mr == omr).all()
 
 
@@ -312,3 +312,14 @@ def test_invalid_arguments_return_status(ctx):
     assert e.value.status == 1
     with pytest.raises(SplatError):
         G.project_all(ctx, planes, 10, 10, Camera.from_record(cam), ProjOpts.make(sh_degree=4))
+
+
+def test_fast_exp_bound_behind_backward_screening(ctx):
+    """The backward pass decides with a fast exp outside a relative band of 3e-5 around its
+    thresholds; its error over every float of the argument range [-(ln 255 + 0.5), 0] must
+    stay far inside that band."""
+    import ctypes as C
+    out = C.c_float()
+    G.check(ctx.lib.splat_diag_fast_exp_error(ctx.h, 0.0, 6.05, 1, C.byref(out)), ctx.h)
+    print(f"\nfast exp max relative error on [-6.05, 0]: {out.value:.3e}")
+    assert 0.0 < out.value < 3e-6

@@ -1,0 +1,265 @@
+"""Parity of the loss, optimiser, density-control kernels and the device trainer with the
+CPU oracle, through the C ABI, plus the reference's training tests (tests/pipeline.rs)
+replayed on the device trainer."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import oracle as O
+from splatrs_b200 import gpu as G
+from splatrs_b200 import scenes
+from splatrs_b200._lib import DensifyConfig, LearningRates
+from tests import fixtures as F
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = G.Context(0)
+    yield c
+    c.close()
+
+
+@pytest.fixture
+def cr_math():
+    O.set_cr_math(True)
+    yield
+    O.set_cr_math(False)
+
+
+def dev(a, dtype=torch.float32):
+    return torch.from_numpy(np.ascontiguousarray(a)).to("cuda", dtype)
+
+
+def to_planes(ctx, aos, cap=None):
+    return G.params_to_planes(ctx, dev(aos), cap)
+
+
+def from_planes(ctx, planes, n, cap):
+    return G.planes_to_params(ctx, planes, n, cap).cpu().numpy()
+
+
+@pytest.mark.parametrize("w,h,lam,u8", [(64, 48, 0.2, True), (97, 53, 0.2, False), (320, 240, 0.8, True),
+                                        (16, 12, 1.0, False)])
+def test_loss_matches_oracle(ctx, w, h, lam, u8):
+    """photometric_loss: gradient bit-identical (same blur order, same formulas); loss and
+    PSNR to summation-order rounding."""
+    rng = np.random.default_rng(w * h)
+    pred = rng.uniform(-0.1, 1.1, w * h * 3).astype(np.float32)
+    if u8:
+        t8 = rng.integers(0, 256, w * h * 3).astype(np.uint8)
+        target = t8.astype(np.float32) / np.float32(255.0)
+        tdev = dev(t8, torch.uint8)
+    else:
+        target = rng.uniform(0, 1, w * h * 3).astype(np.float32)
+        tdev = dev(target)
+    out, grad = G.photometric_loss(ctx, dev(pred), tdev, w, h, lam)
+    loss, ogr = O.photometric_loss(pred, target, w, h, lam)
+    g = grad.cpu().numpy()
+    assert np.array_equal(g, ogr), np.abs(g - ogr).max()
+    o = out.cpu().numpy()
+    assert abs(o[0] - loss) <= 2e-6 * max(1.0, abs(loss))
+    assert abs(o[2] - O.psnr(pred, target)) < 1e-3
+    loss64, g64 = O.photometric_loss(pred.astype(np.float64), target.astype(np.float64), w, h, lam, dtype=np.float64)
+    print(f"\nloss grad vs f64 oracle: {np.abs(g - g64).max() / np.abs(g64).max():.2e}; loss {abs(o[0] - loss64):.2e}")
+
+
+def test_ssim_identity_on_device(ctx):
+    """src/loss.rs:196-207 on the device: SSIM(x, x) = 1 and its gradient vanishes."""
+    w, h = 20, 14
+    img = np.array([((i * 7919) % 255) / 255.0 for i in range(w * h * 3)], np.float32)
+    out, grad = G.photometric_loss(ctx, dev(img), dev(img), w, h, 1.0)
+    o = out.cpu().numpy()
+    assert abs(o[1] - 1.0) < 1e-4
+    assert np.abs(grad.cpu().numpy()).max() < 1e-3
+
+
+def test_adam_bit_exact(ctx):
+    """Adam::step over five steps: parameters and moments bit-identical to the oracle."""
+    rng = np.random.default_rng(7)
+    n = 3000
+    p = rng.normal(0, 1, (n, 59)).astype(np.float32)
+    p_o = p.copy()
+    m_o = np.zeros_like(p)
+    v_o = np.zeros_like(p)
+    planes = to_planes(ctx, p)
+    m = torch.zeros_like(planes)
+    v = torch.zeros_like(planes)
+    lr = LearningRates(0.00016 * 3.3, 0.005, 0.001, 0.025, 0.0025, 0.0025 / 20)
+    lr6 = np.array([lr.mean, lr.log_scale, lr.quat, lr.opacity, lr.sh_dc, lr.sh_rest], np.float32)
+    step = 0
+    for k in range(5):
+        g = rng.normal(0, 1e-3, (n, 59)).astype(np.float32)
+        g[::5] = 0.0  # zero gradients still decay the moments (adam.rs:56-60)
+        step = O.adam_step(p_o, g, m_o, v_o, step, lr6)
+        G.adam_step(ctx, planes, to_planes(ctx, g), m, v, n, n, step, lr)
+    assert np.array_equal(from_planes(ctx, planes, n, n), p_o)
+    assert np.array_equal(from_planes(ctx, m, n, n), m_o)
+    assert np.array_equal(from_planes(ctx, v, n, n), v_o)
+
+
+def densify_case(seed, n=4000):
+    rng = np.random.default_rng(seed)
+    g = scenes.random_gaussians(rng, n, -1.0, 1.0, -3.0, 1.0, 2.5)
+    g[::13, 3:6] = -0.5  # large
+    g[::17, 10] = -8.0   # transparent
+    accum = rng.uniform(0, 3e-3, n).astype(np.float32)
+    denom = rng.integers(0, 6, n).astype(np.uint32)
+    maxr = rng.integers(0, 40, n).astype(np.uint32)
+    m = rng.normal(0, 1e-4, (n, 59)).astype(np.float32)
+    v = np.abs(rng.normal(0, 1e-6, (n, 59))).astype(np.float32)
+    return g, m, v, accum, denom, maxr
+
+
+@pytest.mark.parametrize("opts", [dict(), dict(prune_big_world=True, max_screen_size=20),
+                                  dict(grad_threshold=1e-9, percent_dense=0.05)])
+def test_densify_bit_exact(ctx, cr_math, opts):
+    """densify_and_prune with the same generator state: counts, order and every
+    parameter and moment bit-identical to the oracle (with the correctly rounded exp the
+    kernels use for the scales); the generator advances identically."""
+    g, m, v, accum, denom, maxr = densify_case(5)
+    n = g.shape[0]
+    extent = 4.4
+    cfg = dict(grad_threshold=0.0002, percent_dense=0.01, min_opacity=0.005, prune_big_world=False,
+               max_world_size_frac=0.1, max_screen_size=None, split_children=2)
+    cfg.update(opts)
+    seed = 1234
+    stats = torch.zeros(3 * n, dtype=torch.int32, device="cuda")
+    stats[:n] = dev(accum).view(torch.int32)
+    stats[n:2 * n] = dev(denom.view(np.int32), torch.int32)
+    stats[2 * n:] = dev(maxr.view(np.int32), torch.int32)
+    po, mo, vo, rep, st, cap_out = G.densify_and_prune(ctx, to_planes(ctx, g), to_planes(ctx, m), to_planes(ctx, v), n,
+                                                       n, stats, DensifyConfig.make(**cfg), extent, seed)
+    # The oracle draws from the same generator.
+    state = np.array([seed], np.uint64)
+    normals = np.array([O.lib().ora_splitmix_normal(state.ctypes.data) for _ in range(6 * n)])
+    op, om, ov, orep = O.densify_and_prune(g, m, v, accum, denom, maxr, extent, normals, **cfg)
+    assert (rep.cloned, rep.split, rep.pruned) == orep[:3]
+    assert rep.new_count == op.shape[0]
+    assert rep.cloned > 0 and rep.split > 0
+    k = op.shape[0]
+    assert np.array_equal(from_planes(ctx, po, k, cap_out), op)
+    assert np.array_equal(from_planes(ctx, mo, k, cap_out), om)
+    assert np.array_equal(from_planes(ctx, vo, k, cap_out), ov)
+    s2 = np.array([seed], np.uint64)
+    for _ in range(orep[3]):
+        O.lib().ora_splitmix_normal(s2.ctypes.data)
+    assert st == int(s2[0])
+
+
+def test_densify_matches_libm_oracle(ctx):
+    """densify_and_prune against the faithful oracle: the same decisions and order; split
+    children's means to a few ulps (the scales go through exp)."""
+    g, m, v, accum, denom, maxr = densify_case(9)
+    n = g.shape[0]
+    stats = torch.zeros(3 * n, dtype=torch.int32, device="cuda")
+    stats[:n] = dev(accum).view(torch.int32)
+    stats[n:2 * n] = dev(denom.view(np.int32), torch.int32)
+    stats[2 * n:] = dev(maxr.view(np.int32), torch.int32)
+    po, mo, vo, rep, st, cap_out = G.densify_and_prune(ctx, to_planes(ctx, g), to_planes(ctx, m), to_planes(ctx, v), n,
+                                                       n, stats, DensifyConfig.make(), 4.4, 77)
+    state = np.array([77], np.uint64)
+    normals = np.array([O.lib().ora_splitmix_normal(state.ctypes.data) for _ in range(6 * n)])
+    op, om, ov, orep = O.densify_and_prune(g, m, v, accum, denom, maxr, 4.4, normals)
+    assert (rep.cloned, rep.split, rep.pruned, rep.new_count) == (*orep[:3], op.shape[0])
+    got = from_planes(ctx, po, op.shape[0], cap_out)
+    assert np.allclose(got, op, rtol=1e-6, atol=1e-7)
+    assert np.array_equal(from_planes(ctx, mo, op.shape[0], cap_out), om)
+
+
+def test_densify_capacity_error_leaves_generator(ctx):
+    """Too small an output capacity: SPLAT_ERR_CAPACITY with the needed count, nothing drawn."""
+    from splatrs_b200._lib import SplatError
+    g, m, v, accum, denom, maxr = densify_case(6, n=500)
+    n = g.shape[0]
+    stats = torch.zeros(3 * n, dtype=torch.int32, device="cuda")
+    stats[:n] = dev(accum).view(torch.int32)
+    stats[n:2 * n] = dev(denom.view(np.int32), torch.int32)
+    with pytest.raises(SplatError) as e:
+        G.densify_and_prune(ctx, to_planes(ctx, g), to_planes(ctx, m), to_planes(ctx, v), n, n, stats,
+                            DensifyConfig.make(), 4.4, 99, cap_out=10)
+    assert e.value.status == 2
+
+
+def test_reset_opacity_bit_exact(ctx):
+    g, m, v, *_ = densify_case(8, n=1000)
+    n = g.shape[0]
+    planes, mp, vp = to_planes(ctx, g), to_planes(ctx, m), to_planes(ctx, v)
+    G.reset_opacity(ctx, planes, mp, vp, n, 0.01)
+    O.reset_opacity(g, m, v, 0.01)
+    assert np.array_equal(from_planes(ctx, planes, n, n), g)
+    assert np.array_equal(from_planes(ctx, mp, n, n), m)
+    assert np.array_equal(from_planes(ctx, vp, n, n), v)
+
+
+def _views_and_init(seed_scene, n_gt, n_cams, w, h, bg, truncate=None):
+    rng = np.random.default_rng(seed_scene)
+    gt = F.ground_truth(rng, n_gt)
+    cams = F.ring_cameras(n_cams, w, h, 2.6)
+    views = F.render_views(gt, cams, 1, bg)
+    extent = O.scene_extent(cams)
+    pts, rgb = F.init_points(gt, rng)
+    if truncate:
+        pts, rgb = pts[:truncate], rgb[:truncate]
+    return views, extent, O.from_points(pts, rgb)
+
+
+def _evaluate(trainer, views):
+    tot = 0.0
+    for cam, rgb in views:
+        img = trainer.render(cam)
+        tot += O.psnr(img, rgb.astype(np.float32) / np.float32(255.0))
+    return tot / len(views)
+
+
+def test_device_trainer_trains_without_densification(ctx):
+    """tests/pipeline.rs:17-60 on the device trainer, beside the oracle trainer."""
+    views, extent, init = _views_and_init(100, 40, 10, 64, 48, [0.0, 0.0, 0.0])
+    cfg = dict(iterations=600, densify=0, sh_degree=1, sh_degree_interval=200, position_lr_max_steps=600, seed=3)
+    before = F.evaluate(init, views, 0, [0, 0, 0])
+    t = G.Trainer(ctx, init, extent, views, **cfg)
+    ot = O.Trainer(init, extent, views, **cfg)
+    for _ in range(600):
+        info = t.step()
+        oinfo = ot.step()
+        assert info["view"] == oinfo["view"]
+    assert t.count == 40
+    after = _evaluate(t, views)
+    oafter = F.evaluate(ot.model(), views, ot.sh_degree, [0, 0, 0])
+    print(f"\nno densification: PSNR {before:.2f} -> device {after:.2f} dB, oracle {oafter:.2f} dB")
+    assert after > before + 6.0 and after > 24.0
+    assert abs(after - oafter) < 0.5
+    t.close()
+
+
+def test_device_trainer_trains_with_densification(ctx):
+    """tests/pipeline.rs:62-130 on the device trainer, beside the oracle trainer."""
+    views, extent, init = _views_and_init(200, 30, 8, 48, 36, [1.0, 1.0, 1.0], truncate=10)
+    cfg = dict(iterations=500, densify=1, densify_from_iter=40, densify_until_iter=400, densification_interval=40,
+               opacity_reset_interval=200, densify_grad_threshold=0.0005, white_background=1, sh_degree=1,
+               sh_degree_interval=150, position_lr_max_steps=500, seed=5)
+    before = F.evaluate(init, views, 0, [1, 1, 1])
+    t = G.Trainer(ctx, init, extent, views, **cfg)
+    ot = O.Trainer(init, extent, views, **cfg)
+    for _ in range(500):
+        info = t.step()
+        ot.step()
+        assert np.isfinite(info["loss"])
+    assert t.count > 10
+    assert t.sh_degree == 1
+    after = _evaluate(t, views)
+    oafter = F.evaluate(ot.model(), views, ot.sh_degree, [1, 1, 1])
+    print(f"\nwith densification: PSNR {before:.2f} -> device {after:.2f} dB ({t.count} Gaussians), "
+          f"oracle {oafter:.2f} dB ({ot.count} Gaussians)")
+    assert after > before + 4.0
+    assert np.isfinite(t.model()[:, 0:10]).all()
+    t.close()
+
+
+def test_trainer_rejects_zero_iterations(ctx):
+    """src/train.rs:353-375."""
+    from splatrs_b200._lib import SplatError
+    with pytest.raises(SplatError) as e:
+        G.Trainer(ctx, np.zeros((0, 59), np.float32), 1.0, [], iterations=0, sh_degree=0)
+    assert e.value.status == 1

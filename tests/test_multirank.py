@@ -1,0 +1,49 @@
+"""The N > 1 host logic of bench.py (replicas, max over ranks) on two gloo ranks on CPU."""
+import os
+import socket
+import subprocess
+import sys
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+WORKER = r"""
+import os, sys
+sys.path.insert(0, {root!r})
+import torch.distributed as dist
+from datetime import timedelta
+dist.init_process_group("gloo", timeout=timedelta(seconds=60))
+import bench
+rank, world, local = bench.dist_info()
+assert world == 2
+v = bench.max_over_ranks(10.0 + 5.0 * rank, world)
+assert v == 15.0, v
+w = bench.max_over_ranks(3.0 - rank, world)
+assert w == 3.0, w
+dist.barrier()
+dist.destroy_process_group()
+print("rank", rank, "ok")
+"""
+
+
+def free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    p = s.getsockname()[1]
+    s.close()
+    return p
+
+
+def test_max_over_ranks_with_two_gloo_ranks():
+    port = free_port()
+    procs = []
+    for r in range(2):
+        env = dict(os.environ, RANK=str(r), WORLD_SIZE="2", LOCAL_RANK=str(r), MASTER_ADDR="127.0.0.1",
+                   MASTER_PORT=str(port), CUDA_VISIBLE_DEVICES="")
+        procs.append(subprocess.Popen([sys.executable, "-c", WORKER.format(root=ROOT)], env=env,
+                                      stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True))
+    outs = []
+    for p in procs:
+        out, _ = p.communicate(timeout=120)
+        outs.append(out)
+        assert p.returncode == 0, out
+    assert all("ok" in o for o in outs)
