@@ -33,12 +33,6 @@ __device__ __forceinline__ PixelGeom pixel_geom(uint32_t tile, uint32_t tiles_x,
   return p;
 }
 
-// Entry rectangle against the warp's 8x4 sub-block (warp-uniform).
-__device__ __forceinline__ bool rect_hits_block(uint32_t rx, uint32_t ry, const PixelGeom& p) {
-  const uint32_t x0 = rx & 0xffffu, x1 = rx >> 16, y0 = ry & 0xffffu, y1 = ry >> 16;
-  return !(x1 <= p.bx0 || x0 >= p.bx0 + 8u || y1 <= p.by0 || y0 >= p.by0 + 4u);
-}
-
 __device__ __forceinline__ bool pixel_in_rect(uint32_t rx, uint32_t ry, const PixelGeom& p) {
   const uint32_t x0 = rx & 0xffffu, x1 = rx >> 16, y0 = ry & 0xffffu, y1 = ry >> 16;
   return p.px_i >= x0 && p.px_i < x1 && p.py_j >= y0 && p.py_j < y1;
@@ -120,15 +114,53 @@ Status launch_diag_fast_exp(Ctx* c, float magnitude_lo, float magnitude_hi, int 
   return Status::ok();
 }
 
+// Bit w of the result is set when the pixel rectangle (x0|x1<<16, y0|y1<<16, absolute
+// pixels) overlaps warp w's 8x4 sub-block of the tile whose top-left pixel is (ox, oy).
+__device__ __forceinline__ uint32_t subblock_mask(uint32_t rx, uint32_t ry, uint32_t ox, uint32_t oy) {
+  const uint32_t x0 = rx & 0xffffu, x1 = rx >> 16, y0 = ry & 0xffffu, y1 = ry >> 16;
+  const bool left = x0 < ox + 8u && x1 > ox;
+  const bool right = x0 < ox + 16u && x1 > ox + 8u;
+  uint32_t m = 0;
+#pragma unroll
+  for (uint32_t q = 0; q < 4; q++) {
+    const bool row = y0 < oy + 4u * q + 4u && y1 > oy + 4u * q;
+    if (row && left) m |= 1u << (2 * q);
+    if (row && right) m |= 1u << (2 * q + 1);
+  }
+  return m;
+}
+
+// Compacts, in order, the chunk-local indices k < cnt whose mask has this warp's bit (and,
+// when `limit` is finite, k < limit) into list[]; returns how many.
+__device__ __forceinline__ uint32_t build_warp_list(const uint8_t* __restrict__ smask, uint32_t cnt, uint32_t limit,
+                                                    uint8_t* __restrict__ list) {
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t lt = (1u << lane) - 1u;
+  uint32_t n = 0;
+  for (uint32_t b = 0; b < cnt; b += 32) {
+    const uint32_t k = b + lane;
+    const bool hit = k < cnt && k < limit && ((smask[k] >> warp) & 1u);
+    const uint32_t bal = __ballot_sync(0xffffffffu, hit);
+    if (hit) list[n + __popc(bal & lt)] = (uint8_t)k;
+    n += __popc(bal);
+  }
+  __syncwarp();
+  return n;
+}
+
 // forward_tile (rasterize.rs:249-302) for one tile per block.
 __global__ void __launch_bounds__(kRasterThreads) raster_fwd_kernel(
     const float4* __restrict__ rec, const uint32_t* __restrict__ gauss, const uint2* __restrict__ ranges,
     uint32_t width, uint32_t height, uint32_t tiles_x, float bg0, float bg1, float bg2, float* __restrict__ image,
     float* __restrict__ final_t, uint32_t* __restrict__ n_contrib, unsigned long long* __restrict__ pairs) {
   __shared__ float4 s0[kChunk], s1[kChunk], s2[kChunk];
+  __shared__ uint8_t smask[kChunk];
+  __shared__ uint8_t slist[kRasterThreads / 32][kChunk];
   const PixelGeom pg = pixel_geom(blockIdx.x, tiles_x, width, height);
+  const uint32_t ox = (blockIdx.x % tiles_x) * kTile, oy = (blockIdx.x / tiles_x) * kTile;
   const float px = (float)pg.px_i + 0.5f, py = (float)pg.py_j + 0.5f;
   const uint2 range = ranges[blockIdx.x];
+  uint8_t* list = slist[threadIdx.x >> 5];
   float T = 1.0f, cr = 0.0f, cg = 0.0f, cb = 0.0f;
   uint32_t ncon = 0;
   bool done = !pg.inside;
@@ -136,20 +168,24 @@ __global__ void __launch_bounds__(kRasterThreads) raster_fwd_kernel(
   for (uint32_t base = range.x; base < range.y; base += kChunk) {
     if (__syncthreads_count(!done) == 0) break;
     const uint32_t idx = base + threadIdx.x;
+    uint32_t m = 0;
     if (idx < range.y) {
       const uint32_t g = gauss[idx];
       s0[threadIdx.x] = rec[4 * (size_t)g];
       s1[threadIdx.x] = rec[4 * (size_t)g + 1];
-      s2[threadIdx.x] = rec[4 * (size_t)g + 2];
+      const float4 e2 = rec[4 * (size_t)g + 2];
+      s2[threadIdx.x] = e2;
+      m = subblock_mask(fbits(e2.z), fbits(e2.w), ox, oy);
     }
+    smask[threadIdx.x] = (uint8_t)m;
     __syncthreads();
     const uint32_t cnt = min((uint32_t)kChunk, range.y - base);
-    for (uint32_t k = 0; k < cnt; k++) {
+    const uint32_t nl = build_warp_list(smask, cnt, 0xffffffffu, list);
+    for (uint32_t i = 0; i < nl; i++) {
       if (__all_sync(0xffffffffu, done)) break;
+      const uint32_t k = list[i];
       const float4 e2 = s2[k];
-      const uint32_t rx = fbits(e2.z), ry = fbits(e2.w);
-      if (!rect_hits_block(rx, ry, pg)) continue;
-      if (done || !pixel_in_rect(rx, ry, pg)) continue;
+      if (done || !pixel_in_rect(fbits(e2.z), fbits(e2.w), pg)) continue;
       npairs++;
       const float4 e0 = s0[k], e1 = s1[k];
       float gval, alpha;
@@ -183,9 +219,41 @@ __global__ void __launch_bounds__(kRasterThreads) raster_fwd_kernel(
 }
 
 // backward_tile (rasterize.rs:354-455) for one tile per block. Per-pixel contributions to
-// an entry's 11 gradient slots are summed across the warp with shuffles, across the
-// block's warps in shared memory, and across tiles with one vector atomic per plane.
+// an entry's 11 gradient slots are summed across the warp by a transposing butterfly
+// (16 shuffles leave slot j's warp total in lanes 2j and 2j+1), across the block's warps
+// with one shared-memory atomic instruction per warp, and across tiles with three float4
+// vector atomics per entry.
 constexpr int kSlots = 12;  // 11 used, padded for float4 flushes
+
+// v[0..15] per lane in, warp total of slot ((lane >> 1) & 15) out.
+__device__ __forceinline__ float warp_transpose_reduce16(float v[16]) {
+  const uint32_t lane = threadIdx.x & 31;
+  float w[8], x[4], y[2];
+  const bool b4 = lane & 16u, b3 = lane & 8u, b2 = lane & 4u, b1 = lane & 2u;
+#pragma unroll
+  for (int i = 0; i < 8; i++) {
+    const float send = b4 ? v[i] : v[i + 8];
+    const float keep = b4 ? v[i + 8] : v[i];
+    w[i] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+  }
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    const float send = b3 ? w[i] : w[i + 4];
+    const float keep = b3 ? w[i + 4] : w[i];
+    x[i] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+  }
+#pragma unroll
+  for (int i = 0; i < 2; i++) {
+    const float send = b2 ? x[i] : x[i + 2];
+    const float keep = b2 ? x[i + 2] : x[i];
+    y[i] = keep + __shfl_xor_sync(0xffffffffu, send, 4);
+  }
+  const float send = b1 ? y[0] : y[1];
+  const float keep = b1 ? y[1] : y[0];
+  float z = keep + __shfl_xor_sync(0xffffffffu, send, 2);
+  z += __shfl_xor_sync(0xffffffffu, z, 1);
+  return z;
+}
 
 __global__ void __launch_bounds__(kRasterThreads) raster_bwd_kernel(
     const float4* __restrict__ rec, const uint32_t* __restrict__ gauss, const uint2* __restrict__ ranges,
@@ -195,11 +263,15 @@ __global__ void __launch_bounds__(kRasterThreads) raster_bwd_kernel(
   __shared__ float4 s0[kChunk], s1[kChunk], s2[kChunk];
   __shared__ uint32_t sg[kChunk];
   __shared__ float acc[kChunk * kSlots];
+  __shared__ uint8_t smask[kChunk];
+  __shared__ uint8_t slist[kRasterThreads / 32][kChunk];
   __shared__ uint32_t s_max_last;
   const PixelGeom pg = pixel_geom(blockIdx.x, tiles_x, width, height);
+  const uint32_t ox = (blockIdx.x % tiles_x) * kTile, oy = (blockIdx.x / tiles_x) * kTile;
   const float px = (float)pg.px_i + 0.5f, py = (float)pg.py_j + 0.5f;
   const uint2 range = ranges[blockIdx.x];
-  const int lane = threadIdx.x & 31;
+  const uint32_t lane = threadIdx.x & 31;
+  uint8_t* list = slist[threadIdx.x >> 5];
 
   uint32_t last = 0;
   float T = 1.0f, t_fin = 1.0f, d0 = 0.0f, d1 = 0.0f, d2 = 0.0f, bg_dot = 0.0f;
@@ -217,10 +289,8 @@ __global__ void __launch_bounds__(kRasterThreads) raster_bwd_kernel(
   if (threadIdx.x == 0) s_max_last = 0;
   for (int i = threadIdx.x; i < kChunk * kSlots; i += kRasterThreads) acc[i] = 0.0f;
   __syncthreads();
-  {
-    const uint32_t m = __reduce_max_sync(0xffffffffu, last);
-    if (lane == 0) atomicMax(&s_max_last, m);
-  }
+  const uint32_t warp_max_last = __reduce_max_sync(0xffffffffu, last);
+  if (lane == 0) atomicMax(&s_max_last, warp_max_last);
   __syncthreads();
   const uint32_t max_last = s_max_last;
   float acc_r = 0.0f, acc_g = 0.0f, acc_b = 0.0f;  // accum (rasterize.rs:347)
@@ -230,24 +300,30 @@ __global__ void __launch_bounds__(kRasterThreads) raster_bwd_kernel(
   for (uint32_t cend = max_last; cend > 0;) {
     const uint32_t cstart = cend > (uint32_t)kChunk ? cend - kChunk : 0u;
     const uint32_t cnt = cend - cstart;
+    uint32_t m = 0;
     if (threadIdx.x < cnt) {
       const uint32_t g = gauss[range.x + cstart + threadIdx.x];
       sg[threadIdx.x] = g;
       s0[threadIdx.x] = rec[4 * (size_t)g];
       s1[threadIdx.x] = rec[4 * (size_t)g + 1];
-      s2[threadIdx.x] = rec[4 * (size_t)g + 2];
+      const float4 e2 = rec[4 * (size_t)g + 2];
+      s2[threadIdx.x] = e2;
+      m = subblock_mask(fbits(e2.z), fbits(e2.w), ox, oy);
     }
+    smask[threadIdx.x] = (uint8_t)m;
     __syncthreads();
-    for (int kk = (int)cnt - 1; kk >= 0; kk--) {
-      const uint32_t k = cstart + (uint32_t)kk;
+    // Entries at or past every lane's n_contrib contribute nothing to this warp.
+    const uint32_t limit = warp_max_last > cstart ? warp_max_last - cstart : 0u;
+    const uint32_t nl = build_warp_list(smask, cnt, limit, list);
+    for (int i = (int)nl - 1; i >= 0; i--) {
+      const uint32_t kk = list[i];
+      const uint32_t k = cstart + kk;
       const float4 e2 = s2[kk];
-      const uint32_t rx = fbits(e2.z), ry = fbits(e2.w);
-      if (!rect_hits_block(rx, ry, pg)) continue;
-      float c[11];
+      float c[16];
 #pragma unroll
-      for (int s = 0; s < 11; s++) c[s] = 0.0f;
+      for (int q = 0; q < 16; q++) c[q] = 0.0f;
       bool active = false;
-      if (k < last && pixel_in_rect(rx, ry, pg)) {
+      if (k < last && pixel_in_rect(fbits(e2.z), fbits(e2.w), pg)) {
         npairs++;
         const float4 e0 = s0[kk], e1 = s1[kk];
         float gval, alpha;
@@ -296,17 +372,9 @@ __global__ void __launch_bounds__(kRasterThreads) raster_bwd_kernel(
         }
       }
       if (__any_sync(0xffffffffu, active)) {
-#pragma unroll
-        for (int s = 0; s < 11; s++) {
-          float v = c[s];
-#pragma unroll
-          for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-          c[s] = v;
-        }
-        if (lane == 0) {
-#pragma unroll
-          for (int s = 0; s < 11; s++) atomicAdd(&acc[kk * kSlots + s], c[s]);
-        }
+        const float tot = warp_transpose_reduce16(c);
+        const uint32_t slot = (lane >> 1) & 15u;
+        if (!(lane & 1u) && slot < 11u) atomicAdd(&acc[kk * kSlots + slot], tot);
       }
     }
     __syncthreads();
@@ -320,7 +388,7 @@ __global__ void __launch_bounds__(kRasterThreads) raster_bwd_kernel(
       if (v1.x != 0.0f || v1.y != 0.0f || v1.z != 0.0f || v1.w != 0.0f) atomicAdd(&pgrad[cap + g], v1);
       if (v2.x != 0.0f || v2.y != 0.0f || v2.z != 0.0f) atomicAdd(&pgrad[2 * cap + g], v2);
 #pragma unroll
-      for (int s = 0; s < kSlots; s++) a[s] = 0.0f;
+      for (int q = 0; q < kSlots; q++) a[q] = 0.0f;
     }
     __syncthreads();
     cend = cstart;

@@ -233,17 +233,29 @@ __global__ void __launch_bounds__(kSortThreads) radix_upsweep_kernel(const K* __
   hist[(int64_t)threadIdx.x * nblocks + blockIdx.x] = cnt[threadIdx.x];
 }
 
+// Dynamic shared memory of the downsweep: the block's keys and values reordered by digit,
+// the per-warp digit counters and the block's digit starts.
+template <typename K> constexpr size_t downsweep_smem() {
+  return (size_t)kSortTile * (sizeof(K) + 4) + (size_t)kSortWarps * 256 * 4 + 256 * 4 + 64;
+}
+
 template <typename K>
 __global__ void __launch_bounds__(kSortThreads) radix_downsweep_kernel(const K* __restrict__ keys_in,
                                                                        const uint32_t* __restrict__ vals_in, int64_t n,
                                                                        int shift, const uint32_t* __restrict__ offsets,
                                                                        uint32_t nblocks, K* __restrict__ keys_out,
                                                                        uint32_t* __restrict__ vals_out) {
-  __shared__ uint32_t wcnt[kSortWarps][256];
+  extern __shared__ __align__(16) unsigned char dsm[];
+  K* sk = reinterpret_cast<K*>(dsm);
+  uint32_t* sv = reinterpret_cast<uint32_t*>(sk + kSortTile);
+  uint32_t(*wcnt)[256] = reinterpret_cast<uint32_t(*)[256]>(sv + kSortTile);
+  uint32_t* dstart = reinterpret_cast<uint32_t*>(wcnt) + kSortWarps * 256;
+  uint32_t* wsum = dstart + 256;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int d = lane; d < 256; d += 32) wcnt[warp][d] = 0;
   __syncwarp();
-  const int64_t wbase = (int64_t)blockIdx.x * kSortTile + (int64_t)warp * (32 * kSortRounds);
+  const int64_t bbase = (int64_t)blockIdx.x * kSortTile;
+  const int64_t wbase = bbase + (int64_t)warp * (32 * kSortRounds);
   K k[kSortRounds];
   uint32_t v[kSortRounds];
   uint32_t rank[kSortRounds];
@@ -263,27 +275,48 @@ __global__ void __launch_bounds__(kSortThreads) radix_downsweep_kernel(const K* 
     __syncwarp();
   }
   __syncthreads();
-  // Per-digit exclusive prefix over the warps (thread d owns digit d).
-  {
-    const int d = threadIdx.x;
-    uint32_t run = 0;
+  // Per digit (thread d): exclusive prefix over the warps and the block total.
+  const int d = threadIdx.x;
+  uint32_t total = 0;
 #pragma unroll
-    for (int w = 0; w < kSortWarps; w++) {
-      const uint32_t c = wcnt[w][d];
-      wcnt[w][d] = run;
-      run += c;
-    }
+  for (int w = 0; w < kSortWarps; w++) {
+    const uint32_t c = wcnt[w][d];
+    wcnt[w][d] = total;
+    total += c;
   }
+  // Block-wide exclusive scan of the totals over the digits.
+  uint32_t incl = total;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  if (lane == 31) wsum[warp] = incl;
   __syncthreads();
+  uint32_t wprefix = 0;
+  for (int w = 0; w < warp; w++) wprefix += wsum[w];
+  dstart[d] = wprefix + incl - total;
+  __syncthreads();
+  // Reorder the block's keys by digit in shared memory (stable).
 #pragma unroll
   for (int r = 0; r < kSortRounds; r++) {
     const int64_t idx = wbase + r * 32 + lane;
     if (idx < n) {
-      const uint32_t d = (uint32_t)(k[r] >> shift) & 0xffu;
-      const uint32_t pos = offsets[(int64_t)d * nblocks + blockIdx.x] + wcnt[warp][d] + rank[r];
-      keys_out[pos] = k[r];
-      vals_out[pos] = v[r];
+      const uint32_t dg = (uint32_t)(k[r] >> shift) & 0xffu;
+      const uint32_t pos = dstart[dg] + wcnt[warp][dg] + rank[r];
+      sk[pos] = k[r];
+      sv[pos] = v[r];
     }
+  }
+  __syncthreads();
+  // Write out runs of equal digits contiguously.
+  const int64_t nb = n - bbase < kSortTile ? n - bbase : kSortTile;
+  for (int i = threadIdx.x; i < nb; i += kSortThreads) {
+    const K key = sk[i];
+    const uint32_t dg = (uint32_t)(key >> shift) & 0xffu;
+    const uint32_t pos = offsets[(int64_t)dg * nblocks + blockIdx.x] + (uint32_t)i - dstart[dg];
+    keys_out[pos] = key;
+    vals_out[pos] = sv[i];
   }
 }
 
@@ -310,6 +343,8 @@ static Status sort_and_range(Ctx* c, const float* proj, const uint32_t* entry_of
                              const uint32_t* depth_range, int dbits, int total_bits, uint32_t tiles_x,
                              uint32_t num_tiles, uint32_t* gauss_out, uint64_t* keys_out, uint32_t* ranges) {
   const int passes = (total_bits + 7) / 8;
+  SPLAT_CUDA(cudaFuncSetAttribute(radix_downsweep_kernel<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)downsweep_smem<K>()));
   K *ka = nullptr, *kb = nullptr;
   uint32_t* vb = nullptr;
   SPLAT_TRY(arena_reserve(c, (size_t)E * sizeof(K), (void**)&ka));
@@ -338,7 +373,8 @@ static Status sort_and_range(Ctx* c, const float* proj, const uint32_t* entry_of
     const int shift = 8 * p;
     radix_upsweep_kernel<K><<<nblocks, kSortThreads, 0, c->stream>>>(kin, E, shift, hist, nblocks);
     SPLAT_TRY(launch_scan_u32(c, hist, (int64_t)nblocks * 256, offs, 0, tot));
-    radix_downsweep_kernel<K><<<nblocks, kSortThreads, 0, c->stream>>>(kin, vin, E, shift, offs, nblocks, kout, vout);
+    radix_downsweep_kernel<K><<<nblocks, kSortThreads, downsweep_smem<K>(), c->stream>>>(kin, vin, E, shift, offs,
+                                                                                         nblocks, kout, vout);
     c->launches.count += 2;
     SPLAT_LAUNCHED("radix sort pass");
     std::swap(kin, kout);
