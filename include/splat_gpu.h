@@ -171,6 +171,17 @@ SPLAT_API int splat_proj_to_reference(splat_ctx* ctx, const float* proj_dev, int
  * -------------------------------------------------------------------------------------- */
 SPLAT_API int splat_bin_count(splat_ctx* ctx, const uint32_t* num_tiles_dev, int64_t n,
                               uint32_t* entry_offset_dev, int64_t* num_entries);
+/* splat_bin_count for callers that cannot let this library allocate device memory: hosts
+ * that plan all device memory themselves (a fixed per-frame budget, or their own allocator
+ * owning the device) and cannot afford the synchronisation cudaMalloc/cudaFree may cause.
+ * It has no counterpart in the reference. Same inputs, outputs and result as
+ * splat_bin_count, but its scratch is a fixed 32 KiB array in device memory held by every
+ * GPU that loads the library, so n may be at most 16,777,216 (larger n returns
+ * SPLAT_ERR_CAPACITY). The first call on each device looks the array's address up; make
+ * it before any stream capture. All calls share the array: calls that overlap on the GPU
+ * race. Allocates nothing; synchronises to return the count. */
+SPLAT_API int splat_bin_count_noalloc(splat_ctx* ctx, const uint32_t* num_tiles_dev, int64_t n,
+                                      uint32_t* entry_offset_dev, int64_t* num_entries);
 SPLAT_API int splat_bin_sort(splat_ctx* ctx, const float* proj_dev, const uint32_t* entry_offset_dev, int64_t n,
                              int64_t num_entries, const uint32_t* depth_range_dev, uint32_t width, uint32_t height,
                              uint32_t* gauss_dev, uint64_t* keys_dev, uint32_t* tile_range_dev);

@@ -144,6 +144,7 @@ def _declare(L):
         "splat_proj_from_reference": ([vp, vp, i64, u32, u32, vp, vp, vp], C.c_int),
         "splat_proj_to_reference": ([vp, vp, i64, vp], C.c_int),
         "splat_bin_count": ([vp, vp, i64, vp, P(i64)], C.c_int),
+        "splat_bin_count_noalloc": ([vp, vp, i64, vp, P(i64)], C.c_int),
         "splat_bin_sort": ([vp, vp, vp, i64, i64, vp, u32, u32, vp, vp, vp], C.c_int),
         "splat_rasterize_fwd": ([vp, vp, vp, vp, u32, u32, P(C.c_float), vp, vp, vp, vp], C.c_int),
         "splat_rasterize_bwd": ([vp, vp, vp, vp, u32, u32, P(C.c_float), vp, vp, vp, vp, i64, vp], C.c_int),

@@ -18,6 +18,9 @@ Status launch_project_bwd(Ctx* c, const float* planes, int64_t n, int64_t cap, c
                           void* stats, int absgrad);
 
 Status launch_scan_u32(Ctx* c, const uint32_t* in, int64_t n, uint32_t* out, int write_total, uint64_t* total_dev);
+Status launch_scan_u32_into(Ctx* c, const uint32_t* in, int64_t n, uint32_t* out, int write_total,
+                            uint64_t* partial, uint64_t* total);
+constexpr int kScanValuesPerBlock = 4096;
 Status launch_bin_sort(Ctx* c, const float* proj, const uint32_t* entry_offset, int64_t n, int64_t E,
                        const uint32_t* depth_range_dev, uint32_t depth_min, uint32_t depth_max, uint32_t width,
                        uint32_t height, uint32_t* gauss_out, uint64_t* keys_out, uint32_t* ranges);

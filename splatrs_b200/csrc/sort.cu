@@ -408,3 +408,20 @@ Status launch_bin_sort(Ctx* c, const float* proj, const uint32_t* entry_offset, 
 }
 
 }  // namespace splat
+
+namespace splat {
+
+// The scan of launch_scan_u32 with caller-provided scratch: `partial` holds one uint64 per
+// 4096 input values and `total` one uint64. Allocates nothing.
+Status launch_scan_u32_into(Ctx* c, const uint32_t* in, int64_t n, uint32_t* out, int write_total,
+                            uint64_t* partial, uint64_t* total) {
+  const uint32_t blocks = ceil_div((uint64_t)std::max<int64_t>(n, 1), kScanTile);
+  scan_reduce_kernel<<<blocks, kScanThreads, 0, c->stream>>>(in, n, partial);
+  scan_partials_kernel<<<1, 1024, 0, c->stream>>>(partial, blocks, total);
+  scan_apply_kernel<<<blocks, kScanThreads, 0, c->stream>>>(in, n, partial, total, out, write_total);
+  c->launches.count += 3;
+  SPLAT_LAUNCHED("scan kernels");
+  return Status::ok();
+}
+
+}  // namespace splat
