@@ -42,6 +42,7 @@ def parse():
     ap.add_argument("--n", type=int, default=1_000_000)
     ap.add_argument("--cpu-steps", type=int, default=3, help="steps of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-train", action="store_true", help="skip the config-0 training run")
     ap.add_argument("--profile-small", action="store_true",
                     help="a reduced case for ncu captures (fewer Gaussians, one step)")
     return ap.parse_args()
@@ -297,6 +298,68 @@ def run_ours(args, rank, world, local):
     return line
 
 
+# Plain training on the small scene (config 0): 2,000 iterations, densification every 100
+# from 500 to 1,500 (threshold 2e-4), lambda 0.2, SH degree 3 with the reference's ramp.
+C0_TRAIN = dict(iterations=2000, densify=1, densify_from_iter=500, densify_until_iter=1500, densification_interval=100,
+                densify_grad_threshold=0.0002, lambda_dssim=0.2, sh_degree=3, position_lr_max_steps=2000, seed=0)
+
+
+def c0_views_gpu(ctx, s):
+    """Targets of config 0 rendered by the device renderer from the ground truth."""
+    from splatrs_b200 import gpu as G
+    from splatrs_b200 import scenes
+    from splatrs_b200._lib import Camera, ProjOpts
+    r = G.Renderer(ctx)
+    r.set_model(s["gt"], 3)
+    views = [(cam, scenes.to_rgb8(r.render(Camera.from_record(cam), ProjOpts.make(sh_degree=3), (0, 0, 0))))
+             for cam in s["cams"]]
+    r.close()
+    return views
+
+
+def run_train_c0_gpu(local):
+    """Full config-0 training run on the device trainer: wall time, iterations/s, PSNR."""
+    import torch
+    from splatrs_b200 import gpu as G
+    from splatrs_b200 import scenes
+    s = scenes.config0()
+    ctx = G.Context(local, torch.cuda.current_stream(local))
+    views = c0_views_gpu(ctx, s)
+    init_planes = G.init_from_points(ctx, s["init_points"], s["init_rgb"])
+    n0 = len(s["init_points"])
+    init = G.planes_to_params(ctx, init_planes, n0, n0).cpu().numpy()
+    extent = scenes.scene_extent(s["cams"])
+    t = G.Trainer(ctx, init, extent, views, **C0_TRAIN)
+    torch.cuda.synchronize(local)
+    tw = time.perf_counter()
+    for _ in range(C0_TRAIN["iterations"]):
+        t.step()
+    torch.cuda.synchronize(local)
+    wall = time.perf_counter() - tw
+    ps = float(np.mean([scenes.psnr(t.render(cam), rgb) for cam, rgb in views]))
+    out = {"iterations": C0_TRAIN["iterations"], "wall_s": round(wall, 3),
+           "iters_per_s": round(C0_TRAIN["iterations"] / wall, 1), "psnr_train_views": round(ps, 2),
+           "gaussians": t.count}
+    t.close()
+    ctx.close()
+    return out, init, views, extent
+
+
+def run_train_c0_cpu(init, views, extent):
+    """The same run on the CPU oracle trainer (all host threads)."""
+    from oracle import oracle as O
+    from splatrs_b200 import scenes
+    ot = O.Trainer(init, extent, views, **C0_TRAIN)
+    tw = time.perf_counter()
+    for _ in range(C0_TRAIN["iterations"]):
+        ot.step()
+    wall = time.perf_counter() - tw
+    ps = float(np.mean([scenes.psnr(ot.render(cam), rgb) for cam, rgb in views]))
+    return {"iterations": C0_TRAIN["iterations"], "wall_s": round(wall, 3),
+            "iters_per_s": round(C0_TRAIN["iterations"] / wall, 2), "psnr_train_views": round(ps, 2),
+            "gaussians": ot.count, "cores": O.threads(), "kind": "port"}
+
+
 def cpu_reference_steps(args, steps):
     """The CPU oracle (the reference's hot path restated in C++, all host threads) on the
     same workload: `steps` full forward+backward passes of the 1920x1080 view."""
@@ -357,7 +420,14 @@ def main():
         return
 
     line = run_ours(args, rank, world, local)
+    c0 = None
+    if not args.profile_small and not args.no_train:
+        gpu_c0, init, views, extent = run_train_c0_gpu(local)
+        line["train_c0"] = {"gpu": gpu_c0}
+        c0 = (init, views, extent)
     if rank == 0:
+        if c0 is not None and not args.no_cpu_baseline and world == 1:
+            line["train_c0"]["cpu"] = run_train_c0_cpu(*c0)
         if not args.no_cpu_baseline and world == 1:
             dt, cores = cpu_reference_steps(args, args.cpu_steps)
             line["cpu_baseline"] = {"value": round(WIDTH * HEIGHT / 1e6 / dt, 4), "unit": UNIT, "cores": cores,

@@ -292,6 +292,33 @@ SPLAT_API int splat_reset_opacity(splat_ctx* ctx, float* planes_dev, float* m_de
                                   float max_alpha);
 
 /* ----------------------------------------------------------------------------------------
+ * Initialisation from a sparse point cloud: Model::from_points (reference
+ * src/model.rs:77-104) with mean_nn_dist2 (:128-186), an exact brute-force 3-NN search.
+ *   splat_mean_nn_dist2: points (n x 3 float, device) -> mean squared distance to the three
+ *     nearest other points (n doubles, device); coincident points count as neighbours.
+ *   splat_init_from_points: points (n x 3 float) and colours (n x 3 uint8) on the host ->
+ *     n Gaussians in parameter planes (capacity cap) on the device. Synchronises.
+ * -------------------------------------------------------------------------------------- */
+SPLAT_API int splat_mean_nn_dist2(splat_ctx* ctx, const float* points_dev, int64_t n, double* out_dev);
+SPLAT_API int splat_init_from_points(splat_ctx* ctx, const float* points_host, const uint8_t* rgb_host, int64_t n,
+                                     float* planes_dev, int64_t cap);
+
+/* ----------------------------------------------------------------------------------------
+ * PLY codec: the standard 3DGS binary little-endian float32 layout (reference
+ * src/ply.rs:19-181) straight into / out of parameter planes on the device.
+ *   splat_ply_read_header: vertex count and SH degree (from the f_rest count) of a file.
+ *   splat_ply_read: read (ply.rs:73-181) into planes of capacity cap (SPLAT_ERR_CAPACITY if
+ *     the file holds more Gaussians); property order is taken from the header; format
+ *     errors return SPLAT_ERR_INVALID with the reference's messages.
+ *   splat_ply_write: write (ply.rs:19-69) n Gaussians with coefficients up to sh_degree.
+ * -------------------------------------------------------------------------------------- */
+SPLAT_API int splat_ply_read_header(splat_ctx* ctx, const char* path, int64_t* count, int32_t* sh_degree);
+SPLAT_API int splat_ply_read(splat_ctx* ctx, const char* path, float* planes_dev, int64_t cap, int64_t* count,
+                             int32_t* sh_degree);
+SPLAT_API int splat_ply_write(splat_ctx* ctx, const char* path, const float* planes_dev, int64_t n, int64_t cap,
+                              int32_t sh_degree);
+
+/* ----------------------------------------------------------------------------------------
  * Trainer: train::train (reference src/train.rs:161-306) one iteration per call, with the
  * model, Adam state, statistics and the training views (8-bit pixels) resident in device
  * memory. The view order and split offsets come from a SplitMix64 generator seeded with

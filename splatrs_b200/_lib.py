@@ -164,6 +164,11 @@ def _declare(L):
         "splat_densify": ([vp, vp, vp, vp, i64, i64, vp, P(DensifyConfig), C.c_float, P(C.c_uint64), vp, vp, vp, i64,
                            P(DensifyReport)], C.c_int),
         "splat_reset_opacity": ([vp, vp, vp, vp, i64, C.c_float], C.c_int),
+        "splat_mean_nn_dist2": ([vp, vp, i64, vp], C.c_int),
+        "splat_init_from_points": ([vp, vp, vp, i64, vp, i64], C.c_int),
+        "splat_ply_read_header": ([vp, C.c_char_p, P(i64), P(i32)], C.c_int),
+        "splat_ply_read": ([vp, C.c_char_p, vp, i64, P(i64), P(i32)], C.c_int),
+        "splat_ply_write": ([vp, C.c_char_p, vp, i64, i64, i32], C.c_int),
         "splat_trainer_create": ([vp, P(TrainConfig), C.c_float, P(vp)], C.c_int),
         "splat_trainer_destroy": ([vp], C.c_int),
         "splat_trainer_set_model": ([vp, vp, i64], C.c_int),

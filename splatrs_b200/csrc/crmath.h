@@ -88,6 +88,51 @@ CRM_HD float expf_cr(float x) {
   return (float)(p * s);
 }
 
+// 2^(j/64), j = 0..63, each correctly rounded to double.
+#define CRM_EXP2_TAB64                                                                          \
+  {0x1.0000000000000p+0, 0x1.02c9a3e778061p+0, 0x1.059b0d3158574p+0, 0x1.0874518759bc8p+0,     \
+   0x1.0b5586cf9890fp+0, 0x1.0e3ec32d3d1a2p+0, 0x1.11301d0125b51p+0, 0x1.1429aaea92de0p+0,     \
+   0x1.172b83c7d517bp+0, 0x1.1a35beb6fcb75p+0, 0x1.1d4873168b9aap+0, 0x1.2063b88628cd6p+0,     \
+   0x1.2387a6e756238p+0, 0x1.26b4565e27cddp+0, 0x1.29e9df51fdee1p+0, 0x1.2d285a6e4030bp+0,     \
+   0x1.306fe0a31b715p+0, 0x1.33c08b26416ffp+0, 0x1.371a7373aa9cbp+0, 0x1.3a7db34e59ff7p+0,     \
+   0x1.3dea64c123422p+0, 0x1.4160a21f72e2ap+0, 0x1.44e086061892dp+0, 0x1.486a2b5c13cd0p+0,     \
+   0x1.4bfdad5362a27p+0, 0x1.4f9b2769d2ca7p+0, 0x1.5342b569d4f82p+0, 0x1.56f4736b527dap+0,     \
+   0x1.5ab07dd485429p+0, 0x1.5e76f15ad2148p+0, 0x1.6247eb03a5585p+0, 0x1.6623882552225p+0,     \
+   0x1.6a09e667f3bcdp+0, 0x1.6dfb23c651a2fp+0, 0x1.71f75e8ec5f74p+0, 0x1.75feb564267c9p+0,     \
+   0x1.7a11473eb0187p+0, 0x1.7e2f336cf4e62p+0, 0x1.82589994cce13p+0, 0x1.868d99b4492edp+0,     \
+   0x1.8ace5422aa0dbp+0, 0x1.8f1ae99157736p+0, 0x1.93737b0cdc5e5p+0, 0x1.97d829fde4e50p+0,     \
+   0x1.9c49182a3f090p+0, 0x1.a0c667b5de565p+0, 0x1.a5503b23e255dp+0, 0x1.a9e6b5579fdbfp+0,     \
+   0x1.ae89f995ad3adp+0, 0x1.b33a2b84f15fbp+0, 0x1.b7f76f2fb5e47p+0, 0x1.bcc1e904bc1d2p+0,     \
+   0x1.c199bdd85529cp+0, 0x1.c67f12e57d14bp+0, 0x1.cb720dcef9069p+0, 0x1.d072d4a07897cp+0,     \
+   0x1.d5818dcfba487p+0, 0x1.da9e603db3285p+0, 0x1.dfc97337b9b5fp+0, 0x1.e502ee78b3ff6p+0,     \
+   0x1.ea4afa2a490dap+0, 0x1.efa1bee615a27p+0, 0x1.f50765b6e4540p+0, 0x1.fa7c1819e90d8p+0}
+
+// The same correctly rounded e^x with fewer double operations, for hot loops (table-driven
+// method, Tang 1989): x = (64 m + j) ln2/64 + r with |r| <= ln2/128, ln2/64 split into a
+// 39-bit head and a tail (so the head product and x minus it are exact);
+// e^x = 2^m * 2^(j/64) * (1 + q), q = e^r - 1 by its Taylor series to r^5 (truncation
+// below 4e-17 relative). `tab` is CRM_EXP2_TAB64 (in shared memory on the device). An
+// exhaustive sweep over every float in [-110, 90] gives results identical to expf_cr.
+CRM_HD float expf_cr_tab(float x, const double* tab) {
+  if (!(x == x)) return x;
+  if (x > 88.8f) return (float)INFINITY;
+  if (x < -104.0f) return 0.0f;
+  double d = (double)x;
+  double n = rint(d * 0x1.71547652b82fep+6);  // 64 / ln2
+  double r = fma(-n, 0x1.62e42fefa0000p-7, d);
+  r = fma(-n, 0x1.cf79abc9e3b3ap-46, r);
+  int ni = (int)n;
+  double c = fma(r, 0x1.1111111111111p-7, 0x1.5555555555555p-5);  // 1/120, 1/24
+  c = fma(r, c, 0x1.5555555555555p-3);                            // 1/6
+  c = fma(r, c, 0.5);
+  c = fma(r, c, 1.0);
+  double q = r * c;
+  double t = tab[ni & 63];
+  double y = fma(t, q, t);
+  double s = bits_to_double((uint64_t)((ni >> 6) + 1023) << 52);
+  return (float)(y * s);
+}
+
 // Correctly rounded natural log for float x.
 CRM_HD float logf_cr(float x) {
   if (!(x == x) || x < 0.0f) return (float)NAN;

@@ -704,41 +704,62 @@ __global__ void __launch_bounds__(128) project_bwd_kernel(const float4* __restri
   for (int q = 0; q < 12; q++) out[(3 + q) * cap + i] = make_float4(o_sh[4 * q], o_sh[4 * q + 1], o_sh[4 * q + 2], o_sh[4 * q + 3]);
 }
 
-// Reference Gaussian records <-> planes.
-__global__ void aos_to_planes_kernel(const float* __restrict__ aos, int64_t n, float4* __restrict__ planes, int64_t cap) {
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const float* a = aos + 59 * i;
-  planes[i] = make_float4(a[0], a[1], a[2], a[10]);
-  planes[cap + i] = make_float4(a[6], a[7], a[8], a[9]);
-  planes[2 * cap + i] = make_float4(a[3], a[4], a[5], 0.0f);
-#pragma unroll
-  for (int q = 0; q < 12; q++) planes[(3 + q) * cap + i] = make_float4(a[11 + 4 * q], a[12 + 4 * q], a[13 + 4 * q], a[14 + 4 * q]);
+// Reference Gaussian records <-> planes, 128 Gaussians per block through shared memory so
+// that both the plane side (128-bit loads/stores) and the record side (contiguous 59-float
+// rows) are coalesced.
+constexpr int kConvG = 128;
+
+// Position of record field f (0..58) in the 60-float plane order (mean xyz, opacity, quat,
+// log-scale xyz, pad, sh...).
+__device__ __forceinline__ int plane_slot_of_field(int f) {
+  if (f < 3) return f;          // mean
+  if (f < 6) return 8 + f - 3;  // log_scale
+  if (f < 10) return 4 + f - 6; // quat
+  if (f == 10) return 3;        // opacity
+  return 12 + f - 11;           // sh
 }
 
-__global__ void planes_to_aos_kernel(const float4* __restrict__ planes, int64_t n, int64_t cap, float* __restrict__ aos) {
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  float* a = aos + 59 * i;
-  const float4 p0 = planes[i], p1 = planes[cap + i], p2 = planes[2 * cap + i];
-  a[0] = p0.x;
-  a[1] = p0.y;
-  a[2] = p0.z;
-  a[10] = p0.w;
-  a[6] = p1.x;
-  a[7] = p1.y;
-  a[8] = p1.z;
-  a[9] = p1.w;
-  a[3] = p2.x;
-  a[4] = p2.y;
-  a[5] = p2.z;
+__global__ void __launch_bounds__(kConvG) aos_to_planes_kernel(const float* __restrict__ aos, int64_t n,
+                                                               float4* __restrict__ planes, int64_t cap) {
+  __shared__ float tile[kConvG][61];
+  const int64_t base = (int64_t)blockIdx.x * kConvG;
+  const int cnt = (int)min((int64_t)kConvG, n - base);
+  const float* src = aos + base * 59;
+  for (int L = threadIdx.x; L < cnt * 59; L += kConvG) {
+    const int g = L / 59, f = L - g * 59;
+    tile[g][plane_slot_of_field(f)] = src[L];
+  }
+  __syncthreads();
+  const int t = threadIdx.x;
+  if (t < cnt) {
+    tile[t][11] = 0.0f;  // pad lane of the log-scale plane
 #pragma unroll
-  for (int q = 0; q < 12; q++) {
-    const float4 s = planes[(3 + q) * cap + i];
-    a[11 + 4 * q] = s.x;
-    a[12 + 4 * q] = s.y;
-    a[13 + 4 * q] = s.z;
-    a[14 + 4 * q] = s.w;
+    for (int q = 0; q < kPlanes; q++)
+      planes[q * cap + base + t] = make_float4(tile[t][4 * q], tile[t][4 * q + 1], tile[t][4 * q + 2], tile[t][4 * q + 3]);
+  }
+}
+
+__global__ void __launch_bounds__(kConvG) planes_to_aos_kernel(const float4* __restrict__ planes, int64_t n, int64_t cap,
+                                                               float* __restrict__ aos) {
+  __shared__ float tile[kConvG][61];
+  const int64_t base = (int64_t)blockIdx.x * kConvG;
+  const int cnt = (int)min((int64_t)kConvG, n - base);
+  const int t = threadIdx.x;
+  if (t < cnt) {
+#pragma unroll
+    for (int q = 0; q < kPlanes; q++) {
+      const float4 v = planes[q * cap + base + t];
+      tile[t][4 * q] = v.x;
+      tile[t][4 * q + 1] = v.y;
+      tile[t][4 * q + 2] = v.z;
+      tile[t][4 * q + 3] = v.w;
+    }
+  }
+  __syncthreads();
+  float* dst = aos + base * 59;
+  for (int L = threadIdx.x; L < cnt * 59; L += kConvG) {
+    const int g = L / 59, f = L - g * 59;
+    dst[L] = tile[g][plane_slot_of_field(f)];
   }
 }
 
@@ -816,7 +837,7 @@ Status launch_project_bwd(Ctx* c, const float* planes, int64_t n, int64_t cap, c
 
 Status launch_params_from_aos(Ctx* c, const float* aos, int64_t n, float* planes, int64_t cap) {
   if (n == 0) return Status::ok();
-  aos_to_planes_kernel<<<ceil_div(n, 256), 256, 0, c->stream>>>(aos, n, reinterpret_cast<float4*>(planes), cap);
+  aos_to_planes_kernel<<<ceil_div(n, kConvG), kConvG, 0, c->stream>>>(aos, n, reinterpret_cast<float4*>(planes), cap);
   c->launches.count++;
   SPLAT_LAUNCHED("aos_to_planes_kernel");
   return Status::ok();
@@ -824,7 +845,8 @@ Status launch_params_from_aos(Ctx* c, const float* aos, int64_t n, float* planes
 
 Status launch_params_to_aos(Ctx* c, const float* planes, int64_t n, int64_t cap, float* aos) {
   if (n == 0) return Status::ok();
-  planes_to_aos_kernel<<<ceil_div(n, 256), 256, 0, c->stream>>>(reinterpret_cast<const float4*>(planes), n, cap, aos);
+  planes_to_aos_kernel<<<ceil_div(n, kConvG), kConvG, 0, c->stream>>>(reinterpret_cast<const float4*>(planes), n, cap,
+                                                                      aos);
   c->launches.count++;
   SPLAT_LAUNCHED("planes_to_aos_kernel");
   return Status::ok();

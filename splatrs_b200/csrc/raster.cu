@@ -33,19 +33,19 @@ __device__ __forceinline__ PixelGeom pixel_geom(uint32_t tile, uint32_t tiles_x,
   return p;
 }
 
-__device__ __forceinline__ bool pixel_in_rect(uint32_t rx, uint32_t ry, const PixelGeom& p) {
-  const uint32_t x0 = rx & 0xffffu, x1 = rx >> 16, y0 = ry & 0xffffu, y1 = ry >> 16;
-  return p.px_i >= x0 && p.px_i < x1 && p.py_j >= y0 && p.py_j < y1;
-}
 
-// evaluate (rasterize.rs:231-244). Returns false when skipped.
+__constant__ double kExp2Tab64[64] = CRM_EXP2_TAB64;
+
+// evaluate (rasterize.rs:231-244). Returns false when skipped. `tab` is the exp table in
+// shared memory.
 __device__ __forceinline__ bool evaluate(float px, float py, float mx, float my, float A, float B, float C,
-                                         float opacity, float sigma_max, float* gauss_out, float* alpha_out) {
+                                         float opacity, float sigma_max, const double* tab, float* gauss_out,
+                                         float* alpha_out) {
   const float dx = px - mx;
   const float dy = py - my;
   const float sigma = 0.5f * (A * dx * dx + C * dy * dy) + B * dx * dy;
   if (sigma < 0.0f || sigma > sigma_max) return false;
-  const float gauss = crm::expf_cr(-sigma);
+  const float gauss = crm::expf_cr_tab(-sigma, tab);
   const float og = opacity * gauss;
   if (og < SPLAT_ALPHA_MIN) return false;
   *gauss_out = gauss;
@@ -114,6 +114,18 @@ Status launch_diag_fast_exp(Ctx* c, float magnitude_lo, float magnitude_hi, int 
   return Status::ok();
 }
 
+// The entry's pixel rectangle within the tile whose top-left pixel is (ox, oy) as a 16-bit
+// mask of the columns and a 16-bit mask of the rows it covers (columns in the low half).
+__device__ __forceinline__ uint32_t tile_rect_masks(uint32_t rx, uint32_t ry, uint32_t ox, uint32_t oy) {
+  const int x0 = (int)(rx & 0xffffu) - (int)ox, x1 = (int)(rx >> 16) - (int)ox;
+  const int y0 = (int)(ry & 0xffffu) - (int)oy, y1 = (int)(ry >> 16) - (int)oy;
+  const uint32_t cx0 = (uint32_t)min(max(x0, 0), 16), cx1 = (uint32_t)min(max(x1, 0), 16);
+  const uint32_t cy0 = (uint32_t)min(max(y0, 0), 16), cy1 = (uint32_t)min(max(y1, 0), 16);
+  const uint32_t cols = cx1 > cx0 ? ((0xffffu >> (16u - (cx1 - cx0))) << cx0) : 0u;
+  const uint32_t rows = cy1 > cy0 ? ((0xffffu >> (16u - (cy1 - cy0))) << cy0) : 0u;
+  return cols | (rows << 16);
+}
+
 // Bit w of the result is set when the pixel rectangle (x0|x1<<16, y0|y1<<16, absolute
 // pixels) overlaps warp w's 8x4 sub-block of the tile whose top-left pixel is (ox, oy).
 __device__ __forceinline__ uint32_t subblock_mask(uint32_t rx, uint32_t ry, uint32_t ox, uint32_t oy) {
@@ -149,15 +161,20 @@ __device__ __forceinline__ uint32_t build_warp_list(const uint8_t* __restrict__ 
 }
 
 // forward_tile (rasterize.rs:249-302) for one tile per block.
-__global__ void __launch_bounds__(kRasterThreads) raster_fwd_kernel(
+__global__ void __launch_bounds__(kRasterThreads, 6) raster_fwd_kernel(
     const float4* __restrict__ rec, const uint32_t* __restrict__ gauss, const uint2* __restrict__ ranges,
     uint32_t width, uint32_t height, uint32_t tiles_x, float bg0, float bg1, float bg2, float* __restrict__ image,
     float* __restrict__ final_t, uint32_t* __restrict__ n_contrib, unsigned long long* __restrict__ pairs) {
-  __shared__ float4 s0[kChunk], s1[kChunk], s2[kChunk];
+  __shared__ float4 s0[kChunk], s1[kChunk];
+  __shared__ float2 s2[kChunk];
+  __shared__ uint32_t srect[kChunk];
   __shared__ uint8_t smask[kChunk];
   __shared__ uint8_t slist[kRasterThreads / 32][kChunk];
+  __shared__ double stab[64];
+  if (threadIdx.x < 64) stab[threadIdx.x] = kExp2Tab64[threadIdx.x];
   const PixelGeom pg = pixel_geom(blockIdx.x, tiles_x, width, height);
   const uint32_t ox = (blockIdx.x % tiles_x) * kTile, oy = (blockIdx.x / tiles_x) * kTile;
+  const uint32_t lx = pg.px_i - ox, ly_shift = pg.py_j - oy + 16u;  // bit positions in the rect masks
   const float px = (float)pg.px_i + 0.5f, py = (float)pg.py_j + 0.5f;
   const uint2 range = ranges[blockIdx.x];
   uint8_t* list = slist[threadIdx.x >> 5];
@@ -174,7 +191,8 @@ __global__ void __launch_bounds__(kRasterThreads) raster_fwd_kernel(
       s0[threadIdx.x] = rec[4 * (size_t)g];
       s1[threadIdx.x] = rec[4 * (size_t)g + 1];
       const float4 e2 = rec[4 * (size_t)g + 2];
-      s2[threadIdx.x] = e2;
+      s2[threadIdx.x] = make_float2(e2.x, e2.y);
+      srect[threadIdx.x] = tile_rect_masks(fbits(e2.z), fbits(e2.w), ox, oy);
       m = subblock_mask(fbits(e2.z), fbits(e2.w), ox, oy);
     }
     smask[threadIdx.x] = (uint8_t)m;
@@ -184,12 +202,13 @@ __global__ void __launch_bounds__(kRasterThreads) raster_fwd_kernel(
     for (uint32_t i = 0; i < nl; i++) {
       if (__all_sync(0xffffffffu, done)) break;
       const uint32_t k = list[i];
-      const float4 e2 = s2[k];
-      if (done || !pixel_in_rect(fbits(e2.z), fbits(e2.w), pg)) continue;
+      const uint32_t rm = srect[k];
+      if (done || !((rm >> lx) & (rm >> ly_shift) & 1u)) continue;
       npairs++;
       const float4 e0 = s0[k], e1 = s1[k];
+      const float2 e2 = s2[k];
       float gval, alpha;
-      if (!evaluate(px, py, e0.x, e0.y, e0.z, e0.w, e1.x, e1.y, e1.z, &gval, &alpha)) continue;
+      if (!evaluate(px, py, e0.x, e0.y, e0.z, e0.w, e1.x, e1.y, e1.z, stab, &gval, &alpha)) continue;
       const float test_t = T * (1.0f - alpha);
       if (test_t < SPLAT_T_MIN) {
         done = true;
@@ -260,7 +279,9 @@ __global__ void __launch_bounds__(kRasterThreads) raster_bwd_kernel(
     uint32_t width, uint32_t height, uint32_t tiles_x, float bg0, float bg1, float bg2,
     const float* __restrict__ final_t, const uint32_t* __restrict__ n_contrib, const float* __restrict__ dimage,
     float4* __restrict__ pgrad, int64_t cap, unsigned long long* __restrict__ pairs) {
-  __shared__ float4 s0[kChunk], s1[kChunk], s2[kChunk];
+  __shared__ float4 s0[kChunk], s1[kChunk];
+  __shared__ float2 s2[kChunk];
+  __shared__ uint32_t srect[kChunk];
   __shared__ uint32_t sg[kChunk];
   __shared__ float acc[kChunk * kSlots];
   __shared__ uint8_t smask[kChunk];
@@ -268,6 +289,7 @@ __global__ void __launch_bounds__(kRasterThreads) raster_bwd_kernel(
   __shared__ uint32_t s_max_last;
   const PixelGeom pg = pixel_geom(blockIdx.x, tiles_x, width, height);
   const uint32_t ox = (blockIdx.x % tiles_x) * kTile, oy = (blockIdx.x / tiles_x) * kTile;
+  const uint32_t lx = pg.px_i - ox, ly_shift = pg.py_j - oy + 16u;  // bit positions in the rect masks
   const float px = (float)pg.px_i + 0.5f, py = (float)pg.py_j + 0.5f;
   const uint2 range = ranges[blockIdx.x];
   const uint32_t lane = threadIdx.x & 31;
@@ -307,7 +329,8 @@ __global__ void __launch_bounds__(kRasterThreads) raster_bwd_kernel(
       s0[threadIdx.x] = rec[4 * (size_t)g];
       s1[threadIdx.x] = rec[4 * (size_t)g + 1];
       const float4 e2 = rec[4 * (size_t)g + 2];
-      s2[threadIdx.x] = e2;
+      s2[threadIdx.x] = make_float2(e2.x, e2.y);
+      srect[threadIdx.x] = tile_rect_masks(fbits(e2.z), fbits(e2.w), ox, oy);
       m = subblock_mask(fbits(e2.z), fbits(e2.w), ox, oy);
     }
     smask[threadIdx.x] = (uint8_t)m;
@@ -318,12 +341,13 @@ __global__ void __launch_bounds__(kRasterThreads) raster_bwd_kernel(
     for (int i = (int)nl - 1; i >= 0; i--) {
       const uint32_t kk = list[i];
       const uint32_t k = cstart + kk;
-      const float4 e2 = s2[kk];
+      const uint32_t rm = srect[kk];
       float c[16];
 #pragma unroll
       for (int q = 0; q < 16; q++) c[q] = 0.0f;
       bool active = false;
-      if (k < last && pixel_in_rect(fbits(e2.z), fbits(e2.w), pg)) {
+      if (k < last && ((rm >> lx) & (rm >> ly_shift) & 1u)) {
+        const float2 e2 = s2[kk];
         npairs++;
         const float4 e0 = s0[kk], e1 = s1[kk];
         float gval, alpha;

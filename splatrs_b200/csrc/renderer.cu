@@ -90,6 +90,10 @@ Status render_view(Ctx* c, const float* planes, int64_t n, int64_t cap, const sp
 
 using namespace splat;
 
+// Chunks of the gradient download: the projection backward and the record conversion of
+// chunk i+1 run while chunk i crosses PCIe on the copy stream.
+constexpr int kDownloadChunks = 8;
+
 struct splat_renderer {
   splat_ctx* ctx;
   Ctx* c;
@@ -98,6 +102,8 @@ struct splat_renderer {
   DevBuf planes, aos, pgrad, grad_planes, grad_aos;
   ViewBuffers v;
   int64_t last_entries = 0;
+  cudaStream_t copy = nullptr;  // host<->device transfers overlapping the compute stream
+  cudaEvent_t ev_up = nullptr, ev_img = nullptr, ev_chunk[kDownloadChunks] = {};
 };
 
 namespace {
@@ -133,6 +139,21 @@ SPLAT_API int splat_renderer_create(splat_ctx* ctx, splat_renderer** out) {
   if (!r) return SPLAT_ERR_INVALID;
   r->ctx = ctx;
   r->c = splat_ctx_impl(ctx);
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaSetDevice(r->c->device);
+  bool ok = cudaStreamCreateWithFlags(&r->copy, cudaStreamNonBlocking) == cudaSuccess;
+  ok = ok && cudaEventCreateWithFlags(&r->ev_up, cudaEventDisableTiming) == cudaSuccess;
+  ok = ok && cudaEventCreateWithFlags(&r->ev_img, cudaEventDisableTiming) == cudaSuccess;
+  for (int i = 0; i < kDownloadChunks && ok; i++)
+    ok = cudaEventCreateWithFlags(&r->ev_chunk[i], cudaEventDisableTiming) == cudaSuccess;
+  cudaSetDevice(prev);
+  if (!ok) {
+    cudaGetLastError();
+    r->c->last_error = "splat_renderer_create: stream or event creation failed";
+    delete r;
+    return SPLAT_ERR_CUDA;
+  }
   *out = r;
   return SPLAT_OK;
 }
@@ -142,8 +163,14 @@ SPLAT_API int splat_renderer_destroy(splat_renderer* r) {
   {
     REnter e(r);
     cudaStreamSynchronize(r->c->stream);
+    cudaStreamSynchronize(r->copy);
     for (DevBuf* b : {&r->planes, &r->aos, &r->pgrad, &r->grad_planes, &r->grad_aos}) b->release();
     r->v.release();
+    for (cudaEvent_t ev : r->ev_chunk)
+      if (ev) cudaEventDestroy(ev);
+    if (r->ev_up) cudaEventDestroy(r->ev_up);
+    if (r->ev_img) cudaEventDestroy(r->ev_img);
+    if (r->copy) cudaStreamDestroy(r->copy);
   }
   delete r;
   return SPLAT_OK;
@@ -205,33 +232,49 @@ SPLAT_API int splat_renderer_render_backward(splat_renderer* r, const splat_came
   o.sh_degree = r->sh_degree;
   const size_t npix = (size_t)cam->width * cam->height;
   Status s = r->v.ensure(r->n, cam->width, cam->height);
-  // The upload of dL/dimage overlaps nothing here but is issued first so the copy engine
-  // runs while the projection kernels start.
-  if (s.good()) s = cuda_status(cudaMemcpyAsync(r->v.dimage.ptr, dimage_host, npix * 12, cudaMemcpyHostToDevice,
-                                                c->stream), "upload dimage");
-  if (s.good()) s = render_view(c, r->planes.as<float>(), r->n, r->cap, *cam, o, background, r->v, &r->last_entries);
-  if (s.good() && image_host)
-    s = cuda_status(cudaMemcpyAsync(image_host, r->v.image.ptr, npix * 12, cudaMemcpyDeviceToHost, c->stream),
-                    "download image");
   if (s.good()) s = r->pgrad.ensure((size_t)r->cap * 3 * 16);
   if (s.good()) s = r->grad_planes.ensure((size_t)r->cap * kPlanes * 16);
   if (s.good()) s = r->grad_aos.ensure((size_t)r->cap * 59 * 4);
+  // dL/dimage crosses PCIe while the forward pass runs.
+  if (s.good()) s = cuda_status(cudaMemcpyAsync(r->v.dimage.ptr, dimage_host, npix * 12, cudaMemcpyHostToDevice,
+                                                r->copy), "upload dimage");
+  if (s.good()) s = cuda_status(cudaEventRecord(r->ev_up, r->copy), "cudaEventRecord");
+  if (s.good()) s = render_view(c, r->planes.as<float>(), r->n, r->cap, *cam, o, background, r->v, &r->last_entries);
+  // The image crosses PCIe while the backward pass runs.
+  if (s.good() && image_host) {
+    s = cuda_status(cudaEventRecord(r->ev_img, c->stream), "cudaEventRecord");
+    if (s.good()) s = cuda_status(cudaStreamWaitEvent(r->copy, r->ev_img, 0), "cudaStreamWaitEvent");
+    if (s.good())
+      s = cuda_status(cudaMemcpyAsync(image_host, r->v.image.ptr, npix * 12, cudaMemcpyDeviceToHost, r->copy),
+                      "download image");
+  }
+  if (s.good()) s = cuda_status(cudaStreamWaitEvent(c->stream, r->ev_up, 0), "cudaStreamWaitEvent");
   if (s.good()) s = cuda_status(cudaMemsetAsync(r->pgrad.ptr, 0, (size_t)r->cap * 3 * 16, c->stream), "zero pgrad");
   if (s.good())
     s = launch_raster_bwd(c, r->v.proj.as<float>(), r->v.gauss.as<uint32_t>(), r->v.tile_range.as<uint32_t>(),
                           cam->width, cam->height, background, r->v.final_t.as<float>(), r->v.n_contrib.as<uint32_t>(),
                           r->v.dimage.as<float>(), r->pgrad.as<float>(), r->cap, nullptr);
-  if (s.good())
-    s = launch_project_bwd(c, r->planes.as<float>(), r->n, r->cap, *cam, o, r->v.proj.as<float>(), r->pgrad.as<float>(),
-                           r->grad_planes.as<float>(), nullptr, 0);
-  if (s.good() && grads_aos59_host) {
-    s = launch_params_to_aos(c, r->grad_planes.as<float>(), r->n, r->cap, r->grad_aos.as<float>());
-    if (s.good() && r->n)
-      s = cuda_status(cudaMemcpyAsync(grads_aos59_host, r->grad_aos.ptr, (size_t)r->n * 59 * 4, cudaMemcpyDeviceToHost,
-                                      c->stream),
-                      "download gradients");
+  // Projection backward, record conversion and download in chunks of Gaussians.
+  const int64_t chunk = ((r->n + kDownloadChunks - 1) / kDownloadChunks + 127) / 128 * 128;
+  for (int k = 0; s.good() && k < kDownloadChunks; k++) {
+    const int64_t i0 = (int64_t)k * chunk;
+    if (i0 >= r->n) break;
+    const int64_t cnt = std::min(chunk, r->n - i0);
+    s = launch_project_bwd(c, r->planes.as<float>() + 4 * i0, cnt, r->cap, *cam, o, r->v.proj.as<float>() + 16 * i0,
+                           r->pgrad.as<float>() + 4 * i0, r->grad_planes.as<float>() + 4 * i0, nullptr, 0);
+    if (s.good() && grads_aos59_host) {
+      s = launch_params_to_aos(c, r->grad_planes.as<float>() + 4 * i0, cnt, r->cap, r->grad_aos.as<float>() + 59 * i0);
+      if (s.good()) s = cuda_status(cudaEventRecord(r->ev_chunk[k], c->stream), "cudaEventRecord");
+      if (s.good()) s = cuda_status(cudaStreamWaitEvent(r->copy, r->ev_chunk[k], 0), "cudaStreamWaitEvent");
+      if (s.good())
+        s = cuda_status(cudaMemcpyAsync(grads_aos59_host + 59 * i0, r->grad_aos.as<float>() + 59 * i0,
+                                        (size_t)cnt * 59 * 4, cudaMemcpyDeviceToHost, r->copy),
+                        "download gradients");
+    }
   }
-  if (s.good()) s = cuda_status(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
+  const Status s1 = cuda_status(cudaStreamSynchronize(r->copy), "cudaStreamSynchronize");
+  const Status s2 = cuda_status(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
+  if (s.good()) s = s1.good() ? s2 : s1;
   return s.good() ? SPLAT_OK : rfail(r, s);
 }
 

@@ -398,3 +398,41 @@ class Trainer:
             self.close()
         except Exception:
             pass
+
+
+def ply_read(ctx: Context, path: str, cap: int | None = None):
+    """ply::read (src/ply.rs:73-181) into parameter planes: returns (planes, n, sh_degree)."""
+    n = C.c_int64()
+    d = C.c_int32()
+    check(ctx.lib.splat_ply_read_header(ctx.h, path.encode(), C.byref(n), C.byref(d)), ctx.h)
+    cap = max(1, n.value if cap is None else cap)
+    planes = empty_planes(cap, torch.device("cuda", ctx.device))
+    check(ctx.lib.splat_ply_read(ctx.h, path.encode(), _ptr(planes), cap, C.byref(n), C.byref(d)), ctx.h)
+    return planes, int(n.value), int(d.value), cap
+
+
+def ply_write(ctx: Context, path: str, planes: torch.Tensor, n: int, cap: int, sh_degree: int):
+    """ply::write (src/ply.rs:19-69) from parameter planes."""
+    check(ctx.lib.splat_ply_write(ctx.h, path.encode(), _ptr(planes), n, cap, sh_degree), ctx.h)
+
+
+def mean_nn_dist2(ctx: Context, points: torch.Tensor) -> torch.Tensor:
+    """mean_nn_dist2 (src/model.rs:128-186) on device points (n, 3) float32."""
+    pts = points.contiguous().to(torch.float32)
+    out = torch.empty(pts.shape[0], dtype=torch.float64, device=pts.device)
+    check(ctx.lib.splat_mean_nn_dist2(ctx.h, _ptr(pts), pts.shape[0], _ptr(out)), ctx.h)
+    return out
+
+
+def init_from_points(ctx: Context, points, rgb, cap: int | None = None) -> torch.Tensor:
+    """Model::from_points (src/model.rs:77-104): host points (n, 3) float32 and colours
+    (n, 3) uint8 -> parameter planes of capacity cap."""
+    import numpy as np
+    p = np.ascontiguousarray(points, np.float32).reshape(-1, 3)
+    c = np.ascontiguousarray(rgb, np.uint8).reshape(-1, 3)
+    n = p.shape[0]
+    cap = max(1, n if cap is None else cap)
+    planes = empty_planes(cap, torch.device("cuda", ctx.device))
+    check(ctx.lib.splat_init_from_points(ctx.h, p.ctypes.data_as(C.c_void_p), c.ctypes.data_as(C.c_void_p), n,
+                                         _ptr(planes), cap), ctx.h)
+    return planes

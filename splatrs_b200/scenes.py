@@ -86,3 +86,26 @@ def config1(seed=0, n=1_000_000, width=1920, height=1080, f=1500.0, distance=12.
     cam = look_at(width, height, f, f, (0.0, 0.0, -distance), (0.0, 0.0, 0.0))
     dimage = rng.normal(0.0, 1.0, width * height * 3).astype(np.float32)
     return dict(params=g, cam=cam, dimage=dimage, sh_degree=3, background=(0.0, 0.0, 0.0))
+
+
+def scene_extent(cams):
+    """scene_extent (src/camera.rs:99-118): 1.1 x the largest distance from a camera centre
+    to the mean centre."""
+    cams = np.asarray(cams, np.float64).reshape(-1, 18)
+    centers = np.stack([-(c[6:15].reshape(3, 3).T @ c[15:18]) for c in cams])
+    mean = centers.mean(0)
+    ext = float(np.max(np.linalg.norm(centers - mean, axis=1))) * 1.1
+    return ext if ext > 0 else 1.0
+
+
+def to_rgb8(image):
+    """render::to_rgb8 (src/render.rs:26-31)."""
+    return np.round(np.clip(image, 0.0, 1.0) * 255.0).astype(np.uint8)
+
+
+def psnr(pred, target_u8):
+    """psnr (src/loss.rs:175-190) against an 8-bit view converted as View::to_real."""
+    t = np.asarray(target_u8, np.float32) / np.float32(255.0)
+    d = np.clip(np.asarray(pred, np.float32), 0, 1).astype(np.float64) - np.clip(t, 0, 1).astype(np.float64)
+    mse = float((d * d).mean())
+    return float("inf") if mse <= 0 else -10.0 * np.log10(mse)

@@ -131,3 +131,30 @@ def evaluate(params, views, sh_degree, background, antialias=False):
         img = render(params, cam, sh_degree, background, antialias)
         total += O.psnr(img, rgb.astype(np.float32).ravel() / np.float32(255.0))
     return total / len(views)
+
+
+def write_ply_reference_layout(path, params, degree):
+    """A .ply written as ply::write does (src/ply.rs:19-69), in plain Python: binary
+    little-endian float32 rows x y z nx ny nz f_dc_0..2 f_rest_* (channel-major) opacity
+    scale_0..2 rot_0..3."""
+    K = (degree + 1) ** 2
+    n_rest = 3 * (K - 1)
+    names = ["x", "y", "z", "nx", "ny", "nz", "f_dc_0", "f_dc_1", "f_dc_2"]
+    names += [f"f_rest_{i}" for i in range(n_rest)] + ["opacity", "scale_0", "scale_1", "scale_2"]
+    names += ["rot_0", "rot_1", "rot_2", "rot_3"]
+    header = "ply\nformat binary_little_endian 1.0\n" + f"element vertex {len(params)}\n"
+    header += "".join(f"property float {nm}\n" for nm in names) + "end_header\n"
+    rows = np.zeros((len(params), len(names)), np.float32)
+    p = np.asarray(params, np.float32)
+    sh = p[:, 11:].reshape(-1, 16, 3)
+    rows[:, 0:3] = p[:, 0:3]
+    rows[:, 6:9] = sh[:, 0, :]
+    for c in range(3):
+        for k in range(1, K):
+            rows[:, 9 + c * (K - 1) + (k - 1)] = sh[:, k, c]
+    rows[:, 9 + n_rest] = p[:, 10]
+    rows[:, 10 + n_rest:13 + n_rest] = p[:, 3:6]
+    rows[:, 13 + n_rest:17 + n_rest] = p[:, 6:10]
+    with open(path, "wb") as f:
+        f.write(header.encode())
+        f.write(rows.astype("<f4").tobytes())
