@@ -43,6 +43,10 @@ def parse():
     ap.add_argument("--cpu-steps", type=int, default=3, help="steps of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-train", action="store_true", help="skip the config-0 training run")
+    ap.add_argument("--train-c2", action="store_true",
+                    help="also run plain training on the clustered 500k-Gaussian multi-view scene")
+    ap.add_argument("--train-c2-iters", type=int, default=0, help="iterations of that run (default: all 30,000)")
+    ap.add_argument("--c2-cpu-iters", type=int, default=5, help="iterations of its CPU oracle sample")
     ap.add_argument("--profile-small", action="store_true",
                     help="a reduced case for ncu captures (fewer Gaussians, one step)")
     return ap.parse_args()
@@ -303,9 +307,15 @@ def run_ours(args, rank, world, local):
 C0_TRAIN = dict(iterations=2000, densify=1, densify_from_iter=500, densify_until_iter=1500, densification_interval=100,
                 densify_grad_threshold=0.0002, lambda_dssim=0.2, sh_degree=3, position_lr_max_steps=2000, seed=0)
 
+# Plain training on the clustered multi-view scene (config 2): the reference's defaults
+# (30,000 iterations, densification 500-15,000) with at most 3,000,000 Gaussians.
+C2_TRAIN = dict(iterations=30000, densify=1, densify_from_iter=500, densify_until_iter=15000,
+                densification_interval=100, densify_grad_threshold=0.0002, lambda_dssim=0.2, sh_degree=3,
+                position_lr_max_steps=30000, seed=0, max_gaussians=3_000_000)
 
-def c0_views_gpu(ctx, s):
-    """Targets of config 0 rendered by the device renderer from the ground truth."""
+
+def gt_views_gpu(ctx, s):
+    """Target views: the ground truth rendered by the device renderer, as 8-bit images."""
     from splatrs_b200 import gpu as G
     from splatrs_b200 import scenes
     from splatrs_b200._lib import Camera, ProjOpts
@@ -317,47 +327,49 @@ def c0_views_gpu(ctx, s):
     return views
 
 
-def run_train_c0_gpu(local):
-    """Full config-0 training run on the device trainer: wall time, iterations/s, PSNR."""
+def run_train_gpu(local, s, cfg, iterations):
+    """A plain training run on the device trainer: wall time, iterations/s, PSNR over the
+    training views, final Gaussian count. Targets and initial model are built on the
+    device before the clock starts."""
     import torch
     from splatrs_b200 import gpu as G
     from splatrs_b200 import scenes
-    s = scenes.config0()
     ctx = G.Context(local, torch.cuda.current_stream(local))
-    views = c0_views_gpu(ctx, s)
+    views = gt_views_gpu(ctx, s)
     init_planes = G.init_from_points(ctx, s["init_points"], s["init_rgb"])
     n0 = len(s["init_points"])
     init = G.planes_to_params(ctx, init_planes, n0, n0).cpu().numpy()
+    del init_planes
     extent = scenes.scene_extent(s["cams"])
-    t = G.Trainer(ctx, init, extent, views, **C0_TRAIN)
+    t = G.Trainer(ctx, init, extent, views, **cfg)
     torch.cuda.synchronize(local)
     tw = time.perf_counter()
-    for _ in range(C0_TRAIN["iterations"]):
+    for _ in range(iterations):
         t.step()
     torch.cuda.synchronize(local)
     wall = time.perf_counter() - tw
     ps = float(np.mean([scenes.psnr(t.render(cam), rgb) for cam, rgb in views]))
-    out = {"iterations": C0_TRAIN["iterations"], "wall_s": round(wall, 3),
-           "iters_per_s": round(C0_TRAIN["iterations"] / wall, 1), "psnr_train_views": round(ps, 2),
-           "gaussians": t.count}
+    out = {"iterations": iterations, "wall_s": round(wall, 3), "iters_per_s": round(iterations / wall, 1),
+           "psnr_train_views": round(ps, 2), "gaussians": t.count}
     t.close()
     ctx.close()
     return out, init, views, extent
 
 
-def run_train_c0_cpu(init, views, extent):
-    """The same run on the CPU oracle trainer (all host threads)."""
+def run_train_cpu(init, views, extent, cfg, iterations):
+    """The same run on the CPU oracle trainer (all host threads), for `iterations` steps."""
     from oracle import oracle as O
     from splatrs_b200 import scenes
-    ot = O.Trainer(init, extent, views, **C0_TRAIN)
+    ot = O.Trainer(init, extent, views, **{k: v for k, v in cfg.items() if k != "max_gaussians"})
     tw = time.perf_counter()
-    for _ in range(C0_TRAIN["iterations"]):
+    for _ in range(iterations):
         ot.step()
     wall = time.perf_counter() - tw
-    ps = float(np.mean([scenes.psnr(ot.render(cam), rgb) for cam, rgb in views]))
-    return {"iterations": C0_TRAIN["iterations"], "wall_s": round(wall, 3),
-            "iters_per_s": round(C0_TRAIN["iterations"] / wall, 2), "psnr_train_views": round(ps, 2),
-            "gaussians": ot.count, "cores": O.threads(), "kind": "port"}
+    out = {"iterations": iterations, "wall_s": round(wall, 3), "iters_per_s": round(iterations / wall, 3),
+           "gaussians": ot.count, "cores": O.threads(), "kind": "port"}
+    if iterations == cfg["iterations"]:
+        out["psnr_train_views"] = round(float(np.mean([scenes.psnr(ot.render(cam), rgb) for cam, rgb in views])), 2)
+    return out
 
 
 def cpu_reference_steps(args, steps):
@@ -422,12 +434,23 @@ def main():
     line = run_ours(args, rank, world, local)
     c0 = None
     if not args.profile_small and not args.no_train:
-        gpu_c0, init, views, extent = run_train_c0_gpu(local)
+        from splatrs_b200 import scenes
+        gpu_c0, init, views, extent = run_train_gpu(local, scenes.config0(), C0_TRAIN, C0_TRAIN["iterations"])
         line["train_c0"] = {"gpu": gpu_c0}
         c0 = (init, views, extent)
+    if args.train_c2 and not args.profile_small:
+        from splatrs_b200 import scenes
+        iters = args.train_c2_iters or C2_TRAIN["iterations"]
+        gpu_c2, init2, views2, extent2 = run_train_gpu(local, scenes.config2(), C2_TRAIN, iters)
+        line["train_c2"] = {"gpu": gpu_c2}
+        if rank == 0 and world == 1 and args.c2_cpu_iters > 0:
+            line["train_c2"]["cpu"] = run_train_cpu(init2, views2, extent2, C2_TRAIN, args.c2_cpu_iters)
+            line["train_c2"]["cpu"]["sample"] = (f"first {args.c2_cpu_iters} iterations from the same initial "
+                                                 "model (no densification yet)")
+        del views2
     if rank == 0:
         if c0 is not None and not args.no_cpu_baseline and world == 1:
-            line["train_c0"]["cpu"] = run_train_c0_cpu(*c0)
+            line["train_c0"]["cpu"] = run_train_cpu(*c0, C0_TRAIN, C0_TRAIN["iterations"])
         if not args.no_cpu_baseline and world == 1:
             dt, cores = cpu_reference_steps(args, args.cpu_steps)
             line["cpu_baseline"] = {"value": round(WIDTH * HEIGHT / 1e6 / dt, 4), "unit": UNIT, "cores": cores,

@@ -113,6 +113,9 @@ typedef struct splat_train_config {
   uint32_t sh_degree_interval;
   float near_plane;
   uint64_t seed;
+  /* Not in the reference: 0 = no limit. When a densification would leave more Gaussians
+   * than this, that densification clones and splits nothing and only prunes. */
+  uint64_t max_gaussians;
 } splat_train_config;
 
 typedef struct splat_ctx splat_ctx;
@@ -222,6 +225,16 @@ SPLAT_API int splat_project_bwd(splat_ctx* ctx, const float* planes_dev, int64_t
  * screening against the correctly rounded exp, over every float x with |x| in [lo, hi]
  * (negative != 0 selects -|x|). Synchronises. */
 SPLAT_API int splat_diag_fast_exp_error(splat_ctx* ctx, float lo, float hi, int32_t negative, float* max_rel_error);
+
+/* project_backward_all fused with Adam::step (reference src/project.rs:477-493,
+ * src/adam.rs:77-161): the parameter gradients stay in registers and update planes_dev in
+ * place together with the moments m_dev and v_dev (parameter-plane layout, capacity cap);
+ * `step` is the Adam step count after the increment. Optional densification statistics as
+ * in splat_project_bwd. Results equal splat_project_bwd followed by splat_adam_step. */
+SPLAT_API int splat_project_bwd_adam(splat_ctx* ctx, float* planes_dev, float* m_dev, float* v_dev, int64_t n,
+                                     int64_t cap, const splat_camera* cam, const splat_proj_opts* opts,
+                                     const float* proj_dev, const float* pgrad_dev, void* stats_dev, int32_t absgrad,
+                                     uint64_t step, const splat_lr* lr);
 
 /* Fill `bytes` bytes of device memory with zeros on the context stream. */
 SPLAT_API int splat_zero(splat_ctx* ctx, void* dev, size_t bytes);

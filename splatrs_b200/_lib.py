@@ -82,14 +82,15 @@ class TrainConfig(C.Structure):
                 ("densify_grad_threshold", C.c_float), ("percent_dense", C.c_float), ("min_opacity", C.c_float),
                 ("max_screen_size", C.c_int64), ("absgrad", C.c_int32), ("antialias", C.c_int32),
                 ("white_background", C.c_int32), ("sh_degree", C.c_int32), ("sh_degree_interval", C.c_uint32),
-                ("near_plane", C.c_float), ("seed", C.c_uint64)]
+                ("near_plane", C.c_float), ("seed", C.c_uint64), ("max_gaussians", C.c_uint64)]
 
     DEFAULTS = dict(iterations=30000, position_lr_init=0.00016, position_lr_final=0.0000016,
                     position_lr_max_steps=30000, feature_lr=0.0025, opacity_lr=0.025, scaling_lr=0.005,
                     rotation_lr=0.001, lambda_dssim=0.2, densify=1, densify_from_iter=500, densify_until_iter=15000,
                     densification_interval=100, opacity_reset_interval=3000, densify_grad_threshold=0.0002,
                     percent_dense=0.01, min_opacity=0.005, max_screen_size=-1, absgrad=0, antialias=0,
-                    white_background=0, sh_degree=3, sh_degree_interval=1000, near_plane=0.2, seed=0)
+                    white_background=0, sh_degree=3, sh_degree_interval=1000, near_plane=0.2, seed=0,
+                    max_gaussians=0)
 
     @classmethod
     def make(cls, **kw):
@@ -161,6 +162,8 @@ def _declare(L):
     sig.update({
         "splat_loss_fwd_bwd": ([vp, vp, vp, i32, u32, u32, C.c_float, vp, vp], C.c_int),
         "splat_adam_step": ([vp, vp, vp, vp, vp, i64, i64, C.c_uint64, P(LearningRates)], C.c_int),
+        "splat_project_bwd_adam": ([vp, vp, vp, vp, i64, i64, P(Camera), P(ProjOpts), vp, vp, vp, i32, C.c_uint64,
+                                    P(LearningRates)], C.c_int),
         "splat_densify": ([vp, vp, vp, vp, i64, i64, vp, P(DensifyConfig), C.c_float, P(C.c_uint64), vp, vp, vp, i64,
                            P(DensifyReport)], C.c_int),
         "splat_reset_opacity": ([vp, vp, vp, vp, i64, C.c_float], C.c_int),

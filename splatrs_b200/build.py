@@ -19,7 +19,7 @@ BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libsplatrs_b200.so")
 
 SOURCES = ["capi.cu", "project.cu", "sort.cu", "raster.cu", "renderer.cu", "loss.cu", "optim.cu", "trainer.cu", "noalloc.cu", "ply.cu", "init.cu"]
-HEADERS = ["common.cuh", "kernels.cuh", "renderer.cuh", "crmath.h"]
+HEADERS = ["common.cuh", "kernels.cuh", "renderer.cuh", "crmath.h", "adam.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -314,6 +314,20 @@ SPLAT_API int splat_project_bwd(splat_ctx* ctx, const float* planes_dev, int64_t
                                         grad_planes_dev, stats_dev, absgrad));
 }
 
+SPLAT_API int splat_project_bwd_adam(splat_ctx* ctx, float* planes_dev, float* m_dev, float* v_dev, int64_t n,
+                                     int64_t cap, const splat_camera* cam, const splat_proj_opts* opts,
+                                     const float* proj_dev, const float* pgrad_dev, void* stats_dev, int32_t absgrad,
+                                     uint64_t step, const splat_lr* lr) {
+  if (!ctx) return SPLAT_ERR_INVALID;
+  if (!cam_ok(cam)) return invalid(ctx, "splat_project_bwd_adam: camera size must be in 1..65535");
+  if (!opts_ok(opts)) return invalid(ctx, "splat_project_bwd_adam: sh_degree must be in 0..3");
+  if (!lr || step == 0 || n < 0 || cap < n || (n && (!planes_dev || !m_dev || !v_dev || !proj_dev || !pgrad_dev)))
+    return invalid(ctx, "splat_project_bwd_adam: bad arguments");
+  Enter e(ctx);
+  return finish(ctx, launch_project_bwd_adam(&ctx->c, planes_dev, m_dev, v_dev, n, cap, *cam, *opts, proj_dev,
+                                             pgrad_dev, stats_dev, absgrad, step, *lr));
+}
+
 }  // extern "C"
 
 namespace {

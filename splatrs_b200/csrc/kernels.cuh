@@ -17,6 +17,11 @@ Status launch_project_bwd(Ctx* c, const float* planes, int64_t n, int64_t cap, c
                           const splat_proj_opts& opts, const float* proj, const float* pgrad, float* out,
                           void* stats, int absgrad);
 
+// project_backward_all fused with Adam::step: parameters updated in place.
+Status launch_project_bwd_adam(Ctx* c, float* planes, float* m, float* v, int64_t n, int64_t cap,
+                               const splat_camera& cam, const splat_proj_opts& opts, const float* proj,
+                               const float* pgrad, void* stats, int absgrad, uint64_t step, const splat_lr& lr);
+
 Status launch_scan_u32(Ctx* c, const uint32_t* in, int64_t n, uint32_t* out, int write_total, uint64_t* total_dev);
 Status launch_scan_u32_into(Ctx* c, const uint32_t* in, int64_t n, uint32_t* out, int write_total,
                             uint64_t* partial, uint64_t* total);
@@ -46,11 +51,13 @@ struct DensifyArgs {
   int prune_big_world;
   int64_t max_screen_size;
   int children;
+  int grow;  // 0: clone and split nothing (prune only)
 };
 struct DensifyParams {
   splat_densify_config cfg;
   float extent;
   float shrink;  // ln(0.8 * children), densify.rs:169
+  bool grow = true;
 };
 // Decisions of one densification step; the arrays live in the context arena until the
 // next entry point.

@@ -10,24 +10,9 @@
 // the updated parameters are bit-identical to the reference's given the same inputs.
 #include "common.cuh"
 #include "kernels.cuh"
+#include "adam.cuh"
 
 namespace splat {
-
-// adam.rs:44-61
-__device__ __forceinline__ void adam_update(float& p, float g, float& m, float& v, float lr, float b1, float b2,
-                                            float c1, float c2, float eps) {
-  m = b1 * m + (1.0f - b1) * g;
-  v = b2 * v + (1.0f - b2) * g * g;
-  const float m_hat = m / c1;
-  const float v_hat = v / c2;
-  p -= lr * m_hat / (sqrtf(v_hat) + eps);
-}
-
-struct AdamArgs {
-  float lr[4][4];  // per lane of planes 0..3; planes >= 4 use sh_rest
-  float sh_rest;
-  float b1, b2, c1, c2, eps;
-};
 
 __global__ void __launch_bounds__(256) adam_kernel(float4* __restrict__ p, const float4* __restrict__ g,
                                                    float4* __restrict__ m, float4* __restrict__ v, int64_t n,
@@ -39,19 +24,7 @@ __global__ void __launch_bounds__(256) adam_kernel(float4* __restrict__ p, const
   const int64_t i = t - (int64_t)plane * n;
   const int64_t o = (int64_t)plane * cap + i;
   float4 pp = p[o], gg = g[o], mm = m[o], vv = v[o];
-  float lr0, lr1, lr2, lr3;
-  if (plane < 4) {
-    lr0 = a.lr[plane][0];
-    lr1 = a.lr[plane][1];
-    lr2 = a.lr[plane][2];
-    lr3 = a.lr[plane][3];
-  } else {
-    lr0 = lr1 = lr2 = lr3 = a.sh_rest;
-  }
-  adam_update(pp.x, gg.x, mm.x, vv.x, lr0, a.b1, a.b2, a.c1, a.c2, a.eps);
-  adam_update(pp.y, gg.y, mm.y, vv.y, lr1, a.b1, a.b2, a.c1, a.c2, a.eps);
-  adam_update(pp.z, gg.z, mm.z, vv.z, lr2, a.b1, a.b2, a.c1, a.c2, a.eps);
-  adam_update(pp.w, gg.w, mm.w, vv.w, lr3, a.b1, a.b2, a.c1, a.c2, a.eps);
+  adam_plane(a, plane, pp, gg, mm, vv);
   p[o] = pp;
   m[o] = mm;
   v[o] = vv;
@@ -70,9 +43,7 @@ static float powi_f(float a, int b) {
   return recip ? 1.0f / r : r;
 }
 
-Status launch_adam(Ctx* c, float* params, const float* grads, float* m, float* v, int64_t n, int64_t cap,
-                   uint64_t step, const splat_lr& lr) {
-  if (n == 0) return Status::ok();
+AdamArgs make_adam_args(uint64_t step, const splat_lr& lr) {
   AdamArgs a;
   a.b1 = 0.9f;
   a.b2 = 0.999f;
@@ -88,6 +59,13 @@ Status launch_adam(Ctx* c, float* params, const float* grads, float* m, float* v
   for (int i = 0; i < 4; i++)
     for (int j = 0; j < 4; j++) a.lr[i][j] = L[i][j];
   a.sh_rest = lr.sh_rest;
+  return a;
+}
+
+Status launch_adam(Ctx* c, float* params, const float* grads, float* m, float* v, int64_t n, int64_t cap,
+                   uint64_t step, const splat_lr& lr) {
+  if (n == 0) return Status::ok();
+  const AdamArgs a = make_adam_args(step, lr);
   const int64_t total = (int64_t)kPlanes * n;
   adam_kernel<<<ceil_div(total, 256), 256, 0, c->stream>>>(reinterpret_cast<float4*>(params),
                                                            reinterpret_cast<const float4*>(grads),
@@ -123,7 +101,7 @@ __global__ void densify_mark_kernel(const float4* __restrict__ p, int64_t n, int
   const float4 p0 = p[i], p2 = p[2 * cap + i];
   const float g = denom[i] > 0 ? accum[i] / (float)denom[i] : 0.0f;  // densify.rs:135-143
   const float ms = max_scale_of(p2.x, p2.y, p2.z);
-  const bool hot = g >= a.grad_threshold;
+  const bool hot = a.grow && g >= a.grad_threshold;
   const bool clone = hot && ms <= a.size_limit;
   const bool split = hot && ms > a.size_limit;
   const float alpha = alpha_of(p0.w);
@@ -285,6 +263,7 @@ Status densify_plan(Ctx* c, const float* params, int64_t n, int64_t cap, const f
   a.max_screen_size = dp.cfg.max_screen_size;
   a.children = dp.cfg.split_children;
   a.shrink = dp.shrink;
+  a.grow = dp.grow ? 1 : 0;
   uint32_t *flags, *ko, *kcl, *sp, *kch, *oo, *oc, *os, *ok;
   unsigned long long* counts;
   uint64_t* tot;

@@ -4,6 +4,7 @@
 // active degree needs are touched.
 #include "common.cuh"
 #include "kernels.cuh"
+#include "adam.cuh"
 
 namespace splat {
 
@@ -513,15 +514,19 @@ __global__ void proj_to_reference_kernel(const float4* __restrict__ rec, int64_t
 }
 
 // project_backward_one (project.rs:335-474), plus DensifyStats::accumulate
-// (densify.rs:36-60) when `stats` is given.
-template <int DEG>
+// (densify.rs:36-60) when `stats` is given. With ADAM the 59 gradients never leave the
+// registers: Adam::step (adam.rs:77-161) updates the parameters in place and the moments m
+// and v, over every plane (zero gradients still decay the moments, adam.rs:56-60).
+template <int DEG, bool ADAM>
 __global__ void __launch_bounds__(128) project_bwd_kernel(const float4* __restrict__ planes, int64_t n, int64_t cap,
                                                           splat_camera cam, splat_proj_opts opts,
                                                           const float4* __restrict__ rec,
                                                           const float4* __restrict__ pgrad,
                                                           float4* __restrict__ out, float* __restrict__ stat_accum,
                                                           uint32_t* __restrict__ stat_denom,
-                                                          uint32_t* __restrict__ stat_maxr, int absgrad) {
+                                                          uint32_t* __restrict__ stat_maxr, int absgrad,
+                                                          float4* __restrict__ adam_m, float4* __restrict__ adam_v,
+                                                          AdamArgs adam) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const float4 g0 = pgrad[i], g1 = pgrad[cap + i], g2 = pgrad[2 * cap + i];
@@ -697,11 +702,35 @@ __global__ void __launch_bounds__(128) project_bwd_kernel(const float4* __restri
       for (int ii = 0; ii < 4; ii++) o_q[ii] = (dq[ii] - u[ii] * dot) / nrm;
     }
   }
-  out[i] = make_float4(o_mean[0], o_mean[1], o_mean[2], o_op);
-  out[cap + i] = make_float4(o_q[0], o_q[1], o_q[2], o_q[3]);
-  out[2 * cap + i] = make_float4(o_ls[0], o_ls[1], o_ls[2], 0.0f);
+  if (!ADAM) {
+    out[i] = make_float4(o_mean[0], o_mean[1], o_mean[2], o_op);
+    out[cap + i] = make_float4(o_q[0], o_q[1], o_q[2], o_q[3]);
+    out[2 * cap + i] = make_float4(o_ls[0], o_ls[1], o_ls[2], 0.0f);
 #pragma unroll
-  for (int q = 0; q < 12; q++) out[(3 + q) * cap + i] = make_float4(o_sh[4 * q], o_sh[4 * q + 1], o_sh[4 * q + 2], o_sh[4 * q + 3]);
+    for (int q = 0; q < 12; q++) out[(3 + q) * cap + i] = make_float4(o_sh[4 * q], o_sh[4 * q + 1], o_sh[4 * q + 2], o_sh[4 * q + 3]);
+  } else {
+    // The parameters are read above only through `planes`; each element is read before
+    // this thread writes it and no other thread touches Gaussian i.
+    float4* pw = const_cast<float4*>(planes);
+#pragma unroll
+    for (int q = 0; q < kPlanes; q++) {
+      float4 g;
+      if (q == 0)
+        g = make_float4(o_mean[0], o_mean[1], o_mean[2], o_op);
+      else if (q == 1)
+        g = make_float4(o_q[0], o_q[1], o_q[2], o_q[3]);
+      else if (q == 2)
+        g = make_float4(o_ls[0], o_ls[1], o_ls[2], 0.0f);
+      else
+        g = make_float4(o_sh[4 * (q - 3)], o_sh[4 * (q - 3) + 1], o_sh[4 * (q - 3) + 2], o_sh[4 * (q - 3) + 3]);
+      const int64_t o = (int64_t)q * cap + i;
+      float4 p = pw[o], m = adam_m[o], v = adam_v[o];
+      adam_plane(adam, q, p, g, m, v);
+      pw[o] = p;
+      adam_m[o] = m;
+      adam_v[o] = v;
+    }
+  }
 }
 
 // Reference Gaussian records <-> planes, 128 Gaussians per block through shared memory so
@@ -807,9 +836,10 @@ Status launch_proj_to_reference(Ctx* c, const float* proj, int64_t n, float* p15
   return Status::ok();
 }
 
-Status launch_project_bwd(Ctx* c, const float* planes, int64_t n, int64_t cap, const splat_camera& cam,
-                          const splat_proj_opts& opts, const float* proj, const float* pgrad, float* out,
-                          void* stats, int absgrad) {
+template <bool ADAM>
+static Status project_bwd_dispatch(Ctx* c, const float* planes, int64_t n, int64_t cap, const splat_camera& cam,
+                                   const splat_proj_opts& opts, const float* proj, const float* pgrad, float* out,
+                                   void* stats, int absgrad, float* m, float* v, const AdamArgs& adam) {
   if (n == 0) return Status::ok();
   const int bs = 128;
   const uint32_t grid = ceil_div(n, bs);
@@ -817,6 +847,8 @@ Status launch_project_bwd(Ctx* c, const float* planes, int64_t n, int64_t cap, c
   const float4* r = reinterpret_cast<const float4*>(proj);
   const float4* pg = reinterpret_cast<const float4*>(pgrad);
   float4* o = reinterpret_cast<float4*>(out);
+  float4* am = reinterpret_cast<float4*>(m);
+  float4* av = reinterpret_cast<float4*>(v);
   float* sa = nullptr;
   uint32_t *sd = nullptr, *sm = nullptr;
   if (stats) {
@@ -825,14 +857,28 @@ Status launch_project_bwd(Ctx* c, const float* planes, int64_t n, int64_t cap, c
     sm = sd + cap;
   }
   switch (opts.sh_degree) {
-    case 0: project_bwd_kernel<0><<<grid, bs, 0, c->stream>>>(p, n, cap, cam, opts, r, pg, o, sa, sd, sm, absgrad); break;
-    case 1: project_bwd_kernel<1><<<grid, bs, 0, c->stream>>>(p, n, cap, cam, opts, r, pg, o, sa, sd, sm, absgrad); break;
-    case 2: project_bwd_kernel<2><<<grid, bs, 0, c->stream>>>(p, n, cap, cam, opts, r, pg, o, sa, sd, sm, absgrad); break;
-    default: project_bwd_kernel<3><<<grid, bs, 0, c->stream>>>(p, n, cap, cam, opts, r, pg, o, sa, sd, sm, absgrad); break;
+    case 0: project_bwd_kernel<0, ADAM><<<grid, bs, 0, c->stream>>>(p, n, cap, cam, opts, r, pg, o, sa, sd, sm, absgrad, am, av, adam); break;
+    case 1: project_bwd_kernel<1, ADAM><<<grid, bs, 0, c->stream>>>(p, n, cap, cam, opts, r, pg, o, sa, sd, sm, absgrad, am, av, adam); break;
+    case 2: project_bwd_kernel<2, ADAM><<<grid, bs, 0, c->stream>>>(p, n, cap, cam, opts, r, pg, o, sa, sd, sm, absgrad, am, av, adam); break;
+    default: project_bwd_kernel<3, ADAM><<<grid, bs, 0, c->stream>>>(p, n, cap, cam, opts, r, pg, o, sa, sd, sm, absgrad, am, av, adam); break;
   }
   c->launches.count++;
   SPLAT_LAUNCHED("project_bwd_kernel");
   return Status::ok();
+}
+
+Status launch_project_bwd(Ctx* c, const float* planes, int64_t n, int64_t cap, const splat_camera& cam,
+                          const splat_proj_opts& opts, const float* proj, const float* pgrad, float* out,
+                          void* stats, int absgrad) {
+  return project_bwd_dispatch<false>(c, planes, n, cap, cam, opts, proj, pgrad, out, stats, absgrad, nullptr, nullptr,
+                                     AdamArgs());
+}
+
+Status launch_project_bwd_adam(Ctx* c, float* planes, float* m, float* v, int64_t n, int64_t cap,
+                               const splat_camera& cam, const splat_proj_opts& opts, const float* proj,
+                               const float* pgrad, void* stats, int absgrad, uint64_t step, const splat_lr& lr) {
+  return project_bwd_dispatch<true>(c, planes, n, cap, cam, opts, proj, pgrad, nullptr, stats, absgrad, m, v,
+                                    make_adam_args(step, lr));
 }
 
 Status launch_params_from_aos(Ctx* c, const float* aos, int64_t n, float* planes, int64_t cap) {

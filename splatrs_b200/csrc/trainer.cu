@@ -74,7 +74,7 @@ struct splat_trainer {
   int64_t n = 0;
   int sh_degree = 0;
   ModelBufs cur, next;
-  DevBuf grads, pgrad, stats, pred_grad, loss_out, normals, init;
+  DevBuf pgrad, stats, pred_grad, loss_out, normals, init;
   int64_t stats_cap = 0;
   ViewBuffers vb;
   std::vector<View*> views;
@@ -169,18 +169,14 @@ Status step(splat_trainer* t, splat_step_info* info) {
 
   // Backward (train.rs:226-235).
   SPLAT_TRY(t->pgrad.ensure((size_t)cap * 48));
-  SPLAT_TRY(t->grads.ensure((size_t)cap * kPlanes * 16));
   SPLAT_CUDA(cudaMemsetAsync(t->pgrad.ptr, 0, (size_t)cap * 48, c->stream));
   SPLAT_TRY(launch_raster_bwd(c, t->vb.proj.as<float>(), t->vb.gauss.as<uint32_t>(), t->vb.tile_range.as<uint32_t>(),
                               cam.width, cam.height, bg, t->vb.final_t.as<float>(), t->vb.n_contrib.as<uint32_t>(),
                               t->pred_grad.as<float>(), t->pgrad.as<float>(), cap, nullptr));
   const bool densify_window = cfg.densify && it < cfg.densify_until_iter;
   SPLAT_TRY(ensure_stats(t, cap));
-  SPLAT_TRY(launch_project_bwd(c, t->cur.params.as<float>(), n, cap, cam, opts, t->vb.proj.as<float>(),
-                               t->pgrad.as<float>(), t->grads.as<float>(), densify_window ? t->stats.ptr : nullptr,
-                               cfg.absgrad));
-
-  // Optimiser step (train.rs:238-246).
+  // Optimiser step (train.rs:238-246), fused into the projection backward: the 59
+  // gradients per Gaussian go from registers straight into Adam.
   splat_lr lr;
   lr.mean = position_lr(cfg, it, t->extent);
   lr.log_scale = cfg.scaling_lr;
@@ -189,8 +185,9 @@ Status step(splat_trainer* t, splat_step_info* info) {
   lr.sh_dc = cfg.feature_lr;
   lr.sh_rest = cfg.feature_lr / 20.0f;
   t->adam_step += 1;
-  SPLAT_TRY(launch_adam(c, t->cur.params.as<float>(), t->grads.as<float>(), t->cur.m.as<float>(), t->cur.v.as<float>(),
-                        n, cap, t->adam_step, lr));
+  SPLAT_TRY(launch_project_bwd_adam(c, t->cur.params.as<float>(), t->cur.m.as<float>(), t->cur.v.as<float>(), n, cap,
+                                    cam, opts, t->vb.proj.as<float>(), t->pgrad.as<float>(),
+                                    densify_window ? t->stats.ptr : nullptr, cfg.absgrad, t->adam_step, lr));
 
   // Density control (train.rs:249-272).
   info->densified = 0;
@@ -213,6 +210,11 @@ Status step(splat_trainer* t, splat_step_info* info) {
       uint32_t* maxr = denom + t->stats_cap;
       DensifyPlan plan;
       SPLAT_TRY(densify_plan(c, t->cur.params.as<float>(), n, cap, accum, denom, maxr, dp, &plan));
+      if (cfg.max_gaussians > 0 && plan.new_count() > cfg.max_gaussians) {
+        // Growth would pass the configured limit: this densification only prunes.
+        dp.grow = false;
+        SPLAT_TRY(densify_plan(c, t->cur.params.as<float>(), n, cap, accum, denom, maxr, dp, &plan));
+      }
       const size_t nn = (size_t)plan.split * dp.cfg.split_children * 3;
       std::vector<double> normals(nn);
       for (size_t q = 0; q < nn; q++) normals[q] = t->rng.normal();
@@ -291,7 +293,7 @@ SPLAT_API int splat_trainer_destroy(splat_trainer* t) {
     cudaStreamSynchronize(t->c->stream);
     t->cur.release();
     t->next.release();
-    for (DevBuf* b : {&t->grads, &t->pgrad, &t->stats, &t->pred_grad, &t->loss_out, &t->normals, &t->init}) b->release();
+    for (DevBuf* b : {&t->pgrad, &t->stats, &t->pred_grad, &t->loss_out, &t->normals, &t->init}) b->release();
     t->vb.release();
     for (View* v : t->views) {
       v->rgb.release();

@@ -323,6 +323,16 @@ def adam_step(ctx: Context, planes, grads, m, v, n: int, cap: int, step: int, lr
           ctx.h)
 
 
+def project_backward_adam(ctx: Context, planes, m, v, n: int, cap: int, cam: Camera, opts: ProjOpts,
+                          proj: Projection, pgrad, step: int, lr: LearningRates, stats=None, absgrad=False):
+    """project_backward_all (src/project.rs:477-493) fused with Adam::step
+    (src/adam.rs:77-161): planes, m and v updated in place; `step` is the count after the
+    increment."""
+    check(ctx.lib.splat_project_bwd_adam(ctx.h, _ptr(planes), _ptr(m), _ptr(v), n, cap, C.byref(cam), C.byref(opts),
+                                         _ptr(proj.rec), _ptr(pgrad), _ptr(stats), int(bool(absgrad)), step,
+                                         C.byref(lr)), ctx.h)
+
+
 def densify_and_prune(ctx: Context, planes, m, v, n: int, cap: int, stats, cfg: DensifyConfig, extent: float,
                       rng_state: int, cap_out: int | None = None):
     """densify_and_prune (src/densify.rs:125-221). Returns (planes, m, v, report, rng_state)."""

@@ -88,6 +88,63 @@ def config1(seed=0, n=1_000_000, width=1920, height=1080, f=1500.0, distance=12.
     return dict(params=g, cam=cam, dimage=dimage, sh_degree=3, background=(0.0, 0.0, 0.0))
 
 
+def hemisphere_cameras(n, radius, width, height, f):
+    """n cameras spread over the upper hemisphere (-y is up) by a golden-angle spiral,
+    looking at the origin; none sits exactly at the pole."""
+    ga = math.pi * (3.0 - math.sqrt(5.0))
+    cams = []
+    for i in range(n):
+        y = -(i + 0.5) / n
+        r = math.sqrt(max(0.0, 1.0 - y * y))
+        th = ga * i
+        eye = (radius * r * math.cos(th), radius * y, radius * r * math.sin(th))
+        cams.append(look_at(width, height, f, f, eye, (0.0, 0.0, 0.0)))
+    return np.stack(cams)
+
+
+def config2(seed_gt=0, seed_init=1, n_gt=500_000, n_shells=40, n_cams=200, width=1297, height=840, f=1150.0,
+            n_init=100_000, cube=6.0):
+    """Clustered multi-view scene: n_gt Gaussians on n_shells shells inside a cube of side
+    `cube` centred at the origin, half of them spheres and half planar discs, radius
+    U(0.2, 2), each point jittered N(0, 0.01) per axis; points split over the shells in
+    proportion to their area. Log-scales N(-4.5, 0.3), opacity logits N(0, 1), SH degree 3
+    as in config 0. n_cams cameras on a radius-8 hemisphere at width x height, f = 1150.
+    n_init initial points = ground-truth means + N(0, 0.02), colours from the ground-truth
+    DC band."""
+    rng = np.random.default_rng(seed_gt)
+    radius = rng.uniform(0.2, 2.0, n_shells)
+    planar = rng.uniform(0.0, 1.0, n_shells) < 0.5
+    half = cube / 2.0
+    centre = np.stack([rng.uniform(-half + r, half - r, 3) for r in radius])
+    normal = rng.normal(0.0, 1.0, (n_shells, 3))
+    normal /= np.linalg.norm(normal, axis=1, keepdims=True)
+    area = np.where(planar, math.pi * radius ** 2, 4.0 * math.pi * radius ** 2)
+    counts = np.floor(area / area.sum() * n_gt).astype(np.int64)
+    counts[: n_gt - counts.sum()] += 1
+    pts = []
+    for s in range(n_shells):
+        k = int(counts[s])
+        if planar[s]:
+            a = np.cross(normal[s], [1.0, 0.0, 0.0] if abs(normal[s][0]) < 0.9 else [0.0, 1.0, 0.0])
+            a /= np.linalg.norm(a)
+            b = np.cross(normal[s], a)
+            rr = radius[s] * np.sqrt(rng.uniform(0.0, 1.0, k))
+            th = rng.uniform(0.0, 2.0 * math.pi, k)
+            p = centre[s] + (rr * np.cos(th))[:, None] * a + (rr * np.sin(th))[:, None] * b
+        else:
+            u = rng.normal(0.0, 1.0, (k, 3))
+            p = centre[s] + radius[s] * u / np.linalg.norm(u, axis=1, keepdims=True)
+        pts.append(p + rng.normal(0.0, 0.01, (k, 3)))
+    gt = random_gaussians(rng, n_gt, 0.0, 0.0, -4.5, 0.3, 1.0)
+    gt[:, 0:3] = np.concatenate(pts)
+    cams = hemisphere_cameras(n_cams, 8.0, width, height, f)
+    rng1 = np.random.default_rng(seed_init)
+    pick = rng1.choice(n_gt, size=n_init, replace=False)
+    ip = (gt[pick, 0:3] + rng1.normal(0.0, 0.02, (n_init, 3))).astype(np.float32)
+    rgb = np.round(np.clip(gt[pick, 11:14] * SH_C0 + 0.5, 0.0, 1.0) * 255.0).astype(np.uint8)
+    return dict(gt=gt, cams=cams, init_points=ip, init_rgb=rgb, sh_degree=3, background=(0.0, 0.0, 0.0))
+
+
 def scene_extent(cams):
     """scene_extent (src/camera.rs:99-118): 1.1 x the largest distance from a camera centre
     to the mean centre."""

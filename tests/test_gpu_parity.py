@@ -18,7 +18,7 @@ import torch
 from oracle import oracle as O
 from splatrs_b200 import gpu as G
 from splatrs_b200 import scenes
-from splatrs_b200._lib import Camera, ProjOpts
+from splatrs_b200._lib import Camera, LearningRates, ProjOpts
 from tests import fixtures as F
 
 pytestmark = pytest.mark.gpu
@@ -262,6 +262,35 @@ def test_project_backward_densify_stats(ctx):
         for _ in range(2):
             O.densify_accumulate(p, w, a2 if absgrad else None, int(cam[0]), int(cam[1]), oacc, oden, omr)
         assert (bits(acc) == bits(oacc)).all() and (den == oden).all() and (mr == omr).all()
+
+
+@pytest.mark.parametrize("sh_degree", [0, 3])
+def test_project_backward_adam_equals_separate_steps(ctx, sh_degree):
+    """splat_project_bwd_adam over three steps equals splat_project_bwd followed by
+    splat_adam_step bit for bit: parameters, both moments and the densification stats."""
+    g, cam = small_scene(seed=43, n=3000)
+    n = g.shape[0]
+    rng = np.random.default_rng(43)
+    opts = ProjOpts.make(sh_degree=sh_degree)
+    lr = LearningRates(0.00016 * 3.3, 0.005, 0.001, 0.025, 0.0025, 0.0025 / 20)
+    fused = G.params_to_planes(ctx, dev(g), n)
+    sep = fused.clone()
+    fm, fv = torch.zeros_like(fused), torch.zeros_like(fused)
+    sm, sv = torch.zeros_like(fused), torch.zeros_like(fused)
+    fst = torch.zeros(3 * n, dtype=torch.int32, device="cuda")
+    sst = torch.zeros_like(fst)
+    for step in (1, 2, 3):
+        w = rng.uniform(-1, 1, (n, 9)).astype(np.float32)
+        a2 = np.abs(rng.uniform(-1, 1, (n, 2))).astype(np.float32)
+        pg = G.pgrad_from_reference(dev(w), dev(a2))
+        proj = G.project_all(ctx, sep, n, n, Camera.from_record(cam), opts)
+        gp = G.project_backward_all(ctx, sep, n, n, Camera.from_record(cam), opts, proj, pg, sst, True)
+        G.adam_step(ctx, sep, gp, sm, sv, n, n, step, lr)
+        proj = G.project_all(ctx, fused, n, n, Camera.from_record(cam), opts)
+        G.project_backward_adam(ctx, fused, fm, fv, n, n, Camera.from_record(cam), opts, proj, pg, step, lr, fst, True)
+        assert torch.equal(fused, sep) and torch.equal(fm, sm) and torch.equal(fv, sv)
+        assert torch.equal(fst, sst)
+    assert not torch.equal(fused, G.params_to_planes(ctx, dev(g), n))
 
 
 def test_end_to_end_chain_matches_oracle(ctx):

@@ -263,3 +263,22 @@ def test_trainer_rejects_zero_iterations(ctx):
     with pytest.raises(SplatError) as e:
         G.Trainer(ctx, np.zeros((0, 59), np.float32), 1.0, [], iterations=0, sh_degree=0)
     assert e.value.status == 1
+
+
+def test_trainer_gaussian_limit_stops_growth(ctx):
+    """max_gaussians (not in the reference): a densification that would pass the limit only
+    prunes, so the count never exceeds it; without the limit the same run grows past it."""
+    views, extent, init = _views_and_init(200, 30, 8, 48, 36, [1.0, 1.0, 1.0], truncate=10)
+    cfg = dict(iterations=300, densify=1, densify_from_iter=40, densify_until_iter=280, densification_interval=40,
+               opacity_reset_interval=0, densify_grad_threshold=0.0005, white_background=1, sh_degree=1,
+               sh_degree_interval=150, position_lr_max_steps=300, seed=5)
+    free = G.Trainer(ctx, init, extent, views, **cfg)
+    peak_free = max(free.step()["num_gaussians"] for _ in range(300))
+    free.close()
+    limit = 14
+    assert peak_free > limit
+    t = G.Trainer(ctx, init, extent, views, max_gaussians=limit, **cfg)
+    counts = [t.step()["num_gaussians"] for _ in range(300)]
+    assert max(counts) <= limit
+    assert np.isfinite(t.model()[:, 0:10]).all()
+    t.close()
