@@ -240,8 +240,8 @@ SPLAT_API int splat_project_bwd_adam(splat_ctx* ctx, float* planes_dev, float* m
 SPLAT_API int splat_zero(splat_ctx* ctx, void* dev, size_t bytes);
 
 /* ----------------------------------------------------------------------------------------
- * Renderer: a model resident in device memory, driven with HOST buffers. All calls
- * synchronise before returning.
+ * Renderer: a model resident in device memory, driven with HOST buffers. All calls but
+ * splat_renderer_submit_backward synchronise before returning.
  *   splat_renderer_set_model: upload n reference Gaussian records (aos59, host) and the
  *     model's active SH degree (Model::sh_degree, reference src/model.rs:54-61).
  *   splat_renderer_render: render::render (reference src/render.rs:14-23) into a host
@@ -261,6 +261,18 @@ SPLAT_API int splat_renderer_render(splat_renderer* r, const splat_camera* cam, 
 SPLAT_API int splat_renderer_render_backward(splat_renderer* r, const splat_camera* cam, const splat_proj_opts* opts,
                                              const float background[3], const float* dimage_host, float* image_host,
                                              float* grads_aos59_host);
+/* splat_renderer_render_backward split in two so that consecutive views overlap: submit
+ * queues the step and returns a ticket once its work is queued (it waits on the host only for
+ * the forward pass's entry count and, when two steps are already in flight, for the older of
+ * them); splat_renderer_wait(ticket) returns when that step's image and gradients are in the
+ * host buffers. Up to two steps are in flight, so step k+1 computes while step k's gradients
+ * cross PCIe. The three host buffers belong to the step until its wait returns (pinned host
+ * memory lets the copies run asynchronously). splat_renderer_render_backward is submit
+ * followed by wait. Waiting on a step that is already complete returns SPLAT_OK at once. */
+SPLAT_API int splat_renderer_submit_backward(splat_renderer* r, const splat_camera* cam, const splat_proj_opts* opts,
+                                             const float background[3], const float* dimage_host, float* image_host,
+                                             float* grads_aos59_host, uint64_t* ticket);
+SPLAT_API int splat_renderer_wait(splat_renderer* r, uint64_t ticket);
 /* Tile entries of the last rendered view (Binning::sorted.len()). */
 SPLAT_API int64_t splat_renderer_last_entries(const splat_renderer* r);
 

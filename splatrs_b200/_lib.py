@@ -157,6 +157,9 @@ def _declare(L):
         "splat_renderer_set_model": ([vp, vp, i64, i32], C.c_int),
         "splat_renderer_render": ([vp, P(Camera), P(ProjOpts), P(C.c_float), vp], C.c_int),
         "splat_renderer_render_backward": ([vp, P(Camera), P(ProjOpts), P(C.c_float), vp, vp, vp], C.c_int),
+        "splat_renderer_submit_backward": ([vp, P(Camera), P(ProjOpts), P(C.c_float), vp, vp, vp, P(C.c_uint64)],
+                                           C.c_int),
+        "splat_renderer_wait": ([vp, C.c_uint64], C.c_int),
         "splat_renderer_last_entries": ([vp], i64),
     })
     sig.update({

@@ -91,19 +91,32 @@ Status render_view(Ctx* c, const float* planes, int64_t n, int64_t cap, const sp
 using namespace splat;
 
 // Chunks of the gradient download: the projection backward and the record conversion of
-// chunk i+1 run while chunk i crosses PCIe on the copy stream.
+// chunk i+1 run while chunk i crosses PCIe on the download stream.
 constexpr int kDownloadChunks = 8;
+// Steps in flight. Each slot owns its view buffers, gradient buffers and events, so step k+1
+// computes while step k's gradients cross PCIe; uploads and downloads use separate streams
+// (separate copy engines).
+constexpr int kSlots = 2;
+
+struct RSlot {
+  ViewBuffers v;
+  DevBuf pgrad, grad_planes, grad_aos;
+  cudaEvent_t ev_up = nullptr, ev_img = nullptr, ev_fin = nullptr, ev_done = nullptr;
+  cudaEvent_t ev_chunk[kDownloadChunks] = {};
+  uint64_t ticket = 0;  // step occupying the slot; 0 when idle
+  int64_t entries = 0;
+};
 
 struct splat_renderer {
   splat_ctx* ctx;
   Ctx* c;
   int64_t n = 0, cap = 0;
   int32_t sh_degree = 3;
-  DevBuf planes, aos, pgrad, grad_planes, grad_aos;
-  ViewBuffers v;
+  DevBuf planes, aos;
+  RSlot slots[kSlots];
+  uint64_t next_ticket = 1;
   int64_t last_entries = 0;
-  cudaStream_t copy = nullptr;  // host<->device transfers overlapping the compute stream
-  cudaEvent_t ev_up = nullptr, ev_img = nullptr, ev_chunk[kDownloadChunks] = {};
+  cudaStream_t up = nullptr, down = nullptr;  // host->device and device->host transfers
 };
 
 namespace {
@@ -129,6 +142,73 @@ struct REnter {
 bool cam_ok(const splat_camera* cam) {
   return cam && cam->width > 0 && cam->height > 0 && cam->width <= 65535 && cam->height <= 65535;
 }
+
+// Blocks until the slot's step has finished (its downloads included) and frees the slot.
+Status retire(splat_renderer* r, RSlot& sl) {
+  if (!sl.ticket) return Status::ok();
+  sl.ticket = 0;
+  return cuda_status(cudaEventSynchronize(sl.ev_done), "waiting for a submitted step");
+}
+
+Status retire_all(splat_renderer* r) {
+  Status s = Status::ok();
+  for (RSlot& sl : r->slots) {
+    const Status t = retire(r, sl);
+    if (s.good()) s = t;
+  }
+  return s;
+}
+
+// Queues one differentiable render into slot `sl`: dL/dimage up, forward, backward,
+// projection backward, image and gradient records down. Returns after the queueing (the
+// forward's entry-count read-back is the one host wait inside).
+Status submit_backward(splat_renderer* r, RSlot& sl, const splat_camera& cam, const splat_proj_opts& o,
+                       const float bg[3], const float* dimage_host, float* image_host, float* grads_host) {
+  Ctx* c = r->c;
+  const size_t npix = (size_t)cam.width * cam.height;
+  SPLAT_TRY(sl.v.ensure(r->n, cam.width, cam.height));
+  SPLAT_TRY(sl.pgrad.ensure((size_t)r->cap * 3 * 16));
+  SPLAT_TRY(sl.grad_planes.ensure((size_t)r->cap * kPlanes * 16));
+  if (grads_host) SPLAT_TRY(sl.grad_aos.ensure((size_t)r->cap * 59 * 4));
+  // dL/dimage crosses PCIe while the forward pass runs.
+  SPLAT_CUDA(cudaMemcpyAsync(sl.v.dimage.ptr, dimage_host, npix * 12, cudaMemcpyHostToDevice, r->up));
+  SPLAT_CUDA(cudaEventRecord(sl.ev_up, r->up));
+  SPLAT_TRY(render_view(c, r->planes.as<float>(), r->n, r->cap, cam, o, bg, sl.v, &sl.entries));
+  // The image crosses PCIe while the backward pass runs.
+  if (image_host) {
+    SPLAT_CUDA(cudaEventRecord(sl.ev_img, c->stream));
+    SPLAT_CUDA(cudaStreamWaitEvent(r->down, sl.ev_img, 0));
+    SPLAT_CUDA(cudaMemcpyAsync(image_host, sl.v.image.ptr, npix * 12, cudaMemcpyDeviceToHost, r->down));
+  }
+  SPLAT_CUDA(cudaStreamWaitEvent(c->stream, sl.ev_up, 0));
+  SPLAT_CUDA(cudaMemsetAsync(sl.pgrad.ptr, 0, (size_t)r->cap * 3 * 16, c->stream));
+  SPLAT_TRY(launch_raster_bwd(c, sl.v.proj.as<float>(), sl.v.gauss.as<uint32_t>(), sl.v.tile_range.as<uint32_t>(),
+                              cam.width, cam.height, bg, sl.v.final_t.as<float>(), sl.v.n_contrib.as<uint32_t>(),
+                              sl.v.dimage.as<float>(), sl.pgrad.as<float>(), r->cap, nullptr));
+  // Projection backward, record conversion and download in chunks of Gaussians.
+  const int64_t chunk = ((r->n + kDownloadChunks - 1) / kDownloadChunks + 127) / 128 * 128;
+  for (int k = 0; k < kDownloadChunks; k++) {
+    const int64_t i0 = (int64_t)k * chunk;
+    if (i0 >= r->n) break;
+    const int64_t cnt = std::min(chunk, r->n - i0);
+    SPLAT_TRY(launch_project_bwd(c, r->planes.as<float>() + 4 * i0, cnt, r->cap, cam, o,
+                                 sl.v.proj.as<float>() + 16 * i0, sl.pgrad.as<float>() + 4 * i0,
+                                 sl.grad_planes.as<float>() + 4 * i0, nullptr, 0));
+    if (grads_host) {
+      SPLAT_TRY(launch_params_to_aos(c, sl.grad_planes.as<float>() + 4 * i0, cnt, r->cap,
+                                     sl.grad_aos.as<float>() + 59 * i0));
+      SPLAT_CUDA(cudaEventRecord(sl.ev_chunk[k], c->stream));
+      SPLAT_CUDA(cudaStreamWaitEvent(r->down, sl.ev_chunk[k], 0));
+      SPLAT_CUDA(cudaMemcpyAsync(grads_host + 59 * i0, sl.grad_aos.as<float>() + 59 * i0, (size_t)cnt * 59 * 4,
+                                 cudaMemcpyDeviceToHost, r->down));
+    }
+  }
+  SPLAT_CUDA(cudaEventRecord(sl.ev_fin, c->stream));
+  SPLAT_CUDA(cudaStreamWaitEvent(r->down, sl.ev_fin, 0));
+  SPLAT_CUDA(cudaEventRecord(sl.ev_done, r->down));
+  r->last_entries = sl.entries;
+  return Status::ok();
+}
 }  // namespace
 
 extern "C" {
@@ -142,16 +222,19 @@ SPLAT_API int splat_renderer_create(splat_ctx* ctx, splat_renderer** out) {
   int prev = 0;
   cudaGetDevice(&prev);
   cudaSetDevice(r->c->device);
-  bool ok = cudaStreamCreateWithFlags(&r->copy, cudaStreamNonBlocking) == cudaSuccess;
-  ok = ok && cudaEventCreateWithFlags(&r->ev_up, cudaEventDisableTiming) == cudaSuccess;
-  ok = ok && cudaEventCreateWithFlags(&r->ev_img, cudaEventDisableTiming) == cudaSuccess;
-  for (int i = 0; i < kDownloadChunks && ok; i++)
-    ok = cudaEventCreateWithFlags(&r->ev_chunk[i], cudaEventDisableTiming) == cudaSuccess;
+  bool ok = cudaStreamCreateWithFlags(&r->up, cudaStreamNonBlocking) == cudaSuccess;
+  ok = ok && cudaStreamCreateWithFlags(&r->down, cudaStreamNonBlocking) == cudaSuccess;
+  for (RSlot& sl : r->slots) {
+    for (cudaEvent_t* ev : {&sl.ev_up, &sl.ev_img, &sl.ev_fin, &sl.ev_done})
+      ok = ok && cudaEventCreateWithFlags(ev, cudaEventDisableTiming) == cudaSuccess;
+    for (int i = 0; i < kDownloadChunks && ok; i++)
+      ok = cudaEventCreateWithFlags(&sl.ev_chunk[i], cudaEventDisableTiming) == cudaSuccess;
+  }
   cudaSetDevice(prev);
   if (!ok) {
     cudaGetLastError();
     r->c->last_error = "splat_renderer_create: stream or event creation failed";
-    delete r;
+    splat_renderer_destroy(r);
     return SPLAT_ERR_CUDA;
   }
   *out = r;
@@ -163,14 +246,19 @@ SPLAT_API int splat_renderer_destroy(splat_renderer* r) {
   {
     REnter e(r);
     cudaStreamSynchronize(r->c->stream);
-    cudaStreamSynchronize(r->copy);
-    for (DevBuf* b : {&r->planes, &r->aos, &r->pgrad, &r->grad_planes, &r->grad_aos}) b->release();
-    r->v.release();
-    for (cudaEvent_t ev : r->ev_chunk)
-      if (ev) cudaEventDestroy(ev);
-    if (r->ev_up) cudaEventDestroy(r->ev_up);
-    if (r->ev_img) cudaEventDestroy(r->ev_img);
-    if (r->copy) cudaStreamDestroy(r->copy);
+    if (r->up) cudaStreamSynchronize(r->up);
+    if (r->down) cudaStreamSynchronize(r->down);
+    for (DevBuf* b : {&r->planes, &r->aos}) b->release();
+    for (RSlot& sl : r->slots) {
+      sl.v.release();
+      for (DevBuf* b : {&sl.pgrad, &sl.grad_planes, &sl.grad_aos}) b->release();
+      for (cudaEvent_t ev : sl.ev_chunk)
+        if (ev) cudaEventDestroy(ev);
+      for (cudaEvent_t ev : {sl.ev_up, sl.ev_img, sl.ev_fin, sl.ev_done})
+        if (ev) cudaEventDestroy(ev);
+    }
+    if (r->up) cudaStreamDestroy(r->up);
+    if (r->down) cudaStreamDestroy(r->down);
   }
   delete r;
   return SPLAT_OK;
@@ -185,7 +273,8 @@ SPLAT_API int splat_renderer_set_model(splat_renderer* r, const float* aos59_hos
   REnter e(r);
   Ctx* c = r->c;
   const int64_t cap = std::max<int64_t>(n, 1);
-  Status s = r->planes.ensure((size_t)cap * kPlanes * 16);
+  Status s = retire_all(r);  // in-flight steps read the current model
+  if (s.good()) s = r->planes.ensure((size_t)cap * kPlanes * 16);
   if (s.good()) s = r->aos.ensure((size_t)cap * 59 * 4);
   if (s.good() && n) s = cuda_status(cudaMemcpyAsync(r->aos.ptr, aos59_host, (size_t)n * 59 * 4, cudaMemcpyHostToDevice,
                                                      c->stream), "upload model");
@@ -209,73 +298,69 @@ SPLAT_API int splat_renderer_render(splat_renderer* r, const splat_camera* cam, 
   Ctx* c = r->c;
   splat_proj_opts o = *opts;
   o.sh_degree = r->sh_degree;  // project_all uses the model's active degree (project.rs:321-324)
-  Status s = render_view(c, r->planes.as<float>(), r->n, r->cap, *cam, o, background, r->v, &r->last_entries);
+  Status s = retire_all(r);
+  RSlot& sl = r->slots[0];
+  if (s.good()) s = render_view(c, r->planes.as<float>(), r->n, r->cap, *cam, o, background, sl.v, &sl.entries);
+  if (s.good()) r->last_entries = sl.entries;
   const size_t npix = (size_t)cam->width * cam->height;
   if (s.good() && image_host)
-    s = cuda_status(cudaMemcpyAsync(image_host, r->v.image.ptr, npix * 12, cudaMemcpyDeviceToHost, c->stream),
+    s = cuda_status(cudaMemcpyAsync(image_host, sl.v.image.ptr, npix * 12, cudaMemcpyDeviceToHost, c->stream),
                     "download image");
   if (s.good()) s = cuda_status(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
   return s.good() ? SPLAT_OK : rfail(r, s);
 }
 
-SPLAT_API int splat_renderer_render_backward(splat_renderer* r, const splat_camera* cam, const splat_proj_opts* opts,
+SPLAT_API int splat_renderer_submit_backward(splat_renderer* r, const splat_camera* cam, const splat_proj_opts* opts,
                                              const float background[3], const float* dimage_host, float* image_host,
-                                             float* grads_aos59_host) {
+                                             float* grads_aos59_host, uint64_t* ticket) {
   if (!r) return SPLAT_ERR_INVALID;
-  if (!cam_ok(cam) || !opts || !background || !dimage_host) {
-    r->c->last_error = "splat_renderer_render_backward: bad arguments";
+  if (!cam_ok(cam) || !opts || !background || !dimage_host || !ticket) {
+    r->c->last_error = "splat_renderer_submit_backward: bad arguments";
+    return SPLAT_ERR_INVALID;
+  }
+  *ticket = 0;
+  REnter e(r);
+  splat_proj_opts o = *opts;
+  o.sh_degree = r->sh_degree;
+  // The slot of the oldest step in flight (the next in round-robin order) is reused.
+  RSlot& sl = r->slots[r->next_ticket % kSlots];
+  Status s = retire(r, sl);
+  if (s.good()) s = submit_backward(r, sl, *cam, o, background, dimage_host, image_host, grads_aos59_host);
+  if (!s.good()) {
+    // Leave nothing in flight behind an error.
+    cudaStreamSynchronize(r->c->stream);
+    cudaStreamSynchronize(r->up);
+    cudaStreamSynchronize(r->down);
+    cudaGetLastError();
+    return rfail(r, s);
+  }
+  sl.ticket = r->next_ticket++;
+  *ticket = sl.ticket;
+  return SPLAT_OK;
+}
+
+SPLAT_API int splat_renderer_wait(splat_renderer* r, uint64_t ticket) {
+  if (!r) return SPLAT_ERR_INVALID;
+  if (ticket == 0 || ticket >= r->next_ticket) {
+    r->c->last_error = "splat_renderer_wait: no such submitted step";
     return SPLAT_ERR_INVALID;
   }
   REnter e(r);
-  Ctx* c = r->c;
-  splat_proj_opts o = *opts;
-  o.sh_degree = r->sh_degree;
-  const size_t npix = (size_t)cam->width * cam->height;
-  Status s = r->v.ensure(r->n, cam->width, cam->height);
-  if (s.good()) s = r->pgrad.ensure((size_t)r->cap * 3 * 16);
-  if (s.good()) s = r->grad_planes.ensure((size_t)r->cap * kPlanes * 16);
-  if (s.good()) s = r->grad_aos.ensure((size_t)r->cap * 59 * 4);
-  // dL/dimage crosses PCIe while the forward pass runs.
-  if (s.good()) s = cuda_status(cudaMemcpyAsync(r->v.dimage.ptr, dimage_host, npix * 12, cudaMemcpyHostToDevice,
-                                                r->copy), "upload dimage");
-  if (s.good()) s = cuda_status(cudaEventRecord(r->ev_up, r->copy), "cudaEventRecord");
-  if (s.good()) s = render_view(c, r->planes.as<float>(), r->n, r->cap, *cam, o, background, r->v, &r->last_entries);
-  // The image crosses PCIe while the backward pass runs.
-  if (s.good() && image_host) {
-    s = cuda_status(cudaEventRecord(r->ev_img, c->stream), "cudaEventRecord");
-    if (s.good()) s = cuda_status(cudaStreamWaitEvent(r->copy, r->ev_img, 0), "cudaStreamWaitEvent");
-    if (s.good())
-      s = cuda_status(cudaMemcpyAsync(image_host, r->v.image.ptr, npix * 12, cudaMemcpyDeviceToHost, r->copy),
-                      "download image");
-  }
-  if (s.good()) s = cuda_status(cudaStreamWaitEvent(c->stream, r->ev_up, 0), "cudaStreamWaitEvent");
-  if (s.good()) s = cuda_status(cudaMemsetAsync(r->pgrad.ptr, 0, (size_t)r->cap * 3 * 16, c->stream), "zero pgrad");
-  if (s.good())
-    s = launch_raster_bwd(c, r->v.proj.as<float>(), r->v.gauss.as<uint32_t>(), r->v.tile_range.as<uint32_t>(),
-                          cam->width, cam->height, background, r->v.final_t.as<float>(), r->v.n_contrib.as<uint32_t>(),
-                          r->v.dimage.as<float>(), r->pgrad.as<float>(), r->cap, nullptr);
-  // Projection backward, record conversion and download in chunks of Gaussians.
-  const int64_t chunk = ((r->n + kDownloadChunks - 1) / kDownloadChunks + 127) / 128 * 128;
-  for (int k = 0; s.good() && k < kDownloadChunks; k++) {
-    const int64_t i0 = (int64_t)k * chunk;
-    if (i0 >= r->n) break;
-    const int64_t cnt = std::min(chunk, r->n - i0);
-    s = launch_project_bwd(c, r->planes.as<float>() + 4 * i0, cnt, r->cap, *cam, o, r->v.proj.as<float>() + 16 * i0,
-                           r->pgrad.as<float>() + 4 * i0, r->grad_planes.as<float>() + 4 * i0, nullptr, 0);
-    if (s.good() && grads_aos59_host) {
-      s = launch_params_to_aos(c, r->grad_planes.as<float>() + 4 * i0, cnt, r->cap, r->grad_aos.as<float>() + 59 * i0);
-      if (s.good()) s = cuda_status(cudaEventRecord(r->ev_chunk[k], c->stream), "cudaEventRecord");
-      if (s.good()) s = cuda_status(cudaStreamWaitEvent(r->copy, r->ev_chunk[k], 0), "cudaStreamWaitEvent");
-      if (s.good())
-        s = cuda_status(cudaMemcpyAsync(grads_aos59_host + 59 * i0, r->grad_aos.as<float>() + 59 * i0,
-                                        (size_t)cnt * 59 * 4, cudaMemcpyDeviceToHost, r->copy),
-                        "download gradients");
+  for (RSlot& sl : r->slots)
+    if (sl.ticket == ticket) {
+      const Status s = retire(r, sl);
+      return s.good() ? SPLAT_OK : rfail(r, s);
     }
-  }
-  const Status s1 = cuda_status(cudaStreamSynchronize(r->copy), "cudaStreamSynchronize");
-  const Status s2 = cuda_status(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
-  if (s.good()) s = s1.good() ? s2 : s1;
-  return s.good() ? SPLAT_OK : rfail(r, s);
+  return SPLAT_OK;  // already retired
+}
+
+SPLAT_API int splat_renderer_render_backward(splat_renderer* r, const splat_camera* cam, const splat_proj_opts* opts,
+                                             const float background[3], const float* dimage_host, float* image_host,
+                                             float* grads_aos59_host) {
+  uint64_t t = 0;
+  const int st = splat_renderer_submit_backward(r, cam, opts, background, dimage_host, image_host, grads_aos59_host, &t);
+  if (st != SPLAT_OK) return st;
+  return splat_renderer_wait(r, t);
 }
 
 SPLAT_API int64_t splat_renderer_last_entries(const splat_renderer* r) { return r ? r->last_entries : -1; }

@@ -286,6 +286,23 @@ class Renderer:
             grads_out.ctypes.data_as(C.c_void_p) if want_grads else None), self.ctx.h)
         return image_out, grads_out
 
+    def submit_backward(self, cam: Camera, opts: ProjOpts, background, dimage, image_out, grads_out) -> int:
+        """Queues render_backward into caller-owned host buffers (numpy or pinned torch CPU
+        tensors, None to skip an output) and returns a ticket for ``wait``. The buffers
+        belong to the step until its wait returns."""
+        def ptr(a):
+            if a is None:
+                return None
+            return C.c_void_p(a.data_ptr()) if hasattr(a, "data_ptr") else a.ctypes.data_as(C.c_void_p)
+        bgp, keep = _bg(background)
+        t = C.c_uint64()
+        check(self.lib.splat_renderer_submit_backward(self.h, C.byref(cam), C.byref(opts), bgp, ptr(dimage),
+                                                      ptr(image_out), ptr(grads_out), C.byref(t)), self.ctx.h)
+        return int(t.value)
+
+    def wait(self, ticket: int):
+        check(self.lib.splat_renderer_wait(self.h, ticket), self.ctx.h)
+
     @property
     def last_entries(self) -> int:
         return int(self.lib.splat_renderer_last_entries(self.h))

@@ -84,7 +84,44 @@ def test_renderer_host_api_matches_stage_api(ctx):
     gp = G.project_backward_all(ctx, planes, g.shape[0], g.shape[0], cam, opts, proj, pg)
     want = G.planes_to_params(ctx, gp, g.shape[0], g.shape[0]).cpu().numpy()
     assert np.array_equal(out.image.cpu().numpy(), image)
+    # The compositing backward sums across tiles with float atomics, whose order differs
+    # from run to run; 1e-4 of each column's largest magnitude covers that reordering.
     scale = np.maximum(np.abs(want).max(0), 1e-30)
-    assert (np.abs(grads - want).max(0) / scale).max() < 1e-5
+    assert (np.abs(grads - want).max(0) / scale).max() < 1e-4
     assert r.last_entries == b.num_entries
+    r.close()
+
+
+def test_renderer_pipelined_steps_match_synchronous(ctx):
+    """splat_renderer_submit_backward / splat_renderer_wait with three views of different
+    sizes in flight (pinned host buffers, waits out of order): every image equals the
+    synchronous call's bit for bit and every gradient record agrees to float-atomic order."""
+    rng = np.random.default_rng(9)
+    g = scenes.random_gaussians(rng, 20000, -1.0, 1.0, -3.6, 0.5, 1.0)
+    opts = ProjOpts.make(sh_degree=3)
+    bg = (0.0, 0.1, 0.2)
+    views = []
+    for k, (w, h) in enumerate([(640, 480), (333, 217), (800, 600)]):
+        cam = Camera.from_record(scenes.look_at(w, h, 0.9 * w, 0.9 * w, (0.3 * k, -0.4, -3.3), (0, 0, 0)))
+        dimage = torch.from_numpy(rng.normal(0, 1, w * h * 3).astype(np.float32)).pin_memory()
+        views.append((cam, dimage))
+    r = G.Renderer(ctx)
+    r.set_model(g, 3)
+    want = [r.render_backward(cam, opts, bg, d.numpy()) for cam, d in views]
+    outs = [(torch.empty(cam.width * cam.height * 3).pin_memory(), torch.empty(g.shape[0], 59).pin_memory())
+            for cam, _ in views]
+    t0 = r.submit_backward(views[0][0], opts, bg, views[0][1], *outs[0])
+    t1 = r.submit_backward(views[1][0], opts, bg, views[1][1], *outs[1])
+    t2 = r.submit_backward(views[2][0], opts, bg, views[2][1], *outs[2])  # retires t0's slot first
+    r.wait(t2)
+    r.wait(t1)
+    r.wait(t0)
+    r.wait(t0)  # already complete
+    for (img, grads), (wi, wg) in zip(outs, want):
+        assert np.array_equal(img.numpy(), wi)
+        scale = np.maximum(np.abs(wg).max(0), 1e-30)
+        assert (np.abs(grads.numpy() - wg).max(0) / scale).max() < 1e-4
+    from splatrs_b200._lib import SplatError
+    with pytest.raises(SplatError):
+        r.wait(t2 + 1)
     r.close()
