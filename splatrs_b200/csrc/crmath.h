@@ -133,6 +133,36 @@ CRM_HD float expf_cr_tab(float x, const double* tab) {
   return (float)(y * s);
 }
 
+// expf_cr_tab for the compositing range. The argument there is -sigma with
+// 0 <= sigma <= sigma_max = ln(255 * opacity) <= ln 255, so n = rint(64 x / ln2) lies in
+// [-512, 0]. A table of 2^(n/64) for n in [-(kExpNegEntries-1), 0] folds the 2^m scale into
+// the table entry (entry k = table64[(-k) & 63] * 2^((-k) >> 6), exact), so
+// fma(t', q, t') = 2^m * fma(t, q, t) exactly and the result equals expf_cr_tab bit for
+// bit; arguments below kExpNegMin (never produced by a valid projection) and NaN take
+// expf_cr.
+constexpr int kExpNegEntries = 577;
+constexpr float kExpNegMin = -6.2f;  // rint(-6.2 * 64 / ln2) = -572
+
+CRM_HD double exp2_neg_entry(int k, const double* tab64) {
+  const int n = -k;
+  return bits_to_double(double_to_bits(tab64[n & 63]) + ((uint64_t)(int64_t)(n >> 6) << 52));
+}
+
+CRM_HD float expf_cr_neg(float x, const double* tab_neg) {
+  if (!(x >= kExpNegMin)) return expf_cr(x);
+  const double d = (double)x;
+  const double n = rint(d * 0x1.71547652b82fep+6);  // 64 / ln2
+  double r = fma(-n, 0x1.62e42fefa0000p-7, d);
+  r = fma(-n, 0x1.cf79abc9e3b3ap-46, r);
+  double c = fma(r, 0x1.1111111111111p-7, 0x1.5555555555555p-5);  // 1/120, 1/24
+  c = fma(r, c, 0x1.5555555555555p-3);                            // 1/6
+  c = fma(r, c, 0.5);
+  c = fma(r, c, 1.0);
+  const double q = r * c;
+  const double t = tab_neg[-(int)n];
+  return (float)fma(t, q, t);
+}
+
 // Correctly rounded natural log for float x.
 CRM_HD float logf_cr(float x) {
   if (!(x == x) || x < 0.0f) return (float)NAN;

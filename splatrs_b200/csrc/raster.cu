@@ -36,8 +36,8 @@ __device__ __forceinline__ PixelGeom pixel_geom(uint32_t tile, uint32_t tiles_x,
 
 __constant__ double kExp2Tab64[64] = CRM_EXP2_TAB64;
 
-// evaluate (rasterize.rs:231-244). Returns false when skipped. `tab` is the exp table in
-// shared memory.
+// evaluate (rasterize.rs:231-244). Returns false when skipped. `tab` is the table of
+// crm::expf_cr_neg in shared memory.
 __device__ __forceinline__ bool evaluate(float px, float py, float mx, float my, float A, float B, float C,
                                          float opacity, float sigma_max, const double* tab, float* gauss_out,
                                          float* alpha_out) {
@@ -45,7 +45,7 @@ __device__ __forceinline__ bool evaluate(float px, float py, float mx, float my,
   const float dy = py - my;
   const float sigma = 0.5f * (A * dx * dx + C * dy * dy) + B * dx * dy;
   if (sigma < 0.0f || sigma > sigma_max) return false;
-  const float gauss = crm::expf_cr_tab(-sigma, tab);
+  const float gauss = crm::expf_cr_neg(-sigma, tab);
   const float og = opacity * gauss;
   if (og < SPLAT_ALPHA_MIN) return false;
   *gauss_out = gauss;
@@ -142,6 +142,21 @@ __device__ __forceinline__ uint32_t subblock_mask(uint32_t rx, uint32_t ry, uint
   return m;
 }
 
+// 32x32 bit-matrix transpose across a warp: lane j holds row j on entry; on return lane L
+// holds column L (bit j of the result = bit L of lane j's input). Five exchange stages,
+// each swapping the off-diagonal blocks of size s.
+__device__ __forceinline__ uint32_t warp_transpose_bits(uint32_t x) {
+  const uint32_t lane = threadIdx.x & 31;
+  const uint32_t masks[5] = {0x0000ffffu, 0x00ff00ffu, 0x0f0f0f0fu, 0x33333333u, 0x55555555u};
+#pragma unroll
+  for (int i = 0; i < 5; i++) {
+    const uint32_t sh = 16u >> i, m = masks[i];
+    const uint32_t y = __shfl_xor_sync(0xffffffffu, x, sh);
+    x = (lane & sh) ? ((x & ~m) | ((y & ~m) >> sh)) : ((x & m) | ((y & m) << sh));
+  }
+  return x;
+}
+
 // Compacts, in order, the chunk-local indices k < cnt whose mask has this warp's bit (and,
 // when `limit` is finite, k < limit) into list[]; returns how many.
 __device__ __forceinline__ uint32_t build_warp_list(const uint8_t* __restrict__ smask, uint32_t cnt, uint32_t limit,
@@ -160,7 +175,12 @@ __device__ __forceinline__ uint32_t build_warp_list(const uint8_t* __restrict__ 
   return n;
 }
 
-// forward_tile (rasterize.rs:249-302) for one tile per block.
+// forward_tile (rasterize.rs:249-302) for one tile per block. Each warp walks, 32 at a
+// time, the chunk's entries whose pixel rectangle touches its 8x4 sub-block; a lane takes
+// only the entries whose rectangle covers its own pixel (the rectangle test of the
+// reference), found from the batch's coverage masks transposed across the warp, so the
+// warp runs as many rounds as its busiest lane rather than one round per entry. Each lane
+// still composites its entries in list (depth) order.
 __global__ void __launch_bounds__(kRasterThreads, 6) raster_fwd_kernel(
     const float4* __restrict__ rec, const uint32_t* __restrict__ gauss, const uint2* __restrict__ ranges,
     uint32_t width, uint32_t height, uint32_t tiles_x, float bg0, float bg1, float bg2, float* __restrict__ image,
@@ -170,14 +190,15 @@ __global__ void __launch_bounds__(kRasterThreads, 6) raster_fwd_kernel(
   __shared__ uint32_t srect[kChunk];
   __shared__ uint8_t smask[kChunk];
   __shared__ uint8_t slist[kRasterThreads / 32][kChunk];
-  __shared__ double stab[64];
-  if (threadIdx.x < 64) stab[threadIdx.x] = kExp2Tab64[threadIdx.x];
+  __shared__ double stab[crm::kExpNegEntries];
+  for (int i = threadIdx.x; i < crm::kExpNegEntries; i += kRasterThreads) stab[i] = crm::exp2_neg_entry(i, kExp2Tab64);
   const PixelGeom pg = pixel_geom(blockIdx.x, tiles_x, width, height);
   const uint32_t ox = (blockIdx.x % tiles_x) * kTile, oy = (blockIdx.x / tiles_x) * kTile;
-  const uint32_t lx = pg.px_i - ox, ly_shift = pg.py_j - oy + 16u;  // bit positions in the rect masks
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t sbx = (warp & 1u) * 8u, sby = (warp >> 1) * 4u;  // sub-block origin in the tile
   const float px = (float)pg.px_i + 0.5f, py = (float)pg.py_j + 0.5f;
   const uint2 range = ranges[blockIdx.x];
-  uint8_t* list = slist[threadIdx.x >> 5];
+  uint8_t* list = slist[warp];
   float T = 1.0f, cr = 0.0f, cg = 0.0f, cb = 0.0f;
   uint32_t ncon = 0;
   bool done = !pg.inside;
@@ -199,27 +220,44 @@ __global__ void __launch_bounds__(kRasterThreads, 6) raster_fwd_kernel(
     __syncthreads();
     const uint32_t cnt = min((uint32_t)kChunk, range.y - base);
     const uint32_t nl = build_warp_list(smask, cnt, 0xffffffffu, list);
-    for (uint32_t i = 0; i < nl; i++) {
+    for (uint32_t b0 = 0; b0 < nl; b0 += 32) {
       if (__all_sync(0xffffffffu, done)) break;
-      const uint32_t k = list[i];
-      const uint32_t rm = srect[k];
-      if (done || !((rm >> lx) & (rm >> ly_shift) & 1u)) continue;
-      npairs++;
-      const float4 e0 = s0[k], e1 = s1[k];
-      const float2 e2 = s2[k];
-      float gval, alpha;
-      if (!evaluate(px, py, e0.x, e0.y, e0.z, e0.w, e1.x, e1.y, e1.z, stab, &gval, &alpha)) continue;
-      const float test_t = T * (1.0f - alpha);
-      if (test_t < SPLAT_T_MIN) {
-        done = true;
-        continue;
+      // Lane j loads entry j of the batch and expands its rectangle to a 32-bit mask of the
+      // sub-block's pixels (bit 8 * row + column); the transpose gives each lane the mask of
+      // the batch entries that cover its pixel.
+      const uint32_t j = b0 + lane;
+      uint32_t kl = 0, cov = 0;
+      if (j < nl) {
+        kl = list[j];
+        const uint32_t rm = srect[kl];
+        const uint32_t c8 = (rm >> sbx) & 0xffu;
+        const uint32_t r4 = (rm >> (16u + sby)) & 0xfu;
+        cov = c8 * ((r4 & 1u) | ((r4 & 2u) << 7) | ((r4 & 4u) << 14) | ((r4 & 8u) << 21));
       }
-      const float at = alpha * T;
-      cr += at * e1.w;
-      cg += at * e2.x;
-      cb += at * e2.y;
-      T = test_t;
-      ncon = base - range.x + k + 1;
+      uint32_t mine = warp_transpose_bits(cov);
+      if (done) mine = 0;
+      while (__any_sync(0xffffffffu, mine != 0u)) {
+        const uint32_t k = __shfl_sync(0xffffffffu, kl, (__ffs(mine) - 1) & 31);
+        if (mine == 0u) continue;
+        mine &= mine - 1u;
+        npairs++;
+        const float4 e0 = s0[k], e1 = s1[k];
+        const float2 e2 = s2[k];
+        float gval, alpha;
+        if (!evaluate(px, py, e0.x, e0.y, e0.z, e0.w, e1.x, e1.y, e1.z, stab, &gval, &alpha)) continue;
+        const float test_t = T * (1.0f - alpha);
+        if (test_t < SPLAT_T_MIN) {
+          done = true;
+          mine = 0;
+          continue;
+        }
+        const float at = alpha * T;
+        cr += at * e1.w;
+        cg += at * e2.x;
+        cb += at * e2.y;
+        T = test_t;
+        ncon = base - range.x + k + 1;
+      }
     }
     __syncthreads();
   }
@@ -233,7 +271,7 @@ __global__ void __launch_bounds__(kRasterThreads, 6) raster_fwd_kernel(
   }
   if (pairs) {
     for (int o = 16; o > 0; o >>= 1) npairs += __shfl_xor_sync(0xffffffffu, npairs, o);
-    if ((threadIdx.x & 31) == 0 && npairs) atomicAdd(pairs, npairs);
+    if (lane == 0 && npairs) atomicAdd(pairs, npairs);
   }
 }
 
