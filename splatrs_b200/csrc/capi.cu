@@ -133,7 +133,9 @@ SPLAT_API int splat_ctx_create(int device, void* stream, splat_ctx** out) {
   cudaGetDevice(&prev);
   cudaSetDevice(device);
   cudaDeviceGetAttribute(&ctx->c.sm_count, cudaDevAttrMultiProcessorCount, device);
-  if (cudaMallocHost(&ctx->c.host_small, 4096) != cudaSuccess) {
+  if (cudaHostAlloc(&ctx->c.host_small, 4096, cudaHostAllocMapped) != cudaSuccess ||
+      cudaHostGetDevicePointer(&ctx->c.host_small_dev, ctx->c.host_small, 0) != cudaSuccess) {
+    if (ctx->c.host_small) cudaFreeHost(ctx->c.host_small);
     cudaGetLastError();
     cudaSetDevice(prev);
     delete ctx;

@@ -71,8 +71,10 @@ struct Ctx {
   LaunchCounter launches;
   std::string last_error;
   int sm_count = 148;
-  // Pinned host staging for small read-backs.
+  // Mapped pinned host memory for small read-backs: kernels store into it through
+  // host_small_dev, so a read-back never queues on a copy engine behind large transfers.
   void* host_small = nullptr;
+  void* host_small_dev = nullptr;
 };
 
 // Reserve `bytes` of scratch (256-byte aligned) from the context arena. The arena is

@@ -23,6 +23,15 @@ Status launch_project_bwd_adam(Ctx* c, float* planes, float* m, float* v, int64_
                                const float* pgrad, void* stats, int absgrad, uint64_t step, const splat_lr& lr);
 
 Status launch_scan_u32(Ctx* c, const uint32_t* in, int64_t n, uint32_t* out, int write_total, uint64_t* total_dev);
+
+// Fills `words` 32-bit words at `dst` with `value` by a kernel on the context stream (in
+// place of cudaMemsetAsync, so the compute stream holds kernels only).
+Status launch_fill_u32(Ctx* c, void* dst, size_t words, uint32_t value);
+
+// Copies na words from a and then nb words from b (device memory, na + nb <= 32) into the
+// context's mapped host buffer (c->host_small) with a one-warp kernel; the host reads them
+// after synchronising the stream.
+Status launch_publish_u32(Ctx* c, const uint32_t* a, int na, const uint32_t* b, int nb);
 Status launch_scan_u32_into(Ctx* c, const uint32_t* in, int64_t n, uint32_t* out, int write_total,
                             uint64_t* partial, uint64_t* total);
 constexpr int kScanValuesPerBlock = 4096;

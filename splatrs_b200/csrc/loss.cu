@@ -250,7 +250,7 @@ Status launch_loss(Ctx* c, const float* pred, const void* target, int target_u8,
   double* sums = nullptr;
   SPLAT_TRY(arena_reserve(c, npix3 * 3 * 4, (void**)&dmaps));
   SPLAT_TRY(arena_reserve(c, 3 * 8, (void**)&sums));
-  SPLAT_CUDA(cudaMemsetAsync(sums, 0, 3 * 8, c->stream));
+  SPLAT_TRY(launch_fill_u32(c, sums, 3 * 2, 0u));
   const LossKernel K = make_loss_kernel();
   const dim3 grid(ceil_div(width, kLT), ceil_div(height, kLT));
   ssim_fwd_kernel<<<grid, kLossThreads, 0, c->stream>>>(pred, target, target_u8, width, height, K, dmaps, sums);

@@ -797,8 +797,8 @@ __global__ void __launch_bounds__(kConvG) planes_to_aos_kernel(const float4* __r
 // ---------------------------------------------------------------------------------------
 Status launch_project_fwd(Ctx* c, const float* planes, int64_t n, int64_t cap, const splat_camera& cam,
                           const splat_proj_opts& opts, float* proj, uint32_t* num_tiles, uint32_t* depth_range) {
-  SPLAT_CUDA(cudaMemsetAsync(depth_range, 0xff, 4, c->stream));
-  SPLAT_CUDA(cudaMemsetAsync(depth_range + 1, 0, 4, c->stream));
+  SPLAT_TRY(launch_fill_u32(c, depth_range, 1, 0xffffffffu));
+  SPLAT_TRY(launch_fill_u32(c, depth_range + 1, 1, 0u));
   if (n == 0) return Status::ok();
   const int bs = 256;
   const uint32_t grid = ceil_div(n, bs);
@@ -817,8 +817,8 @@ Status launch_project_fwd(Ctx* c, const float* planes, int64_t n, int64_t cap, c
 
 Status launch_proj_from_reference(Ctx* c, const float* p15, int64_t n, uint32_t width, uint32_t height, float* proj,
                                   uint32_t* num_tiles, uint32_t* depth_range) {
-  SPLAT_CUDA(cudaMemsetAsync(depth_range, 0xff, 4, c->stream));
-  SPLAT_CUDA(cudaMemsetAsync(depth_range + 1, 0, 4, c->stream));
+  SPLAT_TRY(launch_fill_u32(c, depth_range, 1, 0xffffffffu));
+  SPLAT_TRY(launch_fill_u32(c, depth_range + 1, 1, 0u));
   if (n == 0) return Status::ok();
   proj_from_reference_kernel<<<ceil_div(n, 256), 256, 0, c->stream>>>(p15, n, width, height,
                                                                        reinterpret_cast<float4*>(proj), num_tiles,

@@ -68,14 +68,16 @@ Status render_view(Ctx* c, const float* planes, int64_t n, int64_t cap, const sp
   uint64_t* total = nullptr;
   SPLAT_TRY(arena_reserve(c, 8, (void**)&total));
   SPLAT_TRY(launch_scan_u32(c, nt, n, v.entry_offset.as<uint32_t>(), 1, total));
-  // One read-back per view: the entry count and the depth range size the sort.
-  uint64_t* h = reinterpret_cast<uint64_t*>(c->host_small);
-  SPLAT_CUDA(cudaMemcpyAsync(h, total, 8, cudaMemcpyDeviceToHost, c->stream));
-  SPLAT_CUDA(cudaMemcpyAsync(h + 1, dr, 8, cudaMemcpyDeviceToHost, c->stream));
+  // One read-back per view: the entry count and the depth range size the sort. A kernel
+  // stores them into mapped host memory, so the read does not wait behind transfers queued
+  // on a copy engine (a renderer step's downloads overlap the next step).
+  SPLAT_TRY(launch_publish_u32(c, reinterpret_cast<const uint32_t*>(total), 2, dr, 2));
   SPLAT_CUDA(cudaStreamSynchronize(c->stream));
+  const volatile uint64_t* h = reinterpret_cast<const volatile uint64_t*>(c->host_small);
   const uint64_t E = h[0];
   if (E >= 0xffffffffull) return Status::make(SPLAT_ERR_CAPACITY, "too many tile entries for 32-bit offsets");
-  const uint32_t* drh = reinterpret_cast<const uint32_t*>(h + 1);
+  const uint64_t drw = h[1];
+  const uint32_t drh[2] = {(uint32_t)drw, (uint32_t)(drw >> 32)};
   SPLAT_TRY(v.gauss.ensure((size_t)std::max<uint64_t>(E, 1) * 4));
   SPLAT_TRY(launch_bin_sort(c, proj, v.entry_offset.as<uint32_t>(), n, (int64_t)E, dr, drh[0],
                             E > 0 ? drh[1] : drh[0], cam.width, cam.height, v.gauss.as<uint32_t>(), nullptr,
@@ -181,7 +183,7 @@ Status submit_backward(splat_renderer* r, RSlot& sl, const splat_camera& cam, co
     SPLAT_CUDA(cudaMemcpyAsync(image_host, sl.v.image.ptr, npix * 12, cudaMemcpyDeviceToHost, r->down));
   }
   SPLAT_CUDA(cudaStreamWaitEvent(c->stream, sl.ev_up, 0));
-  SPLAT_CUDA(cudaMemsetAsync(sl.pgrad.ptr, 0, (size_t)r->cap * 3 * 16, c->stream));
+  SPLAT_TRY(launch_fill_u32(c, sl.pgrad.ptr, (size_t)r->cap * 12, 0u));
   SPLAT_TRY(launch_raster_bwd(c, sl.v.proj.as<float>(), sl.v.gauss.as<uint32_t>(), sl.v.tile_range.as<uint32_t>(),
                               cam.width, cam.height, bg, sl.v.final_t.as<float>(), sl.v.n_contrib.as<uint32_t>(),
                               sl.v.dimage.as<float>(), sl.pgrad.as<float>(), r->cap, nullptr));

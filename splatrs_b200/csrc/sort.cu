@@ -126,6 +126,42 @@ __global__ void __launch_bounds__(kScanThreads) scan_apply_kernel(const uint32_t
   if (write_total && blockIdx.x == 0 && threadIdx.x == 0) out[n] = (uint32_t)*total;
 }
 
+__global__ void fill_u32_kernel(uint32_t* __restrict__ dst, size_t words, uint32_t value, int vector) {
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  const size_t quads = vector ? words / 4 : 0;
+  uint4* d4 = reinterpret_cast<uint4*>(dst);
+  const uint4 v4 = make_uint4(value, value, value, value);
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < quads; i += stride) d4[i] = v4;
+  for (size_t i = quads * 4 + (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < words; i += stride) dst[i] = value;
+}
+
+Status launch_fill_u32(Ctx* c, void* dst, size_t words, uint32_t value) {
+  if (words == 0) return Status::ok();
+  const int vector = (reinterpret_cast<uintptr_t>(dst) & 15u) == 0;
+  const size_t items = vector ? (words + 3) / 4 : words;
+  const uint32_t grid = (uint32_t)std::min<size_t>((items + 255) / 256, (size_t)c->sm_count * 8);
+  fill_u32_kernel<<<grid, 256, 0, c->stream>>>(reinterpret_cast<uint32_t*>(dst), words, value, vector);
+  c->launches.count++;
+  SPLAT_LAUNCHED("fill_u32_kernel");
+  return Status::ok();
+}
+
+__global__ void publish_u32_kernel(const uint32_t* __restrict__ a, int na, const uint32_t* __restrict__ b, int nb,
+                                   volatile uint32_t* out) {
+  const int lane = threadIdx.x;
+  if (lane < na) out[lane] = a[lane];
+  if (lane < nb) out[na + lane] = b[lane];
+  __threadfence_system();
+}
+
+Status launch_publish_u32(Ctx* c, const uint32_t* a, int na, const uint32_t* b, int nb) {
+  if (na < 0 || nb < 0 || na + nb > 32) return Status::make(SPLAT_ERR_INVALID, "publish: at most 32 words");
+  publish_u32_kernel<<<1, 32, 0, c->stream>>>(a, na, b, nb, reinterpret_cast<volatile uint32_t*>(c->host_small_dev));
+  c->launches.count++;
+  SPLAT_LAUNCHED("publish_u32_kernel");
+  return Status::ok();
+}
+
 Status launch_scan_u32(Ctx* c, const uint32_t* in, int64_t n, uint32_t* out, int write_total, uint64_t* total_dev) {
   const uint32_t blocks = ceil_div((uint64_t)std::max<int64_t>(n, 1), kScanTile);
   uint64_t* partial = nullptr;
@@ -380,7 +416,7 @@ static Status sort_and_range(Ctx* c, const float* proj, const uint32_t* entry_of
     std::swap(kin, kout);
     std::swap(vin, vout);
   }
-  SPLAT_CUDA(cudaMemsetAsync(ranges, 0, (size_t)num_tiles * 8, c->stream));
+  SPLAT_TRY(launch_fill_u32(c, ranges, (size_t)num_tiles * 2, 0u));
   tile_ranges_kernel<K><<<ceil_div(E, 256), 256, 0, c->stream>>>(kin, E, dbits, depth_range, ranges, keys_out);
   c->launches.count++;
   SPLAT_LAUNCHED("tile_ranges_kernel");
@@ -393,7 +429,7 @@ Status launch_bin_sort(Ctx* c, const float* proj, const uint32_t* entry_offset, 
   const uint32_t tiles_x = (width + kTile - 1) / kTile, tiles_y = (height + kTile - 1) / kTile;
   const uint32_t num_tiles = tiles_x * tiles_y;
   if (E == 0) {
-    SPLAT_CUDA(cudaMemsetAsync(ranges, 0, (size_t)num_tiles * 8, c->stream));
+    SPLAT_TRY(launch_fill_u32(c, ranges, (size_t)num_tiles * 2, 0u));
     return Status::ok();
   }
   const uint32_t span = depth_max - depth_min;

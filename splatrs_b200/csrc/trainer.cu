@@ -124,12 +124,12 @@ Status ensure_stats(splat_trainer* t, int64_t cap) {
   SPLAT_CUDA(cudaStreamSynchronize(t->c->stream));
   SPLAT_TRY(t->stats.ensure((size_t)cap * 12));
   t->stats_cap = cap;
-  SPLAT_CUDA(cudaMemsetAsync(t->stats.ptr, 0, t->stats.bytes, t->c->stream));
+  SPLAT_TRY(launch_fill_u32(t->c, t->stats.ptr, t->stats.bytes / 4, 0u));
   return Status::ok();
 }
 
 Status reset_stats(splat_trainer* t) {
-  return cuda_status(cudaMemsetAsync(t->stats.ptr, 0, t->stats.bytes, t->c->stream), "reset stats");
+  return launch_fill_u32(t->c, t->stats.ptr, t->stats.bytes / 4, 0u);
 }
 
 Status step(splat_trainer* t, splat_step_info* info) {
@@ -169,7 +169,7 @@ Status step(splat_trainer* t, splat_step_info* info) {
 
   // Backward (train.rs:226-235).
   SPLAT_TRY(t->pgrad.ensure((size_t)cap * 48));
-  SPLAT_CUDA(cudaMemsetAsync(t->pgrad.ptr, 0, (size_t)cap * 48, c->stream));
+  SPLAT_TRY(launch_fill_u32(c, t->pgrad.ptr, (size_t)cap * 12, 0u));
   SPLAT_TRY(launch_raster_bwd(c, t->vb.proj.as<float>(), t->vb.gauss.as<uint32_t>(), t->vb.tile_range.as<uint32_t>(),
                               cam.width, cam.height, bg, t->vb.final_t.as<float>(), t->vb.n_contrib.as<uint32_t>(),
                               t->pred_grad.as<float>(), t->pgrad.as<float>(), cap, nullptr));
