@@ -277,28 +277,32 @@ __global__ void __launch_bounds__(kRasterThreads, 6) raster_fwd_kernel(
 
 // backward_tile (rasterize.rs:354-455) for one tile per block. Per-pixel contributions to
 // an entry's 11 gradient slots are summed across the warp by a transposing butterfly
-// (16 shuffles leave slot j's warp total in lanes 2j and 2j+1), across the block's warps
+// (13 shuffles leave each slot's warp total in a pair of lanes), across the block's warps
 // with one shared-memory atomic instruction per warp, and across tiles with three float4
 // vector atomics per entry.
 constexpr int kSlots = 12;  // 11 used, padded for float4 flushes
 
-// v[0..15] per lane in, warp total of slot ((lane >> 1) & 15) out.
-__device__ __forceinline__ float warp_transpose_reduce16(float v[16]) {
+// v[0..11] per lane in (v[11] unused); out, the warp total of slot
+// 6*b4 + 3*b3 + 2*b2 + b1 (b_i = bit i of the lane) when 2*b2 + b1 < 3, in both lanes of a
+// pair. Each exchange stage keeps the half of the values selected by the lane's bit and
+// adds the partner's copy of that half: 6 + 3 + 2 + 1 + 1 = 13 shuffles for 11 slots.
+__device__ __forceinline__ float warp_transpose_reduce12(const float v[12]) {
   const uint32_t lane = threadIdx.x & 31;
-  float w[8], x[4], y[2];
   const bool b4 = lane & 16u, b3 = lane & 8u, b2 = lane & 4u, b1 = lane & 2u;
+  float w[6], x[4], y[2];
 #pragma unroll
-  for (int i = 0; i < 8; i++) {
-    const float send = b4 ? v[i] : v[i + 8];
-    const float keep = b4 ? v[i + 8] : v[i];
+  for (int i = 0; i < 6; i++) {
+    const float send = b4 ? v[i] : v[i + 6];
+    const float keep = b4 ? v[i + 6] : v[i];
     w[i] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
   }
 #pragma unroll
-  for (int i = 0; i < 4; i++) {
-    const float send = b3 ? w[i] : w[i + 4];
-    const float keep = b3 ? w[i + 4] : w[i];
+  for (int i = 0; i < 3; i++) {
+    const float send = b3 ? w[i] : w[i + 3];
+    const float keep = b3 ? w[i + 3] : w[i];
     x[i] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
   }
+  x[3] = 0.0f;
 #pragma unroll
   for (int i = 0; i < 2; i++) {
     const float send = b2 ? x[i] : x[i + 2];
@@ -310,6 +314,14 @@ __device__ __forceinline__ float warp_transpose_reduce16(float v[16]) {
   float z = keep + __shfl_xor_sync(0xffffffffu, send, 2);
   z += __shfl_xor_sync(0xffffffffu, z, 1);
   return z;
+}
+
+// 1 / x for x in [0.01, 1]: the MUFU approximation refined by one Newton step (values only;
+// used to recover transmittance, never for a decision).
+__device__ __forceinline__ float rcp_refined(float x) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return __fmaf_rn(r, __fmaf_rn(-x, r, 1.0f), r);
 }
 
 __global__ void __launch_bounds__(kRasterThreads) raster_bwd_kernel(
@@ -380,9 +392,9 @@ __global__ void __launch_bounds__(kRasterThreads) raster_bwd_kernel(
       const uint32_t kk = list[i];
       const uint32_t k = cstart + kk;
       const uint32_t rm = srect[kk];
-      float c[16];
+      float c[kSlots];
 #pragma unroll
-      for (int q = 0; q < 16; q++) c[q] = 0.0f;
+      for (int q = 0; q < kSlots; q++) c[q] = 0.0f;
       bool active = false;
       if (k < last && ((rm >> lx) & (rm >> ly_shift) & 1u)) {
         const float2 e2 = s2[kk];
@@ -395,7 +407,7 @@ __global__ void __launch_bounds__(kRasterThreads) raster_bwd_kernel(
           // Values only from here on: the arithmetic is fused and the divisions are
           // reciprocals; every decision was taken above exactly as in the forward pass.
           const float col_r = e1.w, col_g = e2.x, col_b = e2.y;
-          const float inv = __frcp_rn(1.0f - alpha);
+          const float inv = rcp_refined(1.0f - alpha);
           T = T * inv;
           const float t = T;
           const float keep = 1.0f - last_alpha;
@@ -434,9 +446,10 @@ __global__ void __launch_bounds__(kRasterThreads) raster_bwd_kernel(
         }
       }
       if (__any_sync(0xffffffffu, active)) {
-        const float tot = warp_transpose_reduce16(c);
-        const uint32_t slot = (lane >> 1) & 15u;
-        if (!(lane & 1u) && slot < 11u) atomicAdd(&acc[kk * kSlots + slot], tot);
+        const float tot = warp_transpose_reduce12(c);
+        const uint32_t local = (lane >> 1) & 3u;
+        const uint32_t slot = 6u * ((lane >> 4) & 1u) + 3u * ((lane >> 3) & 1u) + local;
+        if (!(lane & 1u) && local < 3u && slot < 11u) atomicAdd(&acc[kk * kSlots + slot], tot);
       }
     }
     __syncthreads();
