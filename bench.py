@@ -362,8 +362,7 @@ def run_train_gpu(local, s, cfg, iterations):
     t = G.Trainer(ctx, init, extent, views, **cfg)
     torch.cuda.synchronize(local)
     tw = time.perf_counter()
-    for _ in range(iterations):
-        t.step()
+    t.run(iterations)  # splat_trainer_run: the whole run in one call, queued ahead of the device
     torch.cuda.synchronize(local)
     wall = time.perf_counter() - tw
     ps = float(np.mean([scenes.psnr(t.render(cam), rgb) for cam, rgb in views]))

@@ -116,6 +116,9 @@ typedef struct splat_train_config {
   /* Not in the reference: 0 = no limit. When a densification would leave more Gaussians
    * than this, that densification clones and splits nothing and only prunes. */
   uint64_t max_gaussians;
+  /* Not in the reference: tile entries the binning buffers hold at first (0 = automatic).
+   * An iteration whose view needs more is redone with larger buffers. */
+  uint64_t entry_capacity;
 } splat_train_config;
 
 typedef struct splat_ctx splat_ctx;
@@ -188,6 +191,23 @@ SPLAT_API int splat_bin_count_noalloc(splat_ctx* ctx, const uint32_t* num_tiles_
 SPLAT_API int splat_bin_sort(splat_ctx* ctx, const float* proj_dev, const uint32_t* entry_offset_dev, int64_t n,
                              int64_t num_entries, const uint32_t* depth_range_dev, uint32_t width, uint32_t height,
                              uint32_t* gauss_dev, uint64_t* keys_dev, uint32_t* tile_range_dev);
+
+/* The same binning with no host read-back, for callers that queue whole steps ahead (or
+ * capture them in a CUDA graph): splat_bin_count_device writes the entry count to device
+ * memory (*num_entries_dev, uint64) instead of returning it, and splat_bin_sort_device
+ * reads it there. Buffers are sized for `capacity` entries: gauss_dev holds capacity
+ * values and scratch_dev splat_bin_sort_device_scratch_bytes(capacity) bytes. When the
+ * count exceeds capacity the call sorts only the first `capacity` entries and sets
+ * *overflow_dev to 1 (it is never cleared here): the view must then be redone with larger
+ * buffers. Otherwise gauss_dev and tile_range_dev equal splat_bin_sort's. */
+SPLAT_API int splat_bin_count_device(splat_ctx* ctx, const uint32_t* num_tiles_dev, int64_t n,
+                                     uint32_t* entry_offset_dev, uint64_t* num_entries_dev);
+SPLAT_API size_t splat_bin_sort_device_scratch_bytes(int64_t capacity);
+SPLAT_API int splat_bin_sort_device(splat_ctx* ctx, const float* proj_dev, const uint32_t* entry_offset_dev, int64_t n,
+                                    const uint64_t* num_entries_dev, int64_t capacity,
+                                    const uint32_t* depth_range_dev, uint32_t width, uint32_t height,
+                                    void* scratch_dev, uint32_t* gauss_dev, uint32_t* tile_range_dev,
+                                    uint32_t* overflow_dev);
 
 /* ----------------------------------------------------------------------------------------
  * Compositing forward: rasterize_forward (reference src/rasterize.rs:305-337,
@@ -361,6 +381,7 @@ typedef struct splat_step_info {
   uint64_t num_gaussians;
   uint64_t cloned, split, pruned;
   uint64_t entries;
+  uint32_t replayed; /* not in the reference: 1 when the iteration ran as a replayed CUDA graph */
 } splat_step_info;
 
 /* Fails with SPLAT_ERR_INVALID for zero iterations or sh_degree > 3 (train.rs:169-183). */
@@ -372,6 +393,10 @@ SPLAT_API int splat_trainer_set_model(splat_trainer* t, const float* aos59_host,
 SPLAT_API int splat_trainer_add_view(splat_trainer* t, const splat_camera* cam, const uint8_t* rgb_host);
 /* Reset generator, optimiser state and statistics; SH degree 0 (train.rs:184-189). */
 SPLAT_API int splat_trainer_start(splat_trainer* t);
+/* `iterations` iterations of splat_trainer_step in one call, queued one iteration ahead of
+ * the device (no host wait inside an iteration); `info` describes the last one, with the
+ * densification fields of the last iteration that densified. */
+SPLAT_API int splat_trainer_run(splat_trainer* t, uint32_t iterations, splat_step_info* info);
 SPLAT_API int splat_trainer_step(splat_trainer* t, splat_step_info* info);
 SPLAT_API int64_t splat_trainer_count(const splat_trainer* t);
 SPLAT_API int32_t splat_trainer_sh_degree(const splat_trainer* t);

@@ -82,7 +82,8 @@ class TrainConfig(C.Structure):
                 ("densify_grad_threshold", C.c_float), ("percent_dense", C.c_float), ("min_opacity", C.c_float),
                 ("max_screen_size", C.c_int64), ("absgrad", C.c_int32), ("antialias", C.c_int32),
                 ("white_background", C.c_int32), ("sh_degree", C.c_int32), ("sh_degree_interval", C.c_uint32),
-                ("near_plane", C.c_float), ("seed", C.c_uint64), ("max_gaussians", C.c_uint64)]
+                ("near_plane", C.c_float), ("seed", C.c_uint64), ("max_gaussians", C.c_uint64),
+                ("entry_capacity", C.c_uint64)]
 
     DEFAULTS = dict(iterations=30000, position_lr_init=0.00016, position_lr_final=0.0000016,
                     position_lr_max_steps=30000, feature_lr=0.0025, opacity_lr=0.025, scaling_lr=0.005,
@@ -90,7 +91,7 @@ class TrainConfig(C.Structure):
                     densification_interval=100, opacity_reset_interval=3000, densify_grad_threshold=0.0002,
                     percent_dense=0.01, min_opacity=0.005, max_screen_size=-1, absgrad=0, antialias=0,
                     white_background=0, sh_degree=3, sh_degree_interval=1000, near_plane=0.2, seed=0,
-                    max_gaussians=0)
+                    max_gaussians=0, entry_capacity=0)
 
     @classmethod
     def make(cls, **kw):
@@ -116,7 +117,7 @@ class StepInfo(C.Structure):
     """splat_step_info (reference src/train.rs:142-157)."""
     _fields_ = [("loss", C.c_double), ("psnr", C.c_double), ("view", C.c_uint32), ("densified", C.c_int32),
                 ("reset", C.c_int32), ("num_gaussians", C.c_uint64), ("cloned", C.c_uint64), ("split", C.c_uint64),
-                ("pruned", C.c_uint64), ("entries", C.c_uint64)]
+                ("pruned", C.c_uint64), ("entries", C.c_uint64), ("replayed", C.c_uint32)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
@@ -147,6 +148,9 @@ def _declare(L):
         "splat_bin_count": ([vp, vp, i64, vp, P(i64)], C.c_int),
         "splat_bin_count_noalloc": ([vp, vp, i64, vp, P(i64)], C.c_int),
         "splat_bin_sort": ([vp, vp, vp, i64, i64, vp, u32, u32, vp, vp, vp], C.c_int),
+        "splat_bin_count_device": ([vp, vp, i64, vp, vp], C.c_int),
+        "splat_bin_sort_device_scratch_bytes": ([i64], sz),
+        "splat_bin_sort_device": ([vp, vp, vp, i64, vp, i64, vp, u32, u32, vp, vp, vp, vp], C.c_int),
         "splat_rasterize_fwd": ([vp, vp, vp, vp, u32, u32, P(C.c_float), vp, vp, vp, vp], C.c_int),
         "splat_rasterize_bwd": ([vp, vp, vp, vp, u32, u32, P(C.c_float), vp, vp, vp, vp, i64, vp], C.c_int),
         "splat_project_bwd": ([vp, vp, i64, i64, P(Camera), P(ProjOpts), vp, vp, vp, vp, i32], C.c_int),
@@ -181,6 +185,7 @@ def _declare(L):
         "splat_trainer_add_view": ([vp, P(Camera), vp], C.c_int),
         "splat_trainer_start": ([vp], C.c_int),
         "splat_trainer_step": ([vp, P(StepInfo)], C.c_int),
+        "splat_trainer_run": ([vp, u32, P(StepInfo)], C.c_int),
         "splat_trainer_count": ([vp], i64),
         "splat_trainer_sh_degree": ([vp], i32),
         "splat_trainer_iteration": ([vp], u32),

@@ -29,6 +29,7 @@ Status arena_reserve(Ctx* c, size_t bytes, void** out) {
     }
     a.chunks.push_back(ArenaChunk{p, want});
     a.used = 0;
+    a.generation++;
   }
   *out = static_cast<char*>(a.chunks.back().ptr) + a.used;
   a.used += bytes;
@@ -43,6 +44,7 @@ void arena_reset(Ctx* c) {
     cudaStreamSynchronize(c->stream);
     for (auto& ch : a.chunks) cudaFree(ch.ptr);
     a.chunks.clear();
+    a.generation++;
     void* p = nullptr;
     if (cudaMalloc(&p, total) == cudaSuccess)
       a.chunks.push_back(ArenaChunk{p, total});
@@ -56,6 +58,7 @@ void arena_free(Ctx* c) {
   for (auto& ch : c->arena.chunks) cudaFree(ch.ptr);
   c->arena.chunks.clear();
   c->arena.used = 0;
+  c->arena.generation++;
 }
 
 }  // namespace splat
@@ -272,6 +275,36 @@ SPLAT_API int splat_bin_sort(splat_ctx* ctx, const float* proj_dev, const uint32
   return finish(ctx, launch_bin_sort(&ctx->c, proj_dev, entry_offset_dev, n, num_entries, depth_range_dev, dmin,
                                      num_entries > 0 ? dmax : dmin, width, height, gauss_dev, keys_dev,
                                      tile_range_dev));
+}
+
+SPLAT_API int splat_bin_count_device(splat_ctx* ctx, const uint32_t* num_tiles_dev, int64_t n,
+                                     uint32_t* entry_offset_dev, uint64_t* num_entries_dev) {
+  if (!ctx) return SPLAT_ERR_INVALID;
+  if (n < 0 || !entry_offset_dev || !num_entries_dev || (n && !num_tiles_dev))
+    return invalid(ctx, "splat_bin_count_device: bad buffers");
+  Enter e(ctx);
+  return finish(ctx, launch_scan_u32(&ctx->c, num_tiles_dev, n, entry_offset_dev, 1, num_entries_dev));
+}
+
+SPLAT_API size_t splat_bin_sort_device_scratch_bytes(int64_t capacity) {
+  return capacity < 0 ? 0 : dev_sort_scratch_bytes(capacity);
+}
+
+SPLAT_API int splat_bin_sort_device(splat_ctx* ctx, const float* proj_dev, const uint32_t* entry_offset_dev, int64_t n,
+                                    const uint64_t* num_entries_dev, int64_t capacity,
+                                    const uint32_t* depth_range_dev, uint32_t width, uint32_t height,
+                                    void* scratch_dev, uint32_t* gauss_dev, uint32_t* tile_range_dev,
+                                    uint32_t* overflow_dev) {
+  if (!ctx) return SPLAT_ERR_INVALID;
+  if (width == 0 || height == 0 || width > 65535 || height > 65535)
+    return invalid(ctx, "splat_bin_sort_device: image size must be in 1..65535");
+  if (n < 0 || capacity < 0 || capacity >= 0xffffffffLL || !num_entries_dev || !depth_range_dev || !scratch_dev ||
+      !gauss_dev || !tile_range_dev || !overflow_dev || (n && (!proj_dev || !entry_offset_dev)))
+    return invalid(ctx, "splat_bin_sort_device: bad buffers");
+  Enter e(ctx);
+  return finish(ctx, launch_bin_sort_dev(&ctx->c, proj_dev, entry_offset_dev, n, num_entries_dev, capacity,
+                                         depth_range_dev, width, height, scratch_dev, gauss_dev, tile_range_dev,
+                                         overflow_dev));
 }
 
 SPLAT_API int splat_rasterize_fwd(splat_ctx* ctx, const float* proj_dev, const uint32_t* gauss_dev,

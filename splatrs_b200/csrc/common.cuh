@@ -56,7 +56,8 @@ struct ArenaChunk {
 };
 struct Arena {
   std::vector<ArenaChunk> chunks;
-  size_t used = 0;  // bytes used in the last chunk
+  size_t used = 0;       // bytes used in the last chunk
+  uint64_t generation = 0;  // changes whenever chunks are allocated or freed
 };
 
 // Launch bookkeeping shared by all launchers.

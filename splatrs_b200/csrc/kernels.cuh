@@ -2,14 +2,25 @@
 // context stream.
 #pragma once
 #include "common.cuh"
+#include "adam.cuh"
 
 namespace splat {
+
+// Per-iteration arguments read from device memory, so that a captured training step
+// (a CUDA graph) replays with a new view, camera and Adam step. Kernels given a non-NULL
+// StepParams* use its fields in place of the corresponding by-value arguments.
+struct StepParams {
+  splat_camera cam;
+  AdamArgs adam;
+  const void* target;  // the view's 8-bit pixels
+};
 
 Status launch_params_from_aos(Ctx* c, const float* aos, int64_t n, float* planes, int64_t cap);
 Status launch_params_to_aos(Ctx* c, const float* planes, int64_t n, int64_t cap, float* aos);
 
 Status launch_project_fwd(Ctx* c, const float* planes, int64_t n, int64_t cap, const splat_camera& cam,
-                          const splat_proj_opts& opts, float* proj, uint32_t* num_tiles, uint32_t* depth_range);
+                          const splat_proj_opts& opts, float* proj, uint32_t* num_tiles, uint32_t* depth_range,
+                          const StepParams* sp = nullptr);
 Status launch_proj_from_reference(Ctx* c, const float* p15, int64_t n, uint32_t width, uint32_t height, float* proj,
                                   uint32_t* num_tiles, uint32_t* depth_range);
 Status launch_proj_to_reference(Ctx* c, const float* proj, int64_t n, float* p15);
@@ -18,11 +29,22 @@ Status launch_project_bwd(Ctx* c, const float* planes, int64_t n, int64_t cap, c
                           void* stats, int absgrad);
 
 // project_backward_all fused with Adam::step: parameters updated in place.
+// A nonzero *skip (may be NULL) makes the kernel return without touching anything (a view
+// whose binning overflowed).
 Status launch_project_bwd_adam(Ctx* c, float* planes, float* m, float* v, int64_t n, int64_t cap,
                                const splat_camera& cam, const splat_proj_opts& opts, const float* proj,
-                               const float* pgrad, void* stats, int absgrad, uint64_t step, const splat_lr& lr);
+                               const float* pgrad, void* stats, int absgrad, uint64_t step, const splat_lr& lr,
+                               const uint32_t* skip = nullptr, const StepParams* sp = nullptr);
 
 Status launch_scan_u32(Ctx* c, const uint32_t* in, int64_t n, uint32_t* out, int write_total, uint64_t* total_dev);
+
+// Binning without a host read-back: the entry count (*E_dev, from the entry-offset scan)
+// and the depth range stay on the device; `scratch` holds dev_sort_scratch_bytes(E_cap)
+// bytes. Counts above E_cap set *overflow and leave the view's results invalid.
+size_t dev_sort_scratch_bytes(int64_t E_cap);
+Status launch_bin_sort_dev(Ctx* c, const float* proj, const uint32_t* entry_offset, int64_t n, const uint64_t* E_dev,
+                           int64_t E_cap, const uint32_t* depth_range_dev, uint32_t width, uint32_t height,
+                           void* scratch, uint32_t* gauss_out, uint32_t* ranges, uint32_t* overflow);
 
 // Fills `words` 32-bit words at `dst` with `value` by a kernel on the context stream (in
 // place of cudaMemsetAsync, so the compute stream holds kernels only).
@@ -32,6 +54,8 @@ Status launch_fill_u32(Ctx* c, void* dst, size_t words, uint32_t value);
 // context's mapped host buffer (c->host_small) with a one-warp kernel; the host reads them
 // after synchronising the stream.
 Status launch_publish_u32(Ctx* c, const uint32_t* a, int na, const uint32_t* b, int nb);
+// The same into another mapped host buffer (its device alias `out_dev`).
+Status launch_publish_u32_to(Ctx* c, const uint32_t* a, int na, const uint32_t* b, int nb, void* out_dev);
 Status launch_scan_u32_into(Ctx* c, const uint32_t* in, int64_t n, uint32_t* out, int write_total,
                             uint64_t* partial, uint64_t* total);
 constexpr int kScanValuesPerBlock = 4096;
@@ -49,7 +73,11 @@ Status launch_raster_bwd(Ctx* c, const float* proj, const uint32_t* gauss, const
 Status launch_diag_fast_exp(Ctx* c, float magnitude_lo, float magnitude_hi, int negative, float* out_host);
 
 Status launch_loss(Ctx* c, const float* pred, const void* target, int target_u8, uint32_t width, uint32_t height,
-                   float lambda, float* grad, float* out3);
+                   float lambda, float* grad, float* out3, const StepParams* sp = nullptr);
+
+// Copies `words` 32-bit words (a StepParams) from mapped host memory to device memory with
+// one warp.
+Status launch_load_words(Ctx* c, const void* src_mapped_dev, void* dst, int words);
 
 Status launch_adam(Ctx* c, float* params, const float* grads, float* m, float* v, int64_t n, int64_t cap,
                    uint64_t step, const splat_lr& lr);

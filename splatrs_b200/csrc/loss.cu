@@ -33,9 +33,11 @@ __device__ __forceinline__ float load_target(const void* target, int target_u8, 
 
 // Sums: [0] SSIM, [1] |x - y|, [2] squared clamped error (PSNR).
 __global__ void __launch_bounds__(kLossThreads) ssim_fwd_kernel(const float* __restrict__ pred,
-                                                                const void* __restrict__ target, int target_u8,
+                                                                const void* __restrict__ target_arg, int target_u8,
                                                                 uint32_t width, uint32_t height, LossKernel K,
-                                                                float* __restrict__ dmaps, double* __restrict__ sums) {
+                                                                float* __restrict__ dmaps, double* __restrict__ sums,
+                                                                const StepParams* __restrict__ sp) {
+  const void* target = sp ? sp->target : target_arg;
   __shared__ float sx[kLE][kLE], sy[kLE][kLE];
   __shared__ float h[5][kLE][kLT];
   __shared__ double red[3][kLossThreads / 32];
@@ -146,10 +148,12 @@ __global__ void __launch_bounds__(kLossThreads) ssim_fwd_kernel(const float* __r
 
 // Gradient of the loss w.r.t. the prediction (loss.rs:124-133, :155-169).
 __global__ void __launch_bounds__(kLossThreads) ssim_bwd_kernel(const float* __restrict__ pred,
-                                                                const void* __restrict__ target, int target_u8,
+                                                                const void* __restrict__ target_arg, int target_u8,
                                                                 uint32_t width, uint32_t height, LossKernel K,
                                                                 const float* __restrict__ dmaps, float lambda,
-                                                                float* __restrict__ grad) {
+                                                                float* __restrict__ grad,
+                                                                const StepParams* __restrict__ sp) {
+  const void* target = sp ? sp->target : target_arg;
   __shared__ float sm[3][kLE][kLE];
   __shared__ float h[3][kLE][kLT];
   const int ox0 = blockIdx.x * kLT, oy0 = blockIdx.y * kLT;
@@ -244,7 +248,7 @@ LossKernel make_loss_kernel() {
 }
 
 Status launch_loss(Ctx* c, const float* pred, const void* target, int target_u8, uint32_t width, uint32_t height,
-                   float lambda, float* grad, float* out3) {
+                   float lambda, float* grad, float* out3, const StepParams* sp) {
   const size_t npix3 = (size_t)width * height * 3;
   float* dmaps = nullptr;
   double* sums = nullptr;
@@ -253,9 +257,9 @@ Status launch_loss(Ctx* c, const float* pred, const void* target, int target_u8,
   SPLAT_TRY(launch_fill_u32(c, sums, 3 * 2, 0u));
   const LossKernel K = make_loss_kernel();
   const dim3 grid(ceil_div(width, kLT), ceil_div(height, kLT));
-  ssim_fwd_kernel<<<grid, kLossThreads, 0, c->stream>>>(pred, target, target_u8, width, height, K, dmaps, sums);
+  ssim_fwd_kernel<<<grid, kLossThreads, 0, c->stream>>>(pred, target, target_u8, width, height, K, dmaps, sums, sp);
   ssim_bwd_kernel<<<grid, kLossThreads, 0, c->stream>>>(pred, target, target_u8, width, height, K, dmaps, lambda,
-                                                         grad);
+                                                         grad, sp);
   loss_finalize_kernel<<<1, 1, 0, c->stream>>>(sums, npix3, lambda, out3);
   c->launches.count += 3;
   SPLAT_LAUNCHED("loss kernels");

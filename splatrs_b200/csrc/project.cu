@@ -422,9 +422,11 @@ __device__ __forceinline__ void depth_range_update(uint32_t* depth_range, bool v
 // project_one (project.rs:277-317) for every Gaussian.
 template <int DEG>
 __global__ void __launch_bounds__(256) project_fwd_kernel(const float4* __restrict__ planes, int64_t n, int64_t cap,
-                                                          splat_camera cam, splat_proj_opts opts,
+                                                          splat_camera cam_arg, splat_proj_opts opts,
                                                           float4* __restrict__ rec, uint32_t* __restrict__ num_tiles,
-                                                          uint32_t* __restrict__ depth_range) {
+                                                          uint32_t* __restrict__ depth_range,
+                                                          const StepParams* __restrict__ sp) {
+  const splat_camera cam = sp ? sp->cam : cam_arg;
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   bool visible = false;
   float depth = 0.0f;
@@ -519,16 +521,20 @@ __global__ void proj_to_reference_kernel(const float4* __restrict__ rec, int64_t
 // and v, over every plane (zero gradients still decay the moments, adam.rs:56-60).
 template <int DEG, bool ADAM>
 __global__ void __launch_bounds__(128) project_bwd_kernel(const float4* __restrict__ planes, int64_t n, int64_t cap,
-                                                          splat_camera cam, splat_proj_opts opts,
+                                                          splat_camera cam_arg, splat_proj_opts opts,
                                                           const float4* __restrict__ rec,
                                                           const float4* __restrict__ pgrad,
                                                           float4* __restrict__ out, float* __restrict__ stat_accum,
                                                           uint32_t* __restrict__ stat_denom,
                                                           uint32_t* __restrict__ stat_maxr, int absgrad,
                                                           float4* __restrict__ adam_m, float4* __restrict__ adam_v,
-                                                          AdamArgs adam) {
+                                                          AdamArgs adam_arg, const uint32_t* __restrict__ skip,
+                                                          const StepParams* __restrict__ sp) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
+  if (ADAM && skip && *skip) return;
+  const splat_camera cam = sp ? sp->cam : cam_arg;
+  const AdamArgs adam = (ADAM && sp) ? sp->adam : adam_arg;
   const float4 g0 = pgrad[i], g1 = pgrad[cap + i], g2 = pgrad[2 * cap + i];
   // ProjGrad fields.
   const float dp_mean2d[2] = {g0.x, g0.y};
@@ -796,7 +802,8 @@ __global__ void __launch_bounds__(kConvG) planes_to_aos_kernel(const float4* __r
 // Launchers
 // ---------------------------------------------------------------------------------------
 Status launch_project_fwd(Ctx* c, const float* planes, int64_t n, int64_t cap, const splat_camera& cam,
-                          const splat_proj_opts& opts, float* proj, uint32_t* num_tiles, uint32_t* depth_range) {
+                          const splat_proj_opts& opts, float* proj, uint32_t* num_tiles, uint32_t* depth_range,
+                          const StepParams* sp) {
   SPLAT_TRY(launch_fill_u32(c, depth_range, 1, 0xffffffffu));
   SPLAT_TRY(launch_fill_u32(c, depth_range + 1, 1, 0u));
   if (n == 0) return Status::ok();
@@ -805,10 +812,10 @@ Status launch_project_fwd(Ctx* c, const float* planes, int64_t n, int64_t cap, c
   const float4* p = reinterpret_cast<const float4*>(planes);
   float4* r = reinterpret_cast<float4*>(proj);
   switch (opts.sh_degree) {
-    case 0: project_fwd_kernel<0><<<grid, bs, 0, c->stream>>>(p, n, cap, cam, opts, r, num_tiles, depth_range); break;
-    case 1: project_fwd_kernel<1><<<grid, bs, 0, c->stream>>>(p, n, cap, cam, opts, r, num_tiles, depth_range); break;
-    case 2: project_fwd_kernel<2><<<grid, bs, 0, c->stream>>>(p, n, cap, cam, opts, r, num_tiles, depth_range); break;
-    default: project_fwd_kernel<3><<<grid, bs, 0, c->stream>>>(p, n, cap, cam, opts, r, num_tiles, depth_range); break;
+    case 0: project_fwd_kernel<0><<<grid, bs, 0, c->stream>>>(p, n, cap, cam, opts, r, num_tiles, depth_range, sp); break;
+    case 1: project_fwd_kernel<1><<<grid, bs, 0, c->stream>>>(p, n, cap, cam, opts, r, num_tiles, depth_range, sp); break;
+    case 2: project_fwd_kernel<2><<<grid, bs, 0, c->stream>>>(p, n, cap, cam, opts, r, num_tiles, depth_range, sp); break;
+    default: project_fwd_kernel<3><<<grid, bs, 0, c->stream>>>(p, n, cap, cam, opts, r, num_tiles, depth_range, sp); break;
   }
   c->launches.count++;
   SPLAT_LAUNCHED("project_fwd_kernel");
@@ -839,7 +846,8 @@ Status launch_proj_to_reference(Ctx* c, const float* proj, int64_t n, float* p15
 template <bool ADAM>
 static Status project_bwd_dispatch(Ctx* c, const float* planes, int64_t n, int64_t cap, const splat_camera& cam,
                                    const splat_proj_opts& opts, const float* proj, const float* pgrad, float* out,
-                                   void* stats, int absgrad, float* m, float* v, const AdamArgs& adam) {
+                                   void* stats, int absgrad, float* m, float* v, const AdamArgs& adam,
+                                   const uint32_t* skip, const StepParams* sp) {
   if (n == 0) return Status::ok();
   const int bs = 128;
   const uint32_t grid = ceil_div(n, bs);
@@ -857,10 +865,10 @@ static Status project_bwd_dispatch(Ctx* c, const float* planes, int64_t n, int64
     sm = sd + cap;
   }
   switch (opts.sh_degree) {
-    case 0: project_bwd_kernel<0, ADAM><<<grid, bs, 0, c->stream>>>(p, n, cap, cam, opts, r, pg, o, sa, sd, sm, absgrad, am, av, adam); break;
-    case 1: project_bwd_kernel<1, ADAM><<<grid, bs, 0, c->stream>>>(p, n, cap, cam, opts, r, pg, o, sa, sd, sm, absgrad, am, av, adam); break;
-    case 2: project_bwd_kernel<2, ADAM><<<grid, bs, 0, c->stream>>>(p, n, cap, cam, opts, r, pg, o, sa, sd, sm, absgrad, am, av, adam); break;
-    default: project_bwd_kernel<3, ADAM><<<grid, bs, 0, c->stream>>>(p, n, cap, cam, opts, r, pg, o, sa, sd, sm, absgrad, am, av, adam); break;
+    case 0: project_bwd_kernel<0, ADAM><<<grid, bs, 0, c->stream>>>(p, n, cap, cam, opts, r, pg, o, sa, sd, sm, absgrad, am, av, adam, skip, sp); break;
+    case 1: project_bwd_kernel<1, ADAM><<<grid, bs, 0, c->stream>>>(p, n, cap, cam, opts, r, pg, o, sa, sd, sm, absgrad, am, av, adam, skip, sp); break;
+    case 2: project_bwd_kernel<2, ADAM><<<grid, bs, 0, c->stream>>>(p, n, cap, cam, opts, r, pg, o, sa, sd, sm, absgrad, am, av, adam, skip, sp); break;
+    default: project_bwd_kernel<3, ADAM><<<grid, bs, 0, c->stream>>>(p, n, cap, cam, opts, r, pg, o, sa, sd, sm, absgrad, am, av, adam, skip, sp); break;
   }
   c->launches.count++;
   SPLAT_LAUNCHED("project_bwd_kernel");
@@ -871,14 +879,15 @@ Status launch_project_bwd(Ctx* c, const float* planes, int64_t n, int64_t cap, c
                           const splat_proj_opts& opts, const float* proj, const float* pgrad, float* out,
                           void* stats, int absgrad) {
   return project_bwd_dispatch<false>(c, planes, n, cap, cam, opts, proj, pgrad, out, stats, absgrad, nullptr, nullptr,
-                                     AdamArgs());
+                                     AdamArgs(), nullptr, nullptr);
 }
 
 Status launch_project_bwd_adam(Ctx* c, float* planes, float* m, float* v, int64_t n, int64_t cap,
                                const splat_camera& cam, const splat_proj_opts& opts, const float* proj,
-                               const float* pgrad, void* stats, int absgrad, uint64_t step, const splat_lr& lr) {
+                               const float* pgrad, void* stats, int absgrad, uint64_t step, const splat_lr& lr,
+                               const uint32_t* skip, const StepParams* sp) {
   return project_bwd_dispatch<true>(c, planes, n, cap, cam, opts, proj, pgrad, nullptr, stats, absgrad, m, v,
-                                    make_adam_args(step, lr));
+                                    make_adam_args(step, lr), skip, sp);
 }
 
 Status launch_params_from_aos(Ctx* c, const float* aos, int64_t n, float* planes, int64_t cap) {

@@ -53,8 +53,32 @@ Status ViewBuffers::ensure(int64_t n, uint32_t width, uint32_t height) {
 
 void ViewBuffers::release() {
   for (DevBuf* b : {&proj, &num_tiles, &entry_offset, &depth_range, &tile_range, &gauss, &image, &final_t, &n_contrib,
-                    &dimage, &pairs})
+                    &dimage, &pairs, &sort_scratch, &scan_partial, &counters})
     b->release();
+}
+
+Status render_view_dev(Ctx* c, const float* planes, int64_t n, int64_t cap, const splat_camera& cam,
+                       const splat_proj_opts& opts, const float bg[3], ViewBuffers& v, const StepParams* sp) {
+  SPLAT_TRY(v.ensure(n, cam.width, cam.height));
+  const int64_t e_cap = std::max<int64_t>(v.e_cap, 1);
+  SPLAT_TRY(v.gauss.ensure((size_t)e_cap * 4));
+  SPLAT_TRY(v.sort_scratch.ensure(dev_sort_scratch_bytes(e_cap)));
+  SPLAT_TRY(v.scan_partial.ensure(((size_t)std::max<int64_t>(n, 1) / kScanValuesPerBlock + 2) * 8));
+  if (v.counters.bytes == 0) {
+    SPLAT_TRY(v.counters.ensure(64));
+    SPLAT_TRY(launch_fill_u32(c, v.counters.ptr, 16, 0u));
+  }
+  float* proj = v.proj.as<float>();
+  uint32_t* nt = v.num_tiles.as<uint32_t>();
+  uint32_t* dr = v.depth_range.as<uint32_t>();
+  SPLAT_TRY(launch_project_fwd(c, planes, n, cap, cam, opts, proj, nt, dr, sp));
+  SPLAT_TRY(launch_scan_u32_into(c, nt, n, v.entry_offset.as<uint32_t>(), 1, v.scan_partial.as<uint64_t>(),
+                                 v.entry_count()));
+  SPLAT_TRY(launch_bin_sort_dev(c, proj, v.entry_offset.as<uint32_t>(), n, v.entry_count(), e_cap, dr, cam.width,
+                                cam.height, v.sort_scratch.ptr, v.gauss.as<uint32_t>(), v.tile_range.as<uint32_t>(),
+                                v.overflow_flag()));
+  return launch_raster_fwd(c, proj, v.gauss.as<uint32_t>(), v.tile_range.as<uint32_t>(), cam.width, cam.height, bg,
+                           v.image.as<float>(), v.final_t.as<float>(), v.n_contrib.as<uint32_t>(), nullptr);
 }
 
 // Projection, binning and forward compositing of one view into `v`.

@@ -10,6 +10,8 @@
 // of keys, so the sort runs over ceil((tile bits + depth bits) / 8) passes instead of 8.
 // The sort is stable, and entries enter it in entry order, which reproduces the
 // reference's tie-break on the entry index.
+#include <atomic>
+
 #include "common.cuh"
 #include "kernels.cuh"
 
@@ -154,9 +156,25 @@ __global__ void publish_u32_kernel(const uint32_t* __restrict__ a, int na, const
   __threadfence_system();
 }
 
+__global__ void load_words_kernel(const volatile uint32_t* src, uint32_t* __restrict__ dst, int words) {
+  for (int i = threadIdx.x; i < words; i += 32) dst[i] = src[i];
+}
+
+Status launch_load_words(Ctx* c, const void* src_mapped_dev, void* dst, int words) {
+  load_words_kernel<<<1, 32, 0, c->stream>>>(static_cast<const volatile uint32_t*>(src_mapped_dev),
+                                             static_cast<uint32_t*>(dst), words);
+  c->launches.count++;
+  SPLAT_LAUNCHED("load_words_kernel");
+  return Status::ok();
+}
+
 Status launch_publish_u32(Ctx* c, const uint32_t* a, int na, const uint32_t* b, int nb) {
+  return launch_publish_u32_to(c, a, na, b, nb, c->host_small_dev);
+}
+
+Status launch_publish_u32_to(Ctx* c, const uint32_t* a, int na, const uint32_t* b, int nb, void* out_dev) {
   if (na < 0 || nb < 0 || na + nb > 32) return Status::make(SPLAT_ERR_INVALID, "publish: at most 32 words");
-  publish_u32_kernel<<<1, 32, 0, c->stream>>>(a, na, b, nb, reinterpret_cast<volatile uint32_t*>(c->host_small_dev));
+  publish_u32_kernel<<<1, 32, 0, c->stream>>>(a, na, b, nb, reinterpret_cast<volatile uint32_t*>(out_dev));
   c->launches.count++;
   SPLAT_LAUNCHED("publish_u32_kernel");
   return Status::ok();
@@ -180,10 +198,10 @@ Status launch_scan_u32(Ctx* c, const uint32_t* in, int64_t n, uint32_t* out, int
 // Each warp takes 32 consecutive Gaussians and writes their entries contiguously.
 // ---------------------------------------------------------------------------------------
 template <typename K>
-__global__ void __launch_bounds__(256) emit_keys_kernel(const float4* __restrict__ rec,
-                                                        const uint32_t* __restrict__ entry_offset, int64_t n,
-                                                        uint32_t tiles_x, const uint32_t* __restrict__ depth_range,
-                                                        int dbits, K* __restrict__ keys, uint32_t* __restrict__ vals) {
+__device__ __forceinline__ void emit_keys_body(const float4* __restrict__ rec, const uint32_t* __restrict__ entry_offset,
+                                               int64_t n, uint32_t tiles_x, const uint32_t* __restrict__ depth_range,
+                                               int dbits, int64_t limit, K* __restrict__ keys,
+                                               uint32_t* __restrict__ vals) {
   const int lane = threadIdx.x & 31;
   const int64_t warp_id = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t g = warp_id * 32 + lane;
@@ -226,7 +244,7 @@ __global__ void __launch_bounds__(256) emit_keys_kernel(const float4* __restrict
     const uint32_t o_ty0 = __shfl_sync(0xffffffffu, ty0, lo);
     const uint32_t o_w = __shfl_sync(0xffffffffu, w, lo);
     const uint32_t o_dkey = __shfl_sync(0xffffffffu, dkey, lo);
-    if (j < total) {
+    if (j < total && (int64_t)start + j < limit) {
       const uint32_t local = j - (o_incl - o_cnt);
       const uint32_t ty = o_ty0 + local / o_w;
       const uint32_t tx = o_tx0 + local % o_w;
@@ -235,6 +253,14 @@ __global__ void __launch_bounds__(256) emit_keys_kernel(const float4* __restrict
       vals[start + j] = (uint32_t)(first + lo);
     }
   }
+}
+
+template <typename K>
+__global__ void __launch_bounds__(256) emit_keys_kernel(const float4* __restrict__ rec,
+                                                        const uint32_t* __restrict__ entry_offset, int64_t n,
+                                                        uint32_t tiles_x, const uint32_t* __restrict__ depth_range,
+                                                        int dbits, K* __restrict__ keys, uint32_t* __restrict__ vals) {
+  emit_keys_body<K>(rec, entry_offset, n, tiles_x, depth_range, dbits, INT64_MAX, keys, vals);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -249,9 +275,8 @@ constexpr int kSortRounds = 16;
 constexpr int kSortTile = kSortThreads * kSortRounds;  // 4096
 
 template <typename K>
-__global__ void __launch_bounds__(kSortThreads) radix_upsweep_kernel(const K* __restrict__ keys, int64_t n, int shift,
-                                                                     uint32_t* __restrict__ hist, uint32_t nblocks) {
-  __shared__ uint32_t cnt[256];
+__device__ __forceinline__ void upsweep_body(const K* __restrict__ keys, int64_t n, int shift,
+                                             uint32_t* __restrict__ hist, uint32_t nblocks, uint32_t* cnt) {
   cnt[threadIdx.x] = 0;
   __syncthreads();
   const int64_t base = (int64_t)blockIdx.x * kSortTile;
@@ -269,6 +294,13 @@ __global__ void __launch_bounds__(kSortThreads) radix_upsweep_kernel(const K* __
   hist[(int64_t)threadIdx.x * nblocks + blockIdx.x] = cnt[threadIdx.x];
 }
 
+template <typename K>
+__global__ void __launch_bounds__(kSortThreads) radix_upsweep_kernel(const K* __restrict__ keys, int64_t n, int shift,
+                                                                     uint32_t* __restrict__ hist, uint32_t nblocks) {
+  __shared__ uint32_t cnt[256];
+  upsweep_body<K>(keys, n, shift, hist, nblocks, cnt);
+}
+
 // Dynamic shared memory of the downsweep: the block's keys and values reordered by digit,
 // the per-warp digit counters and the block's digit starts.
 template <typename K> constexpr size_t downsweep_smem() {
@@ -276,12 +308,10 @@ template <typename K> constexpr size_t downsweep_smem() {
 }
 
 template <typename K>
-__global__ void __launch_bounds__(kSortThreads) radix_downsweep_kernel(const K* __restrict__ keys_in,
-                                                                       const uint32_t* __restrict__ vals_in, int64_t n,
-                                                                       int shift, const uint32_t* __restrict__ offsets,
-                                                                       uint32_t nblocks, K* __restrict__ keys_out,
-                                                                       uint32_t* __restrict__ vals_out) {
-  extern __shared__ __align__(16) unsigned char dsm[];
+__device__ __forceinline__ void downsweep_body(const K* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
+                                               int64_t n, int shift, const uint32_t* __restrict__ offsets,
+                                               uint32_t nblocks, K* __restrict__ keys_out,
+                                               uint32_t* __restrict__ vals_out, unsigned char* dsm) {
   K* sk = reinterpret_cast<K*>(dsm);
   uint32_t* sv = reinterpret_cast<uint32_t*>(sk + kSortTile);
   uint32_t(*wcnt)[256] = reinterpret_cast<uint32_t(*)[256]>(sv + kSortTile);
@@ -354,6 +384,16 @@ __global__ void __launch_bounds__(kSortThreads) radix_downsweep_kernel(const K* 
     keys_out[pos] = key;
     vals_out[pos] = sv[i];
   }
+}
+
+template <typename K>
+__global__ void __launch_bounds__(kSortThreads) radix_downsweep_kernel(const K* __restrict__ keys_in,
+                                                                       const uint32_t* __restrict__ vals_in, int64_t n,
+                                                                       int shift, const uint32_t* __restrict__ offsets,
+                                                                       uint32_t nblocks, K* __restrict__ keys_out,
+                                                                       uint32_t* __restrict__ vals_out) {
+  extern __shared__ __align__(16) unsigned char dsm[];
+  downsweep_body<K>(keys_in, vals_in, n, shift, offsets, nblocks, keys_out, vals_out, dsm);
 }
 
 // Tile ranges (rasterize.rs:108-119) and, optionally, the reference 64-bit keys.
@@ -441,6 +481,147 @@ Status launch_bin_sort(Ctx* c, const float* proj, const uint32_t* entry_offset, 
                                     gauss_out, keys_out, ranges);
   return sort_and_range<uint64_t>(c, proj, entry_offset, n, E, depth_range_dev, dbits, total, tiles_x, num_tiles,
                                   gauss_out, keys_out, ranges);
+}
+
+// ---------------------------------------------------------------------------------------
+// Device-driven binning: the entry count and the depth range stay in device memory, so the
+// host never waits for them. Grids and buffers are sized for a capacity E_cap; every
+// kernel reads the count (clamped to E_cap) and the key width from device memory, skips
+// passes the keys do not need, and the last needed pass writes the caller's buffer. An
+// entry count above E_cap sets *overflow (sticky) and sorts only the first E_cap entries;
+// the caller must discard that view's results. Keys are the compacted keys of
+// launch_bin_sort held in 64 bits, and the passes are the same, so the output equals it.
+// ---------------------------------------------------------------------------------------
+struct DevSortPlan {
+  int64_t E;
+  int dbits;
+  int passes;
+};
+
+__device__ __forceinline__ DevSortPlan dev_sort_plan(const uint64_t* __restrict__ E_dev, int64_t E_cap,
+                                                     const uint32_t* __restrict__ dr, int tbits) {
+  DevSortPlan p;
+  const uint64_t e = *E_dev;
+  p.E = e < (uint64_t)E_cap ? (int64_t)e : E_cap;
+  const uint32_t span = p.E > 0 ? dr[1] - dr[0] : 0u;
+  p.dbits = span == 0 ? 0 : 32 - __clz(span);
+  const int total = p.dbits + tbits;
+  p.passes = total == 0 ? 1 : (total + 7) / 8;
+  return p;
+}
+
+__global__ void __launch_bounds__(256) emit_keys_dev_kernel(const float4* __restrict__ rec,
+                                                            const uint32_t* __restrict__ entry_offset, int64_t n,
+                                                            uint32_t tiles_x, const uint32_t* __restrict__ depth_range,
+                                                            const uint64_t* __restrict__ E_dev, int64_t E_cap, int tbits,
+                                                            uint64_t* __restrict__ keys, uint32_t* __restrict__ vals,
+                                                            uint32_t* __restrict__ overflow) {
+  const DevSortPlan p = dev_sort_plan(E_dev, E_cap, depth_range, tbits);
+  if (blockIdx.x == 0 && threadIdx.x == 0 && *E_dev > (uint64_t)E_cap) atomicOr(overflow, 1u);
+  emit_keys_body<uint64_t>(rec, entry_offset, n, tiles_x, depth_range, p.dbits, E_cap, keys, vals);
+}
+
+__global__ void __launch_bounds__(kSortThreads) radix_upsweep_dev_kernel(const uint64_t* __restrict__ ka,
+                                                                         const uint64_t* __restrict__ kb,
+                                                                         const uint64_t* __restrict__ E_dev,
+                                                                         int64_t E_cap,
+                                                                         const uint32_t* __restrict__ dr, int tbits,
+                                                                         int pass, uint32_t* __restrict__ hist,
+                                                                         uint32_t nblocks) {
+  __shared__ uint32_t cnt[256];
+  const DevSortPlan p = dev_sort_plan(E_dev, E_cap, dr, tbits);
+  if (pass >= p.passes) return;
+  upsweep_body<uint64_t>((pass & 1) ? kb : ka, p.E, 8 * pass, hist, nblocks, cnt);
+}
+
+__global__ void __launch_bounds__(kSortThreads) radix_downsweep_dev_kernel(
+    uint64_t* __restrict__ ka, uint64_t* __restrict__ kb, uint32_t* __restrict__ va, uint32_t* __restrict__ vb,
+    const uint64_t* __restrict__ E_dev, int64_t E_cap, const uint32_t* __restrict__ dr, int tbits, int pass,
+    const uint32_t* __restrict__ offsets, uint32_t nblocks, uint32_t* __restrict__ vals_final) {
+  extern __shared__ __align__(16) unsigned char dsm[];
+  const DevSortPlan p = dev_sort_plan(E_dev, E_cap, dr, tbits);
+  if (pass >= p.passes) return;
+  const bool odd = pass & 1;
+  uint32_t* vout = pass == p.passes - 1 ? vals_final : (odd ? va : vb);
+  downsweep_body<uint64_t>(odd ? kb : ka, odd ? vb : va, p.E, 8 * pass, offsets, nblocks, odd ? ka : kb, vout, dsm);
+}
+
+__global__ void tile_ranges_dev_kernel(const uint64_t* __restrict__ ka, const uint64_t* __restrict__ kb,
+                                       const uint64_t* __restrict__ E_dev, int64_t E_cap,
+                                       const uint32_t* __restrict__ dr, int tbits, uint32_t* __restrict__ ranges) {
+  const DevSortPlan p = dev_sort_plan(E_dev, E_cap, dr, tbits);
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= p.E) return;
+  const uint64_t* keys = ((p.passes - 1) & 1) ? ka : kb;  // written by the last pass
+  const uint64_t tile = keys[i] >> p.dbits;
+  if (i == 0 || (keys[i - 1] >> p.dbits) != tile) ranges[2 * tile] = (uint32_t)i;
+  if (i == p.E - 1 || (keys[i + 1] >> p.dbits) != tile) ranges[2 * tile + 1] = (uint32_t)(i + 1);
+}
+
+size_t dev_sort_scratch_bytes(int64_t E_cap) {
+  const uint64_t cap = (uint64_t)std::max<int64_t>(E_cap, 1);
+  const uint64_t nblocks = ceil_div(cap, kSortTile);
+  const uint64_t scan_blocks = ceil_div(nblocks * 256, kScanTile);
+  return 2 * cap * 8 + 2 * cap * 4 + 2 * nblocks * 256 * 4 + scan_blocks * 8 + 8 + 8 * 256;  // 8 pieces, 256-aligned
+}
+
+Status launch_bin_sort_dev(Ctx* c, const float* proj, const uint32_t* entry_offset, int64_t n, const uint64_t* E_dev,
+                           int64_t E_cap, const uint32_t* depth_range_dev, uint32_t width, uint32_t height,
+                           void* scratch, uint32_t* gauss_out, uint32_t* ranges, uint32_t* overflow) {
+  const uint32_t tiles_x = (width + kTile - 1) / kTile, tiles_y = (height + kTile - 1) / kTile;
+  const uint32_t num_tiles = tiles_x * tiles_y;
+  const int tbits = num_tiles <= 1 ? 0 : 32 - __builtin_clz(num_tiles - 1);
+  const int max_passes = (tbits + 32 + 7) / 8;
+  const uint64_t cap = (uint64_t)std::max<int64_t>(E_cap, 1);
+  const uint32_t nblocks = ceil_div(cap, kSortTile);
+  const uint64_t scan_blocks = ceil_div((uint64_t)nblocks * 256, kScanTile);
+  // Carve the scratch (256-byte aligned pieces).
+  auto carve = [&](size_t bytes) {
+    void* p = scratch;
+    scratch = static_cast<char*>(scratch) + ((bytes + 255) & ~(size_t)255);
+    return p;
+  };
+  uint64_t* ka = static_cast<uint64_t*>(carve(cap * 8));
+  uint64_t* kb = static_cast<uint64_t*>(carve(cap * 8));
+  uint32_t* va = static_cast<uint32_t*>(carve(cap * 4));
+  uint32_t* vb = static_cast<uint32_t*>(carve(cap * 4));
+  uint32_t* hist = static_cast<uint32_t*>(carve((size_t)nblocks * 256 * 4));
+  uint32_t* offs = static_cast<uint32_t*>(carve((size_t)nblocks * 256 * 4));
+  uint64_t* partial = static_cast<uint64_t*>(carve(scan_blocks * 8));
+  uint64_t* tot = static_cast<uint64_t*>(carve(8));
+  // Once per device (and never inside a stream capture after the first call).
+  static std::atomic<uint64_t> attr_done{0};
+  if (c->device < 64 && !(attr_done.load() & (1ull << c->device))) {
+    SPLAT_CUDA(cudaFuncSetAttribute(radix_downsweep_dev_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)downsweep_smem<uint64_t>()));
+    attr_done.fetch_or(1ull << c->device);
+  } else if (c->device >= 64) {
+    SPLAT_CUDA(cudaFuncSetAttribute(radix_downsweep_dev_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)downsweep_smem<uint64_t>()));
+  }
+  SPLAT_TRY(launch_fill_u32(c, ranges, (size_t)num_tiles * 2, 0u));
+  if (n > 0) {
+    const uint32_t warps = ceil_div(n, 32);
+    emit_keys_dev_kernel<<<ceil_div((uint64_t)warps * 32, 256), 256, 0, c->stream>>>(
+        reinterpret_cast<const float4*>(proj), entry_offset, n, tiles_x, depth_range_dev, E_dev, E_cap, tbits, ka, va,
+        overflow);
+    c->launches.count++;
+    SPLAT_LAUNCHED("emit_keys_dev_kernel");
+  }
+  for (int pass = 0; pass < max_passes; pass++) {
+    radix_upsweep_dev_kernel<<<nblocks, kSortThreads, 0, c->stream>>>(ka, kb, E_dev, E_cap, depth_range_dev, tbits,
+                                                                       pass, hist, nblocks);
+    SPLAT_TRY(launch_scan_u32_into(c, hist, (int64_t)nblocks * 256, offs, 0, partial, tot));
+    radix_downsweep_dev_kernel<<<nblocks, kSortThreads, downsweep_smem<uint64_t>(), c->stream>>>(
+        ka, kb, va, vb, E_dev, E_cap, depth_range_dev, tbits, pass, offs, nblocks, gauss_out);
+    c->launches.count += 2;
+    SPLAT_LAUNCHED("radix sort pass (device-driven)");
+  }
+  tile_ranges_dev_kernel<<<ceil_div(cap, 256), 256, 0, c->stream>>>(ka, kb, E_dev, E_cap, depth_range_dev, tbits,
+                                                                     ranges);
+  c->launches.count++;
+  SPLAT_LAUNCHED("tile_ranges_dev_kernel");
+  return Status::ok();
 }
 
 }  // namespace splat

@@ -82,7 +82,25 @@ struct splat_trainer {
   std::vector<uint32_t> order;
   uint32_t iteration = 0;
   uint64_t adam_step = 0;
-  float* loss_host = nullptr;  // pinned
+  // Mapped pinned read-back slots, one per iteration in flight: loss, ssim, psnr (f32),
+  // entry count (u64), overflow flag; written by a kernel at the end of an iteration.
+  uint32_t* slots_host = nullptr;
+  void* slots_dev = nullptr;
+  cudaEvent_t slot_done[2] = {nullptr, nullptr};
+  // Per-iteration arguments: one mapped host slot per iteration in flight, loaded into
+  // params_dev by the iteration's first kernel.
+  StepParams* params_host = nullptr;
+  void* params_host_dev = nullptr;
+  DevBuf params_dev;
+  // The iteration captured as a CUDA graph, one per read-back slot, and the state it was
+  // captured for (sizes, SH degree, buffer addresses); a change of state re-captures.
+  cudaStream_t cap_stream = nullptr;
+  cudaGraphExec_t exec[2] = {nullptr, nullptr};
+  std::vector<uint64_t> gkey;
+  int g_uses = 0;           // uncaptured iterations run with the current key
+  uint64_t g_launches = 0;  // kernels in one captured iteration
+  bool graphs = true;       // false after a failed capture: plain launches from then on
+  bool last_replayed = false;
 };
 
 namespace {
@@ -132,21 +150,76 @@ Status reset_stats(splat_trainer* t) {
   return launch_fill_u32(t->c, t->stats.ptr, t->stats.bytes / 4, 0u);
 }
 
-Status step(splat_trainer* t, splat_step_info* info) {
-  Ctx* c = t->c;
+// The host side of one iteration (train.rs:196-247): its number, view, SH degree,
+// learning rates, Adam step and what density control runs after it.
+struct IterPlan {
+  uint32_t it = 0, view = 0;
+  int sh_degree = 0;
+  splat_lr lr{};
+  uint64_t adam_step = 0;
+  bool densify_window = false, densify_now = false, reset_now = false;
+};
+
+IterPlan schedule(splat_trainer* t) {
   const splat_train_config& cfg = t->cfg;
+  IterPlan p;
   t->iteration += 1;
-  const uint32_t it = t->iteration;
-  if (cfg.sh_degree_interval > 0 && it % cfg.sh_degree_interval == 0 && t->sh_degree < cfg.sh_degree) t->sh_degree++;
+  p.it = t->iteration;
+  if (cfg.sh_degree_interval > 0 && p.it % cfg.sh_degree_interval == 0 && t->sh_degree < cfg.sh_degree) t->sh_degree++;
+  p.sh_degree = t->sh_degree;
   if (t->order.empty()) {
     const uint32_t nv = (uint32_t)t->views.size();
     t->order.resize(nv);
     for (uint32_t i = 0; i < nv; i++) t->order[i] = i;
     for (uint32_t i = nv; i-- > 1;) std::swap(t->order[i], t->order[t->rng.index(i + 1)]);
   }
-  const uint32_t vi = t->order.back();
+  p.view = t->order.back();
   t->order.pop_back();
-  View& view = *t->views[vi];
+  p.lr.mean = position_lr(cfg, p.it, t->extent);
+  p.lr.log_scale = cfg.scaling_lr;
+  p.lr.quat = cfg.rotation_lr;
+  p.lr.opacity = cfg.opacity_lr;
+  p.lr.sh_dc = cfg.feature_lr;
+  p.lr.sh_rest = cfg.feature_lr / 20.0f;
+  t->adam_step += 1;
+  p.adam_step = t->adam_step;
+  p.densify_window = cfg.densify && p.it < cfg.densify_until_iter;
+  p.densify_now = p.densify_window && p.it > cfg.densify_from_iter && p.it % cfg.densification_interval == 0;
+  p.reset_now = p.densify_window && cfg.opacity_reset_interval > 0 &&
+                (p.it % cfg.opacity_reset_interval == 0 || (cfg.white_background && p.it == cfg.densify_from_iter));
+  return p;
+}
+
+std::vector<uint64_t> graph_key(splat_trainer* t, const IterPlan& p) {
+  const splat_camera& cam = t->views[p.view]->cam;
+  std::vector<uint64_t> k = {(uint64_t)t->n, (uint64_t)t->cur.cap, (uint64_t)t->vb.e_cap, (uint64_t)p.sh_degree,
+                             (uint64_t)p.densify_window, cam.width, cam.height, t->c->arena.generation,
+                             (uint64_t)t->stats_cap};
+  for (const DevBuf* b : {&t->cur.params, &t->cur.m, &t->cur.v, &t->stats, &t->pgrad, &t->pred_grad, &t->loss_out,
+                          &t->params_dev, &t->vb.proj, &t->vb.num_tiles, &t->vb.entry_offset, &t->vb.depth_range,
+                          &t->vb.tile_range, &t->vb.gauss, &t->vb.image, &t->vb.final_t, &t->vb.n_contrib,
+                          &t->vb.sort_scratch, &t->vb.scan_partial, &t->vb.counters})
+    k.push_back((uint64_t)(uintptr_t)b->ptr);
+  return k;
+}
+
+void drop_graphs(splat_trainer* t) {
+  for (cudaGraphExec_t& e : t->exec)
+    if (e) {
+      cudaGraphExecDestroy(e);
+      e = nullptr;
+    }
+}
+
+// The kernels of one iteration (train.rs:212-246): forward with device-driven binning,
+// loss, backward, and the projection backward fused with Adam, which does nothing if the
+// binning overflowed; then the read-back kernel for slot `slot`. The camera, Adam step and
+// target view come from params_dev (loaded first from the slot's host parameters), so a
+// captured copy replays for any view of the same size.
+Status body(splat_trainer* t, const IterPlan& p, int slot) {
+  Ctx* c = t->c;
+  const splat_train_config& cfg = t->cfg;
+  View& view = *t->views[p.view];
   const splat_camera& cam = view.cam;
   const float bgv = cfg.white_background ? 1.0f : 0.0f;
   const float bg[3] = {bgv, bgv, bgv};
@@ -154,106 +227,279 @@ Status step(splat_trainer* t, splat_step_info* info) {
   opts.near_plane = cfg.near_plane;
   opts.eps2d = 0.3f;
   opts.antialias = cfg.antialias;
-  opts.sh_degree = t->sh_degree;
+  opts.sh_degree = p.sh_degree;
   const int64_t n = t->n, cap = t->cur.cap;
-
-  // Forward (train.rs:212-223).
-  int64_t entries = 0;
-  SPLAT_TRY(render_view(c, t->cur.params.as<float>(), n, cap, cam, opts, bg, t->vb, &entries));
+  const StepParams* sp = t->params_dev.as<StepParams>();
+  SPLAT_TRY(launch_load_words(c, static_cast<const char*>(t->params_host_dev) + slot * sizeof(StepParams),
+                              t->params_dev.ptr, (int)(sizeof(StepParams) / 4)));
+  SPLAT_TRY(render_view_dev(c, t->cur.params.as<float>(), n, cap, cam, opts, bg, t->vb, sp));
   const size_t npix = (size_t)cam.width * cam.height;
   SPLAT_TRY(t->pred_grad.ensure(npix * 12));
   SPLAT_TRY(t->loss_out.ensure(16));
   SPLAT_TRY(launch_loss(c, t->vb.image.as<float>(), view.rgb.ptr, 1, cam.width, cam.height, cfg.lambda_dssim,
-                        t->pred_grad.as<float>(), t->loss_out.as<float>()));
-  SPLAT_CUDA(cudaMemcpyAsync(t->loss_host, t->loss_out.ptr, 12, cudaMemcpyDeviceToHost, c->stream));
-
-  // Backward (train.rs:226-235).
+                        t->pred_grad.as<float>(), t->loss_out.as<float>(), sp));
   SPLAT_TRY(t->pgrad.ensure((size_t)cap * 48));
   SPLAT_TRY(launch_fill_u32(c, t->pgrad.ptr, (size_t)cap * 12, 0u));
   SPLAT_TRY(launch_raster_bwd(c, t->vb.proj.as<float>(), t->vb.gauss.as<uint32_t>(), t->vb.tile_range.as<uint32_t>(),
                               cam.width, cam.height, bg, t->vb.final_t.as<float>(), t->vb.n_contrib.as<uint32_t>(),
                               t->pred_grad.as<float>(), t->pgrad.as<float>(), cap, nullptr));
-  const bool densify_window = cfg.densify && it < cfg.densify_until_iter;
-  SPLAT_TRY(ensure_stats(t, cap));
   // Optimiser step (train.rs:238-246), fused into the projection backward: the 59
   // gradients per Gaussian go from registers straight into Adam.
-  splat_lr lr;
-  lr.mean = position_lr(cfg, it, t->extent);
-  lr.log_scale = cfg.scaling_lr;
-  lr.quat = cfg.rotation_lr;
-  lr.opacity = cfg.opacity_lr;
-  lr.sh_dc = cfg.feature_lr;
-  lr.sh_rest = cfg.feature_lr / 20.0f;
-  t->adam_step += 1;
   SPLAT_TRY(launch_project_bwd_adam(c, t->cur.params.as<float>(), t->cur.m.as<float>(), t->cur.v.as<float>(), n, cap,
                                     cam, opts, t->vb.proj.as<float>(), t->pgrad.as<float>(),
-                                    densify_window ? t->stats.ptr : nullptr, cfg.absgrad, t->adam_step, lr));
+                                    p.densify_window ? t->stats.ptr : nullptr, cfg.absgrad, p.adam_step, p.lr,
+                                    t->vb.overflow_flag(), sp));
+  SPLAT_TRY(launch_publish_u32_to(c, t->loss_out.as<uint32_t>(), 3, t->vb.counters.as<uint32_t>(), 3,
+                                  static_cast<uint32_t*>(t->slots_dev) + 16 * slot));
+  return Status::ok();
+}
 
-  // Density control (train.rs:249-272).
+// Captures body() for `slot` into a graph; on any failure graphs are switched off and the
+// trainer keeps launching kernels one by one.
+void capture(splat_trainer* t, const IterPlan& p, int slot) {
+  Ctx* c = t->c;
+  if (cudaStreamBeginCapture(t->cap_stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+    cudaGetLastError();
+    t->graphs = false;
+    return;
+  }
+  cudaStream_t orig = c->stream;
+  c->stream = t->cap_stream;
+  const uint64_t l0 = c->launches.count;
+  const Status s = body(t, p, slot);
+  cudaGraph_t g = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(t->cap_stream, &g);
+  c->stream = orig;
+  const uint64_t nl = c->launches.count - l0;
+  c->launches.count = l0;
+  if (!s.good() || e != cudaSuccess || !g) {
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError();
+    t->graphs = false;
+    return;
+  }
+  const cudaError_t ei = cudaGraphInstantiate(&t->exec[slot], g, 0);
+  cudaGraphDestroy(g);
+  if (ei != cudaSuccess) {
+    t->exec[slot] = nullptr;
+    cudaGetLastError();
+    t->graphs = false;
+    drop_graphs(t);
+    return;
+  }
+  t->g_launches = nl;
+}
+
+// Queues one iteration without any host wait and records slot `slot`'s event: the captured
+// graph when one matches the current state, else the kernels one by one (the first
+// iteration after a change of state, which also sizes every buffer before a capture).
+Status enqueue(splat_trainer* t, const IterPlan& p, int slot) {
+  Ctx* c = t->c;
+  // Scratch of the previous iteration is free for reuse: all of it is consumed on this
+  // stream before anything queued now runs.
+  arena_reset(c);
+  View& view = *t->views[p.view];
+  StepParams& hp = t->params_host[slot];
+  hp.cam = view.cam;
+  hp.adam = make_adam_args(p.adam_step, p.lr);
+  hp.target = view.rgb.ptr;
+  SPLAT_TRY(t->params_dev.ensure(sizeof(StepParams)));
+  if (t->graphs) {
+    const std::vector<uint64_t> key = graph_key(t, p);
+    if (key != t->gkey) {
+      drop_graphs(t);
+      t->g_uses = 0;
+    } else if (!t->exec[slot] && t->g_uses > 0) {
+      capture(t, p, slot);
+    }
+    if (t->graphs && t->exec[slot]) {
+      t->last_replayed = true;
+      SPLAT_CUDA(cudaGraphLaunch(t->exec[slot], c->stream));
+      c->launches.count += t->g_launches;
+      SPLAT_CUDA(cudaEventRecord(t->slot_done[slot], c->stream));
+      return Status::ok();
+    }
+  }
+  t->last_replayed = false;
+  SPLAT_TRY(body(t, p, slot));
+  SPLAT_CUDA(cudaEventRecord(t->slot_done[slot], c->stream));
+  if (t->graphs) {
+    t->gkey = graph_key(t, p);  // the state after this iteration's allocations
+    t->g_uses++;
+  }
+  return Status::ok();
+}
+
+struct SlotResult {
+  float loss, psnr;
+  uint64_t entries;
+  bool overflow;
+};
+
+SlotResult read_slot(splat_trainer* t, int slot) {
+  const volatile uint32_t* w = t->slots_host + 16 * slot;
+  SlotResult r;
+  uint32_t b0 = w[0], b2 = w[2];
+  std::memcpy(&r.loss, &b0, 4);
+  std::memcpy(&r.psnr, &b2, 4);
+  r.entries = (uint64_t)w[3] | ((uint64_t)w[4] << 32);
+  r.overflow = w[5] != 0;
+  return r;
+}
+
+// After an overflow: room for the view that overflowed with a margin, the flag cleared.
+Status grow_entries(splat_trainer* t, uint64_t entries) {
+  t->vb.e_cap = std::max<int64_t>(t->vb.e_cap * 2, (int64_t)(entries + entries / 4 + 4096));
+  if (t->vb.e_cap >= 0xffffffffLL) return Status::make(SPLAT_ERR_CAPACITY, "too many tile entries for 32-bit offsets");
+  return launch_fill_u32(t->c, t->vb.overflow_flag(), 1, 0u);
+}
+
+// Density control after iteration p (train.rs:249-272); synchronises.
+Status density_control(splat_trainer* t, const IterPlan& p, splat_step_info* info) {
+  Ctx* c = t->c;
+  const splat_train_config& cfg = t->cfg;
+  const int64_t n = t->n, cap = t->cur.cap;
+  if (p.densify_now) {
+    DensifyParams dp;
+    dp.cfg.grad_threshold = cfg.densify_grad_threshold;
+    dp.cfg.percent_dense = cfg.percent_dense;
+    dp.cfg.min_opacity = cfg.min_opacity;
+    dp.cfg.prune_big_world = cfg.opacity_reset_interval > 0 && p.it > cfg.opacity_reset_interval;
+    dp.cfg.max_world_size_frac = 0.1f;
+    dp.cfg.max_screen_size = cfg.max_screen_size;
+    dp.cfg.split_children = 2;
+    dp.extent = t->extent;
+    dp.shrink = logf(0.8f * (float)dp.cfg.split_children);
+    float* accum = t->stats.as<float>();
+    uint32_t* denom = reinterpret_cast<uint32_t*>(accum + t->stats_cap);
+    uint32_t* maxr = denom + t->stats_cap;
+    DensifyPlan plan;
+    SPLAT_TRY(densify_plan(c, t->cur.params.as<float>(), n, cap, accum, denom, maxr, dp, &plan));
+    if (cfg.max_gaussians > 0 && plan.new_count() > cfg.max_gaussians) {
+      // Growth would pass the configured limit: this densification only prunes.
+      dp.grow = false;
+      SPLAT_TRY(densify_plan(c, t->cur.params.as<float>(), n, cap, accum, denom, maxr, dp, &plan));
+    }
+    const size_t nn = (size_t)plan.split * dp.cfg.split_children * 3;
+    std::vector<double> normals(nn);
+    for (size_t q = 0; q < nn; q++) normals[q] = t->rng.normal();
+    SPLAT_TRY(t->normals.ensure(std::max<size_t>(nn, 1) * 8));
+    if (nn) SPLAT_CUDA(cudaMemcpyAsync(t->normals.ptr, normals.data(), nn * 8, cudaMemcpyHostToDevice, c->stream));
+    const int64_t new_n = (int64_t)plan.new_count();
+    const int64_t want = std::max<int64_t>(new_n, 1);
+    if (t->next.cap < want) SPLAT_TRY(t->next.ensure(std::max<int64_t>(want, cap)));
+    SPLAT_TRY(densify_apply(c, t->cur.params.as<float>(), t->cur.m.as<float>(), t->cur.v.as<float>(), n, cap, plan,
+                            t->normals.as<double>(), t->next.params.as<float>(), t->next.m.as<float>(),
+                            t->next.v.as<float>(), t->next.cap));
+    // The normals buffer is read by the scatter; keep the host vector alive until done.
+    SPLAT_CUDA(cudaStreamSynchronize(c->stream));
+    std::swap(t->cur, t->next);
+    t->n = new_n;
+    SPLAT_TRY(ensure_stats(t, t->cur.cap));
+    SPLAT_TRY(reset_stats(t));
+    info->densified = 1;
+    info->cloned = plan.cloned;
+    info->split = plan.split;
+    info->pruned = plan.pruned;
+  }
+  if (p.reset_now) {
+    const float x = 0.01f;
+    const float limit = logf(x / (1.0f - x));  // inverse_sigmoid (math.rs:454)
+    SPLAT_TRY(launch_reset_opacity(c, t->cur.params.as<float>(), t->cur.m.as<float>(), t->cur.v.as<float>(), t->n,
+                                   limit));
+    info->reset = 1;
+  }
+  return Status::ok();
+}
+
+void fill_info(splat_trainer* t, const IterPlan& p, const SlotResult& r, splat_step_info* info) {
+  info->loss = r.loss;
+  info->psnr = r.psnr;
+  info->view = p.view;
+  info->num_gaussians = (uint64_t)t->n;
+  info->entries = r.entries;
+  info->replayed = t->last_replayed ? 1u : 0u;
+}
+
+Status initial_capacity(splat_trainer* t) {
+  if (t->vb.e_cap == 0)
+    t->vb.e_cap = t->cfg.entry_capacity > 0 ? (int64_t)std::min<uint64_t>(t->cfg.entry_capacity, 0xfffffffeull)
+                                            : std::max<int64_t>(8 * std::max<int64_t>(t->n, 1), 1 << 16);
+  return ensure_stats(t, t->cur.cap);
+}
+
+// Runs iteration p to completion, redoing it with more room if its binning overflowed.
+Status run_one(splat_trainer* t, const IterPlan& p, int slot, SlotResult* out) {
+  for (;;) {
+    SPLAT_TRY(enqueue(t, p, slot));
+    SPLAT_CUDA(cudaEventSynchronize(t->slot_done[slot]));
+    *out = read_slot(t, slot);
+    if (!out->overflow) return Status::ok();
+    SPLAT_TRY(grow_entries(t, out->entries));
+  }
+}
+
+Status step(splat_trainer* t, splat_step_info* info) {
+  SPLAT_TRY(initial_capacity(t));
+  const IterPlan p = schedule(t);
   info->densified = 0;
   info->reset = 0;
   info->cloned = info->split = info->pruned = 0;
-  if (densify_window) {
-    if (it > cfg.densify_from_iter && it % cfg.densification_interval == 0) {
-      DensifyParams dp;
-      dp.cfg.grad_threshold = cfg.densify_grad_threshold;
-      dp.cfg.percent_dense = cfg.percent_dense;
-      dp.cfg.min_opacity = cfg.min_opacity;
-      dp.cfg.prune_big_world = cfg.opacity_reset_interval > 0 && it > cfg.opacity_reset_interval;
-      dp.cfg.max_world_size_frac = 0.1f;
-      dp.cfg.max_screen_size = cfg.max_screen_size;
-      dp.cfg.split_children = 2;
-      dp.extent = t->extent;
-      dp.shrink = logf(0.8f * (float)dp.cfg.split_children);
-      float* accum = t->stats.as<float>();
-      uint32_t* denom = reinterpret_cast<uint32_t*>(accum + t->stats_cap);
-      uint32_t* maxr = denom + t->stats_cap;
-      DensifyPlan plan;
-      SPLAT_TRY(densify_plan(c, t->cur.params.as<float>(), n, cap, accum, denom, maxr, dp, &plan));
-      if (cfg.max_gaussians > 0 && plan.new_count() > cfg.max_gaussians) {
-        // Growth would pass the configured limit: this densification only prunes.
-        dp.grow = false;
-        SPLAT_TRY(densify_plan(c, t->cur.params.as<float>(), n, cap, accum, denom, maxr, dp, &plan));
+  SlotResult r;
+  SPLAT_TRY(run_one(t, p, 0, &r));
+  SPLAT_TRY(density_control(t, p, info));
+  if (p.densify_now || p.reset_now) SPLAT_CUDA(cudaStreamSynchronize(t->c->stream));
+  fill_info(t, p, r, info);
+  return Status::ok();
+}
+
+// `count` iterations with the host one iteration ahead of the device: iteration i+1 is
+// queued before iteration i's read-back is checked. Iterations followed by density
+// control run to completion first. An overflow at iteration i also voids i+1 (the flag is
+// sticky, so i+1's update was skipped too): both are redone, in order, with more room.
+Status run(splat_trainer* t, uint32_t count, splat_step_info* info) {
+  SPLAT_TRY(initial_capacity(t));
+  info->densified = 0;
+  info->reset = 0;
+  info->cloned = info->split = info->pruned = 0;
+  IterPlan pending;
+  bool has_pending = false;
+  int pending_slot = 0;
+  SlotResult r{};
+  IterPlan last{};
+  for (uint32_t k = 0; k < count; k++) {
+    const IterPlan p = schedule(t);
+    const int slot = has_pending ? 1 - pending_slot : 0;
+    SPLAT_TRY(enqueue(t, p, slot));
+    if (has_pending) {
+      SPLAT_CUDA(cudaEventSynchronize(t->slot_done[pending_slot]));
+      const SlotResult pr = read_slot(t, pending_slot);
+      if (pr.overflow) {
+        SPLAT_CUDA(cudaEventSynchronize(t->slot_done[slot]));
+        SPLAT_TRY(grow_entries(t, pr.entries));
+        SlotResult tmp;
+        SPLAT_TRY(run_one(t, pending, pending_slot, &tmp));
+        SPLAT_TRY(run_one(t, p, slot, &tmp));
       }
-      const size_t nn = (size_t)plan.split * dp.cfg.split_children * 3;
-      std::vector<double> normals(nn);
-      for (size_t q = 0; q < nn; q++) normals[q] = t->rng.normal();
-      SPLAT_TRY(t->normals.ensure(std::max<size_t>(nn, 1) * 8));
-      if (nn)
-        SPLAT_CUDA(cudaMemcpyAsync(t->normals.ptr, normals.data(), nn * 8, cudaMemcpyHostToDevice, c->stream));
-      const int64_t new_n = (int64_t)plan.new_count();
-      const int64_t want = std::max<int64_t>(new_n, 1);
-      if (t->next.cap < want) SPLAT_TRY(t->next.ensure(std::max<int64_t>(want, cap)));
-      SPLAT_TRY(densify_apply(c, t->cur.params.as<float>(), t->cur.m.as<float>(), t->cur.v.as<float>(), n, cap, plan,
-                              t->normals.as<double>(), t->next.params.as<float>(), t->next.m.as<float>(),
-                              t->next.v.as<float>(), t->next.cap));
-      // The normals buffer is read by the scatter; keep the host vector alive until done.
-      SPLAT_CUDA(cudaStreamSynchronize(c->stream));
-      std::swap(t->cur, t->next);
-      t->n = new_n;
-      SPLAT_TRY(ensure_stats(t, t->cur.cap));
-      SPLAT_TRY(reset_stats(t));
-      info->densified = 1;
-      info->cloned = plan.cloned;
-      info->split = plan.split;
-      info->pruned = plan.pruned;
+      has_pending = false;
     }
-    const bool reset = cfg.opacity_reset_interval > 0 &&
-                       (it % cfg.opacity_reset_interval == 0 || (cfg.white_background && it == cfg.densify_from_iter));
-    if (reset) {
-      const float x = 0.01f;
-      const float limit = logf(x / (1.0f - x));  // inverse_sigmoid (math.rs:454)
-      SPLAT_TRY(launch_reset_opacity(c, t->cur.params.as<float>(), t->cur.m.as<float>(), t->cur.v.as<float>(), t->n,
-                                     limit));
-      info->reset = 1;
+    if (p.densify_now || p.reset_now || k + 1 == count) {
+      SPLAT_CUDA(cudaEventSynchronize(t->slot_done[slot]));
+      r = read_slot(t, slot);
+      if (r.overflow) {
+        SPLAT_TRY(grow_entries(t, r.entries));
+        SPLAT_TRY(run_one(t, p, slot, &r));
+      }
+      SPLAT_TRY(density_control(t, p, info));
+      last = p;
+    } else {
+      pending = p;
+      pending_slot = slot;
+      has_pending = true;
     }
   }
-  SPLAT_CUDA(cudaStreamSynchronize(c->stream));
-  info->loss = t->loss_host[0];
-  info->psnr = t->loss_host[2];
-  info->view = vi;
-  info->num_gaussians = (uint64_t)t->n;
-  info->entries = (uint64_t)entries;
+  SPLAT_CUDA(cudaStreamSynchronize(t->c->stream));
+  fill_info(t, last, r, info);
   return Status::ok();
 }
 }  // namespace
@@ -277,9 +523,31 @@ SPLAT_API int splat_trainer_create(splat_ctx* ctx, const splat_train_config* cfg
   t->c = splat_ctx_impl(ctx);
   t->cfg = *cfg;
   t->extent = extent;
-  if (cudaMallocHost(&t->loss_host, 64) != cudaSuccess) {
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaSetDevice(t->c->device);
+  bool ok = cudaHostAlloc((void**)&t->slots_host, 2 * 16 * 4, cudaHostAllocMapped) == cudaSuccess;
+  ok = ok && cudaHostGetDevicePointer(&t->slots_dev, t->slots_host, 0) == cudaSuccess;
+  for (cudaEvent_t& ev : t->slot_done) ok = ok && cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) == cudaSuccess;
+  cudaSetDevice(prev);
+  if (!ok) {
     cudaGetLastError();
+    for (cudaEvent_t ev : t->slot_done)
+      if (ev) cudaEventDestroy(ev);
+    if (t->slots_host) cudaFreeHost(t->slots_host);
     delete t;
+    return SPLAT_ERR_CUDA;
+  }
+  std::memset(t->slots_host, 0, 2 * 16 * 4);
+  cudaSetDevice(t->c->device);
+  ok = cudaHostAlloc((void**)&t->params_host, 2 * sizeof(StepParams), cudaHostAllocMapped) == cudaSuccess;
+  ok = ok && cudaHostGetDevicePointer(&t->params_host_dev, t->params_host, 0) == cudaSuccess;
+  ok = ok && cudaStreamCreateWithFlags(&t->cap_stream, cudaStreamNonBlocking) == cudaSuccess;
+  cudaSetDevice(prev);
+  if (!ok) {
+    cudaGetLastError();
+    t->c->last_error = "splat_trainer_create: host or stream allocation failed";
+    splat_trainer_destroy(t);
     return SPLAT_ERR_CUDA;
   }
   *out = t;
@@ -300,7 +568,13 @@ SPLAT_API int splat_trainer_destroy(splat_trainer* t) {
       delete v;
     }
     t->views.clear();
-    if (t->loss_host) cudaFreeHost(t->loss_host);
+    drop_graphs(t);
+    t->params_dev.release();
+    for (cudaEvent_t ev : t->slot_done)
+      if (ev) cudaEventDestroy(ev);
+    if (t->slots_host) cudaFreeHost(t->slots_host);
+    if (t->params_host) cudaFreeHost(t->params_host);
+    if (t->cap_stream) cudaStreamDestroy(t->cap_stream);
   }
   delete t;
   return SPLAT_OK;
@@ -381,6 +655,18 @@ SPLAT_API int splat_trainer_step(splat_trainer* t, splat_step_info* info) {
   }
   TEnter e(t);
   Status s = step(t, info);
+  return s.good() ? SPLAT_OK : tfail(t, s);
+}
+
+SPLAT_API int splat_trainer_run(splat_trainer* t, uint32_t iterations, splat_step_info* info) {
+  if (!t || !info) return SPLAT_ERR_INVALID;
+  if (t->views.empty()) {
+    t->c->last_error = "no training views";
+    return SPLAT_ERR_INVALID;
+  }
+  if (iterations == 0) return SPLAT_OK;
+  TEnter e(t);
+  Status s = run(t, iterations, info);
   return s.good() ? SPLAT_OK : tfail(t, s);
 }
 

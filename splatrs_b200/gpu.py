@@ -160,6 +160,28 @@ def bin(ctx: Context, proj: Projection, want_keys: bool = False) -> Binning:
     return Binning(off, gauss[:E], keys[:E] if keys is not None else None, tr, E, tx, ty)
 
 
+def bin_device(ctx: Context, proj: Projection, capacity: int, scratch: torch.Tensor | None = None):
+    """bin without a host read-back (splat_bin_count_device + splat_bin_sort_device).
+    Returns (gauss (capacity,), tile ranges, entry count (device uint64), overflow flag
+    (device), scratch); results are valid only when the flag is 0."""
+    dev = proj.rec.device
+    off = torch.empty(proj.n + 1, dtype=torch.int32, device=dev)
+    e_dev = torch.zeros(1, dtype=torch.int64, device=dev)
+    check(ctx.lib.splat_bin_count_device(ctx.h, _ptr(proj.num_tiles), proj.n, _ptr(off), _ptr(e_dev)), ctx.h)
+    tx = (proj.width + 15) // 16
+    ty = (proj.height + 15) // 16
+    need = int(ctx.lib.splat_bin_sort_device_scratch_bytes(capacity))
+    if scratch is None or scratch.numel() < need:
+        scratch = torch.empty(need, dtype=torch.uint8, device=dev)
+    gauss = torch.empty(max(capacity, 1), dtype=torch.int32, device=dev)
+    tr = torch.empty((tx * ty, 2), dtype=torch.int32, device=dev)
+    flag = torch.zeros(1, dtype=torch.int32, device=dev)
+    check(ctx.lib.splat_bin_sort_device(ctx.h, _ptr(proj.rec), _ptr(off), proj.n, _ptr(e_dev), capacity,
+                                        _ptr(proj.depth_range), proj.width, proj.height, _ptr(scratch), _ptr(gauss),
+                                        _ptr(tr), _ptr(flag)), ctx.h)
+    return gauss, tr, e_dev, flag, scratch
+
+
 def _bg(background):
     arr = (C.c_float * 3)(*[float(x) for x in background])
     return C.cast(arr, C.POINTER(C.c_float)), arr
@@ -392,6 +414,12 @@ class Trainer:
     def step(self) -> dict:
         info = StepInfo()
         check(self.lib.splat_trainer_step(self.h, C.byref(info)), self.ctx.h)
+        return info.as_dict()
+
+    def run(self, iterations: int) -> dict:
+        """``iterations`` steps in one call, queued ahead of the device; info of the last."""
+        info = StepInfo()
+        check(self.lib.splat_trainer_run(self.h, iterations, C.byref(info)), self.ctx.h)
         return info.as_dict()
 
     @property

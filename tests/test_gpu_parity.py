@@ -131,6 +131,30 @@ def test_binning_large_single_view(ctx):
     assert (b.tile_range.cpu().numpy().view(np.uint32) == a["tile_range"]).all()
 
 
+@pytest.mark.parametrize("seed,size", [(8, (320, 240)), (9, (1024, 64)), (10, (1920, 1080))])
+def test_device_driven_binning_equals_host_driven(ctx, seed, size):
+    """splat_bin_count_device + splat_bin_sort_device (no host read-back, capacity-sized
+    buffers): per-tile lists and ranges identical to splat_bin_sort; a second, smaller
+    view through the same scratch too; a capacity below the count raises the overflow
+    flag instead of writing past the buffers."""
+    g, cam = small_scene(seed=seed, n=20000, size=size)
+    _, proj = gpu_project(ctx, g, cam, sh_degree=3)
+    want = G.bin(ctx, proj)
+    E = want.num_entries
+    gauss, tr, e_dev, flag, scratch = G.bin_device(ctx, proj, E + 4097)
+    assert int(e_dev.item()) == E and int(flag.item()) == 0
+    assert torch.equal(tr, want.tile_range)
+    assert torch.equal(gauss[:E], want.gauss)
+    g2, cam2 = small_scene(seed=seed + 100, n=3000, size=(size[0] // 2 + 1, size[1] // 2 + 1))
+    _, proj2 = gpu_project(ctx, g2, cam2, sh_degree=1)
+    want2 = G.bin(ctx, proj2)
+    gauss2, tr2, e2, flag2, _ = G.bin_device(ctx, proj2, E + 4097, scratch)
+    assert int(flag2.item()) == 0 and torch.equal(tr2, want2.tile_range)
+    assert torch.equal(gauss2[:want2.num_entries], want2.gauss)
+    _, _, _, flag3, _ = G.bin_device(ctx, proj, E // 2)
+    assert int(flag3.item()) == 1
+
+
 def test_binning_empty_and_offscreen(ctx):
     """No visible Gaussian: zero entries, every tile range empty."""
     g, cam = small_scene(n=50)

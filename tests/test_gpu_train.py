@@ -282,3 +282,54 @@ def test_trainer_gaussian_limit_stops_growth(ctx):
     assert max(counts) <= limit
     assert np.isfinite(t.model()[:, 0:10]).all()
     t.close()
+
+
+def _cfg_small():
+    return dict(iterations=300, densify=1, densify_from_iter=40, densify_until_iter=280, densification_interval=40,
+                opacity_reset_interval=200, densify_grad_threshold=0.0005, white_background=1, sh_degree=1,
+                sh_degree_interval=150, position_lr_max_steps=300, seed=5)
+
+
+def test_trainer_run_matches_step(ctx):
+    """splat_trainer_run (iterations queued one ahead of the device) follows the schedule of
+    splat_trainer_step: the same views at the same iterations, the same SH degree, and a
+    model of the same quality. Without densification the view order depends on the seed
+    alone (the split offsets share its generator, and the compositing backward's float
+    atomics can change a split count, so with densification the orders may part)."""
+    views, extent, init = _views_and_init(200, 30, 8, 48, 36, [1.0, 1.0, 1.0])
+    cfg = dict(_cfg_small(), densify=0)
+    a = G.Trainer(ctx, init, extent, views, **cfg)
+    infos = [a.step() for _ in range(300)]
+    b = G.Trainer(ctx, init, extent, views, **cfg)
+    done = 0
+    for k in (1, 136, 163):
+        ib = b.run(k)
+        done += k
+        assert ib["view"] == infos[done - 1]["view"]
+    assert a.sh_degree == b.sh_degree == 1
+    pa, pb = _evaluate(a, views), _evaluate(b, views)
+    print(f"\nstep x300: {pa:.2f} dB; run 1+136+163: {pb:.2f} dB")
+    assert abs(pa - pb) < 0.3
+    a.close()
+    b.close()
+
+
+@pytest.mark.parametrize("use_run", [False, True])
+def test_trainer_entry_overflow_is_redone(ctx, use_run):
+    """With room for only 64 tile entries the first iterations overflow the binning; each is
+    redone with larger buffers (and its Adam update applied once), so training matches a
+    run that never overflowed."""
+    views, extent, init = _views_and_init(200, 30, 8, 48, 36, [1.0, 1.0, 1.0], truncate=10)
+    ref = G.Trainer(ctx, init, extent, views, **_cfg_small())
+    ref.run(300)
+    t = G.Trainer(ctx, init, extent, views, entry_capacity=64, **_cfg_small())
+    if use_run:
+        t.run(300)
+    else:
+        for _ in range(300):
+            t.step()
+    assert np.isfinite(t.model()[:, 0:10]).all()
+    pr, pt = _evaluate(ref, views), _evaluate(t, views)
+    assert abs(pr - pt) < 0.5, (pr, pt)
+    ref.close()
+    t.close()
