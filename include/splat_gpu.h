@@ -81,6 +81,12 @@ typedef struct splat_proj_opts {
   float eps2d;      /* 0.3 */
   int32_t antialias;
   int32_t sh_degree;
+  /* Not in the reference (0 reproduces it): when the f32 determinant of the projected 2x2
+   * covariance is ill-conditioned, rebuild that covariance, its determinant and inverse in
+   * f64. The test is det < 1e-4 * trace^2 on the f32 values, so that every covariance with
+   * det < 1e-6 * trace^2 is caught although the f32 determinant tested is itself off by up
+   * to ~10% near that ratio. */
+  int32_t fp64_conic;
 } splat_proj_opts;
 
 /* Per-group learning rates (reference src/adam.rs:11-24). */
@@ -119,6 +125,11 @@ typedef struct splat_train_config {
   /* Not in the reference: tile entries the binning buffers hold at first (0 = automatic).
    * An iteration whose view needs more is redone with larger buffers. */
   uint64_t entry_capacity;
+  /* Not in the reference: render from a BF16 copy of quaternion, log-scales and SH (the
+   * f32 parameters stay the optimiser's master copy), and re-solve ill-conditioned 2x2
+   * conics in f64 (splat_proj_opts.fp64_conic). */
+  int32_t bf16_storage;
+  int32_t fp64_conic;
 } splat_train_config;
 
 typedef struct splat_ctx splat_ctx;
@@ -154,6 +165,17 @@ SPLAT_API int splat_params_to_aos(splat_ctx* ctx, const float* planes_dev, int64
 SPLAT_API int splat_project_fwd(splat_ctx* ctx, const float* planes_dev, int64_t n, int64_t cap,
                                 const splat_camera* cam, const splat_proj_opts* opts, float* proj_dev,
                                 uint32_t* num_tiles_dev, uint32_t* depth_range_dev);
+
+/* BF16 storage (not in the reference). splat_params_to_bf16 writes the BF16 render copy of
+ * parameter planes 1..14 (quaternion, log-scales, SH: 4 x bf16 per Gaussian and plane,
+ * plane q at offset (q - 1) * cap, 8 * 14 * cap bytes, rounded to nearest even); means and
+ * opacity stay in f32 plane 0. splat_project_fwd_bf16 is splat_project_fwd reading those
+ * planes from the copy (112 bytes per Gaussian instead of 224): its records equal
+ * splat_project_fwd's on planes rounded to bf16. */
+SPLAT_API int splat_params_to_bf16(splat_ctx* ctx, const float* planes_dev, int64_t n, int64_t cap, void* bf16_dev);
+SPLAT_API int splat_project_fwd_bf16(splat_ctx* ctx, const float* planes_dev, const void* bf16_dev, int64_t n,
+                                     int64_t cap, const splat_camera* cam, const splat_proj_opts* opts,
+                                     float* proj_dev, uint32_t* num_tiles_dev, uint32_t* depth_range_dev);
 
 /* Build projection records from reference-layout Proj records (proj15, device), e.g. to
  * bin and composite projections made elsewhere. Also writes tile counts and depth range. */
@@ -250,11 +272,13 @@ SPLAT_API int splat_diag_fast_exp_error(splat_ctx* ctx, float lo, float hi, int3
  * src/adam.rs:77-161): the parameter gradients stay in registers and update planes_dev in
  * place together with the moments m_dev and v_dev (parameter-plane layout, capacity cap);
  * `step` is the Adam step count after the increment. Optional densification statistics as
- * in splat_project_bwd. Results equal splat_project_bwd followed by splat_adam_step. */
+ * in splat_project_bwd. Results equal splat_project_bwd followed by splat_adam_step. With a
+ * BF16 render copy (bf16_dev, see splat_params_to_bf16; may be NULL) the gradient is taken
+ * at the copy's values and the copy is rewritten from the updated f32 planes. */
 SPLAT_API int splat_project_bwd_adam(splat_ctx* ctx, float* planes_dev, float* m_dev, float* v_dev, int64_t n,
                                      int64_t cap, const splat_camera* cam, const splat_proj_opts* opts,
                                      const float* proj_dev, const float* pgrad_dev, void* stats_dev, int32_t absgrad,
-                                     uint64_t step, const splat_lr* lr);
+                                     uint64_t step, const splat_lr* lr, void* bf16_dev);
 
 /* Fill `bytes` bytes of device memory with zeros on the context stream. */
 SPLAT_API int splat_zero(splat_ctx* ctx, void* dev, size_t bytes);

@@ -47,11 +47,12 @@ class Camera(C.Structure):
 
 class ProjOpts(C.Structure):
     """splat_proj_opts (reference src/project.rs:22-43)."""
-    _fields_ = [("near_plane", C.c_float), ("eps2d", C.c_float), ("antialias", C.c_int32), ("sh_degree", C.c_int32)]
+    _fields_ = [("near_plane", C.c_float), ("eps2d", C.c_float), ("antialias", C.c_int32), ("sh_degree", C.c_int32),
+                ("fp64_conic", C.c_int32)]
 
     @classmethod
-    def make(cls, near=0.2, eps2d=0.3, antialias=False, sh_degree=3):
-        return cls(near, eps2d, int(bool(antialias)), int(sh_degree))
+    def make(cls, near=0.2, eps2d=0.3, antialias=False, sh_degree=3, fp64_conic=False):
+        return cls(near, eps2d, int(bool(antialias)), int(sh_degree), int(bool(fp64_conic)))
 
 
 class LearningRates(C.Structure):
@@ -83,7 +84,7 @@ class TrainConfig(C.Structure):
                 ("max_screen_size", C.c_int64), ("absgrad", C.c_int32), ("antialias", C.c_int32),
                 ("white_background", C.c_int32), ("sh_degree", C.c_int32), ("sh_degree_interval", C.c_uint32),
                 ("near_plane", C.c_float), ("seed", C.c_uint64), ("max_gaussians", C.c_uint64),
-                ("entry_capacity", C.c_uint64)]
+                ("entry_capacity", C.c_uint64), ("bf16_storage", C.c_int32), ("fp64_conic", C.c_int32)]
 
     DEFAULTS = dict(iterations=30000, position_lr_init=0.00016, position_lr_final=0.0000016,
                     position_lr_max_steps=30000, feature_lr=0.0025, opacity_lr=0.025, scaling_lr=0.005,
@@ -91,7 +92,7 @@ class TrainConfig(C.Structure):
                     densification_interval=100, opacity_reset_interval=3000, densify_grad_threshold=0.0002,
                     percent_dense=0.01, min_opacity=0.005, max_screen_size=-1, absgrad=0, antialias=0,
                     white_background=0, sh_degree=3, sh_degree_interval=1000, near_plane=0.2, seed=0,
-                    max_gaussians=0, entry_capacity=0)
+                    max_gaussians=0, entry_capacity=0, bf16_storage=0, fp64_conic=0)
 
     @classmethod
     def make(cls, **kw):
@@ -170,7 +171,9 @@ def _declare(L):
         "splat_loss_fwd_bwd": ([vp, vp, vp, i32, u32, u32, C.c_float, vp, vp], C.c_int),
         "splat_adam_step": ([vp, vp, vp, vp, vp, i64, i64, C.c_uint64, P(LearningRates)], C.c_int),
         "splat_project_bwd_adam": ([vp, vp, vp, vp, i64, i64, P(Camera), P(ProjOpts), vp, vp, vp, i32, C.c_uint64,
-                                    P(LearningRates)], C.c_int),
+                                    P(LearningRates), vp], C.c_int),
+        "splat_params_to_bf16": ([vp, vp, i64, i64, vp], C.c_int),
+        "splat_project_fwd_bf16": ([vp, vp, vp, i64, i64, P(Camera), P(ProjOpts), vp, vp, vp], C.c_int),
         "splat_densify": ([vp, vp, vp, vp, i64, i64, vp, P(DensifyConfig), C.c_float, P(C.c_uint64), vp, vp, vp, i64,
                            P(DensifyReport)], C.c_int),
         "splat_reset_opacity": ([vp, vp, vp, vp, i64, C.c_float], C.c_int),

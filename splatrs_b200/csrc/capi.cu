@@ -218,6 +218,26 @@ SPLAT_API int splat_project_fwd(splat_ctx* ctx, const float* planes_dev, int64_t
                                         depth_range_dev));
 }
 
+SPLAT_API int splat_params_to_bf16(splat_ctx* ctx, const float* planes_dev, int64_t n, int64_t cap, void* bf16_dev) {
+  if (!ctx) return SPLAT_ERR_INVALID;
+  if (n < 0 || cap < n || (n && (!planes_dev || !bf16_dev))) return invalid(ctx, "splat_params_to_bf16: bad buffers");
+  Enter e(ctx);
+  return finish(ctx, launch_planes_to_bf16(&ctx->c, planes_dev, n, cap, bf16_dev));
+}
+
+SPLAT_API int splat_project_fwd_bf16(splat_ctx* ctx, const float* planes_dev, const void* bf16_dev, int64_t n,
+                                     int64_t cap, const splat_camera* cam, const splat_proj_opts* opts,
+                                     float* proj_dev, uint32_t* num_tiles_dev, uint32_t* depth_range_dev) {
+  if (!ctx) return SPLAT_ERR_INVALID;
+  if (!cam_ok(cam)) return invalid(ctx, "splat_project_fwd_bf16: camera size must be in 1..65535");
+  if (!opts_ok(opts)) return invalid(ctx, "splat_project_fwd_bf16: sh_degree must be in 0..3");
+  if (n < 0 || cap < n || !depth_range_dev || (n && (!planes_dev || !bf16_dev || !proj_dev || !num_tiles_dev)))
+    return invalid(ctx, "splat_project_fwd_bf16: bad buffers");
+  Enter e(ctx);
+  return finish(ctx, launch_project_fwd(&ctx->c, planes_dev, n, cap, *cam, *opts, proj_dev, num_tiles_dev,
+                                        depth_range_dev, nullptr, bf16_dev));
+}
+
 SPLAT_API int splat_proj_from_reference(splat_ctx* ctx, const float* proj15_dev, int64_t n, uint32_t width,
                                         uint32_t height, float* proj_dev, uint32_t* num_tiles_dev,
                                         uint32_t* depth_range_dev) {
@@ -352,7 +372,7 @@ SPLAT_API int splat_project_bwd(splat_ctx* ctx, const float* planes_dev, int64_t
 SPLAT_API int splat_project_bwd_adam(splat_ctx* ctx, float* planes_dev, float* m_dev, float* v_dev, int64_t n,
                                      int64_t cap, const splat_camera* cam, const splat_proj_opts* opts,
                                      const float* proj_dev, const float* pgrad_dev, void* stats_dev, int32_t absgrad,
-                                     uint64_t step, const splat_lr* lr) {
+                                     uint64_t step, const splat_lr* lr, void* bf16_dev) {
   if (!ctx) return SPLAT_ERR_INVALID;
   if (!cam_ok(cam)) return invalid(ctx, "splat_project_bwd_adam: camera size must be in 1..65535");
   if (!opts_ok(opts)) return invalid(ctx, "splat_project_bwd_adam: sh_degree must be in 0..3");
@@ -360,7 +380,7 @@ SPLAT_API int splat_project_bwd_adam(splat_ctx* ctx, float* planes_dev, float* m
     return invalid(ctx, "splat_project_bwd_adam: bad arguments");
   Enter e(ctx);
   return finish(ctx, launch_project_bwd_adam(&ctx->c, planes_dev, m_dev, v_dev, n, cap, *cam, *opts, proj_dev,
-                                             pgrad_dev, stats_dev, absgrad, step, *lr));
+                                             pgrad_dev, stats_dev, absgrad, step, *lr, nullptr, nullptr, bf16_dev));
 }
 
 }  // extern "C"

@@ -20,7 +20,7 @@ Status launch_params_to_aos(Ctx* c, const float* planes, int64_t n, int64_t cap,
 
 Status launch_project_fwd(Ctx* c, const float* planes, int64_t n, int64_t cap, const splat_camera& cam,
                           const splat_proj_opts& opts, float* proj, uint32_t* num_tiles, uint32_t* depth_range,
-                          const StepParams* sp = nullptr);
+                          const StepParams* sp = nullptr, const void* bf16 = nullptr);
 Status launch_proj_from_reference(Ctx* c, const float* p15, int64_t n, uint32_t width, uint32_t height, float* proj,
                                   uint32_t* num_tiles, uint32_t* depth_range);
 Status launch_proj_to_reference(Ctx* c, const float* proj, int64_t n, float* p15);
@@ -34,7 +34,14 @@ Status launch_project_bwd(Ctx* c, const float* planes, int64_t n, int64_t cap, c
 Status launch_project_bwd_adam(Ctx* c, float* planes, float* m, float* v, int64_t n, int64_t cap,
                                const splat_camera& cam, const splat_proj_opts& opts, const float* proj,
                                const float* pgrad, void* stats, int absgrad, uint64_t step, const splat_lr& lr,
-                               const uint32_t* skip = nullptr, const StepParams* sp = nullptr);
+                               const uint32_t* skip = nullptr, const StepParams* sp = nullptr,
+                               void* bf16 = nullptr);
+
+// The BF16 render copy of parameter planes 1..14 (quaternion, log-scales, SH; 4 x bf16 per
+// Gaussian and plane, plane q at (q - 1) * cap, rounded to nearest even). With a copy,
+// launch_project_fwd reads those planes from it, and launch_project_bwd_adam computes the
+// gradient at the copy's values, updates the f32 master and rewrites the copy.
+Status launch_planes_to_bf16(Ctx* c, const float* planes, int64_t n, int64_t cap, void* bf16);
 
 Status launch_scan_u32(Ctx* c, const uint32_t* in, int64_t n, uint32_t* out, int write_total, uint64_t* total_dev);
 

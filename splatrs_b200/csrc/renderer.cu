@@ -58,7 +58,8 @@ void ViewBuffers::release() {
 }
 
 Status render_view_dev(Ctx* c, const float* planes, int64_t n, int64_t cap, const splat_camera& cam,
-                       const splat_proj_opts& opts, const float bg[3], ViewBuffers& v, const StepParams* sp) {
+                       const splat_proj_opts& opts, const float bg[3], ViewBuffers& v, const StepParams* sp,
+                       const void* bf16) {
   SPLAT_TRY(v.ensure(n, cam.width, cam.height));
   const int64_t e_cap = std::max<int64_t>(v.e_cap, 1);
   SPLAT_TRY(v.gauss.ensure((size_t)e_cap * 4));
@@ -71,7 +72,7 @@ Status render_view_dev(Ctx* c, const float* planes, int64_t n, int64_t cap, cons
   float* proj = v.proj.as<float>();
   uint32_t* nt = v.num_tiles.as<uint32_t>();
   uint32_t* dr = v.depth_range.as<uint32_t>();
-  SPLAT_TRY(launch_project_fwd(c, planes, n, cap, cam, opts, proj, nt, dr, sp));
+  SPLAT_TRY(launch_project_fwd(c, planes, n, cap, cam, opts, proj, nt, dr, sp, bf16));
   SPLAT_TRY(launch_scan_u32_into(c, nt, n, v.entry_offset.as<uint32_t>(), 1, v.scan_partial.as<uint64_t>(),
                                  v.entry_count()));
   SPLAT_TRY(launch_bin_sort_dev(c, proj, v.entry_offset.as<uint32_t>(), n, v.entry_count(), e_cap, dr, cam.width,
@@ -83,12 +84,13 @@ Status render_view_dev(Ctx* c, const float* planes, int64_t n, int64_t cap, cons
 
 // Projection, binning and forward compositing of one view into `v`.
 Status render_view(Ctx* c, const float* planes, int64_t n, int64_t cap, const splat_camera& cam,
-                   const splat_proj_opts& opts, const float bg[3], ViewBuffers& v, int64_t* entries_out) {
+                   const splat_proj_opts& opts, const float bg[3], ViewBuffers& v, int64_t* entries_out,
+                   const void* bf16) {
   SPLAT_TRY(v.ensure(n, cam.width, cam.height));
   float* proj = v.proj.as<float>();
   uint32_t* nt = v.num_tiles.as<uint32_t>();
   uint32_t* dr = v.depth_range.as<uint32_t>();
-  SPLAT_TRY(launch_project_fwd(c, planes, n, cap, cam, opts, proj, nt, dr));
+  SPLAT_TRY(launch_project_fwd(c, planes, n, cap, cam, opts, proj, nt, dr, nullptr, bf16));
   uint64_t* total = nullptr;
   SPLAT_TRY(arena_reserve(c, 8, (void**)&total));
   SPLAT_TRY(launch_scan_u32(c, nt, n, v.entry_offset.as<uint32_t>(), 1, total));

@@ -35,13 +35,14 @@ struct ViewBuffers {
 // Projection, binning and forward compositing of one view. Synchronises once to read the
 // number of tile entries back.
 Status render_view(Ctx* c, const float* planes, int64_t n, int64_t cap, const splat_camera& cam,
-                   const splat_proj_opts& opts, const float bg[3], ViewBuffers& v, int64_t* entries_out);
+                   const splat_proj_opts& opts, const float bg[3], ViewBuffers& v, int64_t* entries_out,
+                   const void* bf16 = nullptr);
 
 // The same without any host wait: binning reads the entry count on the device and sorts at
 // most e_cap entries (v.e_cap, set by the caller; buffers grow to it here). If the view
 // has more, *v.overflow_flag() becomes 1 and the view's outputs are invalid.
 Status render_view_dev(Ctx* c, const float* planes, int64_t n, int64_t cap, const splat_camera& cam,
                        const splat_proj_opts& opts, const float bg[3], ViewBuffers& v,
-                       const StepParams* sp = nullptr);
+                       const StepParams* sp = nullptr, const void* bf16 = nullptr);
 
 }  // namespace splat

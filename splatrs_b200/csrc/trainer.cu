@@ -75,6 +75,7 @@ struct splat_trainer {
   int sh_degree = 0;
   ModelBufs cur, next;
   DevBuf pgrad, stats, pred_grad, loss_out, normals, init;
+  DevBuf bf16;  // BF16 render copy of planes 1..14 when cfg.bf16_storage
   int64_t stats_cap = 0;
   ViewBuffers vb;
   std::vector<View*> views;
@@ -146,6 +147,16 @@ Status ensure_stats(splat_trainer* t, int64_t cap) {
   return Status::ok();
 }
 
+// The BF16 render copy follows the f32 parameters after anything but an optimiser step
+// (which rewrites it itself).
+Status refresh_bf16(splat_trainer* t) {
+  if (!t->cfg.bf16_storage) return Status::ok();
+  SPLAT_TRY(t->bf16.ensure((size_t)std::max<int64_t>(t->cur.cap, 1) * (kPlanes - 1) * 8));
+  return launch_planes_to_bf16(t->c, t->cur.params.as<float>(), t->n, t->cur.cap, t->bf16.ptr);
+}
+
+const void* bf16_copy(const splat_trainer* t) { return t->cfg.bf16_storage ? t->bf16.ptr : nullptr; }
+
 Status reset_stats(splat_trainer* t) {
   return launch_fill_u32(t->c, t->stats.ptr, t->stats.bytes / 4, 0u);
 }
@@ -195,7 +206,7 @@ std::vector<uint64_t> graph_key(splat_trainer* t, const IterPlan& p) {
   std::vector<uint64_t> k = {(uint64_t)t->n, (uint64_t)t->cur.cap, (uint64_t)t->vb.e_cap, (uint64_t)p.sh_degree,
                              (uint64_t)p.densify_window, cam.width, cam.height, t->c->arena.generation,
                              (uint64_t)t->stats_cap};
-  for (const DevBuf* b : {&t->cur.params, &t->cur.m, &t->cur.v, &t->stats, &t->pgrad, &t->pred_grad, &t->loss_out,
+  for (const DevBuf* b : {&t->cur.params, &t->cur.m, &t->cur.v, &t->bf16, &t->stats, &t->pgrad, &t->pred_grad, &t->loss_out,
                           &t->params_dev, &t->vb.proj, &t->vb.num_tiles, &t->vb.entry_offset, &t->vb.depth_range,
                           &t->vb.tile_range, &t->vb.gauss, &t->vb.image, &t->vb.final_t, &t->vb.n_contrib,
                           &t->vb.sort_scratch, &t->vb.scan_partial, &t->vb.counters})
@@ -228,11 +239,12 @@ Status body(splat_trainer* t, const IterPlan& p, int slot) {
   opts.eps2d = 0.3f;
   opts.antialias = cfg.antialias;
   opts.sh_degree = p.sh_degree;
+  opts.fp64_conic = cfg.fp64_conic;
   const int64_t n = t->n, cap = t->cur.cap;
   const StepParams* sp = t->params_dev.as<StepParams>();
   SPLAT_TRY(launch_load_words(c, static_cast<const char*>(t->params_host_dev) + slot * sizeof(StepParams),
                               t->params_dev.ptr, (int)(sizeof(StepParams) / 4)));
-  SPLAT_TRY(render_view_dev(c, t->cur.params.as<float>(), n, cap, cam, opts, bg, t->vb, sp));
+  SPLAT_TRY(render_view_dev(c, t->cur.params.as<float>(), n, cap, cam, opts, bg, t->vb, sp, bf16_copy(t)));
   const size_t npix = (size_t)cam.width * cam.height;
   SPLAT_TRY(t->pred_grad.ensure(npix * 12));
   SPLAT_TRY(t->loss_out.ensure(16));
@@ -248,7 +260,7 @@ Status body(splat_trainer* t, const IterPlan& p, int slot) {
   SPLAT_TRY(launch_project_bwd_adam(c, t->cur.params.as<float>(), t->cur.m.as<float>(), t->cur.v.as<float>(), n, cap,
                                     cam, opts, t->vb.proj.as<float>(), t->pgrad.as<float>(),
                                     p.densify_window ? t->stats.ptr : nullptr, cfg.absgrad, p.adam_step, p.lr,
-                                    t->vb.overflow_flag(), sp));
+                                    t->vb.overflow_flag(), sp, const_cast<void*>(bf16_copy(t))));
   SPLAT_TRY(launch_publish_u32_to(c, t->loss_out.as<uint32_t>(), 3, t->vb.counters.as<uint32_t>(), 3,
                                   static_cast<uint32_t*>(t->slots_dev) + 16 * slot));
   return Status::ok();
@@ -397,6 +409,7 @@ Status density_control(splat_trainer* t, const IterPlan& p, splat_step_info* inf
     t->n = new_n;
     SPLAT_TRY(ensure_stats(t, t->cur.cap));
     SPLAT_TRY(reset_stats(t));
+    SPLAT_TRY(refresh_bf16(t));
     info->densified = 1;
     info->cloned = plan.cloned;
     info->split = plan.split;
@@ -561,7 +574,7 @@ SPLAT_API int splat_trainer_destroy(splat_trainer* t) {
     cudaStreamSynchronize(t->c->stream);
     t->cur.release();
     t->next.release();
-    for (DevBuf* b : {&t->pgrad, &t->stats, &t->pred_grad, &t->loss_out, &t->normals, &t->init}) b->release();
+    for (DevBuf* b : {&t->pgrad, &t->stats, &t->pred_grad, &t->loss_out, &t->normals, &t->init, &t->bf16}) b->release();
     t->vb.release();
     for (View* v : t->views) {
       v->rgb.release();
@@ -643,6 +656,7 @@ SPLAT_API int splat_trainer_start(splat_trainer* t) {
   if (s.good()) s = reset_stats(t);
   if (s.good()) s = cuda_status(cudaMemsetAsync(t->cur.m.ptr, 0, t->cur.m.bytes, c->stream), "zero m");
   if (s.good()) s = cuda_status(cudaMemsetAsync(t->cur.v.ptr, 0, t->cur.v.bytes, c->stream), "zero v");
+  if (s.good()) s = refresh_bf16(t);
   if (s.good()) s = cuda_status(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
   return s.good() ? SPLAT_OK : tfail(t, s);
 }
@@ -702,7 +716,8 @@ SPLAT_API int splat_trainer_render(splat_trainer* t, const splat_camera* cam, fl
   opts.eps2d = 0.3f;
   opts.antialias = t->cfg.antialias;
   opts.sh_degree = t->sh_degree;
-  Status s = render_view(c, t->cur.params.as<float>(), t->n, t->cur.cap, *cam, opts, bg, t->vb, nullptr);
+  opts.fp64_conic = t->cfg.fp64_conic;
+  Status s = render_view(c, t->cur.params.as<float>(), t->n, t->cur.cap, *cam, opts, bg, t->vb, nullptr, bf16_copy(t));
   if (s.good())
     s = cuda_status(cudaMemcpyAsync(image_host, t->vb.image.ptr, (size_t)cam->width * cam->height * 12,
                                     cudaMemcpyDeviceToHost, c->stream),

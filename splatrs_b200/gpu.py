@@ -362,14 +362,33 @@ def adam_step(ctx: Context, planes, grads, m, v, n: int, cap: int, step: int, lr
           ctx.h)
 
 
+def params_to_bf16(ctx: Context, planes, n: int, cap: int) -> torch.Tensor:
+    """BF16 render copy of parameter planes 1..14 (splat_params_to_bf16)."""
+    out = torch.empty((PLANES - 1) * cap * 4, dtype=torch.bfloat16, device=planes.device)
+    check(ctx.lib.splat_params_to_bf16(ctx.h, _ptr(planes), n, cap, _ptr(out)), ctx.h)
+    return out
+
+
+def project_all_bf16(ctx: Context, planes, bf16, n: int, cap: int, cam: Camera, opts: ProjOpts) -> Projection:
+    """project_all reading quaternion, log-scales and SH from the BF16 copy."""
+    dev = planes.device
+    rec = torch.empty((n, PROJ_FLOATS), dtype=torch.float32, device=dev)
+    nt = torch.empty(n, dtype=torch.int32, device=dev)
+    dr = torch.empty(2, dtype=torch.int32, device=dev)
+    check(ctx.lib.splat_project_fwd_bf16(ctx.h, _ptr(planes), _ptr(bf16), n, cap, C.byref(cam), C.byref(opts),
+                                         _ptr(rec), _ptr(nt), _ptr(dr)), ctx.h)
+    return Projection(rec, nt, dr, n, cam.width, cam.height)
+
+
 def project_backward_adam(ctx: Context, planes, m, v, n: int, cap: int, cam: Camera, opts: ProjOpts,
-                          proj: Projection, pgrad, step: int, lr: LearningRates, stats=None, absgrad=False):
+                          proj: Projection, pgrad, step: int, lr: LearningRates, stats=None, absgrad=False,
+                          bf16=None):
     """project_backward_all (src/project.rs:477-493) fused with Adam::step
     (src/adam.rs:77-161): planes, m and v updated in place; `step` is the count after the
     increment."""
     check(ctx.lib.splat_project_bwd_adam(ctx.h, _ptr(planes), _ptr(m), _ptr(v), n, cap, C.byref(cam), C.byref(opts),
                                          _ptr(proj.rec), _ptr(pgrad), _ptr(stats), int(bool(absgrad)), step,
-                                         C.byref(lr)), ctx.h)
+                                         C.byref(lr), _ptr(bf16)), ctx.h)
 
 
 def densify_and_prune(ctx: Context, planes, m, v, n: int, cap: int, stats, cfg: DensifyConfig, extent: float,

@@ -376,3 +376,103 @@ def test_fast_exp_bound_behind_backward_screening(ctx):
     G.check(ctx.lib.splat_diag_fast_exp_error(ctx.h, 0.0, 6.05, 1, C.byref(out)), ctx.h)
     print(f"\nfast exp max relative error on [-6.05, 0]: {out.value:.3e}")
     assert 0.0 < out.value < 3e-6
+
+
+def _bf16_round_params(g):
+    """Reference records with quaternion, log-scales and SH rounded to bf16 (nearest even),
+    the values the BF16 render copy holds; means and opacity stay f32."""
+    r = g.copy()
+    cols = list(range(3, 10)) + list(range(11, 59))
+    r[:, cols] = torch.from_numpy(g[:, cols]).to(torch.bfloat16).to(torch.float32).numpy()
+    return r
+
+
+@pytest.mark.parametrize("sh_degree", [0, 3])
+def test_bf16_projection_equals_f32_on_rounded_params(ctx, sh_degree):
+    """splat_project_fwd_bf16 reads quaternion, log-scales and SH from the BF16 copy: its
+    records are bit-identical to splat_project_fwd on parameters rounded to bf16."""
+    g, cam = small_scene(seed=61)
+    n = g.shape[0]
+    opts = ProjOpts.make(sh_degree=sh_degree, antialias=True)
+    planes = G.params_to_planes(ctx, dev(g), n)
+    bf = G.params_to_bf16(ctx, planes, n, n)
+    got = G.project_all_bf16(ctx, planes, bf, n, n, Camera.from_record(cam), opts)
+    want = G.project_all(ctx, G.params_to_planes(ctx, dev(_bf16_round_params(g)), n), n, n, Camera.from_record(cam),
+                         opts)
+    assert torch.equal(got.rec, want.rec) and torch.equal(got.num_tiles, want.num_tiles)
+    assert torch.equal(got.depth_range, want.depth_range)
+    p64 = O.project_all(g.astype(np.float64), cam.astype(np.float64), antialias=True, sh_degree=sh_degree,
+                        dtype=np.float64)
+    vis = p64[:, 6] > 0
+    rel = np.abs(got.to_reference(ctx).cpu().numpy()[vis, 7:11] - p64[vis, 7:11]).max()
+    print(f"\nbf16 storage: opacity/colour max-abs vs the f64 oracle of the f32 parameters {rel:.2e}")
+
+
+def test_bf16_fused_adam_equals_separate_steps(ctx):
+    """splat_project_bwd_adam with a BF16 copy: the gradient is taken at the copy's values
+    and Adam updates the f32 master, bit-identical to splat_project_bwd on the rounded
+    parameters followed by splat_adam_step on the master; the copy is rewritten as the
+    rounding of the updated master."""
+    g, cam = small_scene(seed=62, n=2000)
+    n = g.shape[0]
+    rng = np.random.default_rng(62)
+    opts = ProjOpts.make(sh_degree=3)
+    lr = LearningRates(0.00016 * 3.3, 0.005, 0.001, 0.025, 0.0025, 0.0025 / 20)
+    master = G.params_to_planes(ctx, dev(g), n)
+    bf = G.params_to_bf16(ctx, master, n, n)
+    sep = master.clone()
+    fm, fv = torch.zeros_like(master), torch.zeros_like(master)
+    sm, sv = torch.zeros_like(master), torch.zeros_like(master)
+    for step in (1, 2):
+        pg = G.pgrad_from_reference(dev(rng.uniform(-1, 1, (n, 9)).astype(np.float32)))
+        rounded = G.params_to_planes(ctx, dev(_bf16_round_params(G.planes_to_params(ctx, sep, n, n).cpu().numpy())), n)
+        proj = G.project_all(ctx, rounded, n, n, Camera.from_record(cam), opts)
+        gp = G.project_backward_all(ctx, rounded, n, n, Camera.from_record(cam), opts, proj, pg)
+        G.adam_step(ctx, sep, gp, sm, sv, n, n, step, lr)
+        projb = G.project_all_bf16(ctx, master, bf, n, n, Camera.from_record(cam), opts)
+        assert torch.equal(projb.rec, proj.rec)
+        G.project_backward_adam(ctx, master, fm, fv, n, n, Camera.from_record(cam), opts, projb, pg, step, lr, bf16=bf)
+        assert torch.equal(master, sep) and torch.equal(fm, sm) and torch.equal(fv, sv)
+        assert torch.equal(bf, G.params_to_bf16(ctx, sep, n, n))
+
+
+def _needles(seed, n=3000):
+    """Long thin Gaussians (one axis e^2, two e^-6) close to the camera: their projected
+    2x2 covariances are nearly rank one."""
+    rng = np.random.default_rng(seed)
+    g = scenes.random_gaussians(rng, n, -0.6, 0.6, -6.0, 0.0, 1.0)
+    g[:, 3] = 2.0
+    cam = scenes.look_at(640, 480, 500.0, 500.0, (0.0, 0.0, -3.0), (0, 0, 0))
+    return g, cam
+
+
+def test_fp64_conic_resolves_ill_conditioned_covariances(ctx):
+    """fp64_conic: for needle-like Gaussians whose f32 2x2 determinant is ill-conditioned
+    the conic matches the f64 oracle far better than the f32 path; ordinary scenes never
+    take the f64 path (records identical with and without it)."""
+    g, cam = _needles(63)
+    n = g.shape[0]
+    planes = G.params_to_planes(ctx, dev(g), n)
+    off = G.project_all(ctx, planes, n, n, Camera.from_record(cam), ProjOpts.make(sh_degree=0))
+    on = G.project_all(ctx, planes, n, n, Camera.from_record(cam), ProjOpts.make(sh_degree=0, fp64_conic=True))
+    p64 = O.project_all(g.astype(np.float64), cam.astype(np.float64), sh_degree=0, dtype=np.float64)
+    ro, rn = off.to_reference(ctx).cpu().numpy(), on.to_reference(ctx).cpu().numpy()
+    vis = (p64[:, 6] > 0) & (ro[:, 6] > 0) & (rn[:, 6] > 0)
+    A, B, Cc = p64[vis, 2], p64[vis, 3], p64[vis, 4]
+    det = 1.0 / (A * Cc - B * B)
+    trace = (A + Cc) * det
+    ill = det < 1e-6 * trace * trace
+    assert ill.sum() > 50, ill.sum()
+    scale = np.abs(p64[vis][:, 2:5]).max(1, keepdims=True)
+    e_off = (np.abs(ro[vis][:, 2:5] - p64[vis][:, 2:5]) / scale).max(1)
+    e_on = (np.abs(rn[vis][:, 2:5] - p64[vis][:, 2:5]) / scale).max(1)
+    print(f"\nill-conditioned: {ill.sum()} of {vis.sum()}; conic rel. error vs f64 oracle: "
+          f"f32 median {np.median(e_off[ill]):.2e} max {e_off[ill].max():.2e}, "
+          f"f64 re-solve median {np.median(e_on[ill]):.2e} max {e_on[ill].max():.2e}")
+    assert e_on[ill].max() < 1e-4
+    assert np.median(e_off[ill]) > 10 * np.median(e_on[ill])
+    g2, cam2 = small_scene(seed=64)
+    p2 = G.params_to_planes(ctx, dev(g2), g2.shape[0])
+    a = G.project_all(ctx, p2, g2.shape[0], g2.shape[0], Camera.from_record(cam2), ProjOpts.make())
+    b = G.project_all(ctx, p2, g2.shape[0], g2.shape[0], Camera.from_record(cam2), ProjOpts.make(fp64_conic=True))
+    assert torch.equal(a.rec, b.rec)

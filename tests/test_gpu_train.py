@@ -316,20 +316,40 @@ def test_trainer_run_matches_step(ctx):
 
 @pytest.mark.parametrize("use_run", [False, True])
 def test_trainer_entry_overflow_is_redone(ctx, use_run):
-    """With room for only 64 tile entries the first iterations overflow the binning; each is
-    redone with larger buffers (and its Adam update applied once), so training matches a
-    run that never overflowed."""
-    views, extent, init = _views_and_init(200, 30, 8, 48, 36, [1.0, 1.0, 1.0], truncate=10)
-    ref = G.Trainer(ctx, init, extent, views, **_cfg_small())
+    """With room for only 64 tile entries the first iteration overflows the binning (under
+    splat_trainer_run the iteration queued behind it is voided too); each is redone with
+    larger buffers and its Adam update applied once, so training matches a run that never
+    overflowed (no densification, so runs differ only by float-atomic order)."""
+    views, extent, init = _views_and_init(100, 40, 10, 64, 48, [0.0, 0.0, 0.0])
+    cfg = dict(iterations=300, densify=0, sh_degree=1, sh_degree_interval=100, position_lr_max_steps=300, seed=4)
+    ref = G.Trainer(ctx, init, extent, views, **cfg)
     ref.run(300)
-    t = G.Trainer(ctx, init, extent, views, entry_capacity=64, **_cfg_small())
+    t = G.Trainer(ctx, init, extent, views, entry_capacity=64, **cfg)
+    first = t.step() if not use_run else t.run(1)
+    assert first["entries"] > 64
     if use_run:
-        t.run(300)
+        t.run(299)
     else:
-        for _ in range(300):
+        for _ in range(299):
             t.step()
     assert np.isfinite(t.model()[:, 0:10]).all()
     pr, pt = _evaluate(ref, views), _evaluate(t, views)
-    assert abs(pr - pt) < 0.5, (pr, pt)
+    assert abs(pr - pt) < 0.3, (pr, pt)
     ref.close()
     t.close()
+
+
+def test_trainer_bf16_storage_trains_like_f32(ctx):
+    """bf16_storage + fp64_conic (not in the reference): rendering from the BF16 copy with
+    f32 master parameters trains to the quality of the f32 trainer."""
+    views, extent, init = _views_and_init(100, 40, 10, 64, 48, [0.0, 0.0, 0.0])
+    cfg = dict(iterations=600, densify=0, sh_degree=1, sh_degree_interval=200, position_lr_max_steps=600, seed=3)
+    a = G.Trainer(ctx, init, extent, views, **cfg)
+    a.run(600)
+    b = G.Trainer(ctx, init, extent, views, bf16_storage=1, fp64_conic=1, **cfg)
+    b.run(600)
+    pa, pb = _evaluate(a, views), _evaluate(b, views)
+    print(f"\nf32 {pa:.2f} dB, bf16 storage {pb:.2f} dB")
+    assert pb > pa - 0.5
+    a.close()
+    b.close()
