@@ -130,6 +130,10 @@ typedef struct splat_train_config {
    * conics in f64 (splat_proj_opts.fp64_conic). */
   int32_t bf16_storage;
   int32_t fp64_conic;
+  /* Not in the reference: views per iteration (0 or 1: one, as the reference; at most 8).
+   * A batch renders and back-propagates its views (of any sizes) in one launch per stage
+   * and takes one Adam step on the mean of their gradients. */
+  uint32_t batch_views;
 } splat_train_config;
 
 typedef struct splat_ctx splat_ctx;

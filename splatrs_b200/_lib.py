@@ -84,7 +84,8 @@ class TrainConfig(C.Structure):
                 ("max_screen_size", C.c_int64), ("absgrad", C.c_int32), ("antialias", C.c_int32),
                 ("white_background", C.c_int32), ("sh_degree", C.c_int32), ("sh_degree_interval", C.c_uint32),
                 ("near_plane", C.c_float), ("seed", C.c_uint64), ("max_gaussians", C.c_uint64),
-                ("entry_capacity", C.c_uint64), ("bf16_storage", C.c_int32), ("fp64_conic", C.c_int32)]
+                ("entry_capacity", C.c_uint64), ("bf16_storage", C.c_int32), ("fp64_conic", C.c_int32),
+                ("batch_views", C.c_uint32)]
 
     DEFAULTS = dict(iterations=30000, position_lr_init=0.00016, position_lr_final=0.0000016,
                     position_lr_max_steps=30000, feature_lr=0.0025, opacity_lr=0.025, scaling_lr=0.005,
@@ -92,7 +93,8 @@ class TrainConfig(C.Structure):
                     densification_interval=100, opacity_reset_interval=3000, densify_grad_threshold=0.0002,
                     percent_dense=0.01, min_opacity=0.005, max_screen_size=-1, absgrad=0, antialias=0,
                     white_background=0, sh_degree=3, sh_degree_interval=1000, near_plane=0.2, seed=0,
-                    max_gaussians=0, entry_capacity=0, bf16_storage=0, fp64_conic=0)
+                    max_gaussians=0, entry_capacity=0, bf16_storage=0, fp64_conic=0,
+                    batch_views=0)
 
     @classmethod
     def make(cls, **kw):

@@ -15,12 +15,39 @@ struct StepParams {
   const void* target;  // the view's 8-bit pixels
 };
 
+// A batch of views rendered and back-propagated together, one launch per stage. Records
+// are view-major (record r = v * n + i for Gaussian i), tiles are numbered across the
+// batch (view v owns global tiles [tile_start[v], tile_start[v + 1])), images are
+// concatenated (view v's pixels start at pix_start[v]) and SSIM blocks likewise. Kernels
+// launched for a capacity exit in blocks past the batch's totals, so one captured graph
+// serves any mix of view sizes.
+constexpr int kMaxViews = 8;
+struct BatchTable {
+  splat_camera cam[kMaxViews];
+  const void* target[kMaxViews];
+  uint32_t tiles_x[kMaxViews];
+  uint32_t tile_start[kMaxViews + 1];
+  uint32_t loss_blocks_x[kMaxViews];
+  uint32_t loss_start[kMaxViews + 1];
+  uint64_t pix_start[kMaxViews + 1];
+  AdamArgs adam;
+  int32_t views;
+  float inv_views;
+};
+
+__device__ __forceinline__ int batch_view_of(const uint32_t* start, int views, uint32_t b) {
+  int v = 0;
+  while (v + 1 < views && b >= start[v + 1]) v++;
+  return v;
+}
+
 Status launch_params_from_aos(Ctx* c, const float* aos, int64_t n, float* planes, int64_t cap);
 Status launch_params_to_aos(Ctx* c, const float* planes, int64_t n, int64_t cap, float* aos);
 
 Status launch_project_fwd(Ctx* c, const float* planes, int64_t n, int64_t cap, const splat_camera& cam,
                           const splat_proj_opts& opts, float* proj, uint32_t* num_tiles, uint32_t* depth_range,
-                          const StepParams* sp = nullptr, const void* bf16 = nullptr);
+                          const StepParams* sp = nullptr, const void* bf16 = nullptr,
+                          const BatchTable* bt = nullptr);
 Status launch_proj_from_reference(Ctx* c, const float* p15, int64_t n, uint32_t width, uint32_t height, float* proj,
                                   uint32_t* num_tiles, uint32_t* depth_range);
 Status launch_proj_to_reference(Ctx* c, const float* proj, int64_t n, float* p15);
@@ -37,6 +64,14 @@ Status launch_project_bwd_adam(Ctx* c, float* planes, float* m, float* v, int64_
                                const uint32_t* skip = nullptr, const StepParams* sp = nullptr,
                                void* bf16 = nullptr);
 
+// A batch's projection backward (records view-major, screen-space gradient planes with
+// stride pcap) summed over the views that see each Gaussian, then one Adam step with the
+// batch's AdamArgs (bt->adam); densification statistics accumulate per view.
+Status launch_project_bwd_batch_adam(Ctx* c, float* planes, float* m, float* v, int64_t n, int64_t cap,
+                                     const splat_proj_opts& opts, const float* proj, const float* pgrad, int64_t pcap,
+                                     void* stats, int absgrad, const uint32_t* skip, const BatchTable* bt,
+                                     void* bf16);
+
 // The BF16 render copy of parameter planes 1..14 (quaternion, log-scales, SH; 4 x bf16 per
 // Gaussian and plane, plane q at (q - 1) * cap, rounded to nearest even). With a copy,
 // launch_project_fwd reads those planes from it, and launch_project_bwd_adam computes the
@@ -51,7 +86,8 @@ Status launch_scan_u32(Ctx* c, const uint32_t* in, int64_t n, uint32_t* out, int
 size_t dev_sort_scratch_bytes(int64_t E_cap);
 Status launch_bin_sort_dev(Ctx* c, const float* proj, const uint32_t* entry_offset, int64_t n, const uint64_t* E_dev,
                            int64_t E_cap, const uint32_t* depth_range_dev, uint32_t width, uint32_t height,
-                           void* scratch, uint32_t* gauss_out, uint32_t* ranges, uint32_t* overflow);
+                           void* scratch, uint32_t* gauss_out, uint32_t* ranges, uint32_t* overflow,
+                           const BatchTable* bt = nullptr, int64_t n_view = 1, uint32_t tiles_cap = 0);
 
 // Fills `words` 32-bit words at `dst` with `value` by a kernel on the context stream (in
 // place of cudaMemsetAsync, so the compute stream holds kernels only).
@@ -72,15 +108,17 @@ Status launch_bin_sort(Ctx* c, const float* proj, const uint32_t* entry_offset, 
 
 Status launch_raster_fwd(Ctx* c, const float* proj, const uint32_t* gauss, const uint32_t* ranges, uint32_t width,
                          uint32_t height, const float bg[3], float* image, float* final_t, uint32_t* n_contrib,
-                         uint64_t* pairs);
+                         uint64_t* pairs, const BatchTable* bt = nullptr, uint32_t tiles_cap = 0);
 Status launch_raster_bwd(Ctx* c, const float* proj, const uint32_t* gauss, const uint32_t* ranges, uint32_t width,
                          uint32_t height, const float bg[3], const float* final_t, const uint32_t* n_contrib,
-                         const float* dimage, float* pgrad, int64_t cap, uint64_t* pairs);
+                         const float* dimage, float* pgrad, int64_t cap, uint64_t* pairs,
+                         const BatchTable* bt = nullptr, uint32_t tiles_cap = 0);
 
 Status launch_diag_fast_exp(Ctx* c, float magnitude_lo, float magnitude_hi, int negative, float* out_host);
 
 Status launch_loss(Ctx* c, const float* pred, const void* target, int target_u8, uint32_t width, uint32_t height,
-                   float lambda, float* grad, float* out3, const StepParams* sp = nullptr);
+                   float lambda, float* grad, float* out3, const StepParams* sp = nullptr,
+                   const BatchTable* bt = nullptr, uint32_t blocks_cap = 0, uint64_t pix_cap = 0);
 
 // Copies `words` 32-bit words (a StepParams) from mapped host memory to device memory with
 // one warp.

@@ -36,12 +36,27 @@ __global__ void __launch_bounds__(kLossThreads) ssim_fwd_kernel(const float* __r
                                                                 const void* __restrict__ target_arg, int target_u8,
                                                                 uint32_t width, uint32_t height, LossKernel K,
                                                                 float* __restrict__ dmaps, double* __restrict__ sums,
-                                                                const StepParams* __restrict__ sp) {
+                                                                const StepParams* __restrict__ sp,
+                                                                const BatchTable* __restrict__ bt) {
   const void* target = sp ? sp->target : target_arg;
+  int bxi = blockIdx.x, byi = blockIdx.y;
+  if (bt) {  // a batch: flat block index -> view, block within the view, buffer offsets
+    if (blockIdx.x >= bt->loss_start[bt->views]) return;
+    const int v = batch_view_of(bt->loss_start, bt->views, blockIdx.x);
+    const uint32_t local = blockIdx.x - bt->loss_start[v];
+    bxi = local % bt->loss_blocks_x[v];
+    byi = local / bt->loss_blocks_x[v];
+    width = bt->cam[v].width;
+    height = bt->cam[v].height;
+    pred += 3 * bt->pix_start[v];
+    target = bt->target[v];
+    dmaps += 9 * bt->pix_start[v];
+    sums += 3 * v;
+  }
   __shared__ float sx[kLE][kLE], sy[kLE][kLE];
   __shared__ float h[5][kLE][kLT];
   __shared__ double red[3][kLossThreads / 32];
-  const int ox0 = blockIdx.x * kLT, oy0 = blockIdx.y * kLT;
+  const int ox0 = bxi * kLT, oy0 = byi * kLT;
   const int tid = threadIdx.x;
   const float c1 = 0.01f * 0.01f, c2 = 0.03f * 0.03f;
   double s_ssim = 0.0, s_l1 = 0.0, s_se = 0.0;
@@ -152,11 +167,28 @@ __global__ void __launch_bounds__(kLossThreads) ssim_bwd_kernel(const float* __r
                                                                 uint32_t width, uint32_t height, LossKernel K,
                                                                 const float* __restrict__ dmaps, float lambda,
                                                                 float* __restrict__ grad,
-                                                                const StepParams* __restrict__ sp) {
+                                                                const StepParams* __restrict__ sp,
+                                                                const BatchTable* __restrict__ bt) {
   const void* target = sp ? sp->target : target_arg;
+  int bxi = blockIdx.x, byi = blockIdx.y;
+  float scale = 1.0f;  // a batch averages the views' gradients
+  if (bt) {
+    if (blockIdx.x >= bt->loss_start[bt->views]) return;
+    const int v = batch_view_of(bt->loss_start, bt->views, blockIdx.x);
+    const uint32_t local = blockIdx.x - bt->loss_start[v];
+    bxi = local % bt->loss_blocks_x[v];
+    byi = local / bt->loss_blocks_x[v];
+    width = bt->cam[v].width;
+    height = bt->cam[v].height;
+    pred += 3 * bt->pix_start[v];
+    target = bt->target[v];
+    dmaps += 9 * bt->pix_start[v];
+    grad += 3 * bt->pix_start[v];
+    scale = bt->inv_views;
+  }
   __shared__ float sm[3][kLE][kLE];
   __shared__ float h[3][kLE][kLT];
-  const int ox0 = blockIdx.x * kLT, oy0 = blockIdx.y * kLT;
+  const int ox0 = bxi * kLT, oy0 = byi * kLT;
   const int tid = threadIdx.x;
   const size_t npix3 = (size_t)width * height * 3;
   const float inv_n = 1.0f / (float)npix3;
@@ -216,14 +248,24 @@ __global__ void __launch_bounds__(kLossThreads) ssim_bwd_kernel(const float* __r
       const float dssim = (bmu + 2.0f * x * bexx + y * bexy) * inv_n;
       const float d = x - y;
       const float sign = d > 0.0f ? 1.0f : (d < 0.0f ? -1.0f : 0.0f);
-      grad[idx] = w1 * sign - lambda * dssim;
+      grad[idx] = (w1 * sign - lambda * dssim) * scale;
     }
     __syncthreads();
   }
 }
 
 // loss = (1 - lambda) * l1 + lambda * (1 - ssim) (loss.rs:147-154) and PSNR (loss.rs:175-190).
-__global__ void loss_finalize_kernel(const double* __restrict__ sums, uint64_t n, float lambda, float* __restrict__ out) {
+__global__ void loss_finalize_kernel(const double* __restrict__ sums, uint64_t n, float lambda, float* __restrict__ out,
+                                     const BatchTable* __restrict__ bt) {
+  if (bt) {  // one thread per view: its own sums, pixel count and outputs
+    const int v = threadIdx.x;
+    if (v >= bt->views) return;
+    sums += 3 * v;
+    out += 3 * v;
+    n = 3 * (bt->pix_start[v + 1] - bt->pix_start[v]);
+  } else if (threadIdx.x > 0) {
+    return;
+  }
   const float inv_n = 1.0f / (float)n;
   const float l1 = (float)sums[1] * inv_n;
   const float ssim = (float)(sums[0] / (double)n);
@@ -248,19 +290,22 @@ LossKernel make_loss_kernel() {
 }
 
 Status launch_loss(Ctx* c, const float* pred, const void* target, int target_u8, uint32_t width, uint32_t height,
-                   float lambda, float* grad, float* out3, const StepParams* sp) {
-  const size_t npix3 = (size_t)width * height * 3;
+                   float lambda, float* grad, float* out3, const StepParams* sp, const BatchTable* bt,
+                   uint32_t blocks_cap, uint64_t pix_cap) {
+  const size_t npix3 = bt ? (size_t)pix_cap * 3 : (size_t)width * height * 3;
+  const int nsums = bt ? kMaxViews : 1;
   float* dmaps = nullptr;
   double* sums = nullptr;
   SPLAT_TRY(arena_reserve(c, npix3 * 3 * 4, (void**)&dmaps));
-  SPLAT_TRY(arena_reserve(c, 3 * 8, (void**)&sums));
-  SPLAT_TRY(launch_fill_u32(c, sums, 3 * 2, 0u));
+  SPLAT_TRY(arena_reserve(c, 3 * 8 * nsums, (void**)&sums));
+  SPLAT_TRY(launch_fill_u32(c, sums, 3 * 2 * nsums, 0u));
   const LossKernel K = make_loss_kernel();
-  const dim3 grid(ceil_div(width, kLT), ceil_div(height, kLT));
-  ssim_fwd_kernel<<<grid, kLossThreads, 0, c->stream>>>(pred, target, target_u8, width, height, K, dmaps, sums, sp);
+  const dim3 grid = bt ? dim3(blocks_cap) : dim3(ceil_div(width, kLT), ceil_div(height, kLT));
+  ssim_fwd_kernel<<<grid, kLossThreads, 0, c->stream>>>(pred, target, target_u8, width, height, K, dmaps, sums, sp,
+                                                         bt);
   ssim_bwd_kernel<<<grid, kLossThreads, 0, c->stream>>>(pred, target, target_u8, width, height, K, dmaps, lambda,
-                                                         grad, sp);
-  loss_finalize_kernel<<<1, 1, 0, c->stream>>>(sums, npix3, lambda, out3);
+                                                         grad, sp, bt);
+  loss_finalize_kernel<<<1, bt ? kMaxViews : 1, 0, c->stream>>>(sums, npix3, lambda, out3, bt);
   c->launches.count += 3;
   SPLAT_LAUNCHED("loss kernels");
   return Status::ok();

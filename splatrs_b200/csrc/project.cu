@@ -494,8 +494,16 @@ __global__ void __launch_bounds__(256) project_fwd_kernel(const float4* __restri
                                                           float4* __restrict__ rec, uint32_t* __restrict__ num_tiles,
                                                           uint32_t* __restrict__ depth_range,
                                                           const StepParams* __restrict__ sp,
-                                                          const uint2* __restrict__ bf) {
-  const splat_camera cam = sp ? sp->cam : cam_arg;
+                                                          const uint2* __restrict__ bf,
+                                                          const BatchTable* __restrict__ bt) {
+  // A batch launch has one grid row per view; its records follow view-major.
+  const int view = bt ? (int)blockIdx.y : 0;
+  if (bt && view >= bt->views) return;
+  const splat_camera cam = bt ? bt->cam[view] : (sp ? sp->cam : cam_arg);
+  if (bt) {
+    rec += 4 * (size_t)view * n;
+    num_tiles += (size_t)view * n;
+  }
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   bool visible = false;
   float depth = 0.0f;
@@ -584,53 +592,32 @@ __global__ void proj_to_reference_kernel(const float4* __restrict__ rec, int64_t
   p[14] = (float)(tmax >> 16);
 }
 
-// project_backward_one (project.rs:335-474), plus DensifyStats::accumulate
-// (densify.rs:36-60) when `stats` is given. With ADAM the 59 gradients never leave the
-// registers: Adam::step (adam.rs:77-161) updates the parameters in place and the moments m
-// and v, over every plane (zero gradients still decay the moments, adam.rs:56-60).
-template <int DEG, bool ADAM, bool BF16>
-__global__ void __launch_bounds__(128) project_bwd_kernel(const float4* __restrict__ planes, int64_t n, int64_t cap,
-                                                          splat_camera cam_arg, splat_proj_opts opts,
-                                                          const float4* __restrict__ rec,
-                                                          const float4* __restrict__ pgrad,
-                                                          float4* __restrict__ out, float* __restrict__ stat_accum,
-                                                          uint32_t* __restrict__ stat_denom,
-                                                          uint32_t* __restrict__ stat_maxr, int absgrad,
-                                                          float4* __restrict__ adam_m, float4* __restrict__ adam_v,
-                                                          AdamArgs adam_arg, const uint32_t* __restrict__ skip,
-                                                          const StepParams* __restrict__ sp, uint2* bf) {
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  if (ADAM && skip && *skip) return;
-  const splat_camera cam = sp ? sp->cam : cam_arg;
-  const AdamArgs adam = (ADAM && sp) ? sp->adam : adam_arg;
-  const float4 g0 = pgrad[i], g1 = pgrad[cap + i], g2 = pgrad[2 * cap + i];
-  // ProjGrad fields.
+// project_backward_one (project.rs:335-474) for parameters g seen by camera cam, given the
+// screen-space gradient (g0, g1, g2 as in the ProjGrad planes): the 59 parameter gradients,
+// zero when the Gaussian is culled.
+struct ParamGrad {
+  float mean[3], op, q[4], ls[3], sh[48];
+};
+
+template <int DEG>
+__device__ __forceinline__ void proj_grad_one(const GParams& g, const splat_camera& cam, const splat_proj_opts& opts,
+                                              const float4 g0, const float4 g1, const float4 g2, ParamGrad& out) {
   const float dp_mean2d[2] = {g0.x, g0.y};
   const float dp_conic[3] = {g0.z, g0.w, g1.x};
   const float dp_opacity = g1.y;
   const float dp_color[3] = {g1.z, g1.w, g2.x};
-
-  if (stat_accum != nullptr) {
-    const uint32_t radius = fbits(rec[4 * i + 3].y);
-    if (radius > 0) {
-      const float sx = (float)cam.width * 0.5f;
-      const float sy = (float)cam.height * 0.5f;
-      const float gx = (absgrad ? g2.y : g0.x) * sx;
-      const float gy = (absgrad ? g2.z : g0.y) * sy;
-      stat_accum[i] += sqrtf(gx * gx + gy * gy);
-      stat_denom[i] += 1u;
-      stat_maxr[i] = max(stat_maxr[i], radius);
-    }
-  }
-
-  float o_mean[3] = {0, 0, 0}, o_ls[3] = {0, 0, 0}, o_q[4] = {0, 0, 0, 0}, o_op = 0.0f;
-  float o_sh[48];
+  float* o_mean = out.mean;
+  float* o_ls = out.ls;
+  float* o_q = out.q;
+  float* o_sh = out.sh;
+  float& o_op = out.op;
+#pragma unroll
+  for (int q = 0; q < 3; q++) o_mean[q] = o_ls[q] = 0.0f;
+#pragma unroll
+  for (int q = 0; q < 4; q++) o_q[q] = 0.0f;
+  o_op = 0.0f;
 #pragma unroll
   for (int q = 0; q < 48; q++) o_sh[q] = 0.0f;
-
-  GParams g;
-  load_params<DEG, BF16>(planes, cap, i, g, bf);
   CoreOut k;
   if (core<DEG>(g, cam, opts, k)) {
     constexpr int NC = (DEG + 1) * (DEG + 1);
@@ -777,6 +764,52 @@ __global__ void __launch_bounds__(128) project_bwd_kernel(const float4* __restri
       for (int ii = 0; ii < 4; ii++) o_q[ii] = (dq[ii] - u[ii] * dot) / nrm;
     }
   }
+}
+
+// project_backward_one (project.rs:335-474), plus DensifyStats::accumulate
+// (densify.rs:36-60) when `stats` is given. With ADAM the 59 gradients never leave the
+// registers: Adam::step (adam.rs:77-161) updates the parameters in place and the moments m
+// and v, over every plane (zero gradients still decay the moments, adam.rs:56-60).
+template <int DEG, bool ADAM, bool BF16>
+__global__ void __launch_bounds__(128) project_bwd_kernel(const float4* __restrict__ planes, int64_t n, int64_t cap,
+                                                          splat_camera cam_arg, splat_proj_opts opts,
+                                                          const float4* __restrict__ rec,
+                                                          const float4* __restrict__ pgrad,
+                                                          float4* __restrict__ out, float* __restrict__ stat_accum,
+                                                          uint32_t* __restrict__ stat_denom,
+                                                          uint32_t* __restrict__ stat_maxr, int absgrad,
+                                                          float4* __restrict__ adam_m, float4* __restrict__ adam_v,
+                                                          AdamArgs adam_arg, const uint32_t* __restrict__ skip,
+                                                          const StepParams* __restrict__ sp, uint2* bf) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  if (ADAM && skip && *skip) return;
+  const splat_camera cam = sp ? sp->cam : cam_arg;
+  const AdamArgs adam = (ADAM && sp) ? sp->adam : adam_arg;
+  const float4 g0 = pgrad[i], g1 = pgrad[cap + i], g2 = pgrad[2 * cap + i];
+
+  if (stat_accum != nullptr) {
+    const uint32_t radius = fbits(rec[4 * i + 3].y);
+    if (radius > 0) {
+      const float sx = (float)cam.width * 0.5f;
+      const float sy = (float)cam.height * 0.5f;
+      const float gx = (absgrad ? g2.y : g0.x) * sx;
+      const float gy = (absgrad ? g2.z : g0.y) * sy;
+      stat_accum[i] += sqrtf(gx * gx + gy * gy);
+      stat_denom[i] += 1u;
+      stat_maxr[i] = max(stat_maxr[i], radius);
+    }
+  }
+
+  GParams g;
+  load_params<DEG, BF16>(planes, cap, i, g, bf);
+  ParamGrad pgr;
+  proj_grad_one<DEG>(g, cam, opts, g0, g1, g2, pgr);
+  const float* o_mean = pgr.mean;
+  const float* o_q = pgr.q;
+  const float* o_ls = pgr.ls;
+  const float* o_sh = pgr.sh;
+  const float o_op = pgr.op;
   if (!ADAM) {
     out[i] = make_float4(o_mean[0], o_mean[1], o_mean[2], o_op);
     out[cap + i] = make_float4(o_q[0], o_q[1], o_q[2], o_q[3]);
@@ -874,7 +907,7 @@ __global__ void __launch_bounds__(kConvG) planes_to_aos_kernel(const float4* __r
 // ---------------------------------------------------------------------------------------
 Status launch_project_fwd(Ctx* c, const float* planes, int64_t n, int64_t cap, const splat_camera& cam,
                           const splat_proj_opts& opts, float* proj, uint32_t* num_tiles, uint32_t* depth_range,
-                          const StepParams* sp, const void* bf16) {
+                          const StepParams* sp, const void* bf16, const BatchTable* bt) {
   SPLAT_TRY(launch_fill_u32(c, depth_range, 1, 0xffffffffu));
   SPLAT_TRY(launch_fill_u32(c, depth_range + 1, 1, 0u));
   if (n == 0) return Status::ok();
@@ -884,7 +917,8 @@ Status launch_project_fwd(Ctx* c, const float* planes, int64_t n, int64_t cap, c
   float4* r = reinterpret_cast<float4*>(proj);
   const uint2* bf = static_cast<const uint2*>(bf16);
 #define SPLAT_PFWD(D, B) \
-  project_fwd_kernel<D, B><<<grid, bs, 0, c->stream>>>(p, n, cap, cam, opts, r, num_tiles, depth_range, sp, bf)
+  project_fwd_kernel<D, B><<<dim3(grid, bt ? kMaxViews : 1), bs, 0, c->stream>>>(p, n, cap, cam, opts, r, num_tiles, \
+                                                                                 depth_range, sp, bf, bt)
   if (bf) {
     switch (opts.sh_degree) {
       case 0: SPLAT_PFWD(0, true); break;
@@ -978,6 +1012,113 @@ Status launch_project_bwd_adam(Ctx* c, float* planes, float* m, float* v, int64_
                                           make_adam_args(step, lr), skip, sp, static_cast<uint2*>(bf16));
   return project_bwd_launch<true, false>(c, planes, n, cap, cam, opts, proj, pgrad, nullptr, stats, absgrad, m, v,
                                          make_adam_args(step, lr), skip, sp, nullptr);
+}
+
+// A batch's projection backward fused with one Adam step: for every view that sees the
+// Gaussian (radius > 0) the view's 59 gradients (project_backward_one with that view's
+// camera and screen-space gradient, already scaled by 1/views through dL/dpixel) are added,
+// in view order, into a per-thread column of shared memory together with the view's
+// densification statistics; Adam then updates the parameters once with the sum.
+constexpr int kBatchBwdThreads = 128;
+
+template <int DEG, bool BF16>
+__global__ void __launch_bounds__(kBatchBwdThreads) project_bwd_batch_adam_kernel(
+    float4* planes, int64_t n, int64_t cap, splat_proj_opts opts, const float4* __restrict__ rec,
+    const float4* __restrict__ pgrad, int64_t pcap, float* __restrict__ stat_accum, uint32_t* __restrict__ stat_denom,
+    uint32_t* __restrict__ stat_maxr, int absgrad, float4* __restrict__ adam_m, float4* __restrict__ adam_v,
+    const uint32_t* __restrict__ skip, const BatchTable* __restrict__ bt, uint2* bf) {
+  __shared__ float acc[kPlanes * 4][kBatchBwdThreads];
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  if (skip && *skip) return;
+  const int tid = threadIdx.x;
+#pragma unroll
+  for (int f = 0; f < kPlanes * 4; f++) acc[f][tid] = 0.0f;
+  GParams g;
+  load_params<DEG, BF16>(planes, cap, i, g, bf);
+  const int views = bt->views;
+  for (int v = 0; v < views; v++) {
+    const int64_t r = (int64_t)v * n + i;
+    const uint32_t radius = fbits(rec[4 * r + 3].y);
+    if (radius == 0) continue;  // not drawn in this view: zero gradient, no statistics
+    const float4 g0 = pgrad[r], g1 = pgrad[pcap + r], g2 = pgrad[2 * pcap + r];
+    const splat_camera cam = bt->cam[v];
+    if (stat_accum != nullptr) {  // DensifyStats::accumulate per view (densify.rs:36-60)
+      const float sx = (float)cam.width * 0.5f;
+      const float sy = (float)cam.height * 0.5f;
+      const float gx = (absgrad ? g2.y : g0.x) * sx;
+      const float gy = (absgrad ? g2.z : g0.y) * sy;
+      stat_accum[i] += sqrtf(gx * gx + gy * gy);
+      stat_denom[i] += 1u;
+      stat_maxr[i] = max(stat_maxr[i], radius);
+    }
+    ParamGrad pgr;
+    proj_grad_one<DEG>(g, cam, opts, g0, g1, g2, pgr);
+#pragma unroll
+    for (int q = 0; q < 3; q++) acc[q][tid] += pgr.mean[q];
+    acc[3][tid] += pgr.op;
+#pragma unroll
+    for (int q = 0; q < 4; q++) acc[4 + q][tid] += pgr.q[q];
+#pragma unroll
+    for (int q = 0; q < 3; q++) acc[8 + q][tid] += pgr.ls[q];
+#pragma unroll
+    for (int q = 0; q < 48; q++) acc[12 + q][tid] += pgr.sh[q];
+  }
+  const AdamArgs adam = bt->adam;
+#pragma unroll
+  for (int q = 0; q < kPlanes; q++) {
+    const float4 gq = make_float4(acc[4 * q][tid], acc[4 * q + 1][tid], acc[4 * q + 2][tid], acc[4 * q + 3][tid]);
+    const int64_t o = (int64_t)q * cap + i;
+    float4 p = planes[o], m = adam_m[o], v = adam_v[o];
+    adam_plane(adam, q, p, gq, m, v);
+    planes[o] = p;
+    adam_m[o] = m;
+    adam_v[o] = v;
+    if (BF16 && q > 0) bf[(int64_t)(q - 1) * cap + i] = pack_bf16x4(p);
+  }
+}
+
+Status launch_project_bwd_batch_adam(Ctx* c, float* planes, float* m, float* v, int64_t n, int64_t cap,
+                                     const splat_proj_opts& opts, const float* proj, const float* pgrad, int64_t pcap,
+                                     void* stats, int absgrad, const uint32_t* skip, const BatchTable* bt,
+                                     void* bf16) {
+  if (n == 0) return Status::ok();
+  const uint32_t grid = ceil_div(n, kBatchBwdThreads);
+  float4* p = reinterpret_cast<float4*>(planes);
+  const float4* r = reinterpret_cast<const float4*>(proj);
+  const float4* pg = reinterpret_cast<const float4*>(pgrad);
+  float* sa = nullptr;
+  uint32_t *sd = nullptr, *sm = nullptr;
+  if (stats) {
+    sa = reinterpret_cast<float*>(stats);
+    sd = reinterpret_cast<uint32_t*>(sa + cap);
+    sm = sd + cap;
+  }
+  float4* am = reinterpret_cast<float4*>(m);
+  float4* av = reinterpret_cast<float4*>(v);
+  uint2* bf = static_cast<uint2*>(bf16);
+#define SPLAT_PBB(D, B)                                                                                          \
+  project_bwd_batch_adam_kernel<D, B><<<grid, kBatchBwdThreads, 0, c->stream>>>(p, n, cap, opts, r, pg, pcap, sa, sd, \
+                                                                                 sm, absgrad, am, av, skip, bt, bf)
+  if (bf) {
+    switch (opts.sh_degree) {
+      case 0: SPLAT_PBB(0, true); break;
+      case 1: SPLAT_PBB(1, true); break;
+      case 2: SPLAT_PBB(2, true); break;
+      default: SPLAT_PBB(3, true); break;
+    }
+  } else {
+    switch (opts.sh_degree) {
+      case 0: SPLAT_PBB(0, false); break;
+      case 1: SPLAT_PBB(1, false); break;
+      case 2: SPLAT_PBB(2, false); break;
+      default: SPLAT_PBB(3, false); break;
+    }
+  }
+#undef SPLAT_PBB
+  c->launches.count++;
+  SPLAT_LAUNCHED("project_bwd_batch_adam_kernel");
+  return Status::ok();
 }
 
 __global__ void planes_to_bf16_kernel(const float4* __restrict__ planes, int64_t n, int64_t cap,

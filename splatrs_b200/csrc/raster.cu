@@ -184,7 +184,9 @@ __device__ __forceinline__ uint32_t build_warp_list(const uint8_t* __restrict__ 
 __global__ void __launch_bounds__(kRasterThreads, 6) raster_fwd_kernel(
     const float4* __restrict__ rec, const uint32_t* __restrict__ gauss, const uint2* __restrict__ ranges,
     uint32_t width, uint32_t height, uint32_t tiles_x, float bg0, float bg1, float bg2, float* __restrict__ image,
-    float* __restrict__ final_t, uint32_t* __restrict__ n_contrib, unsigned long long* __restrict__ pairs) {
+    float* __restrict__ final_t, uint32_t* __restrict__ n_contrib, unsigned long long* __restrict__ pairs,
+    const BatchTable* __restrict__ bt) {
+  if (bt && blockIdx.x >= bt->tile_start[bt->views]) return;  // past the batch's tiles
   __shared__ float4 s0[kChunk], s1[kChunk];
   __shared__ float2 s2[kChunk];
   __shared__ uint32_t srect[kChunk];
@@ -192,8 +194,19 @@ __global__ void __launch_bounds__(kRasterThreads, 6) raster_fwd_kernel(
   __shared__ uint8_t slist[kRasterThreads / 32][kChunk];
   __shared__ double stab[crm::kExpNegEntries];
   for (int i = threadIdx.x; i < crm::kExpNegEntries; i += kRasterThreads) stab[i] = crm::exp2_neg_entry(i, kExp2Tab64);
-  const PixelGeom pg = pixel_geom(blockIdx.x, tiles_x, width, height);
-  const uint32_t ox = (blockIdx.x % tiles_x) * kTile, oy = (blockIdx.x / tiles_x) * kTile;
+  // In a batch the block is a global tile: find its view, local tile and image offset.
+  uint32_t tile = blockIdx.x;
+  size_t pix0 = 0;
+  if (bt) {
+    const int v = batch_view_of(bt->tile_start, bt->views, blockIdx.x);
+    tile = blockIdx.x - bt->tile_start[v];
+    width = bt->cam[v].width;
+    height = bt->cam[v].height;
+    tiles_x = bt->tiles_x[v];
+    pix0 = bt->pix_start[v];
+  }
+  const PixelGeom pg = pixel_geom(tile, tiles_x, width, height);
+  const uint32_t ox = (tile % tiles_x) * kTile, oy = (tile / tiles_x) * kTile;
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t sbx = (warp & 1u) * 8u, sby = (warp >> 1) * 4u;  // sub-block origin in the tile
   const float px = (float)pg.px_i + 0.5f, py = (float)pg.py_j + 0.5f;
@@ -262,7 +275,7 @@ __global__ void __launch_bounds__(kRasterThreads, 6) raster_fwd_kernel(
     __syncthreads();
   }
   if (pg.inside) {
-    const size_t pix = (size_t)pg.py_j * width + pg.px_i;
+    const size_t pix = pix0 + (size_t)pg.py_j * width + pg.px_i;
     image[3 * pix] = cr + T * bg0;
     image[3 * pix + 1] = cg + T * bg1;
     image[3 * pix + 2] = cb + T * bg2;
@@ -328,7 +341,9 @@ __global__ void __launch_bounds__(kRasterThreads) raster_bwd_kernel(
     const float4* __restrict__ rec, const uint32_t* __restrict__ gauss, const uint2* __restrict__ ranges,
     uint32_t width, uint32_t height, uint32_t tiles_x, float bg0, float bg1, float bg2,
     const float* __restrict__ final_t, const uint32_t* __restrict__ n_contrib, const float* __restrict__ dimage,
-    float4* __restrict__ pgrad, int64_t cap, unsigned long long* __restrict__ pairs) {
+    float4* __restrict__ pgrad, int64_t cap, unsigned long long* __restrict__ pairs,
+    const BatchTable* __restrict__ bt) {
+  if (bt && blockIdx.x >= bt->tile_start[bt->views]) return;  // past the batch's tiles
   __shared__ float4 s0[kChunk], s1[kChunk];
   __shared__ float2 s2[kChunk];
   __shared__ uint32_t srect[kChunk];
@@ -337,8 +352,19 @@ __global__ void __launch_bounds__(kRasterThreads) raster_bwd_kernel(
   __shared__ uint8_t smask[kChunk];
   __shared__ uint8_t slist[kRasterThreads / 32][kChunk];
   __shared__ uint32_t s_max_last;
-  const PixelGeom pg = pixel_geom(blockIdx.x, tiles_x, width, height);
-  const uint32_t ox = (blockIdx.x % tiles_x) * kTile, oy = (blockIdx.x / tiles_x) * kTile;
+  // In a batch the block is a global tile: find its view, local tile and image offset.
+  uint32_t tile = blockIdx.x;
+  size_t pix0 = 0;
+  if (bt) {
+    const int v = batch_view_of(bt->tile_start, bt->views, blockIdx.x);
+    tile = blockIdx.x - bt->tile_start[v];
+    width = bt->cam[v].width;
+    height = bt->cam[v].height;
+    tiles_x = bt->tiles_x[v];
+    pix0 = bt->pix_start[v];
+  }
+  const PixelGeom pg = pixel_geom(tile, tiles_x, width, height);
+  const uint32_t ox = (tile % tiles_x) * kTile, oy = (tile / tiles_x) * kTile;
   const uint32_t lx = pg.px_i - ox, ly_shift = pg.py_j - oy + 16u;  // bit positions in the rect masks
   const float px = (float)pg.px_i + 0.5f, py = (float)pg.py_j + 0.5f;
   const uint2 range = ranges[blockIdx.x];
@@ -349,7 +375,7 @@ __global__ void __launch_bounds__(kRasterThreads) raster_bwd_kernel(
   float T = 1.0f, t_fin = 1.0f, d0 = 0.0f, d1 = 0.0f, d2 = 0.0f, bg_dot = 0.0f;
   const uint32_t list_len = range.y - range.x;
   if (pg.inside) {
-    const size_t pix = (size_t)pg.py_j * width + pg.px_i;
+    const size_t pix = pix0 + (size_t)pg.py_j * width + pg.px_i;
     last = min(n_contrib[pix], list_len);  // n_contrib never exceeds its tile's list
     T = final_t[pix];
     t_fin = T;
@@ -476,12 +502,13 @@ __global__ void __launch_bounds__(kRasterThreads) raster_bwd_kernel(
 
 Status launch_raster_fwd(Ctx* c, const float* proj, const uint32_t* gauss, const uint32_t* ranges, uint32_t width,
                          uint32_t height, const float bg[3], float* image, float* final_t, uint32_t* n_contrib,
-                         uint64_t* pairs) {
+                         uint64_t* pairs, const BatchTable* bt, uint32_t tiles_cap) {
   const uint32_t tiles_x = (width + kTile - 1) / kTile, tiles_y = (height + kTile - 1) / kTile;
-  if (tiles_x * tiles_y == 0) return Status::ok();
-  raster_fwd_kernel<<<tiles_x * tiles_y, kRasterThreads, 0, c->stream>>>(
+  const uint32_t blocks = bt ? tiles_cap : tiles_x * tiles_y;
+  if (blocks == 0) return Status::ok();
+  raster_fwd_kernel<<<blocks, kRasterThreads, 0, c->stream>>>(
       reinterpret_cast<const float4*>(proj), gauss, reinterpret_cast<const uint2*>(ranges), width, height, tiles_x,
-      bg[0], bg[1], bg[2], image, final_t, n_contrib, reinterpret_cast<unsigned long long*>(pairs));
+      bg[0], bg[1], bg[2], image, final_t, n_contrib, reinterpret_cast<unsigned long long*>(pairs), bt);
   c->launches.count++;
   SPLAT_LAUNCHED("raster_fwd_kernel");
   return Status::ok();
@@ -489,13 +516,15 @@ Status launch_raster_fwd(Ctx* c, const float* proj, const uint32_t* gauss, const
 
 Status launch_raster_bwd(Ctx* c, const float* proj, const uint32_t* gauss, const uint32_t* ranges, uint32_t width,
                          uint32_t height, const float bg[3], const float* final_t, const uint32_t* n_contrib,
-                         const float* dimage, float* pgrad, int64_t cap, uint64_t* pairs) {
+                         const float* dimage, float* pgrad, int64_t cap, uint64_t* pairs, const BatchTable* bt,
+                         uint32_t tiles_cap) {
   const uint32_t tiles_x = (width + kTile - 1) / kTile, tiles_y = (height + kTile - 1) / kTile;
-  if (tiles_x * tiles_y == 0) return Status::ok();
-  raster_bwd_kernel<<<tiles_x * tiles_y, kRasterThreads, 0, c->stream>>>(
+  const uint32_t blocks = bt ? tiles_cap : tiles_x * tiles_y;
+  if (blocks == 0) return Status::ok();
+  raster_bwd_kernel<<<blocks, kRasterThreads, 0, c->stream>>>(
       reinterpret_cast<const float4*>(proj), gauss, reinterpret_cast<const uint2*>(ranges), width, height, tiles_x,
       bg[0], bg[1], bg[2], final_t, n_contrib, dimage, reinterpret_cast<float4*>(pgrad), cap,
-      reinterpret_cast<unsigned long long*>(pairs));
+      reinterpret_cast<unsigned long long*>(pairs), bt);
   c->launches.count++;
   SPLAT_LAUNCHED("raster_bwd_kernel");
   return Status::ok();

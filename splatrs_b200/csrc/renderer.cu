@@ -51,6 +51,19 @@ Status ViewBuffers::ensure(int64_t n, uint32_t width, uint32_t height) {
   return Status::ok();
 }
 
+Status ViewBuffers::ensure_batch(int64_t records, uint64_t pixels, uint32_t tiles) {
+  SPLAT_TRY(proj.ensure((size_t)std::max<int64_t>(records, 1) * kProjFloats * 4));
+  SPLAT_TRY(num_tiles.ensure((size_t)std::max<int64_t>(records, 1) * 4));
+  SPLAT_TRY(entry_offset.ensure((size_t)(records + 1) * 4));
+  SPLAT_TRY(depth_range.ensure(8));
+  SPLAT_TRY(tile_range.ensure((size_t)tiles * 8));
+  SPLAT_TRY(image.ensure(pixels * 12));
+  SPLAT_TRY(final_t.ensure(pixels * 4));
+  SPLAT_TRY(n_contrib.ensure(pixels * 4));
+  SPLAT_TRY(pairs.ensure(16));
+  return Status::ok();
+}
+
 void ViewBuffers::release() {
   for (DevBuf* b : {&proj, &num_tiles, &entry_offset, &depth_range, &tile_range, &gauss, &image, &final_t, &n_contrib,
                     &dimage, &pairs, &sort_scratch, &scan_partial, &counters})

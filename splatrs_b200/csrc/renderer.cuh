@@ -27,6 +27,8 @@ struct ViewBuffers {
   DevBuf sort_scratch, scan_partial, counters;
   int64_t e_cap = 0;
   Status ensure(int64_t n, uint32_t width, uint32_t height);
+  // A batch: `records` projection records, `pixels` pixels and `tiles` tiles in all.
+  Status ensure_batch(int64_t records, uint64_t pixels, uint32_t tiles);
   void release();
   uint64_t* entry_count() const { return counters.as<uint64_t>(); }
   uint32_t* overflow_flag() const { return counters.as<uint32_t>() + 2; }

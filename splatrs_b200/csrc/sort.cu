@@ -201,14 +201,20 @@ template <typename K>
 __device__ __forceinline__ void emit_keys_body(const float4* __restrict__ rec, const uint32_t* __restrict__ entry_offset,
                                                int64_t n, uint32_t tiles_x, const uint32_t* __restrict__ depth_range,
                                                int dbits, int64_t limit, K* __restrict__ keys,
-                                               uint32_t* __restrict__ vals) {
+                                               uint32_t* __restrict__ vals, const BatchTable* bt = nullptr,
+                                               int64_t n_view = 1) {
   const int lane = threadIdx.x & 31;
   const int64_t warp_id = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t g = warp_id * 32 + lane;
   const int64_t first = warp_id * 32;
   if (first >= n) return;
-  uint32_t cnt = 0, tx0 = 0, ty0 = 0, w = 1, dkey = 0;
+  uint32_t cnt = 0, tx0 = 0, ty0 = 0, w = 1, dkey = 0, toff = 0, txs = tiles_x;
   if (g < n) {
+    if (bt) {  // batch: the record's view sets its tile grid and first global tile
+      const int v = (int)(g / n_view);
+      toff = bt->tile_start[v];
+      txs = bt->tiles_x[v];
+    }
     const uint32_t o0 = entry_offset[g], o1 = entry_offset[g + 1];
     cnt = o1 - o0;
     if (cnt) {
@@ -244,11 +250,13 @@ __device__ __forceinline__ void emit_keys_body(const float4* __restrict__ rec, c
     const uint32_t o_ty0 = __shfl_sync(0xffffffffu, ty0, lo);
     const uint32_t o_w = __shfl_sync(0xffffffffu, w, lo);
     const uint32_t o_dkey = __shfl_sync(0xffffffffu, dkey, lo);
+    const uint32_t o_toff = __shfl_sync(0xffffffffu, toff, lo);
+    const uint32_t o_txs = __shfl_sync(0xffffffffu, txs, lo);
     if (j < total && (int64_t)start + j < limit) {
       const uint32_t local = j - (o_incl - o_cnt);
       const uint32_t ty = o_ty0 + local / o_w;
       const uint32_t tx = o_tx0 + local % o_w;
-      const uint64_t tile = (uint64_t)ty * tiles_x + tx;
+      const uint64_t tile = (uint64_t)o_toff + (uint64_t)ty * o_txs + tx;
       keys[start + j] = (K)((tile << dbits) | (uint64_t)o_dkey);
       vals[start + j] = (uint32_t)(first + lo);
     }
@@ -515,10 +523,11 @@ __global__ void __launch_bounds__(256) emit_keys_dev_kernel(const float4* __rest
                                                             uint32_t tiles_x, const uint32_t* __restrict__ depth_range,
                                                             const uint64_t* __restrict__ E_dev, int64_t E_cap, int tbits,
                                                             uint64_t* __restrict__ keys, uint32_t* __restrict__ vals,
-                                                            uint32_t* __restrict__ overflow) {
+                                                            uint32_t* __restrict__ overflow,
+                                                            const BatchTable* __restrict__ bt, int64_t n_view) {
   const DevSortPlan p = dev_sort_plan(E_dev, E_cap, depth_range, tbits);
   if (blockIdx.x == 0 && threadIdx.x == 0 && *E_dev > (uint64_t)E_cap) atomicOr(overflow, 1u);
-  emit_keys_body<uint64_t>(rec, entry_offset, n, tiles_x, depth_range, p.dbits, E_cap, keys, vals);
+  emit_keys_body<uint64_t>(rec, entry_offset, n, tiles_x, depth_range, p.dbits, E_cap, keys, vals, bt, n_view);
 }
 
 __global__ void __launch_bounds__(kSortThreads) radix_upsweep_dev_kernel(const uint64_t* __restrict__ ka,
@@ -567,9 +576,10 @@ size_t dev_sort_scratch_bytes(int64_t E_cap) {
 
 Status launch_bin_sort_dev(Ctx* c, const float* proj, const uint32_t* entry_offset, int64_t n, const uint64_t* E_dev,
                            int64_t E_cap, const uint32_t* depth_range_dev, uint32_t width, uint32_t height,
-                           void* scratch, uint32_t* gauss_out, uint32_t* ranges, uint32_t* overflow) {
+                           void* scratch, uint32_t* gauss_out, uint32_t* ranges, uint32_t* overflow,
+                           const BatchTable* bt, int64_t n_view, uint32_t tiles_cap) {
   const uint32_t tiles_x = (width + kTile - 1) / kTile, tiles_y = (height + kTile - 1) / kTile;
-  const uint32_t num_tiles = tiles_x * tiles_y;
+  const uint32_t num_tiles = bt ? tiles_cap : tiles_x * tiles_y;
   const int tbits = num_tiles <= 1 ? 0 : 32 - __builtin_clz(num_tiles - 1);
   const int max_passes = (tbits + 32 + 7) / 8;
   const uint64_t cap = (uint64_t)std::max<int64_t>(E_cap, 1);
@@ -604,7 +614,7 @@ Status launch_bin_sort_dev(Ctx* c, const float* proj, const uint32_t* entry_offs
     const uint32_t warps = ceil_div(n, 32);
     emit_keys_dev_kernel<<<ceil_div((uint64_t)warps * 32, 256), 256, 0, c->stream>>>(
         reinterpret_cast<const float4*>(proj), entry_offset, n, tiles_x, depth_range_dev, E_dev, E_cap, tbits, ka, va,
-        overflow);
+        overflow, bt, std::max<int64_t>(n_view, 1));
     c->launches.count++;
     SPLAT_LAUNCHED("emit_keys_dev_kernel");
   }

@@ -102,6 +102,14 @@ struct splat_trainer {
   uint64_t g_launches = 0;  // kernels in one captured iteration
   bool graphs = true;       // false after a failed capture: plain launches from then on
   bool last_replayed = false;
+  // Batches (cfg.batch_views > 1): one mapped table per slot, its device copy, and the
+  // capacities that size every batch launch (the largest view times the batch).
+  int batch = 1;
+  BatchTable* batch_host = nullptr;
+  void* batch_host_dev = nullptr;
+  DevBuf batch_dev;
+  uint32_t tiles_cap = 0, loss_cap = 0;
+  uint64_t pix_cap = 0;
 };
 
 namespace {
@@ -161,9 +169,14 @@ Status reset_stats(splat_trainer* t) {
   return launch_fill_u32(t->c, t->stats.ptr, t->stats.bytes / 4, 0u);
 }
 
-// The host side of one iteration (train.rs:196-247): its number, view, SH degree,
+// Words per read-back slot: 3 per view (loss, ssim, psnr) and the binning counters.
+constexpr int kSlotWords = 32;
+
+// The host side of one iteration (train.rs:196-247): its number, view(s), SH degree,
 // learning rates, Adam step and what density control runs after it.
 struct IterPlan {
+  uint32_t views[kMaxViews] = {};
+  int nviews = 1;
   uint32_t it = 0, view = 0;
   int sh_degree = 0;
   splat_lr lr{};
@@ -184,8 +197,18 @@ IterPlan schedule(splat_trainer* t) {
     for (uint32_t i = 0; i < nv; i++) t->order[i] = i;
     for (uint32_t i = nv; i-- > 1;) std::swap(t->order[i], t->order[t->rng.index(i + 1)]);
   }
-  p.view = t->order.back();
-  t->order.pop_back();
+  p.nviews = t->batch;
+  for (int b = 0; b < p.nviews; b++) {
+    if (t->order.empty()) {  // a new epoch inside the batch
+      const uint32_t nv = (uint32_t)t->views.size();
+      t->order.resize(nv);
+      for (uint32_t i = 0; i < nv; i++) t->order[i] = i;
+      for (uint32_t i = nv; i-- > 1;) std::swap(t->order[i], t->order[t->rng.index(i + 1)]);
+    }
+    p.views[b] = t->order.back();
+    t->order.pop_back();
+  }
+  p.view = p.views[p.nviews - 1];
   p.lr.mean = position_lr(cfg, p.it, t->extent);
   p.lr.log_scale = cfg.scaling_lr;
   p.lr.quat = cfg.rotation_lr;
@@ -203,11 +226,13 @@ IterPlan schedule(splat_trainer* t) {
 
 std::vector<uint64_t> graph_key(splat_trainer* t, const IterPlan& p) {
   const splat_camera& cam = t->views[p.view]->cam;
+  // A batch's launches are sized by the capacities, not by its views' sizes.
+  const uint64_t w = t->batch > 1 ? 0 : cam.width, h = t->batch > 1 ? 0 : cam.height;
   std::vector<uint64_t> k = {(uint64_t)t->n, (uint64_t)t->cur.cap, (uint64_t)t->vb.e_cap, (uint64_t)p.sh_degree,
-                             (uint64_t)p.densify_window, cam.width, cam.height, t->c->arena.generation,
-                             (uint64_t)t->stats_cap};
+                             (uint64_t)p.densify_window, w, h, t->c->arena.generation, (uint64_t)t->stats_cap,
+                             (uint64_t)t->batch, t->tiles_cap, t->pix_cap};
   for (const DevBuf* b : {&t->cur.params, &t->cur.m, &t->cur.v, &t->bf16, &t->stats, &t->pgrad, &t->pred_grad, &t->loss_out,
-                          &t->params_dev, &t->vb.proj, &t->vb.num_tiles, &t->vb.entry_offset, &t->vb.depth_range,
+                          &t->params_dev, &t->batch_dev, &t->vb.proj, &t->vb.num_tiles, &t->vb.entry_offset, &t->vb.depth_range,
                           &t->vb.tile_range, &t->vb.gauss, &t->vb.image, &t->vb.final_t, &t->vb.n_contrib,
                           &t->vb.sort_scratch, &t->vb.scan_partial, &t->vb.counters})
     k.push_back((uint64_t)(uintptr_t)b->ptr);
@@ -262,8 +287,86 @@ Status body(splat_trainer* t, const IterPlan& p, int slot) {
                                     p.densify_window ? t->stats.ptr : nullptr, cfg.absgrad, p.adam_step, p.lr,
                                     t->vb.overflow_flag(), sp, const_cast<void*>(bf16_copy(t))));
   SPLAT_TRY(launch_publish_u32_to(c, t->loss_out.as<uint32_t>(), 3, t->vb.counters.as<uint32_t>(), 3,
-                                  static_cast<uint32_t*>(t->slots_dev) + 16 * slot));
+                                  static_cast<uint32_t*>(t->slots_dev) + kSlotWords * slot));
   return Status::ok();
+}
+
+// One batch: every stage one launch over all the batch's views, sized for the capacities
+// and driven by the batch table loaded first from the slot's host copy.
+Status body_batch(splat_trainer* t, const IterPlan& p, int slot) {
+  Ctx* c = t->c;
+  const splat_train_config& cfg = t->cfg;
+  const float bgv = cfg.white_background ? 1.0f : 0.0f;
+  const float bg[3] = {bgv, bgv, bgv};
+  splat_proj_opts opts;
+  opts.near_plane = cfg.near_plane;
+  opts.eps2d = 0.3f;
+  opts.antialias = cfg.antialias;
+  opts.sh_degree = p.sh_degree;
+  opts.fp64_conic = cfg.fp64_conic;
+  const int64_t n = t->n, cap = t->cur.cap, records = (int64_t)t->batch * n, pcap = (int64_t)t->batch * cap;
+  const splat_camera& cam0 = t->views[p.views[0]]->cam;  // launch arguments only; the table rules
+  const BatchTable* bt = t->batch_dev.as<BatchTable>();
+  ViewBuffers& v = t->vb;
+  SPLAT_TRY(launch_load_words(c, static_cast<const char*>(t->batch_host_dev) + slot * sizeof(BatchTable),
+                              t->batch_dev.ptr, (int)(sizeof(BatchTable) / 4)));
+  SPLAT_TRY(v.ensure_batch(records, t->pix_cap, t->tiles_cap));
+  const int64_t e_cap = std::max<int64_t>(v.e_cap, 1);
+  SPLAT_TRY(v.gauss.ensure((size_t)e_cap * 4));
+  SPLAT_TRY(v.sort_scratch.ensure(dev_sort_scratch_bytes(e_cap)));
+  SPLAT_TRY(v.scan_partial.ensure(((size_t)std::max<int64_t>(records, 1) / kScanValuesPerBlock + 2) * 8));
+  if (v.counters.bytes == 0) {
+    SPLAT_TRY(v.counters.ensure(64));
+    SPLAT_TRY(launch_fill_u32(c, v.counters.ptr, 16, 0u));
+  }
+  float* proj = v.proj.as<float>();
+  uint32_t* dr = v.depth_range.as<uint32_t>();
+  SPLAT_TRY(launch_project_fwd(c, t->cur.params.as<float>(), n, cap, cam0, opts, proj, v.num_tiles.as<uint32_t>(), dr,
+                               nullptr, bf16_copy(t), bt));
+  SPLAT_TRY(launch_scan_u32_into(c, v.num_tiles.as<uint32_t>(), records, v.entry_offset.as<uint32_t>(), 1,
+                                 v.scan_partial.as<uint64_t>(), v.entry_count()));
+  SPLAT_TRY(launch_bin_sort_dev(c, proj, v.entry_offset.as<uint32_t>(), records, v.entry_count(), e_cap, dr, cam0.width,
+                                cam0.height, v.sort_scratch.ptr, v.gauss.as<uint32_t>(), v.tile_range.as<uint32_t>(),
+                                v.overflow_flag(), bt, n, t->tiles_cap));
+  SPLAT_TRY(launch_raster_fwd(c, proj, v.gauss.as<uint32_t>(), v.tile_range.as<uint32_t>(), cam0.width, cam0.height, bg,
+                              v.image.as<float>(), v.final_t.as<float>(), v.n_contrib.as<uint32_t>(), nullptr, bt,
+                              t->tiles_cap));
+  SPLAT_TRY(t->pred_grad.ensure(t->pix_cap * 12));
+  SPLAT_TRY(t->loss_out.ensure(3 * kMaxViews * 4));
+  SPLAT_TRY(launch_loss(c, v.image.as<float>(), nullptr, 1, cam0.width, cam0.height, cfg.lambda_dssim,
+                        t->pred_grad.as<float>(), t->loss_out.as<float>(), nullptr, bt, t->loss_cap, t->pix_cap));
+  SPLAT_TRY(t->pgrad.ensure((size_t)pcap * 48));
+  SPLAT_TRY(launch_fill_u32(c, t->pgrad.ptr, (size_t)pcap * 12, 0u));
+  SPLAT_TRY(launch_raster_bwd(c, proj, v.gauss.as<uint32_t>(), v.tile_range.as<uint32_t>(), cam0.width, cam0.height, bg,
+                              v.final_t.as<float>(), v.n_contrib.as<uint32_t>(), t->pred_grad.as<float>(),
+                              t->pgrad.as<float>(), pcap, nullptr, bt, t->tiles_cap));
+  SPLAT_TRY(launch_project_bwd_batch_adam(c, t->cur.params.as<float>(), t->cur.m.as<float>(), t->cur.v.as<float>(), n,
+                                          cap, opts, proj, t->pgrad.as<float>(), pcap,
+                                          p.densify_window ? t->stats.ptr : nullptr, cfg.absgrad, v.overflow_flag(),
+                                          bt, const_cast<void*>(bf16_copy(t))));
+  SPLAT_TRY(launch_publish_u32_to(c, t->loss_out.as<uint32_t>(), 3 * t->batch, v.counters.as<uint32_t>(), 3,
+                                  static_cast<uint32_t*>(t->slots_dev) + kSlotWords * slot));
+  return Status::ok();
+}
+
+// The batch table of plan p: views, their cameras, targets, tile/pixel/SSIM-block offsets.
+void fill_batch_table(splat_trainer* t, const IterPlan& p, BatchTable& b) {
+  std::memset(&b, 0, sizeof(b));
+  b.views = p.nviews;
+  b.inv_views = 1.0f / (float)p.nviews;
+  b.adam = make_adam_args(p.adam_step, p.lr);
+  for (int k = 0; k < p.nviews; k++) {
+    const View& v = *t->views[p.views[k]];
+    const uint32_t tx = (v.cam.width + kTile - 1) / kTile, ty = (v.cam.height + kTile - 1) / kTile;
+    const uint32_t lx = (v.cam.width + 31) / 32, ly = (v.cam.height + 31) / 32;
+    b.cam[k] = v.cam;
+    b.target[k] = v.rgb.ptr;
+    b.tiles_x[k] = tx;
+    b.tile_start[k + 1] = b.tile_start[k] + tx * ty;
+    b.loss_blocks_x[k] = lx;
+    b.loss_start[k + 1] = b.loss_start[k] + lx * ly;
+    b.pix_start[k + 1] = b.pix_start[k] + (uint64_t)v.cam.width * v.cam.height;
+  }
 }
 
 // Captures body() for `slot` into a graph; on any failure graphs are switched off and the
@@ -278,7 +381,7 @@ void capture(splat_trainer* t, const IterPlan& p, int slot) {
   cudaStream_t orig = c->stream;
   c->stream = t->cap_stream;
   const uint64_t l0 = c->launches.count;
-  const Status s = body(t, p, slot);
+  const Status s = t->batch > 1 ? body_batch(t, p, slot) : body(t, p, slot);
   cudaGraph_t g = nullptr;
   const cudaError_t e = cudaStreamEndCapture(t->cap_stream, &g);
   c->stream = orig;
@@ -310,11 +413,16 @@ Status enqueue(splat_trainer* t, const IterPlan& p, int slot) {
   // Scratch of the previous iteration is free for reuse: all of it is consumed on this
   // stream before anything queued now runs.
   arena_reset(c);
-  View& view = *t->views[p.view];
-  StepParams& hp = t->params_host[slot];
-  hp.cam = view.cam;
-  hp.adam = make_adam_args(p.adam_step, p.lr);
-  hp.target = view.rgb.ptr;
+  if (t->batch > 1) {
+    fill_batch_table(t, p, t->batch_host[slot]);
+    SPLAT_TRY(t->batch_dev.ensure(sizeof(BatchTable)));
+  } else {
+    View& view = *t->views[p.view];
+    StepParams& hp = t->params_host[slot];
+    hp.cam = view.cam;
+    hp.adam = make_adam_args(p.adam_step, p.lr);
+    hp.target = view.rgb.ptr;
+  }
   SPLAT_TRY(t->params_dev.ensure(sizeof(StepParams)));
   if (t->graphs) {
     const std::vector<uint64_t> key = graph_key(t, p);
@@ -333,7 +441,7 @@ Status enqueue(splat_trainer* t, const IterPlan& p, int slot) {
     }
   }
   t->last_replayed = false;
-  SPLAT_TRY(body(t, p, slot));
+  SPLAT_TRY(t->batch > 1 ? body_batch(t, p, slot) : body(t, p, slot));
   SPLAT_CUDA(cudaEventRecord(t->slot_done[slot], c->stream));
   if (t->graphs) {
     t->gkey = graph_key(t, p);  // the state after this iteration's allocations
@@ -349,13 +457,22 @@ struct SlotResult {
 };
 
 SlotResult read_slot(splat_trainer* t, int slot) {
-  const volatile uint32_t* w = t->slots_host + 16 * slot;
+  const volatile uint32_t* w = t->slots_host + kSlotWords * slot;
+  const int nv = t->batch;
   SlotResult r;
-  uint32_t b0 = w[0], b2 = w[2];
-  std::memcpy(&r.loss, &b0, 4);
-  std::memcpy(&r.psnr, &b2, 4);
-  r.entries = (uint64_t)w[3] | ((uint64_t)w[4] << 32);
-  r.overflow = w[5] != 0;
+  double loss = 0.0, psnr = 0.0;
+  for (int v = 0; v < nv; v++) {  // the mean over the batch's views
+    float l, q;
+    uint32_t b0 = w[3 * v], b2 = w[3 * v + 2];
+    std::memcpy(&l, &b0, 4);
+    std::memcpy(&q, &b2, 4);
+    loss += l;
+    psnr += q;
+  }
+  r.loss = (float)(loss / nv);
+  r.psnr = (float)(psnr / nv);
+  r.entries = (uint64_t)w[3 * nv] | ((uint64_t)w[3 * nv + 1] << 32);
+  r.overflow = w[3 * nv + 2] != 0;
   return r;
 }
 
@@ -437,7 +554,7 @@ void fill_info(splat_trainer* t, const IterPlan& p, const SlotResult& r, splat_s
 Status initial_capacity(splat_trainer* t) {
   if (t->vb.e_cap == 0)
     t->vb.e_cap = t->cfg.entry_capacity > 0 ? (int64_t)std::min<uint64_t>(t->cfg.entry_capacity, 0xfffffffeull)
-                                            : std::max<int64_t>(8 * std::max<int64_t>(t->n, 1), 1 << 16);
+                                            : std::max<int64_t>(8 * t->batch * std::max<int64_t>(t->n, 1), 1 << 16);
   return ensure_stats(t, t->cur.cap);
 }
 
@@ -530,6 +647,10 @@ SPLAT_API int splat_trainer_create(splat_ctx* ctx, const splat_train_config* cfg
     splat_ctx_impl(ctx)->last_error = "sh_degree exceeds the maximum of 3";  // train.rs:177-183
     return SPLAT_ERR_INVALID;
   }
+  if (cfg->batch_views > (uint32_t)kMaxViews) {
+    splat_ctx_impl(ctx)->last_error = "batch_views exceeds the maximum of 8";
+    return SPLAT_ERR_INVALID;
+  }
   splat_trainer* t = new (std::nothrow) splat_trainer();
   if (!t) return SPLAT_ERR_INVALID;
   t->ctx = ctx;
@@ -539,7 +660,7 @@ SPLAT_API int splat_trainer_create(splat_ctx* ctx, const splat_train_config* cfg
   int prev = 0;
   cudaGetDevice(&prev);
   cudaSetDevice(t->c->device);
-  bool ok = cudaHostAlloc((void**)&t->slots_host, 2 * 16 * 4, cudaHostAllocMapped) == cudaSuccess;
+  bool ok = cudaHostAlloc((void**)&t->slots_host, 2 * kSlotWords * 4, cudaHostAllocMapped) == cudaSuccess;
   ok = ok && cudaHostGetDevicePointer(&t->slots_dev, t->slots_host, 0) == cudaSuccess;
   for (cudaEvent_t& ev : t->slot_done) ok = ok && cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) == cudaSuccess;
   cudaSetDevice(prev);
@@ -551,10 +672,12 @@ SPLAT_API int splat_trainer_create(splat_ctx* ctx, const splat_train_config* cfg
     delete t;
     return SPLAT_ERR_CUDA;
   }
-  std::memset(t->slots_host, 0, 2 * 16 * 4);
+  std::memset(t->slots_host, 0, 2 * kSlotWords * 4);
   cudaSetDevice(t->c->device);
   ok = cudaHostAlloc((void**)&t->params_host, 2 * sizeof(StepParams), cudaHostAllocMapped) == cudaSuccess;
   ok = ok && cudaHostGetDevicePointer(&t->params_host_dev, t->params_host, 0) == cudaSuccess;
+  ok = ok && cudaHostAlloc((void**)&t->batch_host, 2 * sizeof(BatchTable), cudaHostAllocMapped) == cudaSuccess;
+  ok = ok && cudaHostGetDevicePointer(&t->batch_host_dev, t->batch_host, 0) == cudaSuccess;
   ok = ok && cudaStreamCreateWithFlags(&t->cap_stream, cudaStreamNonBlocking) == cudaSuccess;
   cudaSetDevice(prev);
   if (!ok) {
@@ -587,6 +710,8 @@ SPLAT_API int splat_trainer_destroy(splat_trainer* t) {
       if (ev) cudaEventDestroy(ev);
     if (t->slots_host) cudaFreeHost(t->slots_host);
     if (t->params_host) cudaFreeHost(t->params_host);
+    if (t->batch_host) cudaFreeHost(t->batch_host);
+    t->batch_dev.release();
     if (t->cap_stream) cudaStreamDestroy(t->cap_stream);
   }
   delete t;
@@ -649,6 +774,20 @@ SPLAT_API int splat_trainer_start(splat_trainer* t) {
   Ctx* c = t->c;
   t->rng = SplitMix64(t->cfg.seed);
   t->order.clear();
+  t->batch = t->cfg.batch_views > 1 ? (int)t->cfg.batch_views : 1;
+  if (t->batch > 1) {  // capacities: the largest view, batch times
+    uint32_t max_tiles = 0, max_loss = 0;
+    uint64_t max_pix = 0;
+    for (const View* v : t->views) {
+      const uint32_t w = v->cam.width, h = v->cam.height;
+      max_tiles = std::max(max_tiles, ((w + kTile - 1) / kTile) * ((h + kTile - 1) / kTile));
+      max_loss = std::max(max_loss, ((w + 31) / 32) * ((h + 31) / 32));
+      max_pix = std::max<uint64_t>(max_pix, (uint64_t)w * h);
+    }
+    t->tiles_cap = max_tiles * t->batch;
+    t->loss_cap = max_loss * t->batch;
+    t->pix_cap = max_pix * t->batch;
+  }
   t->iteration = 0;
   t->adam_step = 0;
   t->sh_degree = 0;

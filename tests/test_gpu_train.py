@@ -353,3 +353,76 @@ def test_trainer_bf16_storage_trains_like_f32(ctx):
     assert pb > pa - 0.5
     a.close()
     b.close()
+
+
+def _mixed_size_views(seed, sizes):
+    """Ring views of different sizes (one per entry of `sizes`) of a small ground truth."""
+    rng = np.random.default_rng(seed)
+    gt = F.ground_truth(rng, 40)
+    cams = [F.ring_cameras(len(sizes), w, h, 2.6)[k] for k, (w, h) in enumerate(sizes)]
+    views = F.render_views(gt, cams, 1, [0.0, 0.0, 0.0])
+    pts, rgb = F.init_points(gt, rng)
+    return views, O.scene_extent(np.stack(cams)), O.from_points(pts, rgb)
+
+
+def test_batched_step_matches_per_view_stages(ctx):
+    """batch_views = 3 over three views of different sizes (one epoch per step): the step's
+    loss is the mean of the three views' losses computed view by view with the stage
+    functions (to the rounding of the double-atomic SSIM sums), and its Adam update (a sign
+    step at step 1) moves every parameter with a significant summed gradient against the
+    sign of the sum of the per-view gradients, and no parameter that is unused."""
+    views, extent, init = _mixed_size_views(300, [(64, 48), (80, 60), (50, 70)])
+    n = init.shape[0]
+    cfg = dict(iterations=10, densify=0, sh_degree=1, sh_degree_interval=1000, position_lr_max_steps=10, seed=2,
+               batch_views=3, position_lr_final=0.00016)
+    t = G.Trainer(ctx, init, extent, views, **cfg)
+    info = t.step()
+    after = t.model()
+    from splatrs_b200._lib import Camera, ProjOpts
+    opts = ProjOpts.make(sh_degree=0)
+    planes = G.params_to_planes(ctx, dev(init), n)
+    losses, gsum = [], None
+    for cam, rgb in views:
+        c = Camera.from_record(cam)
+        proj = G.project_all(ctx, planes, n, n, c, opts)
+        b = G.bin(ctx, proj)
+        out = G.rasterize_forward(ctx, proj, b, [0.0, 0.0, 0.0])
+        lv, grad = G.photometric_loss(ctx, out.image, dev(rgb, torch.uint8), c.width, c.height, 0.2)
+        losses.append(float(lv[0].item()))
+        pg = G.rasterize_backward(ctx, proj, b, [0.0, 0.0, 0.0], out, grad / 3.0)
+        gp = G.planes_to_params(ctx, G.project_backward_all(ctx, planes, n, n, c, opts, proj, pg), n, n)
+        gsum = gp if gsum is None else gsum + gp
+    want = float(np.float32(np.mean(np.array(losses, np.float64))))
+    assert abs(info["loss"] - want) <= 1e-6 * want  # SSIM sums are double atomics
+    g = gsum.cpu().numpy()
+    delta = after - init
+    # Significant against the largest gradient: the initial Gaussians are isotropic, so
+    # their rotation gradients are rounding noise (~1e-10) whose sign means nothing.
+    big = np.abs(g) > 1e-5 * np.abs(g).max()
+    assert big.sum() > 200
+    assert (np.sign(delta[big]) == -np.sign(g[big])).all()
+    # Exactly still: Gaussians no view sees, and SH coefficients above degree 0 (unused at
+    # step 1); other exact zeros of the sum can be rounding noise in the batch's sum.
+    assert (delta[(g == 0.0).all(1)] == 0.0).all()
+    assert (delta[:, 14:] == 0.0).all()
+    t.close()
+
+
+def test_batched_training_mixed_sizes(ctx):
+    """batch_views = 4 over eight views of two sizes, queued with splat_trainer_run and
+    replayed as a graph: at an equal number of steps, training on the mean gradient of four
+    views reaches at least the quality of the one-view trainer."""
+    sizes = [(64, 48), (96, 72)] * 4
+    views, extent, init = _mixed_size_views(301, sizes)
+    cfg = dict(iterations=300, densify=0, sh_degree=1, sh_degree_interval=100, position_lr_max_steps=300, seed=3)
+    one = G.Trainer(ctx, init, extent, views, **cfg)
+    one.run(300)
+    bat = G.Trainer(ctx, init, extent, views, batch_views=4, **cfg)
+    info = bat.run(300)
+    assert info["replayed"] == 1
+    assert np.isfinite(bat.model()[:, 0:10]).all()
+    p1, pb = _evaluate(one, views), _evaluate(bat, views)
+    print(f"\n300 steps: one view {p1:.2f} dB; batches of 4 {pb:.2f} dB")
+    assert pb > p1 - 0.3
+    one.close()
+    bat.close()
