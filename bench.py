@@ -47,6 +47,9 @@ def parse():
                     help="also run plain training on the clustered 500k-Gaussian multi-view scene")
     ap.add_argument("--train-c2-iters", type=int, default=0, help="iterations of that run (default: all 30,000)")
     ap.add_argument("--c2-cpu-iters", type=int, default=5, help="iterations of its CPU oracle sample")
+    ap.add_argument("--train-c3", action="store_true",
+                    help="batched mixed-size BF16 training on the same scene (8 views per step)")
+    ap.add_argument("--train-c3-iters", type=int, default=0, help="steps of that run (default: all 3,750)")
     ap.add_argument("--profile-small", action="store_true",
                     help="a reduced case for ncu captures (fewer Gaussians, one step)")
     return ap.parse_args()
@@ -332,6 +335,15 @@ C2_TRAIN = dict(iterations=30000, densify=1, densify_from_iter=500, densify_unti
                 position_lr_max_steps=30000, seed=0, max_gaussians=3_000_000)
 
 
+# Batched mixed-precision training on the same scene (config 3): 8 views of mixed sizes per
+# step, BF16 render copy, f64 conic re-solve, graph replay; as many views as the plain
+# run (3,750 steps of 8) with the plain schedule in views (every step-count divided by 8).
+C3_TRAIN = dict(iterations=3750, densify=1, densify_from_iter=63, densify_until_iter=1875, densification_interval=13,
+                opacity_reset_interval=375, densify_grad_threshold=0.0002, lambda_dssim=0.2, sh_degree=3,
+                sh_degree_interval=125, position_lr_max_steps=3750, seed=0, max_gaussians=3_000_000,
+                batch_views=8, bf16_storage=1, fp64_conic=1)
+
+
 def gt_views_gpu(ctx, s):
     """Target views: the ground truth rendered by the device renderer, as 8-bit images."""
     from splatrs_b200 import gpu as G
@@ -343,6 +355,20 @@ def gt_views_gpu(ctx, s):
              for cam in s["cams"]]
     r.close()
     return views
+
+
+def mean_ssim(trainer, views):
+    """Mean SSIM of the trainer's renders over the views (the loss kernel at lambda 1)."""
+    import torch
+    from splatrs_b200 import gpu as G
+    from splatrs_b200._lib import Camera
+    tot = 0.0
+    for cam, rgb in views:
+        c = Camera.from_record(cam)
+        img = torch.from_numpy(trainer.render(cam)).cuda()
+        out, _ = G.photometric_loss(trainer.ctx, img, torch.from_numpy(rgb).cuda(), c.width, c.height, 1.0)
+        tot += float(out[1].item())
+    return tot / len(views)
 
 
 def run_train_gpu(local, s, cfg, iterations):
@@ -366,8 +392,10 @@ def run_train_gpu(local, s, cfg, iterations):
     torch.cuda.synchronize(local)
     wall = time.perf_counter() - tw
     ps = float(np.mean([scenes.psnr(t.render(cam), rgb) for cam, rgb in views]))
+    bv = max(1, int(cfg.get("batch_views", 1)))
     out = {"iterations": iterations, "wall_s": round(wall, 3), "iters_per_s": round(iterations / wall, 1),
-           "psnr_train_views": round(ps, 2), "gaussians": t.count}
+           "views_per_s": round(iterations * bv / wall, 1), "psnr_train_views": round(ps, 2),
+           "ssim_train_views": round(mean_ssim(t, views), 4), "gaussians": t.count}
     t.close()
     ctx.close()
     return out, init, views, extent
@@ -465,6 +493,13 @@ def main():
             line["train_c2"]["cpu"]["sample"] = (f"first {args.c2_cpu_iters} iterations from the same initial "
                                                  "model (no densification yet)")
         del views2
+    if args.train_c3 and not args.profile_small:
+        from splatrs_b200 import scenes
+        iters = args.train_c3_iters or C3_TRAIN["iterations"]
+        gpu_c3, _, views3, _ = run_train_gpu(local, scenes.config3(), C3_TRAIN, iters)
+        line["train_c3"] = {"gpu": gpu_c3, "views_per_step": C3_TRAIN["batch_views"],
+                            "sizes": "uniform over 640x480, 1024x768, 1297x840, 1600x1200 per view"}
+        del views3
     if rank == 0:
         if c0 is not None and not args.no_cpu_baseline and world == 1:
             line["train_c0"]["cpu"] = run_train_cpu(*c0, C0_TRAIN, C0_TRAIN["iterations"])

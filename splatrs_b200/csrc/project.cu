@@ -1044,8 +1044,9 @@ __global__ void __launch_bounds__(kBatchBwdThreads) project_bwd_batch_adam_kerne
     const float4 g0 = pgrad[r], g1 = pgrad[pcap + r], g2 = pgrad[2 * pcap + r];
     const splat_camera cam = bt->cam[v];
     if (stat_accum != nullptr) {  // DensifyStats::accumulate per view (densify.rs:36-60)
-      const float sx = (float)cam.width * 0.5f;
-      const float sy = (float)cam.height * 0.5f;
+      // The view's own gradient: dL/dpixel carried the batch's 1/views averaging.
+      const float sx = (float)cam.width * 0.5f * (float)views;
+      const float sy = (float)cam.height * 0.5f * (float)views;
       const float gx = (absgrad ? g2.y : g0.x) * sx;
       const float gy = (absgrad ? g2.z : g0.y) * sy;
       stat_accum[i] += sqrtf(gx * gx + gy * gy);

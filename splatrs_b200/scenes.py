@@ -145,6 +145,26 @@ def config2(seed_gt=0, seed_init=1, n_gt=500_000, n_shells=40, n_cams=200, width
     return dict(gt=gt, cams=cams, init_points=ip, init_rgb=rgb, sh_degree=3, background=(0.0, 0.0, 0.0))
 
 
+C3_SIZES = ((640, 480), (1024, 768), (1297, 840), (1600, 1200))
+
+
+def config3(seed_sizes=7, **kw):
+    """The config-2 scene with every camera at a resolution drawn uniformly from C3_SIZES
+    (seeded), its focal length scaled with the width (f = 1150 at 1297 pixels)."""
+    s = config2(**kw)
+    rng = np.random.default_rng(seed_sizes)
+    pick = rng.integers(0, len(C3_SIZES), len(s["cams"]))
+    cams = []
+    for cam, k in zip(s["cams"], pick):
+        w, h = C3_SIZES[k]
+        c = cam.copy()
+        f = 1150.0 * w / 1297.0
+        c[0:6] = [w, h, f, f, w / 2.0, h / 2.0]
+        cams.append(c)
+    s["cams"] = np.stack(cams)
+    return s
+
+
 def scene_extent(cams):
     """scene_extent (src/camera.rs:99-118): 1.1 x the largest distance from a camera centre
     to the mean centre."""

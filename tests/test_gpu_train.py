@@ -426,3 +426,26 @@ def test_batched_training_mixed_sizes(ctx):
     assert pb > p1 - 0.3
     one.close()
     bat.close()
+
+
+def test_batched_densification_statistics_are_per_view(ctx):
+    """A batch of two copies of one view follows the one-view trainer (same mean gradient),
+    and its densification statistics are those of each view's own gradient (not of the
+    batch-averaged one), so the first densification clones and splits as many Gaussians."""
+    views, extent, init = _views_and_init(200, 30, 8, 48, 36, [1.0, 1.0, 1.0])
+    cfg = dict(iterations=100, densify=1, densify_from_iter=20, densify_until_iter=100, densification_interval=40,
+               opacity_reset_interval=0, densify_grad_threshold=0.0002, white_background=1, sh_degree=0,
+               position_lr_max_steps=100, seed=1)
+    one = G.Trainer(ctx, init, extent, views[:1], **cfg)
+    two = G.Trainer(ctx, init, extent, [views[0], views[0]], batch_views=2, **cfg)
+    first = []
+    for t in (one, two):
+        for _ in range(40):
+            info = t.step()
+        assert info["densified"] == 1
+        first.append((info["cloned"], info["split"], info["pruned"]))
+    print(f"\nfirst densification (cloned, split, pruned): one view {first[0]}, batch of two copies {first[1]}")
+    assert first[0][0] + first[0][1] > 0
+    assert abs(first[0][0] - first[1][0]) <= 2 and abs(first[0][1] - first[1][1]) <= 2
+    one.close()
+    two.close()
