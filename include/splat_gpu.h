@@ -284,6 +284,24 @@ SPLAT_API int splat_project_bwd_adam(splat_ctx* ctx, float* planes_dev, float* m
                                      const float* proj_dev, const float* pgrad_dev, void* stats_dev, int32_t absgrad,
                                      uint64_t step, const splat_lr* lr, void* bf16_dev);
 
+/* ----------------------------------------------------------------------------------------
+ * The learned-densification network (no counterpart in the reference): per Gaussian, 16
+ * features -> 64 SiLU -> 64 SiLU -> 3 logits -> softmax over {keep, clone/split, prune},
+ * BF16 operands on the tensor cores with FP32 accumulation. Its parameters are one FP32
+ * vector of splat_mlp_num_params() values: W1 [16][64], b1 [64], W2 [64][64], b2 [64],
+ * W3 [64][3], b3 [3] (W[in][out]).
+ *   splat_mlp_forward: probabilities (n x 3) of n feature rows (n x 16).
+ *   splat_mlp_grad: adds to grad_dev the gradient of the weighted mean cross-entropy
+ *     sum_s w_s * -log p_s[y_s] / sum_s w_s (labels y in 0..2; scale = 1 / sum_s w_s).
+ *   splat_mlp_adam: one Adam step (beta 0.9 / 0.999, eps 1e-8) on the FP32 parameters.
+ * -------------------------------------------------------------------------------------- */
+SPLAT_API int32_t splat_mlp_num_params(void);
+SPLAT_API int splat_mlp_forward(splat_ctx* ctx, const float* x_dev, int64_t n, const float* theta_dev, float* prob_dev);
+SPLAT_API int splat_mlp_grad(splat_ctx* ctx, const float* x_dev, const int32_t* y_dev, const float* w_dev, int64_t n,
+                             float scale, const float* theta_dev, float* grad_dev);
+SPLAT_API int splat_mlp_adam(splat_ctx* ctx, float* theta_dev, const float* grad_dev, float* m_dev, float* v_dev,
+                             uint64_t step, float lr);
+
 /* Fill `bytes` bytes of device memory with zeros on the context stream. */
 SPLAT_API int splat_zero(splat_ctx* ctx, void* dev, size_t bytes);
 

@@ -152,6 +152,10 @@ def _declare(L):
         "splat_bin_count_noalloc": ([vp, vp, i64, vp, P(i64)], C.c_int),
         "splat_bin_sort": ([vp, vp, vp, i64, i64, vp, u32, u32, vp, vp, vp], C.c_int),
         "splat_bin_count_device": ([vp, vp, i64, vp, vp], C.c_int),
+        "splat_mlp_num_params": ([], i32),
+        "splat_mlp_forward": ([vp, vp, i64, vp, vp], C.c_int),
+        "splat_mlp_grad": ([vp, vp, vp, vp, i64, C.c_float, vp, vp], C.c_int),
+        "splat_mlp_adam": ([vp, vp, vp, vp, vp, C.c_uint64, C.c_float], C.c_int),
         "splat_bin_sort_device_scratch_bytes": ([i64], sz),
         "splat_bin_sort_device": ([vp, vp, vp, i64, vp, i64, vp, u32, u32, vp, vp, vp, vp], C.c_int),
         "splat_rasterize_fwd": ([vp, vp, vp, vp, u32, u32, P(C.c_float), vp, vp, vp, vp], C.c_int),

@@ -297,6 +297,32 @@ SPLAT_API int splat_bin_sort(splat_ctx* ctx, const float* proj_dev, const uint32
                                      tile_range_dev));
 }
 
+SPLAT_API int32_t splat_mlp_num_params(void) { return mlp_num_params(); }
+
+SPLAT_API int splat_mlp_forward(splat_ctx* ctx, const float* x_dev, int64_t n, const float* theta_dev, float* prob_dev) {
+  if (!ctx) return SPLAT_ERR_INVALID;
+  if (n < 0 || !theta_dev || (n && (!x_dev || !prob_dev))) return invalid(ctx, "splat_mlp_forward: bad buffers");
+  Enter e(ctx);
+  return finish(ctx, launch_mlp_forward(&ctx->c, x_dev, n, theta_dev, prob_dev));
+}
+
+SPLAT_API int splat_mlp_grad(splat_ctx* ctx, const float* x_dev, const int32_t* y_dev, const float* w_dev, int64_t n,
+                             float scale, const float* theta_dev, float* grad_dev) {
+  if (!ctx) return SPLAT_ERR_INVALID;
+  if (n < 0 || !theta_dev || !grad_dev || (n && (!x_dev || !y_dev || !w_dev)))
+    return invalid(ctx, "splat_mlp_grad: bad buffers");
+  Enter e(ctx);
+  return finish(ctx, launch_mlp_grad(&ctx->c, x_dev, y_dev, w_dev, n, scale, theta_dev, grad_dev));
+}
+
+SPLAT_API int splat_mlp_adam(splat_ctx* ctx, float* theta_dev, const float* grad_dev, float* m_dev, float* v_dev,
+                             uint64_t step, float lr) {
+  if (!ctx) return SPLAT_ERR_INVALID;
+  if (!theta_dev || !grad_dev || !m_dev || !v_dev || step == 0) return invalid(ctx, "splat_mlp_adam: bad arguments");
+  Enter e(ctx);
+  return finish(ctx, launch_mlp_adam(&ctx->c, theta_dev, grad_dev, m_dev, v_dev, step, lr));
+}
+
 SPLAT_API int splat_bin_count_device(splat_ctx* ctx, const uint32_t* num_tiles_dev, int64_t n,
                                      uint32_t* entry_offset_dev, uint64_t* num_entries_dev) {
   if (!ctx) return SPLAT_ERR_INVALID;

@@ -89,6 +89,13 @@ Status launch_bin_sort_dev(Ctx* c, const float* proj, const uint32_t* entry_offs
                            void* scratch, uint32_t* gauss_out, uint32_t* ranges, uint32_t* overflow,
                            const BatchTable* bt = nullptr, int64_t n_view = 1, uint32_t tiles_cap = 0);
 
+// The learned-densification network (mlp.cu): 16 -> 64 -> 64 -> 3, FP32 parameter vector.
+int mlp_num_params();
+Status launch_mlp_forward(Ctx* c, const float* x, int64_t n, const float* theta, float* prob);
+Status launch_mlp_grad(Ctx* c, const float* x, const int32_t* y, const float* w, int64_t n, float scale,
+                       const float* theta, float* grad);
+Status launch_mlp_adam(Ctx* c, float* theta, const float* grad, float* m, float* v, uint64_t step, float lr);
+
 // Fills `words` 32-bit words at `dst` with `value` by a kernel on the context stream (in
 // place of cudaMemsetAsync, so the compute stream holds kernels only).
 Status launch_fill_u32(Ctx* c, void* dst, size_t words, uint32_t value);

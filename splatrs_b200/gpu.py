@@ -510,3 +510,23 @@ def init_from_points(ctx: Context, points, rgb, cap: int | None = None) -> torch
     check(ctx.lib.splat_init_from_points(ctx.h, p.ctypes.data_as(C.c_void_p), c.ctypes.data_as(C.c_void_p), n,
                                          _ptr(planes), cap), ctx.h)
     return planes
+
+
+def mlp_forward(ctx: Context, x: torch.Tensor, theta: torch.Tensor) -> torch.Tensor:
+    """Learned-densification network: probabilities (n, 3) of feature rows (n, 16)."""
+    x = x.contiguous().float()
+    prob = torch.empty((x.shape[0], 3), dtype=torch.float32, device=x.device)
+    check(ctx.lib.splat_mlp_forward(ctx.h, _ptr(x), x.shape[0], _ptr(theta), _ptr(prob)), ctx.h)
+    return prob
+
+
+def mlp_grad(ctx: Context, x, y, w, theta, grad=None):
+    """Gradient of the weighted mean cross-entropy (added into `grad` when given)."""
+    x = x.contiguous().float()
+    y = y.contiguous().to(torch.int32)
+    w = w.contiguous().float()
+    if grad is None:
+        grad = torch.zeros(int(ctx.lib.splat_mlp_num_params()), dtype=torch.float32, device=x.device)
+    scale = 1.0 / float(w.sum().item())
+    check(ctx.lib.splat_mlp_grad(ctx.h, _ptr(x), _ptr(y), _ptr(w), x.shape[0], scale, _ptr(theta), _ptr(grad)), ctx.h)
+    return grad
