@@ -50,6 +50,9 @@ def parse():
     ap.add_argument("--train-c3", action="store_true",
                     help="batched mixed-size BF16 training on the same scene (8 views per step)")
     ap.add_argument("--train-c3-iters", type=int, default=0, help="steps of that run (default: all 3,750)")
+    ap.add_argument("--train-c4", action="store_true",
+                    help="learned densification: learn on scene seeds 2-5, compare with the rule on seed 6")
+    ap.add_argument("--c4-learn-iters", type=int, default=1875, help="steps of each learning run")
     ap.add_argument("--profile-small", action="store_true",
                     help="a reduced case for ncu captures (fewer Gaussians, one step)")
     return ap.parse_args()
@@ -357,6 +360,59 @@ def gt_views_gpu(ctx, s):
     return views
 
 
+def run_c4(local, learn_iters):
+    """Learned densification on the clustered scene in config-3 precision: the network
+    learns online from plain runs on scene seeds 2-5 (the densification window of each),
+    then plain and learned densification train scene seed 6 for the same number of steps."""
+    import torch
+    from splatrs_b200 import gpu as G
+    from splatrs_b200 import scenes
+    ctx = G.Context(local, torch.cuda.current_stream(local))
+
+    def setup(seed):
+        s = scenes.config3(seed_gt=seed, seed_init=seed + 100)
+        views = gt_views_gpu(ctx, s)
+        ip = G.init_from_points(ctx, s["init_points"], s["init_rgb"])
+        n0 = len(s["init_points"])
+        init = G.planes_to_params(ctx, ip, n0, n0).cpu().numpy()
+        return init, views, scenes.scene_extent(s["cams"])
+
+    theta, learn = None, []
+    for seed in (2, 3, 4, 5):
+        init, views, ext = setup(seed)
+        t = G.Trainer(ctx, init, ext, views, **dict(C3_TRAIN, learned_densify=1))
+        if theta is not None:
+            t.set_mlp(theta)
+        tw = time.perf_counter()
+        t.run(learn_iters)
+        torch.cuda.synchronize(local)
+        st = t.mlp_stats()
+        theta = t.get_mlp()
+        learn.append({"seed": seed, "steps": learn_iters, "wall_s": round(time.perf_counter() - tw, 2),
+                      "densifications": st["events"], "records": st["records"],
+                      "labels_keep_densify_prune": [st["label_keep"], st["label_densify"], st["label_prune"]],
+                      "heldout_accuracy_network": round(st["heldout_net"] / max(st["heldout_records"], 1), 4),
+                      "heldout_accuracy_rule": round(st["heldout_rule"] / max(st["heldout_records"], 1), 4)})
+        t.close()
+    init, views, ext = setup(6)
+    ev = {}
+    for name, mode in (("plain", 0), ("learned", 2)):
+        t = G.Trainer(ctx, init, ext, views, **dict(C3_TRAIN, learned_densify=mode))
+        if mode == 2:
+            t.set_mlp(theta)
+        torch.cuda.synchronize(local)
+        tw = time.perf_counter()
+        t.run(C3_TRAIN["iterations"])
+        torch.cuda.synchronize(local)
+        wall = time.perf_counter() - tw
+        ps = float(np.mean([scenes.psnr(t.render(cam), rgb) for cam, rgb in views]))
+        ev[name] = {"steps": C3_TRAIN["iterations"], "wall_s": round(wall, 3), "psnr_train_views": round(ps, 2),
+                    "ssim_train_views": round(mean_ssim(t, views), 4), "gaussians": t.count}
+        t.close()
+    ctx.close()
+    return {"learn": learn, "seed6": ev}
+
+
 def mean_ssim(trainer, views):
     """Mean SSIM of the trainer's renders over the views (the loss kernel at lambda 1)."""
     import torch
@@ -500,6 +556,8 @@ def main():
         line["train_c3"] = {"gpu": gpu_c3, "views_per_step": C3_TRAIN["batch_views"],
                             "sizes": "uniform over 640x480, 1024x768, 1297x840, 1600x1200 per view"}
         del views3
+    if args.train_c4 and not args.profile_small:
+        line["train_c4"] = run_c4(local, args.c4_learn_iters)
     if rank == 0:
         if c0 is not None and not args.no_cpu_baseline and world == 1:
             line["train_c0"]["cpu"] = run_train_cpu(*c0, C0_TRAIN, C0_TRAIN["iterations"])

