@@ -146,6 +146,8 @@ EMIT_BYTES_PER_ENTRY = 12          # key + value written
 RASTER_FWD_BYTES_PER_PIXEL = 20    # image (12) + final T (4) + n_contrib (4) written
 RASTER_BWD_BYTES_PER_PIXEL = 20    # dL/dpix (12) + final T (4) + n_contrib (4) read
 RASTER_BYTES_PER_ENTRY = 52        # sorted index (4) + record gather (48)
+# dram__bytes_read.sum + dram__bytes_write.sum per launch, ncu, default workload.
+NCU_DRAM_BYTES_1M = {"raster_bwd": int((197.05 + 17.84) * 1e6), "raster_fwd": int((82.84 + 20.76) * 1e6)}
 RASTER_FWD_FLOP_PER_PAIR = 20
 RASTER_BWD_FLOP_PER_PAIR = 50
 
@@ -295,8 +297,11 @@ def run_ours(args, rank, world, local):
     else:
         byts = (EMIT_BYTES_PER_ENTRY + SORT_BYTES_PER_KEY_PASS) * entries
     achieved = byts / (stage_ms[dom] / 1e3) / 1e9
+    # DRAM bytes per launch from one ncu capture of this workload (1M Gaussians, 1080p):
+    # profiles/raster_dram_traffic_1M_1080p_ncu.md. Other sizes have no capture.
+    traffic = NCU_DRAM_BYTES_1M.get(dom) if n == 1_000_000 else None
     roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
-                "frac": round(achieved / hbm_peak, 4), "traffic": None, "peak_source": peak_kind,
+                "frac": round(achieved / hbm_peak, 4), "traffic": traffic, "peak_source": peak_kind,
                 "algorithmic_bytes_per_launch": int(byts)}
     flops = {"raster_fwd": RASTER_FWD_FLOP_PER_PAIR * pairs_fwd, "raster_bwd": RASTER_BWD_FLOP_PER_PAIR * pairs_bwd}
     compute = {k: {"pairs": p, "flop": flops[k], "ms": round(stage_ms[k], 4),
