@@ -298,12 +298,18 @@ SPLAT_API int splat_project_bwd_adam(splat_ctx* ctx, float* planes_dev, float* m
  * vector of splat_mlp_num_params() values: W1 [16][64], b1 [64], W2 [64][64], b2 [64],
  * W3 [64][3], b3 [3] (W[in][out]).
  *   splat_mlp_forward: probabilities (n x 3) of n feature rows (n x 16).
+ *   splat_mlp_forward_tc: the same on the 5th-generation tensor cores (tcgen05 MMAs,
+ *     accumulators in tensor memory, persistent blocks of 128-row tiles); x_dev 16-byte
+ *     aligned; same rounding points, sums in another order. Synchronises; a timed-out wait
+ *     for the tensor cores returns SPLAT_ERR_TIMEOUT.
  *   splat_mlp_grad: adds to grad_dev the gradient of the weighted mean cross-entropy
  *     sum_s w_s * -log p_s[y_s] / sum_s w_s (labels y in 0..2; scale = 1 / sum_s w_s).
  *   splat_mlp_adam: one Adam step (beta 0.9 / 0.999, eps 1e-8) on the FP32 parameters.
  * -------------------------------------------------------------------------------------- */
 SPLAT_API int32_t splat_mlp_num_params(void);
 SPLAT_API int splat_mlp_forward(splat_ctx* ctx, const float* x_dev, int64_t n, const float* theta_dev, float* prob_dev);
+SPLAT_API int splat_mlp_forward_tc(splat_ctx* ctx, const float* x_dev, int64_t n, const float* theta_dev,
+                                  float* prob_dev);
 SPLAT_API int splat_mlp_grad(splat_ctx* ctx, const float* x_dev, const int32_t* y_dev, const float* w_dev, int64_t n,
                              float scale, const float* theta_dev, float* grad_dev);
 SPLAT_API int splat_mlp_adam(splat_ctx* ctx, float* theta_dev, const float* grad_dev, float* m_dev, float* v_dev,

@@ -154,6 +154,7 @@ def _declare(L):
         "splat_bin_count_device": ([vp, vp, i64, vp, vp], C.c_int),
         "splat_mlp_num_params": ([], i32),
         "splat_mlp_forward": ([vp, vp, i64, vp, vp], C.c_int),
+        "splat_mlp_forward_tc": ([vp, vp, i64, vp, vp], C.c_int),
         "splat_mlp_grad": ([vp, vp, vp, vp, i64, C.c_float, vp, vp], C.c_int),
         "splat_mlp_adam": ([vp, vp, vp, vp, vp, C.c_uint64, C.c_float], C.c_int),
         "splat_bin_sort_device_scratch_bytes": ([i64], sz),

@@ -306,6 +306,15 @@ SPLAT_API int splat_mlp_forward(splat_ctx* ctx, const float* x_dev, int64_t n, c
   return finish(ctx, launch_mlp_forward(&ctx->c, x_dev, n, theta_dev, prob_dev));
 }
 
+SPLAT_API int splat_mlp_forward_tc(splat_ctx* ctx, const float* x_dev, int64_t n, const float* theta_dev,
+                                  float* prob_dev) {
+  if (!ctx) return SPLAT_ERR_INVALID;
+  if (n < 0 || !theta_dev || (n && (!x_dev || !prob_dev))) return invalid(ctx, "splat_mlp_forward_tc: bad buffers");
+  if (reinterpret_cast<uintptr_t>(x_dev) % 16) return invalid(ctx, "splat_mlp_forward_tc: x_dev not 16-byte aligned");
+  Enter e(ctx);
+  return finish(ctx, mlp_forward_tc_checked(&ctx->c, x_dev, n, theta_dev, prob_dev));
+}
+
 SPLAT_API int splat_mlp_grad(splat_ctx* ctx, const float* x_dev, const int32_t* y_dev, const float* w_dev, int64_t n,
                              float scale, const float* theta_dev, float* grad_dev) {
   if (!ctx) return SPLAT_ERR_INVALID;

@@ -92,6 +92,15 @@ Status launch_bin_sort_dev(Ctx* c, const float* proj, const uint32_t* entry_offs
 // The learned-densification network (mlp.cu): 16 -> 64 -> 64 -> 3, FP32 parameter vector.
 int mlp_num_params();
 Status launch_mlp_forward(Ctx* c, const float* x, int64_t n, const float* theta, float* prob);
+// The same on tcgen05 (TMEM accumulators). `err` is a word the device can store to (the
+// context's mapped host page): set to 1 if a wait for the tensor cores timed out.
+Status launch_mlp_forward_tc(Ctx* c, const float* x, int64_t n, const float* theta, float* prob, uint32_t* err);
+// Word of the context's mapped host page (c->host_small) that the tcgen05 kernels report
+// timeouts in.
+constexpr int kTcErrWord = 1000;
+// Runs the tcgen05 forward with the error word cleared, synchronises and turns a reported
+// timeout into an error status.
+Status mlp_forward_tc_checked(Ctx* c, const float* x, int64_t n, const float* theta, float* prob);
 Status launch_mlp_grad(Ctx* c, const float* x, const int32_t* y, const float* w, int64_t n, float scale,
                        const float* theta, float* grad);
 Status launch_mlp_adam(Ctx* c, float* theta, const float* grad, float* m, float* v, uint64_t step, float lr);

@@ -1,7 +1,9 @@
 // The learned-densification network (no reference counterpart; it proposes, per Gaussian,
 // one of {keep, clone/split, prune} beside the threshold rule of src/densify.rs:125-221):
 // 16 features -> 64 SiLU -> 64 SiLU -> 3 logits -> softmax, BF16 operands on the tensor
-// cores (mma.sync m16n8k16) with FP32 accumulation.
+// cores with FP32 accumulation: the inference forward on tcgen05 (accumulators in tensor
+// memory, further down), the training kernels on mma.sync m16n8k16 (their per-warp
+// transposed products want register fragments).
 //
 // Parameters are one FP32 vector (the optimiser's master copy): W1 [16][64], b1 [64],
 // W2 [64][64], b2 [64], W3 [64][3], b3 [3] with W[in][out]. Each block rounds them to BF16
@@ -13,6 +15,8 @@
 // logit gradient and hidden-layer gradients before each product; biases and their
 // gradients stay FP32.
 #include <cuda_bf16.h>
+
+#include <atomic>
 
 #include "common.cuh"
 #include "kernels.cuh"
@@ -27,10 +31,10 @@ constexpr int kWarps = 4, kThreads = 32 * kWarps, kRows = 16 * kWarps;
 
 typedef __nv_bfloat16 bf;
 
+// Two values rounded to BF16 (nearest even) in one conversion: lo in the low half.
 __device__ __forceinline__ uint32_t pack2(float lo, float hi) {
-  const uint32_t a = __bfloat16_as_ushort(__float2bfloat16_rn(lo));
-  const uint32_t b = __bfloat16_as_ushort(__float2bfloat16_rn(hi));
-  return a | (b << 16);
+  const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+  return *reinterpret_cast<const uint32_t*>(&v);
 }
 __device__ __forceinline__ uint32_t pack2h(bf lo, bf hi) {
   return (uint32_t)__bfloat16_as_ushort(lo) | ((uint32_t)__bfloat16_as_ushort(hi) << 16);
@@ -47,9 +51,19 @@ __device__ __forceinline__ void mma16816(float d[4], uint32_t a0, uint32_t a1, u
       : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
 }
 
-__device__ __forceinline__ float silu(float z) { return z / (1.0f + __expf(-z)); }
+// The logistic function as 0.5 (1 + tanh(z / 2)) with the hardware tanh approximation (one
+// special-function instruction where exp and a reciprocal take two; the epilogues are
+// bound by that unit). Its error, about 2^-11 relative, sits below the BF16 rounding of the
+// activations that follows.
+__device__ __forceinline__ float tanh_fast(float x) {
+  float y;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float sigmoid(float z) { return 0.5f + 0.5f * tanh_fast(0.5f * z); }
+__device__ __forceinline__ float silu(float z) { return z * sigmoid(z); }
 __device__ __forceinline__ float silu_grad(float z) {
-  const float s = 1.0f / (1.0f + __expf(-z));
+  const float s = sigmoid(z);
   return s * (1.0f + z * (1.0f - s));
 }
 
@@ -388,9 +402,282 @@ __global__ void mlp_adam_kernel(float* __restrict__ theta, const float* __restri
   v[i] = 0.999f * v[i] + 0.001f * gi * gi;
   theta[i] -= lr * (m[i] / c1) / (sqrtf(v[i] / c2) + 1e-8f);
 }
+// ---------------------------------------------------------------------------------------
+// The forward on the 5th-generation tensor cores (tcgen05): one CTA of 4 warps per 128
+// Gaussians (M = 128, TMEM lane = row), operands in shared memory in the canonical
+// K-major, no-swizzle layout (8-row x 16-byte core matrices; K-adjacent cores 128 bytes
+// apart, row groups SBO apart), accumulators in 64 TMEM columns that each layer reuses once
+// the previous epilogue has read them. One thread issues each layer's MMAs and
+// commits them to an mbarrier; every thread waits on it (bounded: a timeout sets *err and
+// skips to the end, which waits once more, also bounded, for the MMAs in flight and always
+// frees the TMEM), reads its row with tcgen05.ld, applies bias and SiLU and writes the next
+// layer's A operand back to shared memory.
+// ---------------------------------------------------------------------------------------
+constexpr int kTcRows = 128;
+constexpr uint32_t kTmemCols = 64;
+
+struct TcSmem {
+  alignas(1024) unsigned char ax[kTcRows * kIn * 2];    // A layer 1: [128][16]
+  alignas(1024) unsigned char ah[kTcRows * kHid * 2];   // A layers 2-3: [128][64]
+  alignas(1024) unsigned char bw1[kHid * kIn * 2];      // B layer 1: [64 out][16 in]
+  alignas(1024) unsigned char bw2[kHid * kHid * 2];     // B layer 2: [64 out][64 in]
+  alignas(1024) unsigned char bw3[16 * kHid * 2];       // B layer 3: [16 out (3 used)][64 in]
+  float b1[kHid], b2[kHid], b3[16];
+  alignas(8) uint64_t mbar;
+  uint32_t tmem_base;
+};
+
+// Byte offset of element (row, k) of a K-major operand with `kdim` columns.
+__device__ __forceinline__ uint32_t core_off(int row, int k, int kdim) {
+  return (uint32_t)((row >> 3) * (kdim / 8) * 128 + (k >> 3) * 128 + (row & 7) * 16 + (k & 7) * 2);
+}
+
+__device__ __forceinline__ uint64_t smem_desc(const void* p, uint32_t sbo) {
+  const uint32_t a = (uint32_t)__cvta_generic_to_shared(p);
+  return (uint64_t)((a >> 4) & 0x3FFFu) | ((uint64_t)((128u >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);  // LBO 128 B, version 1, no swizzle
+}
+
+// kind::f16 instruction descriptor: BF16 A and B, F32 accumulator, both K-major, M = 128.
+__host__ __device__ constexpr uint32_t idesc_bf16(uint32_t n) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((n >> 3) << 17) | ((128u >> 4) << 24);
+}
+
+__device__ __forceinline__ void tc_mma(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
+      "l"(a), "l"(b), "r"(idesc), "r"(acc));
+}
+
+__device__ __forceinline__ void tc_commit(uint64_t* bar) {
+  const uint32_t a = (uint32_t)__cvta_generic_to_shared(bar);
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(a) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase) {
+  const uint32_t a = (uint32_t)__cvta_generic_to_shared(bar);
+  for (uint32_t it = 0; it < (1u << 22); it++) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, P1;\n\t}"
+        : "=r"(done)
+        : "r"(a), "r"(phase)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void async_proxy_fence() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// 16 consecutive accumulator columns of this thread's row.
+__device__ __forceinline__ void tmem_ld16(uint32_t addr, float v[16]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(addr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
+}
+
+// Hidden layer epilogue: this thread's row of the accumulator at column col0, plus bias,
+// SiLU, rounded to BF16 into the A operand of the next layer.
+__device__ __forceinline__ void hidden_epilogue(TcSmem& s, uint32_t tmem_row, uint32_t col0, const float* bias,
+                                                int row) {
+#pragma unroll
+  for (int c = 0; c < kHid; c += 16) {
+    float v[16];
+    tmem_ld16(tmem_row + col0 + c, v);
+#pragma unroll
+    for (int h = 0; h < 16; h += 8) {  // one 16-byte core-matrix row per store
+      uint32_t w[4];
+#pragma unroll
+      for (int i = 0; i < 4; i++)
+        w[i] = pack2(silu(v[h + 2 * i] + bias[c + h + 2 * i]), silu(v[h + 2 * i + 1] + bias[c + h + 2 * i + 1]));
+      *reinterpret_cast<uint4*>(s.ah + core_off(row, c + h, kHid)) = make_uint4(w[0], w[1], w[2], w[3]);
+    }
+  }
+}
+
+// A 128-row tile of feature rows (512 float4, contiguous) into registers, coalesced:
+// thread t holds float4s t, t + 128, t + 256 and t + 384 of the tile.
+__device__ __forceinline__ void load_tile(const float* __restrict__ x, int64_t tile, int64_t n, float4 r[4]) {
+  const float4* x4 = reinterpret_cast<const float4*>(x);
+  const int64_t base = tile * kTcRows * (kIn / 4), lim = n * (kIn / 4);
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const int64_t i = base + threadIdx.x + kTcRows * q;
+    r[q] = i < lim ? __ldcs(x4 + i) : make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+}
+
+// Persistent: a CTA lays the weights out once and loops over 128-row tiles with stride
+// gridDim.x, loading the next tile's rows into registers while this tile's MMAs run.
+__global__ void __launch_bounds__(kTcRows) mlp_forward_tc_kernel(const float* __restrict__ x, int64_t n,
+                                                                  const float* __restrict__ th,
+                                                                  float* __restrict__ prob,
+                                                                  volatile uint32_t* __restrict__ err) {
+  extern __shared__ unsigned char tc_raw[];
+  TcSmem& s = *reinterpret_cast<TcSmem*>((reinterpret_cast<uintptr_t>(tc_raw) + 1023) & ~(uintptr_t)1023);
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int64_t tiles = (n + kTcRows - 1) / kTcRows;
+  if (tid == 0) {
+    const uint32_t a = (uint32_t)__cvta_generic_to_shared(&s.mbar);
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(a) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    const uint32_t a = (uint32_t)__cvta_generic_to_shared(&s.tmem_base);
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(a), "r"(kTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  // Weights, rounded to BF16, in the K-major operand layouts.
+  for (int i = tid; i < kIn * kHid; i += kTcRows) {
+    const int in = i / kHid, out = i % kHid;
+    *reinterpret_cast<bf*>(s.bw1 + core_off(out, in, kIn)) = __float2bfloat16_rn(th[kW1 + i]);
+  }
+  for (int i = tid; i < kHid * kHid; i += kTcRows) {
+    const int in = i / kHid, out = i % kHid;
+    *reinterpret_cast<bf*>(s.bw2 + core_off(out, in, kHid)) = __float2bfloat16_rn(th[kW2 + i]);
+  }
+  for (int i = tid; i < 16 * kHid; i += kTcRows) {
+    const int out = i / kHid, in = i % kHid;
+    const float w = out < kOut ? th[kW3 + in * kOut + out] : 0.0f;
+    *reinterpret_cast<bf*>(s.bw3 + core_off(out, in, kHid)) = __float2bfloat16_rn(w);
+  }
+  if (tid < kHid) {
+    s.b1[tid] = th[kB1 + tid];
+    s.b2[tid] = th[kB2 + tid];
+  }
+  if (tid < 16) s.b3[tid] = tid < kOut ? th[kB3 + tid] : 0.0f;
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = s.tmem_base;
+  const uint32_t tmem_row = tmem + ((uint32_t)(32 * warp) << 16);
+  bool ok = true;
+  uint32_t phase = 0;
+  float4 xr[4];
+  int64_t tile = blockIdx.x;
+  if (tile < tiles) load_tile(x, tile, n, xr);
+  for (; tile < tiles; tile += gridDim.x) {
+    const int64_t row_g = tile * kTcRows + tid;
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const int f = tid + kTcRows * q;  // row f / 4, columns 4 (f % 4) .. + 3
+      *reinterpret_cast<uint2*>(s.ax + core_off(f >> 2, (f & 3) * 4, kIn)) =
+          make_uint2(pack2(xr[q].x, xr[q].y), pack2(xr[q].z, xr[q].w));
+    }
+    async_proxy_fence();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    // Layer 1: [128 x 16] x [16 x 64] into columns 0-63.
+    if (tid == 0) {
+      tc_mma(tmem, smem_desc(s.ax, 256), smem_desc(s.bw1, 256), idesc_bf16(kHid), 0u);
+      tc_commit(&s.mbar);
+    }
+    if (tile + gridDim.x < tiles) load_tile(x, tile + gridDim.x, n, xr);
+    ok = !__syncthreads_or(!mbar_wait(&s.mbar, phase));  // the block agrees
+    if (!ok) break;
+    phase ^= 1u;
+    tc_fence_after();
+    hidden_epilogue(s, tmem_row, 0, s.b1, tid);
+    async_proxy_fence();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    // Layer 2: [128 x 64] x [64 x 64] into columns 0-63, four K-steps of 16.
+    if (tid == 0) {
+#pragma unroll
+      for (int k = 0; k < 4; k++)
+        tc_mma(tmem, smem_desc(s.ah + 256 * k, 1024), smem_desc(s.bw2 + 256 * k, 1024), idesc_bf16(kHid),
+               k > 0 ? 1u : 0u);
+      tc_commit(&s.mbar);
+    }
+    ok = !__syncthreads_or(!mbar_wait(&s.mbar, phase));
+    if (!ok) break;
+    phase ^= 1u;
+    tc_fence_after();
+    hidden_epilogue(s, tmem_row, 0, s.b2, tid);
+    async_proxy_fence();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    // Layer 3: [128 x 64] x [64 x 16] into columns 0-15.
+    if (tid == 0) {
+#pragma unroll
+      for (int k = 0; k < 4; k++)
+        tc_mma(tmem, smem_desc(s.ah + 256 * k, 1024), smem_desc(s.bw3 + 256 * k, 1024), idesc_bf16(16),
+               k > 0 ? 1u : 0u);
+      tc_commit(&s.mbar);
+    }
+    ok = !__syncthreads_or(!mbar_wait(&s.mbar, phase));
+    if (!ok) break;
+    phase ^= 1u;
+    tc_fence_after();
+    float v[16];
+    tmem_ld16(tmem_row, v);
+    const float z0 = v[0] + s.b3[0], z1 = v[1] + s.b3[1], z2 = v[2] + s.b3[2];
+    const float m = fmaxf(z0, fmaxf(z1, z2));
+    const float e0 = __expf(z0 - m), e1 = __expf(z1 - m), e2 = __expf(z2 - m);
+    const float inv = 1.0f / (e0 + e1 + e2);
+    if (row_g < n) {
+      prob[row_g * 3] = e0 * inv;
+      prob[row_g * 3 + 1] = e1 * inv;
+      prob[row_g * 3 + 2] = e2 * inv;
+    }
+  }
+  if (!ok) {
+    mbar_wait(&s.mbar, phase);  // the timed-out MMAs, before their TMEM is freed
+    if (tid == 0) *err = 1u;
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+  }
+}
 }  // namespace
 
 int mlp_num_params() { return kParams; }
+
+Status launch_mlp_forward_tc(Ctx* c, const float* x, int64_t n, const float* theta, float* prob, uint32_t* err) {
+  if (n == 0) return Status::ok();
+  const size_t smem = sizeof(TcSmem) + 1024;
+  SPLAT_CUDA(cudaFuncSetAttribute(mlp_forward_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int dev = 0, sms = 0, smem_sm = 0, smem_rsv = 0;
+  SPLAT_CUDA(cudaGetDevice(&dev));
+  SPLAT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  SPLAT_CUDA(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+  SPLAT_CUDA(cudaDeviceGetAttribute(&smem_rsv, cudaDevAttrReservedSharedMemoryPerBlock, dev));
+  // As many CTAs as fit at once: shared memory, and 512 / 64 tensor-memory columns.
+  const int per_sm = std::max(1, std::min<int>(smem_sm / (int)(smem + smem_rsv), 512 / (int)kTmemCols));
+  const int64_t grid = std::min<int64_t>(ceil_div(n, kTcRows), (int64_t)per_sm * sms);
+  mlp_forward_tc_kernel<<<(unsigned)grid, kTcRows, smem, c->stream>>>(x, n, theta, prob, err);
+  c->launches.count++;
+  SPLAT_LAUNCHED("mlp_forward_tc_kernel");
+  return Status::ok();
+}
+
+Status mlp_forward_tc_checked(Ctx* c, const float* x, int64_t n, const float* theta, float* prob) {
+  volatile uint32_t* h = reinterpret_cast<volatile uint32_t*>(c->host_small) + kTcErrWord;
+  *h = 0u;
+  std::atomic_thread_fence(std::memory_order_seq_cst);
+  SPLAT_TRY(launch_mlp_forward_tc(c, x, n, theta, prob, reinterpret_cast<uint32_t*>(c->host_small_dev) + kTcErrWord));
+  SPLAT_CUDA(cudaStreamSynchronize(c->stream));
+  if (*h != 0u) return Status::make(SPLAT_ERR_TIMEOUT, "mlp_forward_tc: a wait for the tensor cores timed out");
+  return Status::ok();
+}
 
 Status launch_mlp_forward(Ctx* c, const float* x, int64_t n, const float* theta, float* prob) {
   if (n == 0) return Status::ok();

@@ -540,7 +540,7 @@ Status learn_from_previous(splat_trainer* t) {
   if (total == 0.0) return Status::ok();
   // Held-out accuracy: the network predicts these labels before it trains on them.
   SPLAT_TRY(t->policy.ensure((size_t)rn * 12));
-  SPLAT_TRY(launch_mlp_forward(c, t->rec_x.as<float>(), rn, t->mlp_theta.as<float>(), t->policy.as<float>()));
+  SPLAT_TRY(mlp_forward_tc_checked(c, t->rec_x.as<float>(), rn, t->mlp_theta.as<float>(), t->policy.as<float>()));
   unsigned long long* acc = t->label_counts.as<unsigned long long>() + 3;
   SPLAT_TRY(launch_fill_u32(c, acc, 6, 0u));
   SPLAT_TRY(launch_label_accuracy(c, t->policy.as<float>(), t->rec_action.as<uint32_t>(), t->labels.as<int32_t>(), rn,
@@ -610,7 +610,7 @@ Status density_control(splat_trainer* t, const IterPlan& p, splat_step_info* inf
     if (learn && t->rec_valid && t->rec_n > 0) SPLAT_TRY(learn_from_previous(t));
     if (apply) {
       SPLAT_TRY(t->policy.ensure((size_t)std::max<int64_t>(n, 1) * 12));
-      SPLAT_TRY(launch_mlp_forward(c, t->feat.as<float>(), n, t->mlp_theta.as<float>(), t->policy.as<float>()));
+      SPLAT_TRY(mlp_forward_tc_checked(c, t->feat.as<float>(), n, t->mlp_theta.as<float>(), t->policy.as<float>()));
       dp.policy = t->policy.as<float>();
     }
     if (learn) {

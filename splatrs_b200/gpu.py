@@ -531,11 +531,13 @@ def init_from_points(ctx: Context, points, rgb, cap: int | None = None) -> torch
     return planes
 
 
-def mlp_forward(ctx: Context, x: torch.Tensor, theta: torch.Tensor) -> torch.Tensor:
-    """Learned-densification network: probabilities (n, 3) of feature rows (n, 16)."""
+def mlp_forward(ctx: Context, x: torch.Tensor, theta: torch.Tensor, tcgen05: bool = False) -> torch.Tensor:
+    """Learned-densification network: probabilities (n, 3) of feature rows (n, 16); with
+    `tcgen05` on the 5th-generation tensor cores (accumulators in tensor memory)."""
     x = x.contiguous().float()
     prob = torch.empty((x.shape[0], 3), dtype=torch.float32, device=x.device)
-    check(ctx.lib.splat_mlp_forward(ctx.h, _ptr(x), x.shape[0], _ptr(theta), _ptr(prob)), ctx.h)
+    fn = ctx.lib.splat_mlp_forward_tc if tcgen05 else ctx.lib.splat_mlp_forward
+    check(fn(ctx.h, _ptr(x), x.shape[0], _ptr(theta), _ptr(prob)), ctx.h)
     return prob
 
 

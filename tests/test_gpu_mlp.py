@@ -1,7 +1,8 @@
 """The learned-densification network's tensor-core kernels against the CPU oracle
 (oracle/mlp.py): probabilities and parameter gradients in the oracle's bf16 mode (same
-rounding points, so differences come from accumulation order and the fast exp in SiLU),
-each also reported against the float64 oracle; Adam; and a learning sanity check."""
+rounding points, so differences come from accumulation order and the hardware tanh in
+SiLU), each also reported against the float64 oracle; the tcgen05 forward against both
+the oracle and the mma.sync forward; Adam; and a learning sanity check."""
 import numpy as np
 import pytest
 import torch
@@ -42,6 +43,34 @@ def test_mlp_forward_matches_oracle(ctx, n):
     p64, _ = M.forward(theta, x)
     print(f"\nn={n}: probabilities max-abs vs bf16 oracle {np.abs(got - want).max():.2e}, "
           f"vs f64 oracle {np.abs(got - p64).max():.2e}")
+
+
+@pytest.mark.parametrize("n", [1, 127, 128, 129, 4099, 100_000])
+def test_mlp_forward_tcgen05_matches_oracle(ctx, n):
+    """The tcgen05 forward (accumulators in tensor memory) against the bf16 oracle and the
+    mma.sync forward: same rounding points, sums in another order, so a hidden activation
+    may round to the neighbouring BF16 value; probabilities agree to well under 5e-3."""
+    theta, x, _, _ = _case(50 + n, n)
+    tx, tth = _t(x), _t(theta)
+    got = G.mlp_forward(ctx, tx, tth, tcgen05=True).cpu().numpy()
+    ref = G.mlp_forward(ctx, tx, tth).cpu().numpy()
+    m = min(n, 4099)
+    want, _ = M.forward(theta, x[:m], bf16_like=True)
+    assert np.isfinite(got).all()
+    assert np.abs(got[:m] - want).max() < 5e-3
+    assert np.abs(got - ref).max() < 5e-3
+    assert np.abs(got.sum(1) - 1.0).max() < 1e-5
+    print(f"\nn={n}: tcgen05 max-abs vs bf16 oracle {np.abs(got[:m] - want).max():.2e}, "
+          f"vs mma.sync {np.abs(got - ref).max():.2e}, equal rows {np.mean(np.all(got == ref, 1)):.3f}")
+
+
+def test_mlp_forward_tcgen05_empty_and_repeated(ctx):
+    theta, x, _, _ = _case(70, 300)
+    empty = G.mlp_forward(ctx, _t(x[:0]), _t(theta), tcgen05=True)
+    assert empty.shape == (0, 3)
+    a = G.mlp_forward(ctx, _t(x), _t(theta), tcgen05=True).cpu().numpy()
+    b = G.mlp_forward(ctx, _t(x), _t(theta), tcgen05=True).cpu().numpy()
+    assert np.array_equal(a, b)
 
 
 @pytest.mark.parametrize("n", [64, 1000])
