@@ -1,6 +1,7 @@
 """Benchmark of the differentiable render path on one B200 (render-only kernel benchmark
-configuration): 1,000,000 Gaussians, one 1920x1080 view, 16x16 tiles, plain FP32 forward
-and backward with an upstream dL/dpixel drawn N(0,1) per channel.
+configuration): 1,000,000 Gaussians, one 1920x1080 view, plain FP32 forward and backward
+with an upstream dL/dpixel drawn N(0,1) per channel. The compositing configuration (tile
+shape x chunk depth) is autotuned on this workload before warm-up (--raster fixes one).
 
 One step = projection + binning (scan, key emission, radix sort, tile ranges) +
 compositing forward + compositing backward + projection backward for that view. The metric
@@ -30,7 +31,7 @@ sys.path.insert(0, ROOT)
 WIDTH, HEIGHT = 1920, 1080
 METRIC = "train iters/s and Mpix/s fwd+bwd at 1 B200 vs plain GPU & CPU, at matched PSNR"
 UNIT = "Mpix/s"
-WORKLOAD = "render fwd+bwd, 1M Gaussians, 1920x1080, 16x16 tiles, SH degree 3, dL/dpix ~ N(0,1)"
+WORKLOAD = "render fwd+bwd, 1M Gaussians, 1920x1080, SH degree 3, dL/dpix ~ N(0,1)"
 
 
 def parse():
@@ -42,6 +43,8 @@ def parse():
     ap.add_argument("--n", type=int, default=1_000_000)
     ap.add_argument("--cpu-steps", type=int, default=3, help="steps of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--raster", default="auto",
+                    help="compositing configuration: 'auto' (autotune) or TWxTHxCHUNK, e.g. 16x16x256")
     ap.add_argument("--no-train", action="store_true", help="skip the config-0 training run")
     ap.add_argument("--train-c2", action="store_true",
                     help="also run plain training on the clustered 500k-Gaussian multi-view scene")
@@ -147,7 +150,8 @@ RASTER_FWD_BYTES_PER_PIXEL = 20    # image (12) + final T (4) + n_contrib (4) wr
 RASTER_BWD_BYTES_PER_PIXEL = 20    # dL/dpix (12) + final T (4) + n_contrib (4) read
 RASTER_BYTES_PER_ENTRY = 52        # sorted index (4) + record gather (48)
 # dram__bytes_read.sum + dram__bytes_write.sum per launch, ncu, default workload.
-NCU_DRAM_BYTES_1M = {"raster_bwd": int((197.05 + 17.84) * 1e6), "raster_fwd": int((82.84 + 20.76) * 1e6)}
+NCU_DRAM_BYTES_1M = {("raster_bwd", 16, 16, 256): int((197.05 + 17.84) * 1e6),
+                     ("raster_fwd", 16, 16, 256): int((82.84 + 20.76) * 1e6)}
 RASTER_FWD_FLOP_PER_PAIR = 20
 RASTER_BWD_FLOP_PER_PAIR = 50
 
@@ -173,6 +177,16 @@ def run_ours(args, rank, world, local):
     dimage = torch.from_numpy(s["dimage"]).to(dev)
     pgrad = torch.zeros((3, n, 4), dtype=torch.float32, device=dev)
     del params
+
+    # Compositing configuration: every candidate timed on this workload, the fastest kept.
+    tuning = None
+    if args.raster == "auto":
+        tuning = ctx.autotune_render(planes, n, n, cam, opts, bg, dimage, reps=3)
+        tuning = {"picked": list(tuning["picked"]),
+                  "ms_per_pass": {f"{a}x{b}x{c}": round(v, 4) for (a, b, c), v in tuning["ms"].items()}}
+    else:
+        ctx.raster_config = tuple(int(v) for v in args.raster.split("x"))
+    raster = ctx.raster_config
 
     # Stage-level step with events between stages.
     def full_step(ev=None):
@@ -299,7 +313,7 @@ def run_ours(args, rank, world, local):
     achieved = byts / (stage_ms[dom] / 1e3) / 1e9
     # DRAM bytes per launch from one ncu capture of this workload (1M Gaussians, 1080p):
     # profiles/raster_dram_traffic_1M_1080p_ncu.md. Other sizes have no capture.
-    traffic = NCU_DRAM_BYTES_1M.get(dom) if n == 1_000_000 else None
+    traffic = NCU_DRAM_BYTES_1M.get((dom,) + tuple(raster)) if n == 1_000_000 else None
     roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
                 "frac": round(achieved / hbm_peak, 4), "traffic": traffic, "peak_source": peak_kind,
                 "algorithmic_bytes_per_launch": int(byts)}
@@ -318,8 +332,11 @@ def run_ours(args, rank, world, local):
         "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded; config-1 distributions)",
-        "config": {"workload": WORKLOAD, "gaussians": n, "width": WIDTH, "height": HEIGHT, "tile": 16,
+        "config": {"workload": WORKLOAD, "gaussians": n, "width": WIDTH, "height": HEIGHT,
+                   "tile": [raster[0], raster[1]], "chunk": raster[2],
+                   "raster": "autotuned" if tuning else "fixed",
                    "l2": "inputs larger than L2 (240 MB parameter planes), no flush", "parallelism": f"replicas x{world}"},
+        "autotune": tuning,
         "iters_per_s": round(1e3 / ms_per_step, 3),
         "stages_ms": {k: round(v, 4) for k, v in stage_ms.items()},
         "entries": entries, "visible": visible, "sort_keys_per_s": round(entries / (stage_ms["bin"] / 1e3), 1),
@@ -349,7 +366,7 @@ C2_TRAIN = dict(iterations=30000, densify=1, densify_from_iter=500, densify_unti
 C3_TRAIN = dict(iterations=3750, densify=1, densify_from_iter=63, densify_until_iter=1875, densification_interval=13,
                 opacity_reset_interval=375, densify_grad_threshold=0.0002, lambda_dssim=0.2, sh_degree=3,
                 sh_degree_interval=125, position_lr_max_steps=3750, seed=0, max_gaussians=3_000_000,
-                batch_views=8, bf16_storage=1, fp64_conic=1)
+                batch_views=8, bf16_storage=1, fp64_conic=1, autotune=1)
 
 
 def gt_views_gpu(ctx, s):
@@ -457,6 +474,10 @@ def run_train_gpu(local, s, cfg, iterations):
     out = {"iterations": iterations, "wall_s": round(wall, 3), "iters_per_s": round(iterations / wall, 1),
            "views_per_s": round(iterations * bv / wall, 1), "psnr_train_views": round(ps, 2),
            "ssim_train_views": round(mean_ssim(t, views), 4), "gaussians": t.count}
+    if cfg.get("autotune"):
+        tu = t.tuning()
+        out["autotune"] = {"tunes": tu["tunes"], "picked": list(tu["picked"]),
+                           "ms_per_pass": {f"{a}x{b}x{c}": round(v, 4) for (a, b, c), v in tu["ms"].items()}}
     t.close()
     ctx.close()
     return out, init, views, extent

@@ -141,6 +141,11 @@ typedef struct splat_train_config {
    * >= 0.9, the rule deciding everything else (with an all-zero network this is exactly
    * the rule). */
   int32_t learned_densify;
+  /* Not in the reference: 1 times the iteration's render stages (no optimiser step) under
+   * every compositing configuration (splat_raster_candidates) before the first iteration
+   * and again whenever the Gaussian count has moved by more than a quarter since, and
+   * keeps the fastest on the context; 0 uses the context's configuration as it is. */
+  int32_t autotune;
 } splat_train_config;
 
 typedef struct splat_ctx splat_ctx;
@@ -315,6 +320,30 @@ SPLAT_API int splat_mlp_grad(splat_ctx* ctx, const float* x_dev, const int32_t* 
 SPLAT_API int splat_mlp_adam(splat_ctx* ctx, float* theta_dev, const float* grad_dev, float* m_dev, float* v_dev,
                              uint64_t step, float lr);
 
+/* ----------------------------------------------------------------------------------------
+ * Compositing configuration (not in the reference): tile shape and shared-memory chunk
+ * depth of the compositing kernels, held by the context and used by every later launch
+ * (projection, binning and compositing must run under the same one). 16x16 tiles are the
+ * reference's and give its tile lists; 8x8 and 16x32 give other lists but identical
+ * images, final transmittances and, up to summation order, gradients (each entry's pixel
+ * rectangle is first narrowed to its 16-pixel tile rectangle). Chunk depth: entries
+ * staged in shared memory per round, 32, 64, 128 or 256. Default 16x16, 256.
+ *   splat_raster_candidates: writes the 12 supported (tile_w, tile_h, chunk) triples to
+ *     out (36 values) and returns 12.
+ *   splat_set_raster_config: SPLAT_ERR_INVALID for an unsupported triple.
+ *   splat_autotune_render: times projection + binning + forward + backward compositing of
+ *     one view (dimage_dev: dL/dimage, H*W*3) under every candidate, `reps` timed passes
+ *     each after an untimed one, sets the fastest on the context and writes the mean
+ *     milliseconds per pass of every candidate to ms_out (12) and the pick to picked (3).
+ *     Synchronises; changes no caller buffer.
+ * -------------------------------------------------------------------------------------- */
+SPLAT_API int32_t splat_raster_candidates(uint32_t* out);
+SPLAT_API int splat_set_raster_config(splat_ctx* ctx, uint32_t tile_w, uint32_t tile_h, uint32_t chunk);
+SPLAT_API int splat_get_raster_config(splat_ctx* ctx, uint32_t* out3);
+SPLAT_API int splat_autotune_render(splat_ctx* ctx, const float* planes_dev, int64_t n, int64_t cap,
+                                    const splat_camera* cam, const splat_proj_opts* opts, const float* background,
+                                    const float* dimage_dev, int32_t reps, float* ms_out, uint32_t* picked);
+
 /* Fill `bytes` bytes of device memory with zeros on the context stream. */
 SPLAT_API int splat_zero(splat_ctx* ctx, void* dev, size_t bytes);
 
@@ -467,6 +496,10 @@ SPLAT_API int64_t splat_trainer_count(const splat_trainer* t);
 SPLAT_API int splat_trainer_get_mlp(splat_trainer* t, float* theta_host);
 SPLAT_API int splat_trainer_set_mlp(splat_trainer* t, const float* theta_host);
 SPLAT_API int splat_trainer_mlp_stats(const splat_trainer* t, uint64_t out[9]);
+/* Autotuning (splat_train_config.autotune): the last tuning's milliseconds per render pass
+ * of every candidate (ms_out, 12, in splat_raster_candidates order; 0 before any), the
+ * configuration in use (picked, 3) and how many tunings ran. Any pointer may be NULL. */
+SPLAT_API int splat_trainer_tuning(const splat_trainer* t, float* ms_out, uint32_t* picked, uint32_t* tunes);
 SPLAT_API int32_t splat_trainer_sh_degree(const splat_trainer* t);
 SPLAT_API uint32_t splat_trainer_iteration(const splat_trainer* t);
 SPLAT_API int splat_trainer_get_model(splat_trainer* t, float* aos59_host);

@@ -85,7 +85,7 @@ class TrainConfig(C.Structure):
                 ("white_background", C.c_int32), ("sh_degree", C.c_int32), ("sh_degree_interval", C.c_uint32),
                 ("near_plane", C.c_float), ("seed", C.c_uint64), ("max_gaussians", C.c_uint64),
                 ("entry_capacity", C.c_uint64), ("bf16_storage", C.c_int32), ("fp64_conic", C.c_int32),
-                ("batch_views", C.c_uint32), ("learned_densify", C.c_int32)]
+                ("batch_views", C.c_uint32), ("learned_densify", C.c_int32), ("autotune", C.c_int32)]
 
     DEFAULTS = dict(iterations=30000, position_lr_init=0.00016, position_lr_final=0.0000016,
                     position_lr_max_steps=30000, feature_lr=0.0025, opacity_lr=0.025, scaling_lr=0.005,
@@ -94,7 +94,7 @@ class TrainConfig(C.Structure):
                     percent_dense=0.01, min_opacity=0.005, max_screen_size=-1, absgrad=0, antialias=0,
                     white_background=0, sh_degree=3, sh_degree_interval=1000, near_plane=0.2, seed=0,
                     max_gaussians=0, entry_capacity=0, bf16_storage=0, fp64_conic=0,
-                    batch_views=0, learned_densify=0)
+                    batch_views=0, learned_densify=0, autotune=0)
 
     @classmethod
     def make(cls, **kw):
@@ -157,6 +157,11 @@ def _declare(L):
         "splat_mlp_forward_tc": ([vp, vp, i64, vp, vp], C.c_int),
         "splat_mlp_grad": ([vp, vp, vp, vp, i64, C.c_float, vp, vp], C.c_int),
         "splat_mlp_adam": ([vp, vp, vp, vp, vp, C.c_uint64, C.c_float], C.c_int),
+        "splat_raster_candidates": ([P(C.c_uint32)], i32),
+        "splat_set_raster_config": ([vp, C.c_uint32, C.c_uint32, C.c_uint32], C.c_int),
+        "splat_get_raster_config": ([vp, P(C.c_uint32)], C.c_int),
+        "splat_autotune_render": ([vp, vp, i64, i64, vp, vp, P(C.c_float), vp, i32, P(C.c_float), P(C.c_uint32)],
+                                  C.c_int),
         "splat_bin_sort_device_scratch_bytes": ([i64], sz),
         "splat_bin_sort_device": ([vp, vp, vp, i64, vp, i64, vp, u32, u32, vp, vp, vp, vp], C.c_int),
         "splat_rasterize_fwd": ([vp, vp, vp, vp, u32, u32, P(C.c_float), vp, vp, vp, vp], C.c_int),
@@ -199,6 +204,7 @@ def _declare(L):
         "splat_trainer_get_mlp": ([vp, vp], C.c_int),
         "splat_trainer_set_mlp": ([vp, vp], C.c_int),
         "splat_trainer_mlp_stats": ([vp, P(C.c_uint64)], C.c_int),
+        "splat_trainer_tuning": ([vp, P(C.c_float), P(C.c_uint32), P(C.c_uint32)], C.c_int),
         "splat_trainer_count": ([vp], i64),
         "splat_trainer_sh_degree": ([vp], i32),
         "splat_trainer_iteration": ([vp], u32),

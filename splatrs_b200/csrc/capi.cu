@@ -297,6 +297,51 @@ SPLAT_API int splat_bin_sort(splat_ctx* ctx, const float* proj_dev, const uint32
                                      tile_range_dev));
 }
 
+SPLAT_API int32_t splat_raster_candidates(uint32_t* out) {
+  if (out)
+    for (int k = 0; k < kRasterCandidates; k++) {
+      out[3 * k] = kRasterCandidateList[k].tile_w;
+      out[3 * k + 1] = kRasterCandidateList[k].tile_h;
+      out[3 * k + 2] = kRasterCandidateList[k].chunk;
+    }
+  return kRasterCandidates;
+}
+
+SPLAT_API int splat_set_raster_config(splat_ctx* ctx, uint32_t tile_w, uint32_t tile_h, uint32_t chunk) {
+  if (!ctx) return SPLAT_ERR_INVALID;
+  if (!RasterConfig::supported(tile_w, tile_h, chunk))
+    return invalid(ctx, "splat_set_raster_config: tiles 8x8, 16x16 or 16x32 and chunk depth 32, 64, 128 or 256");
+  ctx->c.raster.tile_w = tile_w;
+  ctx->c.raster.tile_h = tile_h;
+  ctx->c.raster.chunk = chunk;
+  return SPLAT_OK;
+}
+
+SPLAT_API int splat_get_raster_config(splat_ctx* ctx, uint32_t* out3) {
+  if (!ctx || !out3) return SPLAT_ERR_INVALID;
+  out3[0] = ctx->c.raster.tile_w;
+  out3[1] = ctx->c.raster.tile_h;
+  out3[2] = ctx->c.raster.chunk;
+  return SPLAT_OK;
+}
+
+SPLAT_API int splat_autotune_render(splat_ctx* ctx, const float* planes_dev, int64_t n, int64_t cap,
+                                    const splat_camera* cam, const splat_proj_opts* opts, const float* background,
+                                    const float* dimage_dev, int32_t reps, float* ms_out, uint32_t* picked) {
+  if (!ctx) return SPLAT_ERR_INVALID;
+  if (!cam_ok(cam) || !opts_ok(opts) || !background || !dimage_dev || reps < 1 || n < 0 || cap < n ||
+      (n && !planes_dev))
+    return invalid(ctx, "splat_autotune_render: bad arguments");
+  Enter e(ctx);
+  float ms[kRasterCandidates];
+  const Status s = tune_render(&ctx->c, planes_dev, n, cap, *cam, *opts, background, dimage_dev, reps, ms);
+  if (!s.good()) return fail(ctx, s);
+  if (ms_out)
+    for (int k = 0; k < kRasterCandidates; k++) ms_out[k] = ms[k];
+  if (picked) splat_get_raster_config(ctx, picked);
+  return SPLAT_OK;
+}
+
 SPLAT_API int32_t splat_mlp_num_params(void) { return mlp_num_params(); }
 
 SPLAT_API int splat_mlp_forward(splat_ctx* ctx, const float* x_dev, int64_t n, const float* theta_dev, float* prob_dev) {

@@ -1,6 +1,7 @@
 // Host-side launchers of the device stages; each returns a Status and launches on the
 // context stream.
 #pragma once
+#include <functional>
 #include "common.cuh"
 #include "adam.cuh"
 
@@ -137,6 +138,20 @@ constexpr int kScanValuesPerBlock = 4096;
 Status launch_bin_sort(Ctx* c, const float* proj, const uint32_t* entry_offset, int64_t n, int64_t E,
                        const uint32_t* depth_range_dev, uint32_t depth_min, uint32_t depth_max, uint32_t width,
                        uint32_t height, uint32_t* gauss_out, uint64_t* keys_out, uint32_t* ranges);
+
+// The supported compositing configurations (tile shapes x chunk depths).
+constexpr int kRasterCandidates = 12;
+extern const RasterConfig kRasterCandidateList[kRasterCandidates];
+// Times pass() under every candidate configuration: pass(true) once, untimed (it may
+// synchronise, size buffers and redo work), then pass(false) `reps` times between two
+// events on c->stream. Leaves c->raster at the fastest (at its old value on failure) and
+// writes each candidate's mean milliseconds per pass to ms[].
+Status tune_raster(Ctx* c, const std::function<Status(bool)>& pass, int reps, float ms[kRasterCandidates]);
+// tune_raster over one view's projection, binning and forward + backward compositing
+// (dimage: dL/dimage of the view); allocates and frees its own buffers.
+Status tune_render(Ctx* c, const float* planes, int64_t n, int64_t cap, const splat_camera& cam,
+                   const splat_proj_opts& opts, const float bg[3], const float* dimage, int reps,
+                   float ms[kRasterCandidates]);
 
 Status launch_raster_fwd(Ctx* c, const float* proj, const uint32_t* gauss, const uint32_t* ranges, uint32_t width,
                          uint32_t height, const float bg[3], float* image, float* final_t, uint32_t* n_contrib,

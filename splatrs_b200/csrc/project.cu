@@ -446,7 +446,7 @@ __device__ __forceinline__ void write_record(float4* __restrict__ rec, uint32_t*
                                              const float mean2d[2], const float conic[3], float depth, uint32_t radius,
                                              float opacity, const float color[3], uint32_t tx0, uint32_t ty0,
                                              uint32_t tx1, uint32_t ty1, uint32_t width, uint32_t height,
-                                             uint32_t* depth_range) {
+                                             uint32_t* depth_range, uint32_t tile_w, uint32_t tile_h) {
   const float sigma_max = crm::logf_cr(opacity / SPLAT_ALPHA_MIN);
   const float A = conic[0], B = conic[1], Cc = conic[2];
   const float det = A * Cc - B * B;
@@ -458,6 +458,27 @@ __device__ __forceinline__ void write_record(float4* __restrict__ rec, uint32_t*
     x1 = abs_bound(floorf(mean2d[0] + half_x - 0.5f) + 1.0f, width);
     y0 = abs_bound(ceilf(mean2d[1] - half_y - 0.5f), height);
     y1 = abs_bound(floorf(mean2d[1] + half_y - 0.5f) + 1.0f, height);
+  }
+  if (tile_w != kTile || tile_h != kTile) {
+    // Another tile shape: the pixels the entry may touch are its alpha box within its
+    // 16-pixel tile rectangle (what the reference's tile lists and per-pixel test allow
+    // together), and its tiles are the ones that box overlaps, so every pixel composites
+    // the same entries in the same order as with 16x16 tiles.
+    const uint32_t ex0 = max(x0, tx0 * kTile), ex1 = min(x1, tx1 * kTile);
+    const uint32_t ey0 = max(y0, ty0 * kTile), ey1 = min(y1, ty1 * kTile);
+    if (ex0 < ex1 && ey0 < ey1) {
+      x0 = ex0;
+      x1 = ex1;
+      y0 = ey0;
+      y1 = ey1;
+      tx0 = ex0 / tile_w;
+      tx1 = (ex1 + tile_w - 1) / tile_w;
+      ty0 = ey0 / tile_h;
+      ty1 = (ey1 + tile_h - 1) / tile_h;
+    } else {
+      x0 = x1 = y0 = y1 = 0;
+      tx0 = tx1 = ty0 = ty1 = 0;
+    }
   }
   rec[4 * i + 0] = make_float4(mean2d[0], mean2d[1], A, B);
   rec[4 * i + 1] = make_float4(Cc, opacity, sigma_max, color[0]);
@@ -495,7 +516,8 @@ __global__ void __launch_bounds__(256) project_fwd_kernel(const float4* __restri
                                                           uint32_t* __restrict__ depth_range,
                                                           const StepParams* __restrict__ sp,
                                                           const uint2* __restrict__ bf,
-                                                          const BatchTable* __restrict__ bt) {
+                                                          const BatchTable* __restrict__ bt, uint32_t tile_w,
+                                                          uint32_t tile_h) {
   // A batch launch has one grid row per view; its records follow view-major.
   const int view = bt ? (int)blockIdx.y : 0;
   if (bt && view >= bt->views) return;
@@ -527,7 +549,7 @@ __global__ void __launch_bounds__(256) project_fwd_kernel(const float4* __restri
           for (int ch = 0; ch < 3; ch++) color[ch] = fmaxf(k.color_raw[ch], 0.0f);
           const float opacity = k.o_raw * k.comp;
           write_record(rec, num_tiles, i, k.mean2d, k.conic, k.t[2], sat_u32(r), opacity, color, tx0, ty0, tx1, ty1,
-                       cam.width, cam.height, depth_range);
+                       cam.width, cam.height, depth_range, tile_w, tile_h);
           visible = true;
           depth = k.t[2];
         }
@@ -541,7 +563,7 @@ __global__ void __launch_bounds__(256) project_fwd_kernel(const float4* __restri
 // Records from reference-layout Proj values.
 __global__ void proj_from_reference_kernel(const float* __restrict__ p15, int64_t n, uint32_t width, uint32_t height,
                                            float4* __restrict__ rec, uint32_t* __restrict__ num_tiles,
-                                           uint32_t* __restrict__ depth_range) {
+                                           uint32_t* __restrict__ depth_range, uint32_t tile_w, uint32_t tile_h) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   bool visible = false;
   float depth = 0.0f;
@@ -558,7 +580,7 @@ __global__ void proj_from_reference_kernel(const float* __restrict__ p15, int64_
       const float conic[3] = {p[2], p[3], p[4]};
       const float color[3] = {p[8], p[9], p[10]};
       write_record(rec, num_tiles, i, mean2d, conic, p[5], radius, p[7], color, tx0, ty0, tx1, ty1, width, height,
-                   depth_range);
+                   depth_range, tile_w, tile_h);
       visible = true;
       depth = p[5];
     } else {
@@ -921,7 +943,8 @@ Status launch_project_fwd(Ctx* c, const float* planes, int64_t n, int64_t cap, c
   const uint2* bf = static_cast<const uint2*>(bf16);
 #define SPLAT_PFWD(D, B) \
   project_fwd_kernel<D, B><<<dim3(grid, bt ? kMaxViews : 1), bs, 0, c->stream>>>(p, n, cap, cam, opts, r, num_tiles, \
-                                                                                 depth_range, sp, bf, bt)
+                                                                                 depth_range, sp, bf, bt, \
+                                                                                 c->raster.tile_w, c->raster.tile_h)
   if (bf) {
     switch (opts.sh_degree) {
       case 0: SPLAT_PFWD(0, true); break;
@@ -950,7 +973,8 @@ Status launch_proj_from_reference(Ctx* c, const float* p15, int64_t n, uint32_t 
   if (n == 0) return Status::ok();
   proj_from_reference_kernel<<<ceil_div(n, 256), 256, 0, c->stream>>>(p15, n, width, height,
                                                                        reinterpret_cast<float4*>(proj), num_tiles,
-                                                                       depth_range);
+                                                                       depth_range, c->raster.tile_w,
+                                                                       c->raster.tile_h);
   c->launches.count++;
   SPLAT_LAUNCHED("proj_from_reference_kernel");
   return Status::ok();

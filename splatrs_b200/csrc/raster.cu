@@ -1,19 +1,34 @@
 // Front-to-back alpha compositing, forward and backward (reference src/rasterize.rs).
 //
-// One 256-thread block per 16x16 tile, one pixel per thread. Warps own 8x4 pixel
-// sub-blocks so that an entry whose pixel rectangle misses a sub-block is skipped by the
-// whole warp with one uniform branch. The tile's sorted entries are staged through shared
-// memory in chunks of 256 (each thread gathers one entry's 48-byte record). Every
+// One block per tile (16x16 by default; 8x8 and 16x32 too), one pixel per thread. Warps own
+// 8x4 pixel sub-blocks so that an entry whose pixel rectangle misses a sub-block is skipped
+// by the whole warp with one uniform branch. The tile's sorted entries are staged through
+// shared memory in chunks of CH entries (32-256; each entry's 48-byte record gathered by one
+// thread). Tile shape and chunk depth are template parameters, chosen at run time from the
+// context's configuration (the autotuner's pick). Every
 // per-pixel decision (sigma range, alpha >= 1/255, the 0.99 clamp, T < 1e-4) is taken on
 // values computed exactly as the reference computes them: unfused arithmetic and a
 // correctly rounded exp.
+#include <type_traits>
+
 #include "common.cuh"
 #include "kernels.cuh"
 
 namespace splat {
 
-constexpr int kRasterThreads = 256;
-constexpr int kChunk = 256;
+// Geometry of a TW x TH tile: TW * TH threads, warps over 8x4 sub-blocks row by row. An
+// entry's pixel rectangle within the tile is a column mask and a row mask packed in one
+// word (rows from bit kRowShift), 32 bits while the rows fit in 16, else 64.
+template <int TW, int TH>
+struct TileGeo {
+  static constexpr int kThreads = TW * TH;
+  static constexpr int kWarps = kThreads / 32;
+  static constexpr int kWarpsX = TW / 8;
+  static constexpr int kRowShift = TH > 16 ? 32 : 16;
+  typedef typename std::conditional<(TH > 16), unsigned long long, uint32_t>::type Mask;
+  typedef typename std::conditional<(kWarps > 8), uint16_t, uint8_t>::type WarpMask;
+  static_assert(TW % 8 == 0 && TH % 4 == 0 && TW <= 16 && TH <= 32, "tile shape");
+};
 
 struct PixelGeom {
   uint32_t px_i, py_j;   // absolute pixel
@@ -21,12 +36,14 @@ struct PixelGeom {
   bool inside;
 };
 
+template <int TW, int TH>
 __device__ __forceinline__ PixelGeom pixel_geom(uint32_t tile, uint32_t tiles_x, uint32_t width, uint32_t height) {
+  constexpr int WX = TileGeo<TW, TH>::kWarpsX;
   const uint32_t tx = tile % tiles_x, ty = tile / tiles_x;
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   PixelGeom p;
-  p.bx0 = tx * kTile + (warp & 1u) * 8u;
-  p.by0 = ty * kTile + (warp >> 1) * 4u;
+  p.bx0 = tx * TW + (warp % WX) * 8u;
+  p.by0 = ty * TH + (warp / WX) * 4u;
   p.px_i = p.bx0 + (lane & 7u);
   p.py_j = p.by0 + (lane >> 3);
   p.inside = p.px_i < width && p.py_j < height;
@@ -114,30 +131,37 @@ Status launch_diag_fast_exp(Ctx* c, float magnitude_lo, float magnitude_hi, int 
   return Status::ok();
 }
 
-// The entry's pixel rectangle within the tile whose top-left pixel is (ox, oy) as a 16-bit
-// mask of the columns and a 16-bit mask of the rows it covers (columns in the low half).
-__device__ __forceinline__ uint32_t tile_rect_masks(uint32_t rx, uint32_t ry, uint32_t ox, uint32_t oy) {
+// The entry's pixel rectangle within the TW x TH tile whose top-left pixel is (ox, oy) as a
+// mask of the columns (low bits) and a mask of the rows (from bit kRowShift) it covers.
+template <int TW, int TH>
+__device__ __forceinline__ typename TileGeo<TW, TH>::Mask tile_rect_masks(uint32_t rx, uint32_t ry, uint32_t ox,
+                                                                           uint32_t oy) {
+  typedef typename TileGeo<TW, TH>::Mask Mask;
   const int x0 = (int)(rx & 0xffffu) - (int)ox, x1 = (int)(rx >> 16) - (int)ox;
   const int y0 = (int)(ry & 0xffffu) - (int)oy, y1 = (int)(ry >> 16) - (int)oy;
-  const uint32_t cx0 = (uint32_t)min(max(x0, 0), 16), cx1 = (uint32_t)min(max(x1, 0), 16);
-  const uint32_t cy0 = (uint32_t)min(max(y0, 0), 16), cy1 = (uint32_t)min(max(y1, 0), 16);
-  const uint32_t cols = cx1 > cx0 ? ((0xffffu >> (16u - (cx1 - cx0))) << cx0) : 0u;
-  const uint32_t rows = cy1 > cy0 ? ((0xffffu >> (16u - (cy1 - cy0))) << cy0) : 0u;
-  return cols | (rows << 16);
+  const uint32_t cx0 = (uint32_t)min(max(x0, 0), TW), cx1 = (uint32_t)min(max(x1, 0), TW);
+  const uint32_t cy0 = (uint32_t)min(max(y0, 0), TH), cy1 = (uint32_t)min(max(y1, 0), TH);
+  const uint32_t cols = cx1 > cx0 ? ((0xffffffffu >> (32u - (cx1 - cx0))) << cx0) : 0u;
+  const uint32_t rows = cy1 > cy0 ? ((0xffffffffu >> (32u - (cy1 - cy0))) << cy0) : 0u;
+  return (Mask)cols | ((Mask)rows << TileGeo<TW, TH>::kRowShift);
 }
 
 // Bit w of the result is set when the pixel rectangle (x0|x1<<16, y0|y1<<16, absolute
 // pixels) overlaps warp w's 8x4 sub-block of the tile whose top-left pixel is (ox, oy).
+template <int TW, int TH>
 __device__ __forceinline__ uint32_t subblock_mask(uint32_t rx, uint32_t ry, uint32_t ox, uint32_t oy) {
+  constexpr int WX = TileGeo<TW, TH>::kWarpsX;
   const uint32_t x0 = rx & 0xffffu, x1 = rx >> 16, y0 = ry & 0xffffu, y1 = ry >> 16;
-  const bool left = x0 < ox + 8u && x1 > ox;
-  const bool right = x0 < ox + 16u && x1 > ox + 8u;
+  bool col[WX];
+#pragma unroll
+  for (int qx = 0; qx < WX; qx++) col[qx] = x0 < ox + 8u * qx + 8u && x1 > ox + 8u * qx;
   uint32_t m = 0;
 #pragma unroll
-  for (uint32_t q = 0; q < 4; q++) {
-    const bool row = y0 < oy + 4u * q + 4u && y1 > oy + 4u * q;
-    if (row && left) m |= 1u << (2 * q);
-    if (row && right) m |= 1u << (2 * q + 1);
+  for (uint32_t qy = 0; qy < (uint32_t)(TH / 4); qy++) {
+    const bool row = y0 < oy + 4u * qy + 4u && y1 > oy + 4u * qy;
+#pragma unroll
+    for (int qx = 0; qx < WX; qx++)
+      if (row && col[qx]) m |= 1u << (qy * WX + qx);
   }
   return m;
 }
@@ -159,7 +183,8 @@ __device__ __forceinline__ uint32_t warp_transpose_bits(uint32_t x) {
 
 // Compacts, in order, the chunk-local indices k < cnt whose mask has this warp's bit (and,
 // when `limit` is finite, k < limit) into list[]; returns how many.
-__device__ __forceinline__ uint32_t build_warp_list(const uint8_t* __restrict__ smask, uint32_t cnt, uint32_t limit,
+template <typename WM>
+__device__ __forceinline__ uint32_t build_warp_list(const WM* __restrict__ smask, uint32_t cnt, uint32_t limit,
                                                     uint8_t* __restrict__ list) {
   const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const uint32_t lt = (1u << lane) - 1u;
@@ -181,19 +206,22 @@ __device__ __forceinline__ uint32_t build_warp_list(const uint8_t* __restrict__ 
 // reference), found from the batch's coverage masks transposed across the warp, so the
 // warp runs as many rounds as its busiest lane rather than one round per entry. Each lane
 // still composites its entries in list (depth) order.
-__global__ void __launch_bounds__(kRasterThreads, 6) raster_fwd_kernel(
+template <int TW, int TH, int CH>
+__global__ void __launch_bounds__(TW * TH, 1536 / (TW * TH)) raster_fwd_kernel(
     const float4* __restrict__ rec, const uint32_t* __restrict__ gauss, const uint2* __restrict__ ranges,
     uint32_t width, uint32_t height, uint32_t tiles_x, float bg0, float bg1, float bg2, float* __restrict__ image,
     float* __restrict__ final_t, uint32_t* __restrict__ n_contrib, unsigned long long* __restrict__ pairs,
     const BatchTable* __restrict__ bt) {
+  typedef TileGeo<TW, TH> Geo;
+  constexpr int NT = Geo::kThreads;
   if (bt && blockIdx.x >= bt->tile_start[bt->views]) return;  // past the batch's tiles
-  __shared__ float4 s0[kChunk], s1[kChunk];
-  __shared__ float2 s2[kChunk];
-  __shared__ uint32_t srect[kChunk];
-  __shared__ uint8_t smask[kChunk];
-  __shared__ uint8_t slist[kRasterThreads / 32][kChunk];
+  __shared__ float4 s0[CH], s1[CH];
+  __shared__ float2 s2[CH];
+  __shared__ typename Geo::Mask srect[CH];
+  __shared__ typename Geo::WarpMask smask[CH];
+  __shared__ uint8_t slist[Geo::kWarps][CH];
   __shared__ double stab[crm::kExpNegEntries];
-  for (int i = threadIdx.x; i < crm::kExpNegEntries; i += kRasterThreads) stab[i] = crm::exp2_neg_entry(i, kExp2Tab64);
+  for (int i = threadIdx.x; i < crm::kExpNegEntries; i += NT) stab[i] = crm::exp2_neg_entry(i, kExp2Tab64);
   // In a batch the block is a global tile: find its view, local tile and image offset.
   uint32_t tile = blockIdx.x;
   size_t pix0 = 0;
@@ -205,10 +233,11 @@ __global__ void __launch_bounds__(kRasterThreads, 6) raster_fwd_kernel(
     tiles_x = bt->tiles_x[v];
     pix0 = bt->pix_start[v];
   }
-  const PixelGeom pg = pixel_geom(tile, tiles_x, width, height);
-  const uint32_t ox = (tile % tiles_x) * kTile, oy = (tile / tiles_x) * kTile;
+  const PixelGeom pg = pixel_geom<TW, TH>(tile, tiles_x, width, height);
+  const uint32_t ox = (tile % tiles_x) * TW, oy = (tile / tiles_x) * TH;
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const uint32_t sbx = (warp & 1u) * 8u, sby = (warp >> 1) * 4u;  // sub-block origin in the tile
+  // Sub-block origin in the tile; its rows' bits in the rectangle masks.
+  const uint32_t sbx = (warp % Geo::kWarpsX) * 8u, sby = (warp / Geo::kWarpsX) * 4u + Geo::kRowShift;
   const float px = (float)pg.px_i + 0.5f, py = (float)pg.py_j + 0.5f;
   const uint2 range = ranges[blockIdx.x];
   uint8_t* list = slist[warp];
@@ -216,22 +245,25 @@ __global__ void __launch_bounds__(kRasterThreads, 6) raster_fwd_kernel(
   uint32_t ncon = 0;
   bool done = !pg.inside;
   unsigned long long npairs = 0;
-  for (uint32_t base = range.x; base < range.y; base += kChunk) {
+  for (uint32_t base = range.x; base < range.y; base += CH) {
     if (__syncthreads_count(!done) == 0) break;
-    const uint32_t idx = base + threadIdx.x;
-    uint32_t m = 0;
-    if (idx < range.y) {
-      const uint32_t g = gauss[idx];
-      s0[threadIdx.x] = rec[4 * (size_t)g];
-      s1[threadIdx.x] = rec[4 * (size_t)g + 1];
-      const float4 e2 = rec[4 * (size_t)g + 2];
-      s2[threadIdx.x] = make_float2(e2.x, e2.y);
-      srect[threadIdx.x] = tile_rect_masks(fbits(e2.z), fbits(e2.w), ox, oy);
-      m = subblock_mask(fbits(e2.z), fbits(e2.w), ox, oy);
+#pragma unroll
+    for (uint32_t e = threadIdx.x; e < (uint32_t)CH; e += NT) {
+      const uint32_t idx = base + e;
+      uint32_t m = 0;
+      if (idx < range.y) {
+        const uint32_t g = gauss[idx];
+        s0[e] = rec[4 * (size_t)g];
+        s1[e] = rec[4 * (size_t)g + 1];
+        const float4 e2 = rec[4 * (size_t)g + 2];
+        s2[e] = make_float2(e2.x, e2.y);
+        srect[e] = tile_rect_masks<TW, TH>(fbits(e2.z), fbits(e2.w), ox, oy);
+        m = subblock_mask<TW, TH>(fbits(e2.z), fbits(e2.w), ox, oy);
+      }
+      smask[e] = (typename Geo::WarpMask)m;
     }
-    smask[threadIdx.x] = (uint8_t)m;
     __syncthreads();
-    const uint32_t cnt = min((uint32_t)kChunk, range.y - base);
+    const uint32_t cnt = min((uint32_t)CH, range.y - base);
     const uint32_t nl = build_warp_list(smask, cnt, 0xffffffffu, list);
     for (uint32_t b0 = 0; b0 < nl; b0 += 32) {
       if (__all_sync(0xffffffffu, done)) break;
@@ -242,9 +274,9 @@ __global__ void __launch_bounds__(kRasterThreads, 6) raster_fwd_kernel(
       uint32_t kl = 0, cov = 0;
       if (j < nl) {
         kl = list[j];
-        const uint32_t rm = srect[kl];
-        const uint32_t c8 = (rm >> sbx) & 0xffu;
-        const uint32_t r4 = (rm >> (16u + sby)) & 0xfu;
+        const typename Geo::Mask rm = srect[kl];
+        const uint32_t c8 = (uint32_t)(rm >> sbx) & 0xffu;
+        const uint32_t r4 = (uint32_t)(rm >> sby) & 0xfu;
         cov = c8 * ((r4 & 1u) | ((r4 & 2u) << 7) | ((r4 & 4u) << 14) | ((r4 & 8u) << 21));
       }
       uint32_t mine = warp_transpose_bits(cov);
@@ -337,20 +369,23 @@ __device__ __forceinline__ float rcp_refined(float x) {
   return __fmaf_rn(r, __fmaf_rn(-x, r, 1.0f), r);
 }
 
-__global__ void __launch_bounds__(kRasterThreads) raster_bwd_kernel(
+template <int TW, int TH, int CH>
+__global__ void __launch_bounds__(TW * TH) raster_bwd_kernel(
     const float4* __restrict__ rec, const uint32_t* __restrict__ gauss, const uint2* __restrict__ ranges,
     uint32_t width, uint32_t height, uint32_t tiles_x, float bg0, float bg1, float bg2,
     const float* __restrict__ final_t, const uint32_t* __restrict__ n_contrib, const float* __restrict__ dimage,
     float4* __restrict__ pgrad, int64_t cap, unsigned long long* __restrict__ pairs,
     const BatchTable* __restrict__ bt) {
+  typedef TileGeo<TW, TH> Geo;
+  constexpr int NT = Geo::kThreads;
   if (bt && blockIdx.x >= bt->tile_start[bt->views]) return;  // past the batch's tiles
-  __shared__ float4 s0[kChunk], s1[kChunk];
-  __shared__ float2 s2[kChunk];
-  __shared__ uint32_t srect[kChunk];
-  __shared__ uint32_t sg[kChunk];
-  __shared__ float acc[kChunk * kSlots];
-  __shared__ uint8_t smask[kChunk];
-  __shared__ uint8_t slist[kRasterThreads / 32][kChunk];
+  __shared__ float4 s0[CH], s1[CH];
+  __shared__ float2 s2[CH];
+  __shared__ typename Geo::Mask srect[CH];
+  __shared__ uint32_t sg[CH];
+  __shared__ float acc[CH * kSlots];
+  __shared__ typename Geo::WarpMask smask[CH];
+  __shared__ uint8_t slist[Geo::kWarps][CH];
   __shared__ uint32_t s_max_last;
   // In a batch the block is a global tile: find its view, local tile and image offset.
   uint32_t tile = blockIdx.x;
@@ -363,9 +398,9 @@ __global__ void __launch_bounds__(kRasterThreads) raster_bwd_kernel(
     tiles_x = bt->tiles_x[v];
     pix0 = bt->pix_start[v];
   }
-  const PixelGeom pg = pixel_geom(tile, tiles_x, width, height);
-  const uint32_t ox = (tile % tiles_x) * kTile, oy = (tile / tiles_x) * kTile;
-  const uint32_t lx = pg.px_i - ox, ly_shift = pg.py_j - oy + 16u;  // bit positions in the rect masks
+  const PixelGeom pg = pixel_geom<TW, TH>(tile, tiles_x, width, height);
+  const uint32_t ox = (tile % tiles_x) * TW, oy = (tile / tiles_x) * TH;
+  const uint32_t lx = pg.px_i - ox, ly_shift = pg.py_j - oy + Geo::kRowShift;  // bits in the rect masks
   const float px = (float)pg.px_i + 0.5f, py = (float)pg.py_j + 0.5f;
   const uint2 range = ranges[blockIdx.x];
   const uint32_t lane = threadIdx.x & 31;
@@ -385,7 +420,7 @@ __global__ void __launch_bounds__(kRasterThreads) raster_bwd_kernel(
     bg_dot = bg0 * d0 + bg1 * d1 + bg2 * d2;
   }
   if (threadIdx.x == 0) s_max_last = 0;
-  for (int i = threadIdx.x; i < kChunk * kSlots; i += kRasterThreads) acc[i] = 0.0f;
+  for (int i = threadIdx.x; i < CH * kSlots; i += NT) acc[i] = 0.0f;
   __syncthreads();
   const uint32_t warp_max_last = __reduce_max_sync(0xffffffffu, last);
   if (lane == 0) atomicMax(&s_max_last, warp_max_last);
@@ -396,20 +431,23 @@ __global__ void __launch_bounds__(kRasterThreads) raster_bwd_kernel(
   unsigned long long npairs = 0;
 
   for (uint32_t cend = max_last; cend > 0;) {
-    const uint32_t cstart = cend > (uint32_t)kChunk ? cend - kChunk : 0u;
+    const uint32_t cstart = cend > (uint32_t)CH ? cend - CH : 0u;
     const uint32_t cnt = cend - cstart;
-    uint32_t m = 0;
-    if (threadIdx.x < cnt) {
-      const uint32_t g = gauss[range.x + cstart + threadIdx.x];
-      sg[threadIdx.x] = g;
-      s0[threadIdx.x] = rec[4 * (size_t)g];
-      s1[threadIdx.x] = rec[4 * (size_t)g + 1];
-      const float4 e2 = rec[4 * (size_t)g + 2];
-      s2[threadIdx.x] = make_float2(e2.x, e2.y);
-      srect[threadIdx.x] = tile_rect_masks(fbits(e2.z), fbits(e2.w), ox, oy);
-      m = subblock_mask(fbits(e2.z), fbits(e2.w), ox, oy);
+#pragma unroll
+    for (uint32_t e = threadIdx.x; e < (uint32_t)CH; e += NT) {
+      uint32_t m = 0;
+      if (e < cnt) {
+        const uint32_t g = gauss[range.x + cstart + e];
+        sg[e] = g;
+        s0[e] = rec[4 * (size_t)g];
+        s1[e] = rec[4 * (size_t)g + 1];
+        const float4 e2 = rec[4 * (size_t)g + 2];
+        s2[e] = make_float2(e2.x, e2.y);
+        srect[e] = tile_rect_masks<TW, TH>(fbits(e2.z), fbits(e2.w), ox, oy);
+        m = subblock_mask<TW, TH>(fbits(e2.z), fbits(e2.w), ox, oy);
+      }
+      smask[e] = (typename Geo::WarpMask)m;
     }
-    smask[threadIdx.x] = (uint8_t)m;
     __syncthreads();
     // Entries at or past every lane's n_contrib contribute nothing to this warp.
     const uint32_t limit = warp_max_last > cstart ? warp_max_last - cstart : 0u;
@@ -417,12 +455,12 @@ __global__ void __launch_bounds__(kRasterThreads) raster_bwd_kernel(
     for (int i = (int)nl - 1; i >= 0; i--) {
       const uint32_t kk = list[i];
       const uint32_t k = cstart + kk;
-      const uint32_t rm = srect[kk];
+      const typename Geo::Mask rm = srect[kk];
       float c[kSlots];
 #pragma unroll
       for (int q = 0; q < kSlots; q++) c[q] = 0.0f;
       bool active = false;
-      if (k < last && ((rm >> lx) & (rm >> ly_shift) & 1u)) {
+      if (k < last && ((uint32_t)(rm >> lx) & (uint32_t)(rm >> ly_shift) & 1u)) {
         const float2 e2 = s2[kk];
         npairs++;
         const float4 e0 = s0[kk], e1 = s1[kk];
@@ -479,9 +517,11 @@ __global__ void __launch_bounds__(kRasterThreads) raster_bwd_kernel(
       }
     }
     __syncthreads();
-    if (threadIdx.x < cnt) {
-      float* a = &acc[threadIdx.x * kSlots];
-      const size_t g = sg[threadIdx.x];
+#pragma unroll
+    for (uint32_t e = threadIdx.x; e < (uint32_t)CH; e += NT) {
+      if (e >= cnt) break;
+      float* a = &acc[e * kSlots];
+      const size_t g = sg[e];
       const float4 v0 = make_float4(a[0], a[1], a[2], a[3]);
       const float4 v1 = make_float4(a[4], a[5], a[6], a[7]);
       const float4 v2 = make_float4(a[8], a[9], a[10], 0.0f);
@@ -500,15 +540,38 @@ __global__ void __launch_bounds__(kRasterThreads) raster_bwd_kernel(
   }
 }
 
+// Expands CALL(TW, TH, CH) for the configuration rc; an unsupported one is an error.
+#define SPLAT_RASTER_DISPATCH(rc, CALL)                                                       \
+  do {                                                                                         \
+    const uint32_t w_ = (rc).tile_w, h_ = (rc).tile_h, c_ = (rc).chunk;                        \
+    if (w_ == 16 && h_ == 16 && c_ == 256) CALL(16, 16, 256);                                  \
+    else if (w_ == 16 && h_ == 16 && c_ == 128) CALL(16, 16, 128);                             \
+    else if (w_ == 16 && h_ == 16 && c_ == 64) CALL(16, 16, 64);                               \
+    else if (w_ == 16 && h_ == 16 && c_ == 32) CALL(16, 16, 32);                               \
+    else if (w_ == 8 && h_ == 8 && c_ == 256) CALL(8, 8, 256);                                 \
+    else if (w_ == 8 && h_ == 8 && c_ == 128) CALL(8, 8, 128);                                 \
+    else if (w_ == 8 && h_ == 8 && c_ == 64) CALL(8, 8, 64);                                   \
+    else if (w_ == 8 && h_ == 8 && c_ == 32) CALL(8, 8, 32);                                   \
+    else if (w_ == 16 && h_ == 32 && c_ == 256) CALL(16, 32, 256);                             \
+    else if (w_ == 16 && h_ == 32 && c_ == 128) CALL(16, 32, 128);                             \
+    else if (w_ == 16 && h_ == 32 && c_ == 64) CALL(16, 32, 64);                               \
+    else if (w_ == 16 && h_ == 32 && c_ == 32) CALL(16, 32, 32);                               \
+    else return Status::make(SPLAT_ERR_INVALID, "unsupported raster configuration");           \
+  } while (0)
+
 Status launch_raster_fwd(Ctx* c, const float* proj, const uint32_t* gauss, const uint32_t* ranges, uint32_t width,
                          uint32_t height, const float bg[3], float* image, float* final_t, uint32_t* n_contrib,
                          uint64_t* pairs, const BatchTable* bt, uint32_t tiles_cap) {
-  const uint32_t tiles_x = (width + kTile - 1) / kTile, tiles_y = (height + kTile - 1) / kTile;
-  const uint32_t blocks = bt ? tiles_cap : tiles_x * tiles_y;
+  const RasterConfig& rc = c->raster;
+  const uint32_t tiles_x = rc.tiles_x(width);
+  const uint32_t blocks = bt ? tiles_cap : rc.tiles(width, height);
   if (blocks == 0) return Status::ok();
-  raster_fwd_kernel<<<blocks, kRasterThreads, 0, c->stream>>>(
-      reinterpret_cast<const float4*>(proj), gauss, reinterpret_cast<const uint2*>(ranges), width, height, tiles_x,
-      bg[0], bg[1], bg[2], image, final_t, n_contrib, reinterpret_cast<unsigned long long*>(pairs), bt);
+#define SPLAT_FWD(TW, TH, CH)                                                                                     \
+  raster_fwd_kernel<TW, TH, CH><<<blocks, TW * TH, 0, c->stream>>>(                                              \
+      reinterpret_cast<const float4*>(proj), gauss, reinterpret_cast<const uint2*>(ranges), width, height, tiles_x, \
+      bg[0], bg[1], bg[2], image, final_t, n_contrib, reinterpret_cast<unsigned long long*>(pairs), bt)
+  SPLAT_RASTER_DISPATCH(rc, SPLAT_FWD);
+#undef SPLAT_FWD
   c->launches.count++;
   SPLAT_LAUNCHED("raster_fwd_kernel");
   return Status::ok();
@@ -518,13 +581,17 @@ Status launch_raster_bwd(Ctx* c, const float* proj, const uint32_t* gauss, const
                          uint32_t height, const float bg[3], const float* final_t, const uint32_t* n_contrib,
                          const float* dimage, float* pgrad, int64_t cap, uint64_t* pairs, const BatchTable* bt,
                          uint32_t tiles_cap) {
-  const uint32_t tiles_x = (width + kTile - 1) / kTile, tiles_y = (height + kTile - 1) / kTile;
-  const uint32_t blocks = bt ? tiles_cap : tiles_x * tiles_y;
+  const RasterConfig& rc = c->raster;
+  const uint32_t tiles_x = rc.tiles_x(width);
+  const uint32_t blocks = bt ? tiles_cap : rc.tiles(width, height);
   if (blocks == 0) return Status::ok();
-  raster_bwd_kernel<<<blocks, kRasterThreads, 0, c->stream>>>(
-      reinterpret_cast<const float4*>(proj), gauss, reinterpret_cast<const uint2*>(ranges), width, height, tiles_x,
-      bg[0], bg[1], bg[2], final_t, n_contrib, dimage, reinterpret_cast<float4*>(pgrad), cap,
-      reinterpret_cast<unsigned long long*>(pairs), bt);
+#define SPLAT_BWD(TW, TH, CH)                                                                                     \
+  raster_bwd_kernel<TW, TH, CH><<<blocks, TW * TH, 0, c->stream>>>(                                              \
+      reinterpret_cast<const float4*>(proj), gauss, reinterpret_cast<const uint2*>(ranges), width, height, tiles_x, \
+      bg[0], bg[1], bg[2], final_t, n_contrib, dimage, reinterpret_cast<float4*>(pgrad), cap,                     \
+      reinterpret_cast<unsigned long long*>(pairs), bt)
+  SPLAT_RASTER_DISPATCH(rc, SPLAT_BWD);
+#undef SPLAT_BWD
   c->launches.count++;
   SPLAT_LAUNCHED("raster_bwd_kernel");
   return Status::ok();

@@ -37,7 +37,7 @@ void DevBuf::release() {
 
 Status ViewBuffers::ensure(int64_t n, uint32_t width, uint32_t height) {
   const size_t npix = (size_t)width * height;
-  const uint32_t tiles = ((width + kTile - 1) / kTile) * ((height + kTile - 1) / kTile);
+  const uint32_t tiles = max_tiles(width, height);  // room for every tile shape
   SPLAT_TRY(proj.ensure((size_t)std::max<int64_t>(n, 1) * kProjFloats * 4));
   SPLAT_TRY(num_tiles.ensure((size_t)std::max<int64_t>(n, 1) * 4));
   SPLAT_TRY(entry_offset.ensure((size_t)(n + 1) * 4));

@@ -474,7 +474,7 @@ static Status sort_and_range(Ctx* c, const float* proj, const uint32_t* entry_of
 Status launch_bin_sort(Ctx* c, const float* proj, const uint32_t* entry_offset, int64_t n, int64_t E,
                        const uint32_t* depth_range_dev, uint32_t depth_min, uint32_t depth_max, uint32_t width,
                        uint32_t height, uint32_t* gauss_out, uint64_t* keys_out, uint32_t* ranges) {
-  const uint32_t tiles_x = (width + kTile - 1) / kTile, tiles_y = (height + kTile - 1) / kTile;
+  const uint32_t tiles_x = c->raster.tiles_x(width), tiles_y = c->raster.tiles_y(height);
   const uint32_t num_tiles = tiles_x * tiles_y;
   if (E == 0) {
     SPLAT_TRY(launch_fill_u32(c, ranges, (size_t)num_tiles * 2, 0u));
@@ -578,7 +578,7 @@ Status launch_bin_sort_dev(Ctx* c, const float* proj, const uint32_t* entry_offs
                            int64_t E_cap, const uint32_t* depth_range_dev, uint32_t width, uint32_t height,
                            void* scratch, uint32_t* gauss_out, uint32_t* ranges, uint32_t* overflow,
                            const BatchTable* bt, int64_t n_view, uint32_t tiles_cap) {
-  const uint32_t tiles_x = (width + kTile - 1) / kTile, tiles_y = (height + kTile - 1) / kTile;
+  const uint32_t tiles_x = c->raster.tiles_x(width), tiles_y = c->raster.tiles_y(height);
   const uint32_t num_tiles = bt ? tiles_cap : tiles_x * tiles_y;
   const int tbits = num_tiles <= 1 ? 0 : 32 - __builtin_clz(num_tiles - 1);
   const int max_passes = (tbits + 32 + 7) / 8;

@@ -110,6 +110,11 @@ struct splat_trainer {
   DevBuf batch_dev;
   uint32_t tiles_cap = 0, loss_cap = 0;
   uint64_t pix_cap = 0;
+  // Autotuning (cfg.autotune): Gaussian count at the last tuning, how many tunings ran,
+  // and the last one's milliseconds per render pass of every candidate configuration.
+  int64_t tuned_n = 0;
+  uint32_t tunes = 0;
+  float tune_ms[kRasterCandidates] = {};
   // Learned densification: birth iteration and (learning) origin of every Gaussian, the
   // previous densification's records (features, rule action), the network and its Adam
   // state, and what learning did.
@@ -241,7 +246,8 @@ std::vector<uint64_t> graph_key(splat_trainer* t, const IterPlan& p) {
   const uint64_t w = t->batch > 1 ? 0 : cam.width, h = t->batch > 1 ? 0 : cam.height;
   std::vector<uint64_t> k = {(uint64_t)t->n, (uint64_t)t->cur.cap, (uint64_t)t->vb.e_cap, (uint64_t)p.sh_degree,
                              (uint64_t)p.densify_window, w, h, t->c->arena.generation, (uint64_t)t->stats_cap,
-                             (uint64_t)t->batch, t->tiles_cap, t->pix_cap};
+                             (uint64_t)t->batch, t->tiles_cap, t->pix_cap, t->c->raster.tile_w,
+                             t->c->raster.tile_h, t->c->raster.chunk};
   for (const DevBuf* b : {&t->cur.params, &t->cur.m, &t->cur.v, &t->bf16, &t->stats, &t->pgrad, &t->pred_grad, &t->loss_out,
                           &t->params_dev, &t->batch_dev, &t->vb.proj, &t->vb.num_tiles, &t->vb.entry_offset, &t->vb.depth_range,
                           &t->vb.tile_range, &t->vb.gauss, &t->vb.image, &t->vb.final_t, &t->vb.n_contrib,
@@ -263,7 +269,7 @@ void drop_graphs(splat_trainer* t) {
 // binning overflowed; then the read-back kernel for slot `slot`. The camera, Adam step and
 // target view come from params_dev (loaded first from the slot's host parameters), so a
 // captured copy replays for any view of the same size.
-Status body(splat_trainer* t, const IterPlan& p, int slot) {
+Status body(splat_trainer* t, const IterPlan& p, int slot, bool probe = false) {
   Ctx* c = t->c;
   const splat_train_config& cfg = t->cfg;
   View& view = *t->views[p.view];
@@ -292,8 +298,10 @@ Status body(splat_trainer* t, const IterPlan& p, int slot) {
                               cam.width, cam.height, bg, t->vb.final_t.as<float>(), t->vb.n_contrib.as<uint32_t>(),
                               t->pred_grad.as<float>(), t->pgrad.as<float>(), cap, nullptr));
   // Optimiser step (train.rs:238-246), fused into the projection backward: the 59
-  // gradients per Gaussian go from registers straight into Adam.
-  SPLAT_TRY(launch_project_bwd_adam(c, t->cur.params.as<float>(), t->cur.m.as<float>(), t->cur.v.as<float>(), n, cap,
+  // gradients per Gaussian go from registers straight into Adam. A probe (autotuning)
+  // leaves the model as it is.
+  if (!probe)
+    SPLAT_TRY(launch_project_bwd_adam(c, t->cur.params.as<float>(), t->cur.m.as<float>(), t->cur.v.as<float>(), n, cap,
                                     cam, opts, t->vb.proj.as<float>(), t->pgrad.as<float>(),
                                     p.densify_window ? t->stats.ptr : nullptr, cfg.absgrad, p.adam_step, p.lr,
                                     t->vb.overflow_flag(), sp, const_cast<void*>(bf16_copy(t)), true));
@@ -304,7 +312,7 @@ Status body(splat_trainer* t, const IterPlan& p, int slot) {
 
 // One batch: every stage one launch over all the batch's views, sized for the capacities
 // and driven by the batch table loaded first from the slot's host copy.
-Status body_batch(splat_trainer* t, const IterPlan& p, int slot) {
+Status body_batch(splat_trainer* t, const IterPlan& p, int slot, bool probe = false) {
   Ctx* c = t->c;
   const splat_train_config& cfg = t->cfg;
   const float bgv = cfg.white_background ? 1.0f : 0.0f;
@@ -351,7 +359,8 @@ Status body_batch(splat_trainer* t, const IterPlan& p, int slot) {
   SPLAT_TRY(launch_raster_bwd(c, proj, v.gauss.as<uint32_t>(), v.tile_range.as<uint32_t>(), cam0.width, cam0.height, bg,
                               v.final_t.as<float>(), v.n_contrib.as<uint32_t>(), t->pred_grad.as<float>(),
                               t->pgrad.as<float>(), pcap, nullptr, bt, t->tiles_cap));
-  SPLAT_TRY(launch_project_bwd_batch_adam(c, t->cur.params.as<float>(), t->cur.m.as<float>(), t->cur.v.as<float>(), n,
+  if (!probe)
+    SPLAT_TRY(launch_project_bwd_batch_adam(c, t->cur.params.as<float>(), t->cur.m.as<float>(), t->cur.v.as<float>(), n,
                                           cap, opts, proj, t->pgrad.as<float>(), pcap,
                                           p.densify_window ? t->stats.ptr : nullptr, cfg.absgrad, v.overflow_flag(),
                                           bt, const_cast<void*>(bf16_copy(t)), true));
@@ -368,7 +377,7 @@ void fill_batch_table(splat_trainer* t, const IterPlan& p, BatchTable& b) {
   b.adam = make_adam_args(p.adam_step, p.lr);
   for (int k = 0; k < p.nviews; k++) {
     const View& v = *t->views[p.views[k]];
-    const uint32_t tx = (v.cam.width + kTile - 1) / kTile, ty = (v.cam.height + kTile - 1) / kTile;
+    const uint32_t tx = t->c->raster.tiles_x(v.cam.width), ty = t->c->raster.tiles_y(v.cam.height);
     const uint32_t lx = (v.cam.width + 31) / 32, ly = (v.cam.height + 31) / 32;
     b.cam[k] = v.cam;
     b.target[k] = v.rgb.ptr;
@@ -378,6 +387,38 @@ void fill_batch_table(splat_trainer* t, const IterPlan& p, BatchTable& b) {
     b.loss_start[k + 1] = b.loss_start[k] + lx * ly;
     b.pix_start[k + 1] = b.pix_start[k] + (uint64_t)v.cam.width * v.cam.height;
   }
+}
+
+// The slot's host parameters of iteration p: the batch table, or the step parameters.
+Status prepare(splat_trainer* t, const IterPlan& p, int slot) {
+  if (t->batch > 1) {
+    fill_batch_table(t, p, t->batch_host[slot]);
+    SPLAT_TRY(t->batch_dev.ensure(sizeof(BatchTable)));
+  } else {
+    View& view = *t->views[p.view];
+    StepParams& hp = t->params_host[slot];
+    hp.cam = view.cam;
+    hp.adam = make_adam_args(p.adam_step, p.lr);
+    hp.target = view.rgb.ptr;
+  }
+  return t->params_dev.ensure(sizeof(StepParams));
+}
+
+// Batch capacities under the context's compositing configuration: the largest view's
+// tiles, SSIM blocks and pixels, times the batch.
+void size_batch_caps(splat_trainer* t) {
+  if (t->batch <= 1) return;
+  uint32_t most_tiles = 0, most_loss = 0;
+  uint64_t most_pix = 0;
+  for (const View* v : t->views) {
+    const uint32_t w = v->cam.width, h = v->cam.height;
+    most_tiles = std::max(most_tiles, t->c->raster.tiles(w, h));
+    most_loss = std::max(most_loss, ((w + 31) / 32) * ((h + 31) / 32));
+    most_pix = std::max<uint64_t>(most_pix, (uint64_t)w * h);
+  }
+  t->tiles_cap = most_tiles * t->batch;
+  t->loss_cap = most_loss * t->batch;
+  t->pix_cap = most_pix * t->batch;
 }
 
 // Captures body() for `slot` into a graph; on any failure graphs are switched off and the
@@ -424,17 +465,7 @@ Status enqueue(splat_trainer* t, const IterPlan& p, int slot) {
   // Scratch of the previous iteration is free for reuse: all of it is consumed on this
   // stream before anything queued now runs.
   arena_reset(c);
-  if (t->batch > 1) {
-    fill_batch_table(t, p, t->batch_host[slot]);
-    SPLAT_TRY(t->batch_dev.ensure(sizeof(BatchTable)));
-  } else {
-    View& view = *t->views[p.view];
-    StepParams& hp = t->params_host[slot];
-    hp.cam = view.cam;
-    hp.adam = make_adam_args(p.adam_step, p.lr);
-    hp.target = view.rgb.ptr;
-  }
-  SPLAT_TRY(t->params_dev.ensure(sizeof(StepParams)));
+  SPLAT_TRY(prepare(t, p, slot));
   if (t->graphs) {
     const std::vector<uint64_t> key = graph_key(t, p);
     if (key != t->gkey) {
@@ -689,6 +720,44 @@ Status initial_capacity(splat_trainer* t) {
   return ensure_stats(t, t->cur.cap);
 }
 
+// Autotuning is due before the first iteration and whenever the Gaussian count has moved
+// by more than a quarter since the last tuning.
+bool tune_due(const splat_trainer* t) {
+  if (!t->cfg.autotune) return false;
+  if (t->tunes == 0) return true;
+  const int64_t d = t->n > t->tuned_n ? t->n - t->tuned_n : t->tuned_n - t->n;
+  return 4 * d > t->tuned_n;
+}
+
+// Times iteration p's render stages (a probe: everything but the optimiser step, so the
+// model is left as it is) under every compositing configuration and keeps the fastest.
+// Needs no iteration in flight; uses slot 0.
+Status autotune(splat_trainer* t, const IterPlan& p) {
+  Ctx* c = t->c;
+  auto pass = [&](bool warm) -> Status {
+    arena_reset(c);
+    if (warm) {
+      size_batch_caps(t);
+      SPLAT_TRY(prepare(t, p, 0));
+    }
+    for (;;) {
+      SPLAT_TRY(t->batch > 1 ? body_batch(t, p, 0, true) : body(t, p, 0, true));
+      if (!warm) return Status::ok();
+      SPLAT_CUDA(cudaStreamSynchronize(c->stream));
+      const SlotResult r = read_slot(t, 0);
+      if (!r.overflow) return Status::ok();
+      SPLAT_TRY(grow_entries(t, r.entries));
+      arena_reset(c);
+    }
+  };
+  const Status s = tune_raster(c, pass, 3, t->tune_ms);
+  size_batch_caps(t);
+  SPLAT_TRY(s);
+  t->tuned_n = t->n;
+  t->tunes++;
+  return Status::ok();
+}
+
 // Runs iteration p to completion, redoing it with more room if its binning overflowed.
 Status run_one(splat_trainer* t, const IterPlan& p, int slot, SlotResult* out) {
   for (;;) {
@@ -707,6 +776,7 @@ Status step(splat_trainer* t, splat_step_info* info) {
   info->reset = 0;
   info->cloned = info->split = info->pruned = 0;
   SlotResult r;
+  if (tune_due(t)) SPLAT_TRY(autotune(t, p));
   SPLAT_TRY(run_one(t, p, 0, &r));
   SPLAT_TRY(density_control(t, p, info));
   if (p.densify_now || p.reset_now) SPLAT_CUDA(cudaStreamSynchronize(t->c->stream));
@@ -731,6 +801,7 @@ Status run(splat_trainer* t, uint32_t count, splat_step_info* info) {
   for (uint32_t k = 0; k < count; k++) {
     const IterPlan p = schedule(t);
     const int slot = has_pending ? 1 - pending_slot : 0;
+    if (!has_pending && tune_due(t)) SPLAT_TRY(autotune(t, p));
     SPLAT_TRY(enqueue(t, p, slot));
     if (has_pending) {
       SPLAT_CUDA(cudaEventSynchronize(t->slot_done[pending_slot]));
@@ -910,19 +981,9 @@ SPLAT_API int splat_trainer_start(splat_trainer* t) {
   t->rng = SplitMix64(t->cfg.seed);
   t->order.clear();
   t->batch = t->cfg.batch_views > 1 ? (int)t->cfg.batch_views : 1;
-  if (t->batch > 1) {  // capacities: the largest view, batch times
-    uint32_t max_tiles = 0, max_loss = 0;
-    uint64_t max_pix = 0;
-    for (const View* v : t->views) {
-      const uint32_t w = v->cam.width, h = v->cam.height;
-      max_tiles = std::max(max_tiles, ((w + kTile - 1) / kTile) * ((h + kTile - 1) / kTile));
-      max_loss = std::max(max_loss, ((w + 31) / 32) * ((h + 31) / 32));
-      max_pix = std::max<uint64_t>(max_pix, (uint64_t)w * h);
-    }
-    t->tiles_cap = max_tiles * t->batch;
-    t->loss_cap = max_loss * t->batch;
-    t->pix_cap = max_pix * t->batch;
-  }
+  size_batch_caps(t);
+  t->tuned_n = 0;
+  t->tunes = 0;
   t->iteration = 0;
   t->adam_step = 0;
   t->sh_degree = 0;
@@ -1000,6 +1061,18 @@ SPLAT_API int splat_trainer_mlp_stats(const splat_trainer* t, uint64_t out[9]) {
   out[3] = t->label_hist[1];
   out[4] = t->label_hist[2];
   out[5] = t->mlp_steps;
+  return SPLAT_OK;
+}
+SPLAT_API int splat_trainer_tuning(const splat_trainer* t, float* ms_out, uint32_t* picked, uint32_t* tunes) {
+  if (!t) return SPLAT_ERR_INVALID;
+  if (ms_out)
+    for (int k = 0; k < kRasterCandidates; k++) ms_out[k] = t->tune_ms[k];
+  if (picked) {
+    picked[0] = t->c->raster.tile_w;
+    picked[1] = t->c->raster.tile_h;
+    picked[2] = t->c->raster.chunk;
+  }
+  if (tunes) *tunes = t->tunes;
   return SPLAT_OK;
 }
 SPLAT_API int32_t splat_trainer_sh_degree(const splat_trainer* t) { return t ? t->sh_degree : -1; }

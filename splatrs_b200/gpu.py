@@ -53,6 +53,36 @@ class Context:
     def launches(self) -> int:
         return int(self.lib.splat_ctx_launch_count(self.h))
 
+    @staticmethod
+    def raster_candidates() -> list:
+        """The supported compositing configurations (tile_w, tile_h, chunk depth)."""
+        lib = L.lib()
+        out = (C.c_uint32 * 36)()
+        k = int(lib.splat_raster_candidates(out))
+        return [tuple(int(v) for v in out[3 * i:3 * i + 3]) for i in range(k)]
+
+    @property
+    def raster_config(self) -> tuple:
+        """(tile_w, tile_h, chunk depth) that projection, binning and compositing use."""
+        out = (C.c_uint32 * 3)()
+        check(self.lib.splat_get_raster_config(self.h, out), self.h)
+        return tuple(int(v) for v in out)
+
+    @raster_config.setter
+    def raster_config(self, cfg):
+        check(self.lib.splat_set_raster_config(self.h, *[int(v) for v in cfg]), self.h)
+
+    def autotune_render(self, planes, n, cap, cam, opts, background, dimage, reps: int = 3) -> dict:
+        """Times one view's render + backward under every configuration and keeps the
+        fastest; returns {config: ms per pass} and the pick."""
+        ms = (C.c_float * 12)()
+        picked = (C.c_uint32 * 3)()
+        bgp, _keep = _bg(background)
+        check(self.lib.splat_autotune_render(self.h, _ptr(planes), n, cap, C.byref(cam), C.byref(opts), bgp,
+                                             _ptr(dimage), reps, ms, picked), self.h)
+        cands = Context.raster_candidates()
+        return {"ms": {c: float(ms[i]) for i, c in enumerate(cands)}, "picked": tuple(int(v) for v in picked)}
+
     def zero(self, t: torch.Tensor):
         check(self.lib.splat_zero(self.h, _ptr(t), t.numel() * t.element_size()), self.h)
 
@@ -150,8 +180,9 @@ def bin(ctx: Context, proj: Projection, want_keys: bool = False) -> Binning:
     e = C.c_int64()
     check(ctx.lib.splat_bin_count(ctx.h, _ptr(proj.num_tiles), proj.n, _ptr(off), C.byref(e)), ctx.h)
     E = int(e.value)
-    tx = (proj.width + 15) // 16
-    ty = (proj.height + 15) // 16
+    tw, th, _ = ctx.raster_config
+    tx = (proj.width + tw - 1) // tw
+    ty = (proj.height + th - 1) // th
     gauss = torch.empty(max(E, 1), dtype=torch.int32, device=dev)
     keys = torch.empty(max(E, 1), dtype=torch.int64, device=dev) if want_keys else None
     tr = torch.empty((tx * ty, 2), dtype=torch.int32, device=dev)
@@ -168,8 +199,9 @@ def bin_device(ctx: Context, proj: Projection, capacity: int, scratch: torch.Ten
     off = torch.empty(proj.n + 1, dtype=torch.int32, device=dev)
     e_dev = torch.zeros(1, dtype=torch.int64, device=dev)
     check(ctx.lib.splat_bin_count_device(ctx.h, _ptr(proj.num_tiles), proj.n, _ptr(off), _ptr(e_dev)), ctx.h)
-    tx = (proj.width + 15) // 16
-    ty = (proj.height + 15) // 16
+    tw, th, _ = ctx.raster_config
+    tx = (proj.width + tw - 1) // tw
+    ty = (proj.height + th - 1) // th
     need = int(ctx.lib.splat_bin_sort_device_scratch_bytes(capacity))
     if scratch is None or scratch.numel() < need:
         scratch = torch.empty(need, dtype=torch.uint8, device=dev)
@@ -453,6 +485,17 @@ class Trainer:
         keys = ("events", "records", "label_keep", "label_densify", "label_prune", "adam_steps", "heldout_net",
                 "heldout_rule", "heldout_records")
         return dict(zip(keys, [int(v) for v in out]))
+
+    def tuning(self) -> dict:
+        """The autotuner's last timings (ms per render pass per configuration), the
+        configuration in use and how many tunings ran."""
+        ms = (C.c_float * 12)()
+        picked = (C.c_uint32 * 3)()
+        tunes = C.c_uint32()
+        check(self.lib.splat_trainer_tuning(self.h, ms, picked, C.byref(tunes)), self.ctx.h)
+        cands = Context.raster_candidates()
+        return {"ms": {c: float(ms[i]) for i, c in enumerate(cands)}, "picked": tuple(int(v) for v in picked),
+                "tunes": int(tunes.value)}
 
     def run(self, iterations: int) -> dict:
         """``iterations`` steps in one call, queued ahead of the device; info of the last."""
