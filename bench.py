@@ -382,10 +382,17 @@ def gt_views_gpu(ctx, s):
     return views
 
 
-def run_c4(local, learn_iters):
+# Learned densification's labels and policy: a kept Gaussian whose descendants blended
+# less than 10 pixel-equivalents over a densification window (13 steps of 8 views) is
+# labelled prune, and applying prunes at a prune probability of 0.95.
+C4_LEARN = dict(learn_contribution=10.0, learn_prune_confidence=0.95)
+
+
+def run_c4(local, learn_iters, learn=None, plain=True):
     """Learned densification on the clustered scene in config-3 precision: the network
     learns online from plain runs on scene seeds 2-5 (the densification window of each),
     then plain and learned densification train scene seed 6 for the same number of steps."""
+    learn_cfg = dict(C4_LEARN if learn is None else learn)
     import torch
     from splatrs_b200 import gpu as G
     from splatrs_b200 import scenes
@@ -399,10 +406,10 @@ def run_c4(local, learn_iters):
         init = G.planes_to_params(ctx, ip, n0, n0).cpu().numpy()
         return init, views, scenes.scene_extent(s["cams"])
 
-    theta, learn = None, []
+    theta, learn_log = None, []
     for seed in (2, 3, 4, 5):
         init, views, ext = setup(seed)
-        t = G.Trainer(ctx, init, ext, views, **dict(C3_TRAIN, learned_densify=1))
+        t = G.Trainer(ctx, init, ext, views, **dict(C3_TRAIN, learned_densify=1, **learn_cfg))
         if theta is not None:
             t.set_mlp(theta)
         tw = time.perf_counter()
@@ -410,7 +417,7 @@ def run_c4(local, learn_iters):
         torch.cuda.synchronize(local)
         st = t.mlp_stats()
         theta = t.get_mlp()
-        learn.append({"seed": seed, "steps": learn_iters, "wall_s": round(time.perf_counter() - tw, 2),
+        learn_log.append({"seed": seed, "steps": learn_iters, "wall_s": round(time.perf_counter() - tw, 2),
                       "densifications": st["events"], "records": st["records"],
                       "labels_keep_densify_prune": [st["label_keep"], st["label_densify"], st["label_prune"]],
                       "heldout_accuracy_network": round(st["heldout_net"] / max(st["heldout_records"], 1), 4),
@@ -418,8 +425,8 @@ def run_c4(local, learn_iters):
         t.close()
     init, views, ext = setup(6)
     ev = {}
-    for name, mode in (("plain", 0), ("learned", 2)):
-        t = G.Trainer(ctx, init, ext, views, **dict(C3_TRAIN, learned_densify=mode))
+    for name, mode in ((("plain", 0),) if plain else ()) + (("learned", 2),):
+        t = G.Trainer(ctx, init, ext, views, **dict(C3_TRAIN, learned_densify=mode, **(learn_cfg if mode else {})))
         if mode == 2:
             t.set_mlp(theta)
         torch.cuda.synchronize(local)
@@ -432,7 +439,7 @@ def run_c4(local, learn_iters):
                     "ssim_train_views": round(mean_ssim(t, views), 4), "gaussians": t.count}
         t.close()
     ctx.close()
-    return {"learn": learn, "seed6": ev}
+    return {"labels": learn_cfg, "learn": learn_log, "seed6": ev}
 
 
 def mean_ssim(trainer, views):

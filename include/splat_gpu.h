@@ -146,6 +146,15 @@ typedef struct splat_train_config {
    * and again whenever the Gaussian count has moved by more than a quarter since, and
    * keeps the fastest on the context; 0 uses the context's configuration as it is. */
   int32_t autotune;
+  /* Not in the reference; learned densification only. learn_contribution > 0: hindsight
+   * labels also judge contribution, each Gaussian's blending weight sum(alpha T) over the
+   * pixels of every view between two densifications (pixel units): a kept Gaussian whose
+   * descendants contributed less is labelled prune, and a clone/split descendant counts as
+   * useful only from that contribution on. 0: labels from opacity alone.
+   * learn_prune_confidence > 0: the prune probability at which applying prunes (default
+   * 0.9). */
+  float learn_contribution;
+  float learn_prune_confidence;
 } splat_train_config;
 
 typedef struct splat_ctx splat_ctx;

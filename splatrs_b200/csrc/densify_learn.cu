@@ -3,14 +3,16 @@
 //
 //   densify_features: 16 features per Gaussian at a densification: mean and max
 //     view-space gradient, visibility count, log-scales, opacity, largest screen radius,
-//     SH-DC energy, age, size against the rule's clone/split limit, and five statistics of
-//     its neighbourhood (a hashed grid of cells two rule-limits wide: count, mean opacity,
-//     mean and max gradient, mean log-size).
+//     SH-DC energy, age, size against the rule's clone/split limit, contribution (blending
+//     weight per visible view over the window), and four statistics of its neighbourhood
+//     (a hashed grid of cells two rule-limits wide: count, mean opacity, mean gradient,
+//     mean log-size).
 //   outcome counts / hindsight labels: every Gaussian carries the index of the record it
 //     descends from at the previous densification. At the next one, a record whose
-//     clone/split left fewer than two descendants with opacity >= tau is relabelled keep
-//     (the edit was wasted), a kept record with no descendant left is relabelled prune,
-//     and a pruned one stays prune.
+//     clone/split left fewer than two useful descendants (opacity >= tau and, when tau_c
+//     is set, a window contribution >= tau_c) is relabelled keep (the edit was wasted), a
+//     kept record with no descendant left, or whose descendants contributed less than
+//     tau_c in all, is relabelled prune, and a pruned one stays prune.
 #include "common.cuh"
 #include "kernels.cuh"
 
@@ -26,12 +28,11 @@ __device__ __forceinline__ uint32_t cell_hash(float3 m, float inv_cell, uint32_t
   return ((uint32_t)ix * 73856093u ^ (uint32_t)iy * 19349663u ^ (uint32_t)iz * 83492791u) & mask;
 }
 
-// Grid cell per entry: count, sum opacity, sum gradient, sum log max-scale, max gradient.
+// Grid cell per entry: count, sum opacity, sum gradient, sum log max-scale.
 __global__ void grid_accumulate_kernel(const float4* __restrict__ p, int64_t n, int64_t cap,
                                        const float* __restrict__ accum, const uint32_t* __restrict__ denom,
                                        float inv_cell, uint32_t mask, uint32_t* __restrict__ cnt,
-                                       float* __restrict__ sop, float* __restrict__ sgr, float* __restrict__ sls,
-                                       uint32_t* __restrict__ mgr) {
+                                       float* __restrict__ sop, float* __restrict__ sgr, float* __restrict__ sls) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const float4 p0 = p[i], p2 = p[2 * cap + i];
@@ -41,16 +42,15 @@ __global__ void grid_accumulate_kernel(const float4* __restrict__ p, int64_t n, 
   atomicAdd(&sop[h], sigmoidf_(p0.w));
   atomicAdd(&sgr[h], gr);
   atomicAdd(&sls[h], fmaxf(p2.x, fmaxf(p2.y, p2.z)));
-  atomicMax(&mgr[h], __float_as_uint(gr));  // non-negative floats order as their bits
 }
 
 __global__ void features_kernel(const float4* __restrict__ p, int64_t n, int64_t cap,
                                 const float* __restrict__ accum, const uint32_t* __restrict__ denom,
                                 const uint32_t* __restrict__ maxr, const float* __restrict__ maxg,
-                                const uint32_t* __restrict__ birth, uint32_t now, float size_limit, float inv_cell,
-                                uint32_t mask, const uint32_t* __restrict__ cnt, const float* __restrict__ sop,
-                                const float* __restrict__ sgr, const float* __restrict__ sls,
-                                const uint32_t* __restrict__ mgr, float* __restrict__ x) {
+                                const float* __restrict__ contrib, const uint32_t* __restrict__ birth, uint32_t now,
+                                float size_limit, float inv_cell, uint32_t mask, const uint32_t* __restrict__ cnt,
+                                const float* __restrict__ sop, const float* __restrict__ sgr,
+                                const float* __restrict__ sls, float* __restrict__ x) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const float4 p0 = p[i], p2 = p[2 * cap + i], p3 = p[3 * cap + i];
@@ -74,25 +74,29 @@ __global__ void features_kernel(const float4* __restrict__ p, int64_t n, int64_t
   f[12] = sop[h] / c;
   f[13] = sgr[h] / c * 1e3f;
   f[14] = sls[h] / c + 4.0f;
-  f[15] = __uint_as_float(mgr[h]) * 1e3f;
+  f[15] = contrib ? log1pf(contrib[i] / (float)max(denom[i], 1u)) : 0.0f;
 #pragma unroll
   for (int k = 0; k < kF; k++) x[i * kF + k] = f[k];
 }
 
 __global__ void outcome_counts_kernel(const float4* __restrict__ p, int64_t n, const uint32_t* __restrict__ origin,
-                                      int64_t n_prev, float tau_logit, uint32_t* __restrict__ alive,
-                                      uint32_t* __restrict__ useful) {
+                                      int64_t n_prev, float tau_logit, const float* __restrict__ contrib, float tau_c,
+                                      uint32_t* __restrict__ alive, uint32_t* __restrict__ useful,
+                                      float* __restrict__ csum) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const uint32_t r = origin[i];
   if ((int64_t)r >= n_prev) return;
+  const float cb = contrib ? contrib[i] : 0.0f;
   atomicAdd(&alive[r], 1u);
-  if (p[i].w >= tau_logit) atomicAdd(&useful[r], 1u);
+  atomicAdd(&csum[r], cb);
+  if (p[i].w >= tau_logit && !(tau_c > 0.0f && cb < tau_c)) atomicAdd(&useful[r], 1u);
 }
 
 __global__ void hindsight_labels_kernel(const uint32_t* __restrict__ action, const uint32_t* __restrict__ alive,
-                                        const uint32_t* __restrict__ useful, int64_t n_prev,
-                                        int32_t* __restrict__ y, unsigned long long* __restrict__ counts) {
+                                        const uint32_t* __restrict__ useful, const float* __restrict__ csum,
+                                        float tau_c, int64_t n_prev, int32_t* __restrict__ y,
+                                        unsigned long long* __restrict__ counts) {
   const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= n_prev) return;
   const uint32_t a = action[r];
@@ -100,7 +104,7 @@ __global__ void hindsight_labels_kernel(const uint32_t* __restrict__ action, con
   if (a == 1u)
     lab = useful[r] >= 2u ? 1 : 0;
   else if (a == 0u)
-    lab = alive[r] == 0u ? 2 : 0;
+    lab = (alive[r] == 0u || (tau_c > 0.0f && csum[r] < tau_c)) ? 2 : 0;
   else
     lab = 2;
   y[r] = lab;
@@ -154,12 +158,12 @@ __global__ void gather_training_kernel(const float* __restrict__ x, const int32_
 size_t densify_features_scratch_bytes(int64_t n) {
   uint32_t t = 1024;
   while ((int64_t)t < 2 * n && t < (1u << 24)) t <<= 1;
-  return (size_t)t * 5 * 4;
+  return (size_t)t * 4 * 4;
 }
 
 Status launch_densify_features(Ctx* c, const float* params, int64_t n, int64_t cap, const float* accum,
-                               const uint32_t* denom, const uint32_t* maxr, const float* maxg, const uint32_t* birth,
-                               uint32_t now, float size_limit, void* scratch, float* x_out) {
+                               const uint32_t* denom, const uint32_t* maxr, const float* maxg, const float* contrib,
+                               const uint32_t* birth, uint32_t now, float size_limit, void* scratch, float* x_out) {
   if (n == 0) return Status::ok();
   uint32_t t = 1024;
   while ((int64_t)t < 2 * n && t < (1u << 24)) t <<= 1;
@@ -167,32 +171,34 @@ Status launch_densify_features(Ctx* c, const float* params, int64_t n, int64_t c
   float* sop = reinterpret_cast<float*>(cnt + t);
   float* sgr = sop + t;
   float* sls = sgr + t;
-  uint32_t* mgr = reinterpret_cast<uint32_t*>(sls + t);
-  SPLAT_TRY(launch_fill_u32(c, scratch, (size_t)t * 5, 0u));
+  SPLAT_TRY(launch_fill_u32(c, scratch, (size_t)t * 4, 0u));
   const float inv_cell = 1.0f / (2.0f * size_limit);
   const float4* p = reinterpret_cast<const float4*>(params);
   grid_accumulate_kernel<<<ceil_div(n, 256), 256, 0, c->stream>>>(p, n, cap, accum, denom, inv_cell, t - 1, cnt, sop,
-                                                                   sgr, sls, mgr);
-  features_kernel<<<ceil_div(n, 256), 256, 0, c->stream>>>(p, n, cap, accum, denom, maxr, maxg, birth, now,
-                                                            size_limit, inv_cell, t - 1, cnt, sop, sgr, sls, mgr,
-                                                            x_out);
+                                                                   sgr, sls);
+  features_kernel<<<ceil_div(n, 256), 256, 0, c->stream>>>(p, n, cap, accum, denom, maxr, maxg, contrib, birth, now,
+                                                            size_limit, inv_cell, t - 1, cnt, sop, sgr, sls, x_out);
   c->launches.count += 2;
   SPLAT_LAUNCHED("densify features");
   return Status::ok();
 }
 
 Status launch_hindsight_labels(Ctx* c, const float* params, int64_t n, const uint32_t* origin, int64_t n_prev,
-                               const uint32_t* action, float tau, uint32_t* alive, uint32_t* useful, int32_t* y,
+                               const uint32_t* action, float tau, const float* contrib, float tau_c,
+                               uint32_t* alive, uint32_t* useful, float* csum, int32_t* y,
                                unsigned long long* counts) {
   SPLAT_TRY(launch_fill_u32(c, alive, (size_t)n_prev, 0u));
   SPLAT_TRY(launch_fill_u32(c, useful, (size_t)n_prev, 0u));
+  SPLAT_TRY(launch_fill_u32(c, csum, (size_t)n_prev, 0u));
   SPLAT_TRY(launch_fill_u32(c, counts, 6, 0u));
   const float tau_logit = logf(tau / (1.0f - tau));
   if (n > 0)
     outcome_counts_kernel<<<ceil_div(n, 256), 256, 0, c->stream>>>(reinterpret_cast<const float4*>(params), n, origin,
-                                                                    n_prev, tau_logit, alive, useful);
+                                                                    n_prev, tau_logit, contrib, tau_c, alive, useful,
+                                                                    csum);
   if (n_prev > 0)
-    hindsight_labels_kernel<<<ceil_div(n_prev, 256), 256, 0, c->stream>>>(action, alive, useful, n_prev, y, counts);
+    hindsight_labels_kernel<<<ceil_div(n_prev, 256), 256, 0, c->stream>>>(action, alive, useful, csum, tau_c, n_prev,
+                                                                           y, counts);
   c->launches.count += 2;
   SPLAT_LAUNCHED("hindsight labels");
   return Status::ok();

@@ -64,6 +64,9 @@ Status launch_project_bwd_adam(Ctx* c, float* planes, float* m, float* v, int64_
                                const float* pgrad, void* stats, int absgrad, uint64_t step, const splat_lr& lr,
                                const uint32_t* skip = nullptr, const StepParams* sp = nullptr,
                                void* bf16 = nullptr, bool stats_maxg = false);
+// With stats_maxg the statistics are the trainer's five arrays of cap entries: accum,
+// denom, max radius, max gradient and contribution (each view adds the entry's blending
+// weight sum(alpha T) from plane 2's w of the screen-space gradient).
 
 // A batch's projection backward (records view-major, screen-space gradient planes with
 // stride pcap) summed over the views that see each Gaussian, then one Adam step with the
@@ -107,15 +110,19 @@ Status launch_mlp_grad(Ctx* c, const float* x, const int32_t* y, const float* w,
 Status launch_mlp_adam(Ctx* c, float* theta, const float* grad, float* m, float* v, uint64_t step, float lr);
 
 // Learned densification (densify_learn.cu): features of every Gaussian (n x 16) from its
-// parameters, densification statistics (4 arrays: accum, denom, max radius, max
-// gradient) and birth iteration; hindsight labels of the previous densification's records
-// from the origin of every current Gaussian; a strided, class-weighted training subset.
+// parameters, densification statistics (accum, denom, max radius, max gradient,
+// contribution) and birth iteration; hindsight labels of the previous densification's
+// records from the origin of every current Gaussian (a descendant is useful when its
+// opacity is at least tau and, with tau_c > 0, its contribution over the window at least
+// tau_c; a kept record whose descendants contributed less than tau_c in all is
+// relabelled prune); a strided, class-weighted training subset.
 size_t densify_features_scratch_bytes(int64_t n);
 Status launch_densify_features(Ctx* c, const float* params, int64_t n, int64_t cap, const float* accum,
-                               const uint32_t* denom, const uint32_t* maxr, const float* maxg, const uint32_t* birth,
-                               uint32_t now, float size_limit, void* scratch, float* x_out);
+                               const uint32_t* denom, const uint32_t* maxr, const float* maxg, const float* contrib,
+                               const uint32_t* birth, uint32_t now, float size_limit, void* scratch, float* x_out);
 Status launch_hindsight_labels(Ctx* c, const float* params, int64_t n, const uint32_t* origin, int64_t n_prev,
-                               const uint32_t* action, float tau, uint32_t* alive, uint32_t* useful, int32_t* y,
+                               const uint32_t* action, float tau, const float* contrib, float tau_c,
+                               uint32_t* alive, uint32_t* useful, float* csum, int32_t* y,
                                unsigned long long* counts);
 Status launch_label_accuracy(Ctx* c, const float* prob, const uint32_t* action, const int32_t* y, int64_t n_prev,
                              unsigned long long* acc);

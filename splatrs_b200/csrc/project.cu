@@ -822,7 +822,10 @@ __global__ void __launch_bounds__(128) project_bwd_kernel(const float4* __restri
       stat_accum[i] += gn;
       stat_denom[i] += 1u;
       stat_maxr[i] = max(stat_maxr[i], radius);
-      if (stat_maxg) stat_maxg[i] = fmaxf(stat_maxg[i], gn);
+      if (stat_maxg) {
+        stat_maxg[i] = fmaxf(stat_maxg[i], gn);
+        stat_maxg[cap + i] += g2.w;  // contribution: the view's blending weight sum (alpha T)
+      }
     }
   }
 
@@ -1082,7 +1085,10 @@ __global__ void __launch_bounds__(kBatchBwdThreads) project_bwd_batch_adam_kerne
       stat_accum[i] += gn;
       stat_denom[i] += 1u;
       stat_maxr[i] = max(stat_maxr[i], radius);
-      if (stat_maxg) stat_maxg[i] = fmaxf(stat_maxg[i], gn);
+      if (stat_maxg) {
+        stat_maxg[i] = fmaxf(stat_maxg[i], gn);
+        stat_maxg[cap + i] += g2.w;  // contribution: the view's blending weight sum (alpha T)
+      }
     }
     ParamGrad pgr;
     proj_grad_one<DEG>(g, cam, opts, g0, g1, g2, pgr);

@@ -325,12 +325,14 @@ __global__ void __launch_bounds__(TW * TH, 1536 / (TW * TH)) raster_fwd_kernel(
 // (13 shuffles leave each slot's warp total in a pair of lanes), across the block's warps
 // with one shared-memory atomic instruction per warp, and across tiles with three float4
 // vector atomics per entry.
-constexpr int kSlots = 12;  // 11 used, padded for float4 flushes
+// Slots per entry: ProjGrad (9), the AbsGS accumulators (2) and the entry's blending weight
+// sum(alpha * T) over the tile's pixels (the trainer's contribution statistic).
+constexpr int kSlots = 12;
 
-// v[0..11] per lane in (v[11] unused); out, the warp total of slot
-// 6*b4 + 3*b3 + 2*b2 + b1 (b_i = bit i of the lane) when 2*b2 + b1 < 3, in both lanes of a
-// pair. Each exchange stage keeps the half of the values selected by the lane's bit and
-// adds the partner's copy of that half: 6 + 3 + 2 + 1 + 1 = 13 shuffles for 11 slots.
+// v[0..11] per lane in; out, the warp total of slot 6*b4 + 3*b3 + 2*b2 + b1 (b_i = bit i of
+// the lane) when 2*b2 + b1 < 3, in both lanes of a pair. Each exchange stage keeps the half
+// of the values selected by the lane's bit and adds the partner's copy of that half:
+// 6 + 3 + 2 + 1 + 1 = 13 shuffles for 12 slots.
 __device__ __forceinline__ float warp_transpose_reduce12(const float v[12]) {
   const uint32_t lane = threadIdx.x & 31;
   const bool b4 = lane & 16u, b3 = lane & 8u, b2 = lane & 4u, b1 = lane & 2u;
@@ -485,6 +487,7 @@ __global__ void __launch_bounds__(TW * TH) raster_bwd_kernel(
           c[6] = at * d0;
           c[7] = at * d1;
           c[8] = at * d2;
+          c[11] = at;
           lc_r = col_r;
           lc_g = col_g;
           lc_b = col_b;
@@ -513,7 +516,7 @@ __global__ void __launch_bounds__(TW * TH) raster_bwd_kernel(
         const float tot = warp_transpose_reduce12(c);
         const uint32_t local = (lane >> 1) & 3u;
         const uint32_t slot = 6u * ((lane >> 4) & 1u) + 3u * ((lane >> 3) & 1u) + local;
-        if (!(lane & 1u) && local < 3u && slot < 11u) atomicAdd(&acc[kk * kSlots + slot], tot);
+        if (!(lane & 1u) && local < 3u) atomicAdd(&acc[kk * kSlots + slot], tot);
       }
     }
     __syncthreads();
@@ -524,10 +527,10 @@ __global__ void __launch_bounds__(TW * TH) raster_bwd_kernel(
       const size_t g = sg[e];
       const float4 v0 = make_float4(a[0], a[1], a[2], a[3]);
       const float4 v1 = make_float4(a[4], a[5], a[6], a[7]);
-      const float4 v2 = make_float4(a[8], a[9], a[10], 0.0f);
+      const float4 v2 = make_float4(a[8], a[9], a[10], a[11]);
       if (v0.x != 0.0f || v0.y != 0.0f || v0.z != 0.0f || v0.w != 0.0f) atomicAdd(&pgrad[g], v0);
       if (v1.x != 0.0f || v1.y != 0.0f || v1.z != 0.0f || v1.w != 0.0f) atomicAdd(&pgrad[cap + g], v1);
-      if (v2.x != 0.0f || v2.y != 0.0f || v2.z != 0.0f) atomicAdd(&pgrad[2 * cap + g], v2);
+      if (v2.x != 0.0f || v2.y != 0.0f || v2.z != 0.0f || v2.w != 0.0f) atomicAdd(&pgrad[2 * cap + g], v2);
 #pragma unroll
       for (int q = 0; q < kSlots; q++) a[q] = 0.0f;
     }

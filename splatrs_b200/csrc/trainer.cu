@@ -119,7 +119,7 @@ struct splat_trainer {
   // previous densification's records (features, rule action), the network and its Adam
   // state, and what learning did.
   DevBuf birth, birth_next, origin, origin_next, feat, feat_scratch, policy;
-  DevBuf rec_x, rec_action, alive, useful, labels, label_counts, train_x, train_y, train_w;
+  DevBuf rec_x, rec_action, alive, useful, rec_csum, labels, label_counts, train_x, train_y, train_w;
   DevBuf mlp_theta, mlp_m, mlp_v, mlp_grad;
   int64_t rec_n = 0;
   bool rec_valid = false;
@@ -165,7 +165,7 @@ float position_lr(const splat_train_config& c, uint32_t iteration, float extent)
 Status ensure_stats(splat_trainer* t, int64_t cap) {
   if (t->stats_cap == cap) return Status::ok();
   SPLAT_CUDA(cudaStreamSynchronize(t->c->stream));
-  SPLAT_TRY(t->stats.ensure((size_t)cap * 16));  // accum, denom, max radius, max gradient
+  SPLAT_TRY(t->stats.ensure((size_t)cap * 20));  // accum, denom, max radius, max gradient, contribution
   t->stats_cap = cap;
   SPLAT_TRY(launch_fill_u32(t->c, t->stats.ptr, t->stats.bytes / 4, 0u));
   return Status::ok();
@@ -558,11 +558,14 @@ constexpr float kUsefulOpacity = 0.02f;
 Status learn_from_previous(splat_trainer* t) {
   Ctx* c = t->c;
   const int64_t rn = t->rec_n;
-  for (DevBuf* b : {&t->alive, &t->useful, &t->labels}) SPLAT_TRY(b->ensure((size_t)rn * 4));
+  for (DevBuf* b : {&t->alive, &t->useful, &t->rec_csum, &t->labels}) SPLAT_TRY(b->ensure((size_t)rn * 4));
   SPLAT_TRY(t->label_counts.ensure(64));
+  // The window's contribution of every current Gaussian: the fifth statistics array.
+  const float* contrib = t->stats.as<float>() + 4 * t->stats_cap;
   SPLAT_TRY(launch_hindsight_labels(c, t->cur.params.as<float>(), t->n, t->origin.as<uint32_t>(), rn,
-                                    t->rec_action.as<uint32_t>(), kUsefulOpacity, t->alive.as<uint32_t>(),
-                                    t->useful.as<uint32_t>(), t->labels.as<int32_t>(),
+                                    t->rec_action.as<uint32_t>(), kUsefulOpacity, contrib,
+                                    t->cfg.learn_contribution, t->alive.as<uint32_t>(), t->useful.as<uint32_t>(),
+                                    t->rec_csum.as<float>(), t->labels.as<int32_t>(),
                                     t->label_counts.as<unsigned long long>()));
   unsigned long long cnt[3];
   SPLAT_CUDA(cudaMemcpyAsync(cnt, t->label_counts.ptr, 24, cudaMemcpyDeviceToHost, c->stream));
@@ -626,6 +629,7 @@ Status density_control(splat_trainer* t, const IterPlan& p, splat_step_info* inf
     uint32_t* denom = reinterpret_cast<uint32_t*>(accum + t->stats_cap);
     uint32_t* maxr = denom + t->stats_cap;
     float* maxg = reinterpret_cast<float*>(maxr + t->stats_cap);
+    const float* contrib = maxg + t->stats_cap;
     // Learned densification: features of every Gaussian; learning labels the previous
     // records and trains; applying turns the network's probabilities into a policy.
     const bool learn = cfg.learned_densify == 1, apply = cfg.learned_densify == 2;
@@ -634,7 +638,7 @@ Status density_control(splat_trainer* t, const IterPlan& p, splat_step_info* inf
       SPLAT_TRY(ensure_mlp(t));
       SPLAT_TRY(t->feat.ensure((size_t)std::max<int64_t>(n, 1) * 64));
       SPLAT_TRY(t->feat_scratch.ensure(densify_features_scratch_bytes(n)));
-      SPLAT_TRY(launch_densify_features(c, t->cur.params.as<float>(), n, cap, accum, denom, maxr, maxg,
+      SPLAT_TRY(launch_densify_features(c, t->cur.params.as<float>(), n, cap, accum, denom, maxr, maxg, contrib,
                                         t->birth.as<uint32_t>(), p.it, cfg.percent_dense * t->extent,
                                         t->feat_scratch.ptr, t->feat.as<float>()));
     }
@@ -643,6 +647,7 @@ Status density_control(splat_trainer* t, const IterPlan& p, splat_step_info* inf
       SPLAT_TRY(t->policy.ensure((size_t)std::max<int64_t>(n, 1) * 12));
       SPLAT_TRY(mlp_forward_tc_checked(c, t->feat.as<float>(), n, t->mlp_theta.as<float>(), t->policy.as<float>()));
       dp.policy = t->policy.as<float>();
+      if (cfg.learn_prune_confidence > 0.0f) dp.prune_conf = cfg.learn_prune_confidence;
     }
     if (learn) {
       SPLAT_TRY(t->rec_action.ensure((size_t)std::max<int64_t>(n, 1) * 4));
@@ -901,7 +906,8 @@ SPLAT_API int splat_trainer_destroy(splat_trainer* t) {
     t->next.release();
     for (DevBuf* b : {&t->pgrad, &t->stats, &t->pred_grad, &t->loss_out, &t->normals, &t->init, &t->bf16}) b->release();
     for (DevBuf* b : {&t->birth, &t->birth_next, &t->origin, &t->origin_next, &t->feat, &t->feat_scratch, &t->policy,
-                      &t->rec_x, &t->rec_action, &t->alive, &t->useful, &t->labels, &t->label_counts, &t->train_x,
+                      &t->rec_x, &t->rec_action, &t->alive, &t->useful, &t->rec_csum, &t->labels, &t->label_counts,
+                      &t->train_x,
                       &t->train_y, &t->train_w, &t->mlp_theta, &t->mlp_m, &t->mlp_v, &t->mlp_grad})
       b->release();
     t->vb.release();

@@ -249,3 +249,27 @@ def test_trainer_autotune_retunes_as_the_count_grows(ctx, config):
     assert t.count > 1.25 * n0 and info["tunes"] >= 2
     assert p > 25.0
     t.close()
+
+
+def test_blend_weight_statistic_sums_to_coverage(ctx, config):
+    """The backward's fourth value of gradient plane 2 is each Gaussian's blending weight
+    sum(alpha T) over the view's pixels. Per pixel those weights telescope to 1 - T_final,
+    so over the image they sum to sum(1 - final T); they are non-negative, zero for unseen
+    Gaussians, and the same under every tile shape up to summation order."""
+    g, cam, p, bg, img, ft, nc, pairs, dimage, *_ = oracle_case()
+    per = {}
+    for cfg in [(16, 16, 256), (8, 8, 64), (16, 32, 128)]:
+        config(cfg)
+        proj = G.proj_from_reference(ctx, dev(p), *SIZE)
+        b = G.bin(ctx, proj)
+        out = G.rasterize_forward(ctx, proj, b, bg)
+        pg = G.rasterize_backward(ctx, proj, b, bg, out, dev(dimage))
+        w = pg[2, :, 3].double().cpu().numpy()
+        cover = float((1.0 - out.final_t.double()).sum().item())
+        assert (w >= 0).all()
+        assert (w[p[:, 6] == 0] == 0).all()
+        assert abs(w.sum() - cover) <= 1e-4 * cover, (w.sum(), cover)
+        per[cfg] = w
+    ref = per[(16, 16, 256)]
+    for cfg, w in per.items():
+        assert np.abs(w - ref).max() <= 1e-5 * ref.max(), cfg

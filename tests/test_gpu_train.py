@@ -507,3 +507,44 @@ def test_learned_densification_learns_and_falls_back(ctx):
         firsts.append((info["cloned"], info["split"], info["pruned"]))
         t.close()
     assert abs(firsts[0][0] - firsts[1][0]) <= 2 and abs(firsts[0][1] - firsts[1][1]) <= 2
+
+
+def test_learned_densification_contribution_labels_prune(ctx):
+    """With learn_contribution, a kept Gaussian whose descendants blended less than that
+    many pixel-equivalents over the window is labelled prune: learning sees more prune
+    labels than with opacity-only labels, and applying the network it trained removes
+    Gaussians the rule keeps (at a quality cost this 64x48 scene bounds loosely; the quality
+    bar is measured on the config-3 scene)."""
+    ctx_holder[:] = [ctx]
+    cfg = dict(iterations=900, densify=1, densify_from_iter=100, densify_until_iter=800, densification_interval=50,
+               opacity_reset_interval=0, densify_grad_threshold=0.0002, sh_degree=1, sh_degree_interval=300,
+               position_lr_max_steps=900, seed=0)
+    prunes, theta = [], None
+    for tau in (0.0, 2.0):
+        th = None
+        for seed in (2, 3):
+            init, extent, views = _c0_like(seed)
+            t = G.Trainer(ctx, init, extent, views, learned_densify=1, learn_contribution=tau, **cfg)
+            if th is not None:
+                t.set_mlp(th)
+            t.run(900)
+            st = t.mlp_stats()
+            th = t.get_mlp()
+            t.close()
+        prunes.append(st["label_prune"])
+        theta = th
+    assert prunes[1] > prunes[0]
+    init, extent, views = _c0_like(6)
+    res = []
+    for mode in (0, 2):
+        t = G.Trainer(ctx, init, extent, views, learned_densify=mode, learn_contribution=2.0,
+                      learn_prune_confidence=0.95, **cfg)
+        if mode == 2:
+            t.set_mlp(theta)
+        t.run(900)
+        res.append((t.count, _evaluate(t, views)))
+        t.close()
+    print(f"\nprune labels {prunes[0]} -> {prunes[1]}; seed 6: plain {res[0][0]} Gaussians {res[0][1]:.2f} dB, "
+          f"learned {res[1][0]} Gaussians {res[1][1]:.2f} dB")
+    assert res[1][0] < res[0][0]
+    assert res[1][1] > res[0][1] - 1.5
