@@ -44,7 +44,8 @@ def parse():
     ap.add_argument("--cpu-steps", type=int, default=3, help="steps of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--raster", default="auto",
-                    help="compositing configuration: 'auto' (autotune) or TWxTHxCHUNK, e.g. 16x16x256")
+                    help="compositing configuration: 'auto' (autotune) or TWxTHxCHUNK[/PIXELS_PER_THREAD], "
+                         "e.g. 16x16x256/2")
     ap.add_argument("--no-train", action="store_true", help="skip the config-0 training run")
     ap.add_argument("--train-c2", action="store_true",
                     help="also run plain training on the clustered 500k-Gaussian multi-view scene")
@@ -150,8 +151,8 @@ RASTER_FWD_BYTES_PER_PIXEL = 20    # image (12) + final T (4) + n_contrib (4) wr
 RASTER_BWD_BYTES_PER_PIXEL = 20    # dL/dpix (12) + final T (4) + n_contrib (4) read
 RASTER_BYTES_PER_ENTRY = 52        # sorted index (4) + record gather (48)
 # dram__bytes_read.sum + dram__bytes_write.sum per launch, ncu, default workload.
-NCU_DRAM_BYTES_1M = {("raster_bwd", 16, 16, 256): int((197.05 + 17.84) * 1e6),
-                     ("raster_fwd", 16, 16, 256): int((82.84 + 20.76) * 1e6)}
+NCU_DRAM_BYTES_1M = {("raster_bwd", 16, 16, 256, 1): int((197.05 + 17.84) * 1e6),
+                     ("raster_fwd", 16, 16, 256, 1): int((82.84 + 20.76) * 1e6)}
 RASTER_FWD_FLOP_PER_PAIR = 20
 RASTER_BWD_FLOP_PER_PAIR = 50
 
@@ -183,9 +184,9 @@ def run_ours(args, rank, world, local):
     if args.raster == "auto":
         tuning = ctx.autotune_render(planes, n, n, cam, opts, bg, dimage, reps=3)
         tuning = {"picked": list(tuning["picked"]),
-                  "ms_per_pass": {f"{a}x{b}x{c}": round(v, 4) for (a, b, c), v in tuning["ms"].items()}}
+                  "ms_per_pass": {f"{a}x{b}x{c}/{d}": round(v, 4) for (a, b, c, d), v in tuning["ms"].items()}}
     else:
-        ctx.raster_config = tuple(int(v) for v in args.raster.split("x"))
+        ctx.raster_config = tuple(int(v) for v in args.raster.replace("/", "x").split("x"))
     raster = ctx.raster_config
 
     # Stage-level step with events between stages.
@@ -333,7 +334,7 @@ def run_ours(args, rank, world, local):
         "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded; config-1 distributions)",
         "config": {"workload": WORKLOAD, "gaussians": n, "width": WIDTH, "height": HEIGHT,
-                   "tile": [raster[0], raster[1]], "chunk": raster[2],
+                   "tile": [raster[0], raster[1]], "chunk": raster[2], "bwd_pixels_per_thread": raster[3],
                    "raster": "autotuned" if tuning else "fixed",
                    "l2": "inputs larger than L2 (240 MB parameter planes), no flush", "parallelism": f"replicas x{world}"},
         "autotune": tuning,
@@ -484,7 +485,7 @@ def run_train_gpu(local, s, cfg, iterations):
     if cfg.get("autotune"):
         tu = t.tuning()
         out["autotune"] = {"tunes": tu["tunes"], "picked": list(tu["picked"]),
-                           "ms_per_pass": {f"{a}x{b}x{c}": round(v, 4) for (a, b, c), v in tu["ms"].items()}}
+                           "ms_per_pass": {f"{a}x{b}x{c}/{d}": round(v, 4) for (a, b, c, d), v in tu["ms"].items()}}
     t.close()
     ctx.close()
     return out, init, views, extent

@@ -330,25 +330,27 @@ SPLAT_API int splat_mlp_adam(splat_ctx* ctx, float* theta_dev, const float* grad
                              uint64_t step, float lr);
 
 /* ----------------------------------------------------------------------------------------
- * Compositing configuration (not in the reference): tile shape and shared-memory chunk
- * depth of the compositing kernels, held by the context and used by every later launch
+ * Compositing configuration (not in the reference): tile shape, shared-memory chunk depth
+ * and the backward's pixels per thread, held by the context and used by every later launch
  * (projection, binning and compositing must run under the same one). 16x16 tiles are the
  * reference's and give its tile lists; 8x8 and 16x32 give other lists but identical
  * images, final transmittances and, up to summation order, gradients (each entry's pixel
  * rectangle is first narrowed to its 16-pixel tile rectangle). Chunk depth: entries
- * staged in shared memory per round, 32, 64, 128 or 256. Default 16x16, 256.
- *   splat_raster_candidates: writes the 12 supported (tile_w, tile_h, chunk) triples to
- *     out (36 values) and returns 12.
- *   splat_set_raster_config: SPLAT_ERR_INVALID for an unsupported triple.
+ * staged in shared memory per round, 32, 64, 128 or 256. Pixels per thread of the
+ * backward: 1 or 2 (a warp then covers 8x8 pixels). Default 16x16, 256, 1.
+ *   splat_raster_candidates: writes the 24 supported (tile_w, tile_h, chunk,
+ *     pixels_per_thread) quadruples to out (96 values) and returns 24.
+ *   splat_set_raster_config: SPLAT_ERR_INVALID for an unsupported quadruple.
  *   splat_autotune_render: times projection + binning + forward + backward compositing of
  *     one view (dimage_dev: dL/dimage, H*W*3) under every candidate, `reps` timed passes
  *     each after an untimed one, sets the fastest on the context and writes the mean
- *     milliseconds per pass of every candidate to ms_out (12) and the pick to picked (3).
+ *     milliseconds per pass of every candidate to ms_out (24) and the pick to picked (4).
  *     Synchronises; changes no caller buffer.
  * -------------------------------------------------------------------------------------- */
 SPLAT_API int32_t splat_raster_candidates(uint32_t* out);
-SPLAT_API int splat_set_raster_config(splat_ctx* ctx, uint32_t tile_w, uint32_t tile_h, uint32_t chunk);
-SPLAT_API int splat_get_raster_config(splat_ctx* ctx, uint32_t* out3);
+SPLAT_API int splat_set_raster_config(splat_ctx* ctx, uint32_t tile_w, uint32_t tile_h, uint32_t chunk,
+                                      uint32_t pixels_per_thread);
+SPLAT_API int splat_get_raster_config(splat_ctx* ctx, uint32_t* out4);
 SPLAT_API int splat_autotune_render(splat_ctx* ctx, const float* planes_dev, int64_t n, int64_t cap,
                                     const splat_camera* cam, const splat_proj_opts* opts, const float* background,
                                     const float* dimage_dev, int32_t reps, float* ms_out, uint32_t* picked);
@@ -506,8 +508,8 @@ SPLAT_API int splat_trainer_get_mlp(splat_trainer* t, float* theta_host);
 SPLAT_API int splat_trainer_set_mlp(splat_trainer* t, const float* theta_host);
 SPLAT_API int splat_trainer_mlp_stats(const splat_trainer* t, uint64_t out[9]);
 /* Autotuning (splat_train_config.autotune): the last tuning's milliseconds per render pass
- * of every candidate (ms_out, 12, in splat_raster_candidates order; 0 before any), the
- * configuration in use (picked, 3) and how many tunings ran. Any pointer may be NULL. */
+ * of every candidate (ms_out, 24, in splat_raster_candidates order; 0 before any), the
+ * configuration in use (picked, 4) and how many tunings ran. Any pointer may be NULL. */
 SPLAT_API int splat_trainer_tuning(const splat_trainer* t, float* ms_out, uint32_t* picked, uint32_t* tunes);
 SPLAT_API int32_t splat_trainer_sh_degree(const splat_trainer* t);
 SPLAT_API uint32_t splat_trainer_iteration(const splat_trainer* t);

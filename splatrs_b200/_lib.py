@@ -160,7 +160,7 @@ def _declare(L):
         "splat_mlp_grad": ([vp, vp, vp, vp, i64, C.c_float, vp, vp], C.c_int),
         "splat_mlp_adam": ([vp, vp, vp, vp, vp, C.c_uint64, C.c_float], C.c_int),
         "splat_raster_candidates": ([P(C.c_uint32)], i32),
-        "splat_set_raster_config": ([vp, C.c_uint32, C.c_uint32, C.c_uint32], C.c_int),
+        "splat_set_raster_config": ([vp, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32], C.c_int),
         "splat_get_raster_config": ([vp, P(C.c_uint32)], C.c_int),
         "splat_autotune_render": ([vp, vp, i64, i64, vp, vp, P(C.c_float), vp, i32, P(C.c_float), P(C.c_uint32)],
                                   C.c_int),

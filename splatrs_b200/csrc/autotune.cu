@@ -1,6 +1,7 @@
 // Autotuning of the compositing configuration (not in the reference): tile shape
-// {8x8, 16x16, 16x32} x shared-memory chunk depth {32, 64, 128, 256}, timed on the
-// caller's own workload with CUDA events and kept on the context.
+// {8x8, 16x16, 16x32} x shared-memory chunk depth {32, 64, 128, 256} x the backward's
+// pixels per thread {1, 2}, timed on the caller's own workload with CUDA events and kept on
+// the context.
 #include <cmath>
 #include <functional>
 
@@ -11,8 +12,10 @@
 namespace splat {
 
 const RasterConfig kRasterCandidateList[kRasterCandidates] = {
-    {16, 16, 256}, {16, 16, 128}, {16, 16, 64}, {16, 16, 32}, {8, 8, 256},  {8, 8, 128},
-    {8, 8, 64},    {8, 8, 32},    {16, 32, 256}, {16, 32, 128}, {16, 32, 64}, {16, 32, 32}};
+    {16, 16, 256, 1}, {16, 16, 128, 1}, {16, 16, 64, 1}, {16, 16, 32, 1}, {8, 8, 256, 1},  {8, 8, 128, 1},
+    {8, 8, 64, 1},    {8, 8, 32, 1},    {16, 32, 256, 1}, {16, 32, 128, 1}, {16, 32, 64, 1}, {16, 32, 32, 1},
+    {16, 16, 256, 2}, {16, 16, 128, 2}, {16, 16, 64, 2}, {16, 16, 32, 2}, {8, 8, 256, 2},  {8, 8, 128, 2},
+    {8, 8, 64, 2},    {8, 8, 32, 2},    {16, 32, 256, 2}, {16, 32, 128, 2}, {16, 32, 64, 2}, {16, 32, 32, 2}};
 
 Status tune_raster(Ctx* c, const std::function<Status(bool)>& pass, int reps, float ms[kRasterCandidates]) {
   cudaEvent_t ev[2] = {nullptr, nullptr};

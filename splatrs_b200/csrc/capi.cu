@@ -300,28 +300,33 @@ SPLAT_API int splat_bin_sort(splat_ctx* ctx, const float* proj_dev, const uint32
 SPLAT_API int32_t splat_raster_candidates(uint32_t* out) {
   if (out)
     for (int k = 0; k < kRasterCandidates; k++) {
-      out[3 * k] = kRasterCandidateList[k].tile_w;
-      out[3 * k + 1] = kRasterCandidateList[k].tile_h;
-      out[3 * k + 2] = kRasterCandidateList[k].chunk;
+      out[4 * k] = kRasterCandidateList[k].tile_w;
+      out[4 * k + 1] = kRasterCandidateList[k].tile_h;
+      out[4 * k + 2] = kRasterCandidateList[k].chunk;
+      out[4 * k + 3] = kRasterCandidateList[k].ppl;
     }
   return kRasterCandidates;
 }
 
-SPLAT_API int splat_set_raster_config(splat_ctx* ctx, uint32_t tile_w, uint32_t tile_h, uint32_t chunk) {
+SPLAT_API int splat_set_raster_config(splat_ctx* ctx, uint32_t tile_w, uint32_t tile_h, uint32_t chunk,
+                                      uint32_t pixels_per_thread) {
   if (!ctx) return SPLAT_ERR_INVALID;
-  if (!RasterConfig::supported(tile_w, tile_h, chunk))
-    return invalid(ctx, "splat_set_raster_config: tiles 8x8, 16x16 or 16x32 and chunk depth 32, 64, 128 or 256");
+  if (!RasterConfig::supported(tile_w, tile_h, chunk, pixels_per_thread))
+    return invalid(ctx, "splat_set_raster_config: tiles 8x8, 16x16 or 16x32, chunk depth 32, 64, 128 or 256 and 1 "
+                        "or 2 pixels per thread");
   ctx->c.raster.tile_w = tile_w;
   ctx->c.raster.tile_h = tile_h;
   ctx->c.raster.chunk = chunk;
+  ctx->c.raster.ppl = pixels_per_thread;
   return SPLAT_OK;
 }
 
-SPLAT_API int splat_get_raster_config(splat_ctx* ctx, uint32_t* out3) {
-  if (!ctx || !out3) return SPLAT_ERR_INVALID;
-  out3[0] = ctx->c.raster.tile_w;
-  out3[1] = ctx->c.raster.tile_h;
-  out3[2] = ctx->c.raster.chunk;
+SPLAT_API int splat_get_raster_config(splat_ctx* ctx, uint32_t* out4) {
+  if (!ctx || !out4) return SPLAT_ERR_INVALID;
+  out4[0] = ctx->c.raster.tile_w;
+  out4[1] = ctx->c.raster.tile_h;
+  out4[2] = ctx->c.raster.chunk;
+  out4[3] = ctx->c.raster.ppl;
   return SPLAT_OK;
 }
 

@@ -65,24 +65,26 @@ struct LaunchCounter {
   uint64_t count = 0;
 };
 
-// Compositing configuration: tile shape in pixels and shared-memory chunk depth (entries
-// staged per round). 16x16 is the reference's tile and binning; 8x8 and 16x32 composite the
+// Compositing configuration: tile shape in pixels, shared-memory chunk depth (entries
+// staged per round) and the backward's pixels per thread. 16x16 is the reference's tile and binning; 8x8 and 16x32 composite the
 // same entries per pixel in the same order (the projection narrows each entry's pixel
 // rectangle to its 16-pixel tile rectangle first), so images match the 16x16 path.
 struct RasterConfig {
   uint32_t tile_w = kTile, tile_h = kTile, chunk = 256;
+  uint32_t ppl = 1;  // pixels per thread of the compositing backward (1 or 2)
   bool operator==(const RasterConfig& o) const {
-    return tile_w == o.tile_w && tile_h == o.tile_h && chunk == o.chunk;
+    return tile_w == o.tile_w && tile_h == o.tile_h && chunk == o.chunk && ppl == o.ppl;
   }
   bool operator!=(const RasterConfig& o) const { return !(*this == o); }
   bool reference_tiles() const { return tile_w == kTile && tile_h == kTile; }
   uint32_t tiles_x(uint32_t width) const { return (width + tile_w - 1) / tile_w; }
   uint32_t tiles_y(uint32_t height) const { return (height + tile_h - 1) / tile_h; }
   uint32_t tiles(uint32_t width, uint32_t height) const { return tiles_x(width) * tiles_y(height); }
-  // Tile shapes {8x8, 16x16, 16x32} x chunk depths {32, 64, 128, 256}.
-  static bool supported(uint32_t w, uint32_t h, uint32_t chunk) {
+  // Tile shapes {8x8, 16x16, 16x32} x chunk depths {32, 64, 128, 256} x backward pixels
+  // per thread {1, 2}.
+  static bool supported(uint32_t w, uint32_t h, uint32_t chunk, uint32_t ppl) {
     const bool shape = (w == 8 && h == 8) || (w == 16 && h == 16) || (w == 16 && h == 32);
-    return shape && (chunk == 32 || chunk == 64 || chunk == 128 || chunk == 256);
+    return shape && (chunk == 32 || chunk == 64 || chunk == 128 || chunk == 256) && (ppl == 1 || ppl == 2);
   }
 };
 // Most tiles any supported shape gives an image (8x8): sizes per-tile buffers for all.

@@ -146,8 +146,9 @@ Status launch_bin_sort(Ctx* c, const float* proj, const uint32_t* entry_offset, 
                        const uint32_t* depth_range_dev, uint32_t depth_min, uint32_t depth_max, uint32_t width,
                        uint32_t height, uint32_t* gauss_out, uint64_t* keys_out, uint32_t* ranges);
 
-// The supported compositing configurations (tile shapes x chunk depths).
-constexpr int kRasterCandidates = 12;
+// The supported compositing configurations (tile shapes x chunk depths x backward pixels
+// per thread).
+constexpr int kRasterCandidates = 24;
 extern const RasterConfig kRasterCandidateList[kRasterCandidates];
 // Times pass() under every candidate configuration: pass(true) once, untimed (it may
 // synchronise, size buffers and redo work), then pass(false) `reps` times between two

@@ -147,8 +147,9 @@ __device__ __forceinline__ typename TileGeo<TW, TH>::Mask tile_rect_masks(uint32
 }
 
 // Bit w of the result is set when the pixel rectangle (x0|x1<<16, y0|y1<<16, absolute
-// pixels) overlaps warp w's 8x4 sub-block of the tile whose top-left pixel is (ox, oy).
-template <int TW, int TH>
+// pixels) overlaps warp w's 8 x SBH sub-block of the tile whose top-left pixel is (ox, oy)
+// (warps row by row, TW / 8 across).
+template <int TW, int TH, int SBH = 4>
 __device__ __forceinline__ uint32_t subblock_mask(uint32_t rx, uint32_t ry, uint32_t ox, uint32_t oy) {
   constexpr int WX = TileGeo<TW, TH>::kWarpsX;
   const uint32_t x0 = rx & 0xffffu, x1 = rx >> 16, y0 = ry & 0xffffu, y1 = ry >> 16;
@@ -157,8 +158,8 @@ __device__ __forceinline__ uint32_t subblock_mask(uint32_t rx, uint32_t ry, uint
   for (int qx = 0; qx < WX; qx++) col[qx] = x0 < ox + 8u * qx + 8u && x1 > ox + 8u * qx;
   uint32_t m = 0;
 #pragma unroll
-  for (uint32_t qy = 0; qy < (uint32_t)(TH / 4); qy++) {
-    const bool row = y0 < oy + 4u * qy + 4u && y1 > oy + 4u * qy;
+  for (uint32_t qy = 0; qy < (uint32_t)(TH / SBH); qy++) {
+    const bool row = y0 < oy + (uint32_t)SBH * qy + (uint32_t)SBH && y1 > oy + (uint32_t)SBH * qy;
 #pragma unroll
     for (int qx = 0; qx < WX; qx++)
       if (row && col[qx]) m |= 1u << (qy * WX + qx);
@@ -371,23 +372,28 @@ __device__ __forceinline__ float rcp_refined(float x) {
   return __fmaf_rn(r, __fmaf_rn(-x, r, 1.0f), r);
 }
 
-template <int TW, int TH, int CH>
-__global__ void __launch_bounds__(TW * TH) raster_bwd_kernel(
+// PPL pixels per thread (1 or 2): a warp owns an 8 x (4 PPL) sub-block, lane L the pixels
+// (L % 8, L / 8 + 4 q) of it for q < PPL. With two, a warp-wide reduction sums the
+// contributions of twice as many pixels. Register budgets: 64 per thread with one pixel
+// (32 warps per SM), 85 with two (24).
+template <int TW, int TH, int CH, int PPL>
+__global__ void __launch_bounds__(TW * TH / PPL, (PPL == 1 ? 1024 : 768) / (TW * TH / PPL)) raster_bwd_kernel(
     const float4* __restrict__ rec, const uint32_t* __restrict__ gauss, const uint2* __restrict__ ranges,
     uint32_t width, uint32_t height, uint32_t tiles_x, float bg0, float bg1, float bg2,
     const float* __restrict__ final_t, const uint32_t* __restrict__ n_contrib, const float* __restrict__ dimage,
     float4* __restrict__ pgrad, int64_t cap, unsigned long long* __restrict__ pairs,
     const BatchTable* __restrict__ bt) {
   typedef TileGeo<TW, TH> Geo;
-  constexpr int NT = Geo::kThreads;
+  constexpr int NT = TW * TH / PPL, NW = NT / 32, WX = TW / 8, SBH = 4 * PPL;
+  typedef typename std::conditional<(NW > 8), uint16_t, uint8_t>::type WarpMask;
   if (bt && blockIdx.x >= bt->tile_start[bt->views]) return;  // past the batch's tiles
   __shared__ float4 s0[CH], s1[CH];
   __shared__ float2 s2[CH];
   __shared__ typename Geo::Mask srect[CH];
   __shared__ uint32_t sg[CH];
   __shared__ float acc[CH * kSlots];
-  __shared__ typename Geo::WarpMask smask[CH];
-  __shared__ uint8_t slist[Geo::kWarps][CH];
+  __shared__ WarpMask smask[CH];
+  __shared__ uint8_t slist[NW][CH];
   __shared__ uint32_t s_max_last;
   // In a batch the block is a global tile: find its view, local tile and image offset.
   uint32_t tile = blockIdx.x;
@@ -400,37 +406,49 @@ __global__ void __launch_bounds__(TW * TH) raster_bwd_kernel(
     tiles_x = bt->tiles_x[v];
     pix0 = bt->pix_start[v];
   }
-  const PixelGeom pg = pixel_geom<TW, TH>(tile, tiles_x, width, height);
   const uint32_t ox = (tile % tiles_x) * TW, oy = (tile / tiles_x) * TH;
-  const uint32_t lx = pg.px_i - ox, ly_shift = pg.py_j - oy + Geo::kRowShift;  // bits in the rect masks
-  const float px = (float)pg.px_i + 0.5f, py = (float)pg.py_j + 0.5f;
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t lx = (warp % WX) * 8u + (lane & 7u);        // column in the tile
+  const uint32_t ly0 = (warp / WX) * (uint32_t)SBH + (lane >> 3);  // row of pixel 0 in the tile
+  const float px = (float)(ox + lx) + 0.5f;
   const uint2 range = ranges[blockIdx.x];
-  const uint32_t lane = threadIdx.x & 31;
-  uint8_t* list = slist[threadIdx.x >> 5];
-
-  uint32_t last = 0;
-  float T = 1.0f, t_fin = 1.0f, d0 = 0.0f, d1 = 0.0f, d2 = 0.0f, bg_dot = 0.0f;
+  uint8_t* list = slist[warp];
   const uint32_t list_len = range.y - range.x;
-  if (pg.inside) {
-    const size_t pix = pix0 + (size_t)pg.py_j * width + pg.px_i;
-    last = min(n_contrib[pix], list_len);  // n_contrib never exceeds its tile's list
-    T = final_t[pix];
-    t_fin = T;
-    d0 = dimage[3 * pix];
-    d1 = dimage[3 * pix + 1];
-    d2 = dimage[3 * pix + 2];
-    bg_dot = bg0 * d0 + bg1 * d1 + bg2 * d2;
+
+  // Per pixel: contributor count, transmittance, dL/dpixel and the running sums of the
+  // reverse walk (rasterize.rs:347-455).
+  uint32_t last[PPL];
+  float T[PPL], t_fin[PPL], d0[PPL], d1[PPL], d2[PPL], bg_dot[PPL];
+  float acc_r[PPL], acc_g[PPL], acc_b[PPL], last_alpha[PPL], lc_r[PPL], lc_g[PPL], lc_b[PPL];
+  uint32_t lane_last = 0;
+#pragma unroll
+  for (int q = 0; q < PPL; q++) {
+    const uint32_t y = oy + ly0 + 4u * q, x = ox + lx;
+    last[q] = 0;
+    T[q] = t_fin[q] = 1.0f;
+    d0[q] = d1[q] = d2[q] = bg_dot[q] = 0.0f;
+    if (x < width && y < height) {
+      const size_t pix = pix0 + (size_t)y * width + x;
+      last[q] = min(n_contrib[pix], list_len);  // n_contrib never exceeds its tile's list
+      T[q] = final_t[pix];
+      t_fin[q] = T[q];
+      d0[q] = dimage[3 * pix];
+      d1[q] = dimage[3 * pix + 1];
+      d2[q] = dimage[3 * pix + 2];
+      bg_dot[q] = bg0 * d0[q] + bg1 * d1[q] + bg2 * d2[q];
+    }
+    acc_r[q] = acc_g[q] = acc_b[q] = 0.0f;  // accum (rasterize.rs:347)
+    last_alpha[q] = lc_r[q] = lc_g[q] = lc_b[q] = 0.0f;
+    lane_last = max(lane_last, last[q]);
   }
   if (threadIdx.x == 0) s_max_last = 0;
   for (int i = threadIdx.x; i < CH * kSlots; i += NT) acc[i] = 0.0f;
   __syncthreads();
-  const uint32_t warp_max_last = __reduce_max_sync(0xffffffffu, last);
+  const uint32_t warp_max_last = __reduce_max_sync(0xffffffffu, lane_last);
   if (lane == 0) atomicMax(&s_max_last, warp_max_last);
   __syncthreads();
   const uint32_t max_last = s_max_last;
-  float acc_r = 0.0f, acc_g = 0.0f, acc_b = 0.0f;  // accum (rasterize.rs:347)
-  float last_alpha = 0.0f, lc_r = 0.0f, lc_g = 0.0f, lc_b = 0.0f;
-  unsigned long long npairs = 0;
+  uint32_t npairs = 0;
 
   for (uint32_t cend = max_last; cend > 0;) {
     const uint32_t cstart = cend > (uint32_t)CH ? cend - CH : 0u;
@@ -446,9 +464,9 @@ __global__ void __launch_bounds__(TW * TH) raster_bwd_kernel(
         const float4 e2 = rec[4 * (size_t)g + 2];
         s2[e] = make_float2(e2.x, e2.y);
         srect[e] = tile_rect_masks<TW, TH>(fbits(e2.z), fbits(e2.w), ox, oy);
-        m = subblock_mask<TW, TH>(fbits(e2.z), fbits(e2.w), ox, oy);
+        m = subblock_mask<TW, TH, SBH>(fbits(e2.z), fbits(e2.w), ox, oy);
       }
-      smask[e] = (typename Geo::WarpMask)m;
+      smask[e] = (WarpMask)m;
     }
     __syncthreads();
     // Entries at or past every lane's n_contrib contribute nothing to this warp.
@@ -462,54 +480,57 @@ __global__ void __launch_bounds__(TW * TH) raster_bwd_kernel(
 #pragma unroll
       for (int q = 0; q < kSlots; q++) c[q] = 0.0f;
       bool active = false;
-      if (k < last && ((uint32_t)(rm >> lx) & (uint32_t)(rm >> ly_shift) & 1u)) {
+      const bool col_in = (uint32_t)(rm >> lx) & 1u;
+#pragma unroll
+      for (int q = 0; q < PPL; q++) {
+        if (!(col_in && k < last[q] && ((uint32_t)(rm >> (ly0 + 4u * q + Geo::kRowShift)) & 1u))) continue;
         const float2 e2 = s2[kk];
         npairs++;
         const float4 e0 = s0[kk], e1 = s1[kk];
+        const float py = (float)(oy + ly0 + 4u * q) + 0.5f;
         float gval, alpha;
         bool unclamped;
-        if (evaluate_bwd(px, py, e0.x, e0.y, e0.z, e0.w, e1.x, e1.y, e1.z, &gval, &alpha, &unclamped)) {
-          active = true;
-          // Values only from here on: the arithmetic is fused and the divisions are
-          // reciprocals; every decision was taken above exactly as in the forward pass.
-          const float col_r = e1.w, col_g = e2.x, col_b = e2.y;
-          const float inv = rcp_refined(1.0f - alpha);
-          T = T * inv;
-          const float t = T;
-          const float keep = 1.0f - last_alpha;
-          acc_r = __fmaf_rn(last_alpha, lc_r, keep * acc_r);
-          acc_g = __fmaf_rn(last_alpha, lc_g, keep * acc_g);
-          acc_b = __fmaf_rn(last_alpha, lc_b, keep * acc_b);
-          float dalpha = (col_r - acc_r) * d0;
-          dalpha = __fmaf_rn(col_g - acc_g, d1, dalpha);
-          dalpha = __fmaf_rn(col_b - acc_b, d2, dalpha);
-          const float at = alpha * t;
-          c[6] = at * d0;
-          c[7] = at * d1;
-          c[8] = at * d2;
-          c[11] = at;
-          lc_r = col_r;
-          lc_g = col_g;
-          lc_b = col_b;
-          last_alpha = alpha;
-          dalpha = __fmaf_rn(dalpha, t, -t_fin * inv * bg_dot);
-          if (unclamped) {
-            const float opacity = e1.y;
-            c[5] = gval * dalpha;
-            const float dsigma = -(opacity * dalpha) * gval;
-            const float dx = px - e0.x;
-            const float dy = py - e0.y;
-            const float ddx = dsigma * __fmaf_rn(e0.z, dx, e0.w * dy);
-            const float ddy = dsigma * __fmaf_rn(e0.w, dx, e1.x * dy);
-            c[0] = -ddx;
-            c[1] = -ddy;
-            const float hs = 0.5f * dsigma;
-            c[2] = hs * dx * dx;
-            c[3] = dsigma * dx * dy;
-            c[4] = hs * dy * dy;
-            c[9] = fabsf(ddx);
-            c[10] = fabsf(ddy);
-          }
+        if (!evaluate_bwd(px, py, e0.x, e0.y, e0.z, e0.w, e1.x, e1.y, e1.z, &gval, &alpha, &unclamped)) continue;
+        active = true;
+        // Values only from here on: the arithmetic is fused and the divisions are
+        // reciprocals; every decision was taken above exactly as in the forward pass.
+        const float col_r = e1.w, col_g = e2.x, col_b = e2.y;
+        const float inv = rcp_refined(1.0f - alpha);
+        T[q] = T[q] * inv;
+        const float t = T[q];
+        const float keep = 1.0f - last_alpha[q];
+        acc_r[q] = __fmaf_rn(last_alpha[q], lc_r[q], keep * acc_r[q]);
+        acc_g[q] = __fmaf_rn(last_alpha[q], lc_g[q], keep * acc_g[q]);
+        acc_b[q] = __fmaf_rn(last_alpha[q], lc_b[q], keep * acc_b[q]);
+        float dalpha = (col_r - acc_r[q]) * d0[q];
+        dalpha = __fmaf_rn(col_g - acc_g[q], d1[q], dalpha);
+        dalpha = __fmaf_rn(col_b - acc_b[q], d2[q], dalpha);
+        const float at = alpha * t;
+        c[6] = __fmaf_rn(at, d0[q], c[6]);
+        c[7] = __fmaf_rn(at, d1[q], c[7]);
+        c[8] = __fmaf_rn(at, d2[q], c[8]);
+        c[11] += at;
+        lc_r[q] = col_r;
+        lc_g[q] = col_g;
+        lc_b[q] = col_b;
+        last_alpha[q] = alpha;
+        dalpha = __fmaf_rn(dalpha, t, -t_fin[q] * inv * bg_dot[q]);
+        if (unclamped) {
+          const float opacity = e1.y;
+          c[5] = __fmaf_rn(gval, dalpha, c[5]);
+          const float dsigma = -(opacity * dalpha) * gval;
+          const float dx = px - e0.x;
+          const float dy = py - e0.y;
+          const float ddx = dsigma * __fmaf_rn(e0.z, dx, e0.w * dy);
+          const float ddy = dsigma * __fmaf_rn(e0.w, dx, e1.x * dy);
+          c[0] -= ddx;
+          c[1] -= ddy;
+          const float hs = 0.5f * dsigma;
+          c[2] = __fmaf_rn(hs * dx, dx, c[2]);
+          c[3] = __fmaf_rn(dsigma * dx, dy, c[3]);
+          c[4] = __fmaf_rn(hs * dy, dy, c[4]);
+          c[9] += fabsf(ddx);
+          c[10] += fabsf(ddy);
         }
       }
       if (__any_sync(0xffffffffu, active)) {
@@ -538,8 +559,9 @@ __global__ void __launch_bounds__(TW * TH) raster_bwd_kernel(
     cend = cstart;
   }
   if (pairs) {
-    for (int o = 16; o > 0; o >>= 1) npairs += __shfl_xor_sync(0xffffffffu, npairs, o);
-    if (lane == 0 && npairs) atomicAdd(pairs, npairs);
+    unsigned long long np = npairs;
+    for (int o = 16; o > 0; o >>= 1) np += __shfl_xor_sync(0xffffffffu, np, o);
+    if (lane == 0 && np) atomicAdd(pairs, np);
   }
 }
 
@@ -588,12 +610,19 @@ Status launch_raster_bwd(Ctx* c, const float* proj, const uint32_t* gauss, const
   const uint32_t tiles_x = rc.tiles_x(width);
   const uint32_t blocks = bt ? tiles_cap : rc.tiles(width, height);
   if (blocks == 0) return Status::ok();
-#define SPLAT_BWD(TW, TH, CH)                                                                                     \
-  raster_bwd_kernel<TW, TH, CH><<<blocks, TW * TH, 0, c->stream>>>(                                              \
+#define SPLAT_BWD(TW, TH, CH, P)                                                                                  \
+  raster_bwd_kernel<TW, TH, CH, P><<<blocks, TW * TH / P, 0, c->stream>>>(                                       \
       reinterpret_cast<const float4*>(proj), gauss, reinterpret_cast<const uint2*>(ranges), width, height, tiles_x, \
       bg[0], bg[1], bg[2], final_t, n_contrib, dimage, reinterpret_cast<float4*>(pgrad), cap,                     \
       reinterpret_cast<unsigned long long*>(pairs), bt)
-  SPLAT_RASTER_DISPATCH(rc, SPLAT_BWD);
+#define SPLAT_BWD1(TW, TH, CH) SPLAT_BWD(TW, TH, CH, 1)
+#define SPLAT_BWD2(TW, TH, CH) SPLAT_BWD(TW, TH, CH, 2)
+  if (rc.ppl == 2)
+    SPLAT_RASTER_DISPATCH(rc, SPLAT_BWD2);
+  else
+    SPLAT_RASTER_DISPATCH(rc, SPLAT_BWD1);
+#undef SPLAT_BWD2
+#undef SPLAT_BWD1
 #undef SPLAT_BWD
   c->launches.count++;
   SPLAT_LAUNCHED("raster_bwd_kernel");

@@ -247,7 +247,7 @@ std::vector<uint64_t> graph_key(splat_trainer* t, const IterPlan& p) {
   std::vector<uint64_t> k = {(uint64_t)t->n, (uint64_t)t->cur.cap, (uint64_t)t->vb.e_cap, (uint64_t)p.sh_degree,
                              (uint64_t)p.densify_window, w, h, t->c->arena.generation, (uint64_t)t->stats_cap,
                              (uint64_t)t->batch, t->tiles_cap, t->pix_cap, t->c->raster.tile_w,
-                             t->c->raster.tile_h, t->c->raster.chunk};
+                             t->c->raster.tile_h, t->c->raster.chunk, t->c->raster.ppl};
   for (const DevBuf* b : {&t->cur.params, &t->cur.m, &t->cur.v, &t->bf16, &t->stats, &t->pgrad, &t->pred_grad, &t->loss_out,
                           &t->params_dev, &t->batch_dev, &t->vb.proj, &t->vb.num_tiles, &t->vb.entry_offset, &t->vb.depth_range,
                           &t->vb.tile_range, &t->vb.gauss, &t->vb.image, &t->vb.final_t, &t->vb.n_contrib,
@@ -1077,6 +1077,7 @@ SPLAT_API int splat_trainer_tuning(const splat_trainer* t, float* ms_out, uint32
     picked[0] = t->c->raster.tile_w;
     picked[1] = t->c->raster.tile_h;
     picked[2] = t->c->raster.chunk;
+    picked[3] = t->c->raster.ppl;
   }
   if (tunes) *tunes = t->tunes;
   return SPLAT_OK;

@@ -55,28 +55,33 @@ class Context:
 
     @staticmethod
     def raster_candidates() -> list:
-        """The supported compositing configurations (tile_w, tile_h, chunk depth)."""
+        """The supported compositing configurations (tile_w, tile_h, chunk depth, backward
+        pixels per thread)."""
         lib = L.lib()
-        out = (C.c_uint32 * 36)()
+        out = (C.c_uint32 * 96)()
         k = int(lib.splat_raster_candidates(out))
-        return [tuple(int(v) for v in out[3 * i:3 * i + 3]) for i in range(k)]
+        return [tuple(int(v) for v in out[4 * i:4 * i + 4]) for i in range(k)]
 
     @property
     def raster_config(self) -> tuple:
-        """(tile_w, tile_h, chunk depth) that projection, binning and compositing use."""
-        out = (C.c_uint32 * 3)()
+        """(tile_w, tile_h, chunk depth, backward pixels per thread) that projection,
+        binning and compositing use."""
+        out = (C.c_uint32 * 4)()
         check(self.lib.splat_get_raster_config(self.h, out), self.h)
         return tuple(int(v) for v in out)
 
     @raster_config.setter
     def raster_config(self, cfg):
-        check(self.lib.splat_set_raster_config(self.h, *[int(v) for v in cfg]), self.h)
+        cfg = tuple(int(v) for v in cfg)
+        if len(cfg) == 3:
+            cfg = cfg + (1,)
+        check(self.lib.splat_set_raster_config(self.h, *cfg), self.h)
 
     def autotune_render(self, planes, n, cap, cam, opts, background, dimage, reps: int = 3) -> dict:
         """Times one view's render + backward under every configuration and keeps the
         fastest; returns {config: ms per pass} and the pick."""
-        ms = (C.c_float * 12)()
-        picked = (C.c_uint32 * 3)()
+        ms = (C.c_float * 24)()
+        picked = (C.c_uint32 * 4)()
         bgp, _keep = _bg(background)
         check(self.lib.splat_autotune_render(self.h, _ptr(planes), n, cap, C.byref(cam), C.byref(opts), bgp,
                                              _ptr(dimage), reps, ms, picked), self.h)
@@ -180,7 +185,7 @@ def bin(ctx: Context, proj: Projection, want_keys: bool = False) -> Binning:
     e = C.c_int64()
     check(ctx.lib.splat_bin_count(ctx.h, _ptr(proj.num_tiles), proj.n, _ptr(off), C.byref(e)), ctx.h)
     E = int(e.value)
-    tw, th, _ = ctx.raster_config
+    tw, th = ctx.raster_config[:2]
     tx = (proj.width + tw - 1) // tw
     ty = (proj.height + th - 1) // th
     gauss = torch.empty(max(E, 1), dtype=torch.int32, device=dev)
@@ -199,7 +204,7 @@ def bin_device(ctx: Context, proj: Projection, capacity: int, scratch: torch.Ten
     off = torch.empty(proj.n + 1, dtype=torch.int32, device=dev)
     e_dev = torch.zeros(1, dtype=torch.int64, device=dev)
     check(ctx.lib.splat_bin_count_device(ctx.h, _ptr(proj.num_tiles), proj.n, _ptr(off), _ptr(e_dev)), ctx.h)
-    tw, th, _ = ctx.raster_config
+    tw, th = ctx.raster_config[:2]
     tx = (proj.width + tw - 1) // tw
     ty = (proj.height + th - 1) // th
     need = int(ctx.lib.splat_bin_sort_device_scratch_bytes(capacity))
@@ -489,8 +494,8 @@ class Trainer:
     def tuning(self) -> dict:
         """The autotuner's last timings (ms per render pass per configuration), the
         configuration in use and how many tunings ran."""
-        ms = (C.c_float * 12)()
-        picked = (C.c_uint32 * 3)()
+        ms = (C.c_float * 24)()
+        picked = (C.c_uint32 * 4)()
         tunes = C.c_uint32()
         check(self.lib.splat_trainer_tuning(self.h, ms, picked, C.byref(tunes)), self.ctx.h)
         cands = Context.raster_candidates()

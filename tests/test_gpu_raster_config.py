@@ -1,4 +1,5 @@
-"""Compositing configurations (tile shape x shared-memory chunk depth) and the autotuner.
+"""Compositing configurations (tile shape x shared-memory chunk depth x the backward's pixels
+per thread) and the autotuner.
 
 Every configuration composites the same entries per pixel in the same depth order (the
 projection narrows each entry's pixel rectangle to its 16-pixel tile rectangle before
@@ -22,9 +23,10 @@ from tests import fixtures as F
 
 pytestmark = pytest.mark.gpu
 
-CANDS = [(16, 16, 256), (16, 16, 128), (16, 16, 64), (16, 16, 32), (8, 8, 256), (8, 8, 128), (8, 8, 64),
-         (8, 8, 32), (16, 32, 256), (16, 32, 128), (16, 32, 64), (16, 32, 32)]
-DEFAULT = (16, 16, 256)
+SHAPES = [(16, 16, 256), (16, 16, 128), (16, 16, 64), (16, 16, 32), (8, 8, 256), (8, 8, 128), (8, 8, 64),
+          (8, 8, 32), (16, 32, 256), (16, 32, 128), (16, 32, 64), (16, 32, 32)]
+CANDS = [s + (1,) for s in SHAPES] + [s + (2,) for s in SHAPES]
+DEFAULT = (16, 16, 256, 1)
 SIZE = (640, 480)
 
 
@@ -84,7 +86,8 @@ def config(ctx):
 def test_candidates_and_invalid_configs(ctx):
     assert G.Context.raster_candidates() == CANDS
     assert ctx.raster_config == DEFAULT
-    for bad in [(16, 16, 16), (16, 16, 512), (32, 32, 256), (8, 16, 64), (0, 0, 0)]:
+    for bad in [(16, 16, 16, 1), (16, 16, 512, 1), (32, 32, 256, 1), (8, 16, 64, 1), (0, 0, 0, 1), (16, 16, 256, 3),
+                (16, 16, 256, 0)]:
         with pytest.raises(SplatError):
             ctx.raster_config = bad
     assert ctx.raster_config == DEFAULT
@@ -124,7 +127,7 @@ def test_backward_matches_oracle_under_every_config(ctx, cr_math, config, cfg):
     print(f"\n{cfg}: screen-space gradients max rel. error vs oracle {err:.2e}")
 
 
-@pytest.mark.parametrize("cfg", [(8, 8, 64), (16, 32, 128)])
+@pytest.mark.parametrize("cfg", [(8, 8, 64, 1), (16, 32, 128, 2)])
 def test_device_projection_path_identical_across_configs(ctx, config, cfg):
     """The full device chain (projection, device-driven counts, binning, compositing) gives
     the same image under another tile shape as under 16x16."""
@@ -189,7 +192,7 @@ def test_trainer_same_first_step_under_every_tile_shape(ctx, config, batch):
     cfg = dict(iterations=10, densify=0, sh_degree=1, sh_degree_interval=1000, position_lr_max_steps=10, seed=2,
                batch_views=batch)
     results = []
-    for shape in [(16, 16, 256), (8, 8, 64), (16, 32, 128)]:
+    for shape in [(16, 16, 256, 1), (8, 8, 64, 2), (16, 32, 128, 1), (16, 16, 128, 2)]:
         config(shape)
         t = G.Trainer(ctx, init, extent, views, **cfg)
         info = t.step()
@@ -258,7 +261,7 @@ def test_blend_weight_statistic_sums_to_coverage(ctx, config):
     Gaussians, and the same under every tile shape up to summation order."""
     g, cam, p, bg, img, ft, nc, pairs, dimage, *_ = oracle_case()
     per = {}
-    for cfg in [(16, 16, 256), (8, 8, 64), (16, 32, 128)]:
+    for cfg in [(16, 16, 256, 1), (8, 8, 64, 1), (16, 32, 128, 2), (16, 16, 256, 2)]:
         config(cfg)
         proj = G.proj_from_reference(ctx, dev(p), *SIZE)
         b = G.bin(ctx, proj)
@@ -270,6 +273,6 @@ def test_blend_weight_statistic_sums_to_coverage(ctx, config):
         assert (w[p[:, 6] == 0] == 0).all()
         assert abs(w.sum() - cover) <= 1e-4 * cover, (w.sum(), cover)
         per[cfg] = w
-    ref = per[(16, 16, 256)]
+    ref = per[(16, 16, 256, 1)]
     for cfg, w in per.items():
         assert np.abs(w - ref).max() <= 1e-5 * ref.max(), cfg
