@@ -57,6 +57,9 @@ def parse():
     ap.add_argument("--train-c4", action="store_true",
                     help="learned densification: learn on scene seeds 2-5, compare with the rule on seed 6")
     ap.add_argument("--c4-learn-iters", type=int, default=1875, help="steps of each learning run")
+    ap.add_argument("--profile-mlp", action="store_true",
+                    help="only the densification network's forward (tcgen05) on 4M rows, for an ncu capture")
+    ap.add_argument("--mlp-rows", type=int, default=4_000_000)
     ap.add_argument("--profile-small", action="store_true",
                     help="a reduced case for ncu captures (fewer Gaussians, one step)")
     return ap.parse_args()
@@ -152,7 +155,9 @@ RASTER_BWD_BYTES_PER_PIXEL = 20    # dL/dpix (12) + final T (4) + n_contrib (4) 
 RASTER_BYTES_PER_ENTRY = 52        # sorted index (4) + record gather (48)
 # dram__bytes_read.sum + dram__bytes_write.sum per launch, ncu, default workload.
 NCU_DRAM_BYTES_1M = {("raster_bwd", 16, 16, 256, 1): int((197.05 + 17.84) * 1e6),
-                     ("raster_fwd", 16, 16, 256, 1): int((82.84 + 20.76) * 1e6)}
+                     ("raster_fwd", 16, 16, 256, 1): int((82.84 + 20.76) * 1e6),
+                     ("raster_bwd", 16, 16, 256, 2): int((196.92 + 17.50) * 1e6),
+                     ("raster_fwd", 16, 16, 256, 2): int((83.13 + 20.63) * 1e6)}
 RASTER_FWD_FLOP_PER_PAIR = 20
 RASTER_BWD_FLOP_PER_PAIR = 50
 
@@ -531,8 +536,43 @@ def cpu_reference_steps(args, steps):
     return dt, O.threads()
 
 
+def run_mlp(local, rows, reps=20):
+    """The learned-densification network's forward on `rows` feature rows already on the
+    device: the tcgen05 kernel (what the trainer runs) and the mma.sync kernel, CUDA-event
+    timed per call on the launching stream (each call synchronises once for its timeout
+    check, so the figure includes one host round trip)."""
+    import torch
+    from oracle import mlp as M
+    from splatrs_b200 import gpu as G
+    dev = torch.device("cuda", local)
+    ctx = G.Context(local, torch.cuda.current_stream(local))
+    rng = np.random.default_rng(1)
+    x = torch.from_numpy(rng.normal(0, 1, (rows, 16)).astype(np.float32)).to(dev)
+    th = torch.from_numpy(M.init_params(1).astype(np.float32)).to(dev)
+    out = {"rows": rows, "flop_per_row": 2 * (16 * 64 + 64 * 64 + 64 * 3), "bytes_per_row": 16 * 4 + 3 * 4}
+    stream = torch.cuda.current_stream(dev)
+    for name, tc in (("tcgen05", True), ("mma_sync", False)):
+        for _ in range(3):
+            G.mlp_forward(ctx, x, th, tcgen05=tc)
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            G.mlp_forward(ctx, x, th, tcgen05=tc)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        ms = e0.elapsed_time(e1) / reps
+        out[name] = {"ms": round(ms, 4), "tflops": round(out["flop_per_row"] * rows / ms / 1e9, 2),
+                     "gbs": round(out["bytes_per_row"] * rows / ms / 1e6, 1)}
+    ctx.close()
+    return out
+
+
 def main():
     args = parse()
+    if args.profile_mlp:
+        print(json.dumps({"mlp": run_mlp(0, args.mlp_rows, reps=3)}), flush=True)
+        return
     rank, world, local = dist_info()
     if world > 1:
         import torch
@@ -567,6 +607,8 @@ def main():
         return
 
     line = run_ours(args, rank, world, local)
+    if not args.profile_small:
+        line["mlp"] = run_mlp(local, args.mlp_rows)
     c0 = None
     if not args.profile_small and not args.no_train:
         from splatrs_b200 import scenes
