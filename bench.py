@@ -60,6 +60,9 @@ def parse():
     ap.add_argument("--profile-mlp", action="store_true",
                     help="only the densification network's forward (tcgen05) on 4M rows, for an ncu capture")
     ap.add_argument("--mlp-rows", type=int, default=4_000_000)
+    ap.add_argument("--profile-train", action="store_true",
+                    help="only a short config-2 training run (20 views, 300 iterations) for an ncu launch list; "
+                         "prints the launches before its last 100 iterations")
     ap.add_argument("--profile-small", action="store_true",
                     help="a reduced case for ncu captures (fewer Gaussians, one step)")
     return ap.parse_args()
@@ -568,8 +571,40 @@ def run_mlp(local, rows, reps=20):
     return out
 
 
+def run_profile_train(local):
+    """Config-2 training for an ncu launch list: the scene's first 20 cameras, 300 plain
+    iterations (densification from 100 every 50). Prints how many kernel launches come
+    before the last 100 iterations (skip that many) and how many those take."""
+    import torch
+    from splatrs_b200 import gpu as G
+    from splatrs_b200 import scenes
+    s = scenes.config2()
+    s["cams"] = s["cams"][:20]
+    ctx = G.Context(local, torch.cuda.current_stream(local))
+    views = gt_views_gpu(ctx, s)
+    init_planes = G.init_from_points(ctx, s["init_points"], s["init_rgb"])
+    n0 = len(s["init_points"])
+    init = G.planes_to_params(ctx, init_planes, n0, n0).cpu().numpy()
+    cfg = dict(C2_TRAIN, iterations=300, densify_from_iter=100, densify_until_iter=250, densification_interval=50,
+               position_lr_max_steps=300)
+    t = G.Trainer(ctx, init, scenes.scene_extent(s["cams"]), views, **cfg)
+    t.run(200)
+    torch.cuda.synchronize(local)
+    before = ctx.launches
+    t.run(100)
+    torch.cuda.synchronize(local)
+    out = {"profile_train": {"launches_before_last_100": before, "launches_last_100": ctx.launches - before,
+                             "gaussians": t.count}}
+    t.close()
+    ctx.close()
+    return out
+
+
 def main():
     args = parse()
+    if args.profile_train:
+        print(json.dumps(run_profile_train(0)), flush=True)
+        return
     if args.profile_mlp:
         print(json.dumps({"mlp": run_mlp(0, args.mlp_rows, reps=3)}), flush=True)
         return
