@@ -147,7 +147,7 @@ typedef struct splat_train_config {
    * keeps the fastest on the context; 0 uses the context's configuration as it is. */
   int32_t autotune;
   /* Not in the reference; learned densification only. learn_contribution > 0: hindsight
-   * labels also judge contribution, each Gaussian's blending weight sum(alpha T) over the
+   * labels also weigh contribution, each Gaussian's blending weight sum(alpha T) over the
    * pixels of every view between two densifications (pixel units): a kept Gaussian whose
    * descendants contributed less is labelled prune, and a clone/split descendant counts as
    * useful only from that contribution on. 0: labels from opacity alone.

@@ -1,6 +1,6 @@
 """Parity of the sm_100a kernels with the CPU oracle, stage by stage, through the C ABI.
 
-Bars (north star): tile lists and sort order bit-exact when fed the same projections;
+Bars: tile lists and sort order bit-exact when fed the same projections;
 images within 1e-4 max-abs; per-parameter gradients within 1e-3 relative error; every
 result also reports its error against the FP64 oracle.
 

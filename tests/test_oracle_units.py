@@ -1,7 +1,7 @@
 """The reference's unit tests with exact answers, replayed against the CPU oracle.
 
 Each test names the reference test it replays. These pin the oracle before it is used to
-judge the CUDA kernels."""
+check the CUDA kernels."""
 import math
 
 import numpy as np
