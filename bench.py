@@ -539,6 +539,87 @@ def cpu_reference_steps(args, steps):
     return dt, O.threads()
 
 
+ADAM_BYTES = 4 * 240 + 3 * 240            # params, grads, m, v read; params, m, v written (60 floats padded)
+PROJ_BWD_ADAM_BYTES = 240 + 64 + 48 + 2 * 240 + 3 * 240  # + record and screen gradients; no gradient round trip
+LOSS_BYTES_PER_PIXEL = 12 + 3 + 12        # prediction read, u8 target read, gradient written
+LOSS_FLOP_PER_PIXEL = 1056                # five blurs forward, three back, SSIM and its partials, L1
+
+
+def run_stages(local, reps=20):
+    """The HBM- or FP32-bound stages outside the render step, CUDA-event timed on their own
+    (inputs above L2): the fused SSIM + L1 loss forward and backward on one 1297x840 view,
+    Adam over 1M Gaussians, and the projection backward fused with Adam over 1M Gaussians
+    (the trainer's optimiser step)."""
+    import torch
+    from splatrs_b200 import gpu as G
+    from splatrs_b200 import scenes
+    from splatrs_b200._lib import Camera, LearningRates, ProjOpts
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream(dev)
+    ctx = G.Context(local, stream)
+    hbm, kind = measured_peaks()
+    fp32_nominal = 148 * 128 * 2 * 1.965e9 / 1e12  # TFLOP/s at the maximum SM clock
+
+    def timed(fn):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        return e0.elapsed_time(e1) / reps
+
+    out = {"peak_hbm_gbs": hbm, "peak_source": kind, "fp32_tflops_nominal": round(fp32_nominal, 1)}
+    w, h = 1297, 840
+    rng = np.random.default_rng(3)
+    pred = torch.from_numpy(rng.uniform(0, 1, w * h * 3).astype(np.float32)).to(dev)
+    tgt = torch.from_numpy(rng.integers(0, 256, w * h * 3).astype(np.uint8)).to(dev)
+    grad = torch.empty_like(pred)
+    lo = torch.empty(3, dtype=torch.float32, device=dev)
+    ms = timed(lambda: G.check(ctx.lib.splat_loss_fwd_bwd(ctx.h, G._ptr(pred), G._ptr(tgt), 1, w, h, 0.2,
+                                                          G._ptr(grad), G._ptr(lo)), ctx.h))
+    px = w * h
+    out["ssim_l1_fwd_bwd"] = {"pixels": px, "ms": round(ms, 4), "bytes_per_pixel": LOSS_BYTES_PER_PIXEL,
+                              "gbs": round(LOSS_BYTES_PER_PIXEL * px / ms / 1e6, 1),
+                              "hbm_frac": round(LOSS_BYTES_PER_PIXEL * px / ms / 1e6 / hbm, 4),
+                              "flop_per_pixel": LOSS_FLOP_PER_PIXEL,
+                              "tflops": round(LOSS_FLOP_PER_PIXEL * px / ms / 1e9, 2),
+                              "fp32_frac_nominal": round(LOSS_FLOP_PER_PIXEL * px / ms / 1e9 / fp32_nominal, 4)}
+    del pred, tgt, grad
+    n = 1_000_000
+    sc = scenes.config1(n=n)
+    planes = G.params_to_planes(ctx, torch.from_numpy(sc["params"]).to(dev))
+    grads = torch.randn_like(planes) * 1e-3
+    m, v = torch.zeros_like(planes), torch.zeros_like(planes)
+    lr = LearningRates(mean=1.6e-4, log_scale=0.005, quat=0.001, opacity=0.025, sh_dc=0.0025, sh_rest=0.000125)
+    step = [0]
+
+    def adam():
+        step[0] += 1
+        G.adam_step(ctx, planes, grads, m, v, n, n, step[0], lr)
+
+    ms = timed(adam)
+    out["adam"] = {"gaussians": n, "ms": round(ms, 4), "bytes_per_gaussian": ADAM_BYTES,
+                   "gbs": round(ADAM_BYTES * n / ms / 1e6, 1), "hbm_frac": round(ADAM_BYTES * n / ms / 1e6 / hbm, 4)}
+    cam, opts = Camera.from_record(sc["cam"]), ProjOpts.make(sh_degree=3)
+    proj = G.project_all(ctx, planes, n, n, cam, opts)
+    pgrad = torch.randn((3, n, 4), dtype=torch.float32, device=dev) * 1e-3
+
+    def pba():
+        step[0] += 1
+        G.project_backward_adam(ctx, planes, m, v, n, n, cam, opts, proj, pgrad, step[0], lr)
+
+    ms = timed(pba)
+    out["project_bwd_adam"] = {"gaussians": n, "ms": round(ms, 4), "bytes_per_gaussian": PROJ_BWD_ADAM_BYTES,
+                               "gbs": round(PROJ_BWD_ADAM_BYTES * n / ms / 1e6, 1),
+                               "hbm_frac": round(PROJ_BWD_ADAM_BYTES * n / ms / 1e6 / hbm, 4)}
+    ctx.close()
+    return out
+
+
 def run_mlp(local, rows, reps=20):
     """The learned-densification network's forward on `rows` feature rows already on the
     device: the tcgen05 kernel (what the trainer runs) and the mma.sync kernel, CUDA-event
@@ -644,6 +725,7 @@ def main():
     line = run_ours(args, rank, world, local)
     if not args.profile_small:
         line["mlp"] = run_mlp(local, args.mlp_rows)
+        line["stages"] = run_stages(local)
     c0 = None
     if not args.profile_small and not args.no_train:
         from splatrs_b200 import scenes
