@@ -443,26 +443,12 @@ def run_c4(local, learn_iters, learn=None, plain=True):
         t.run(C3_TRAIN["iterations"])
         torch.cuda.synchronize(local)
         wall = time.perf_counter() - tw
-        ps = float(np.mean([scenes.psnr(t.render(cam), rgb) for cam, rgb in views]))
-        ev[name] = {"steps": C3_TRAIN["iterations"], "wall_s": round(wall, 3), "psnr_train_views": round(ps, 2),
-                    "ssim_train_views": round(mean_ssim(t, views), 4), "gaussians": t.count}
+        sc = t.evaluate()  # splat_trainer_evaluate: every view scored on the device
+        ev[name] = {"steps": C3_TRAIN["iterations"], "wall_s": round(wall, 3), "psnr_train_views": round(sc["psnr"], 2),
+                    "ssim_train_views": round(sc["ssim"], 4), "gaussians": t.count}
         t.close()
     ctx.close()
     return {"labels": learn_cfg, "learn": learn_log, "seed6": ev}
-
-
-def mean_ssim(trainer, views):
-    """Mean SSIM of the trainer's renders over the views (the loss kernel at lambda 1)."""
-    import torch
-    from splatrs_b200 import gpu as G
-    from splatrs_b200._lib import Camera
-    tot = 0.0
-    for cam, rgb in views:
-        c = Camera.from_record(cam)
-        img = torch.from_numpy(trainer.render(cam)).cuda()
-        out, _ = G.photometric_loss(trainer.ctx, img, torch.from_numpy(rgb).cuda(), c.width, c.height, 1.0)
-        tot += float(out[1].item())
-    return tot / len(views)
 
 
 def run_train_gpu(local, s, cfg, iterations):
@@ -485,11 +471,11 @@ def run_train_gpu(local, s, cfg, iterations):
     t.run(iterations)  # splat_trainer_run: the whole run in one call, queued ahead of the device
     torch.cuda.synchronize(local)
     wall = time.perf_counter() - tw
-    ps = float(np.mean([scenes.psnr(t.render(cam), rgb) for cam, rgb in views]))
+    ev = t.evaluate()  # splat_trainer_evaluate: every view scored on the device
     bv = max(1, int(cfg.get("batch_views", 1)))
     out = {"iterations": iterations, "wall_s": round(wall, 3), "iters_per_s": round(iterations / wall, 1),
-           "views_per_s": round(iterations * bv / wall, 1), "psnr_train_views": round(ps, 2),
-           "ssim_train_views": round(mean_ssim(t, views), 4), "gaussians": t.count}
+           "views_per_s": round(iterations * bv / wall, 1), "psnr_train_views": round(ev["psnr"], 2),
+           "ssim_train_views": round(ev["ssim"], 4), "gaussians": t.count}
     if cfg.get("autotune"):
         tu = t.tuning()
         out["autotune"] = {"tunes": tu["tunes"], "picked": list(tu["picked"]),

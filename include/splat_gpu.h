@@ -516,6 +516,12 @@ SPLAT_API uint32_t splat_trainer_iteration(const splat_trainer* t);
 SPLAT_API int splat_trainer_get_model(splat_trainer* t, float* aos59_host);
 /* render::render of the current model at the active SH degree and the config's background. */
 SPLAT_API int splat_trainer_render(splat_trainer* t, const splat_camera* cam, float* image_host);
+/* evaluate (train.rs:309-321) on the device: renders every training view with the current
+ * model (trainer's SH degree and background) and scores it with the loss kernel. Writes
+ * the mean PSNR (loss.rs:175-190; NaN without views) to *mean_psnr and, when per_view3_host
+ * is not NULL, {loss, SSIM, PSNR} of every view (3 floats per view, in the order the views
+ * were added). One host wait for all views. */
+SPLAT_API int splat_trainer_evaluate(splat_trainer* t, float* per_view3_host, double* mean_psnr);
 
 #ifdef __cplusplus
 }

@@ -207,6 +207,7 @@ def _declare(L):
         "splat_trainer_set_mlp": ([vp, vp], C.c_int),
         "splat_trainer_mlp_stats": ([vp, P(C.c_uint64)], C.c_int),
         "splat_trainer_tuning": ([vp, P(C.c_float), P(C.c_uint32), P(C.c_uint32)], C.c_int),
+        "splat_trainer_evaluate": ([vp, vp, P(C.c_double)], C.c_int),
         "splat_trainer_count": ([vp], i64),
         "splat_trainer_sh_degree": ([vp], i32),
         "splat_trainer_iteration": ([vp], u32),

@@ -121,6 +121,7 @@ struct splat_trainer {
   DevBuf birth, birth_next, origin, origin_next, feat, feat_scratch, policy;
   DevBuf rec_x, rec_action, alive, useful, rec_csum, labels, label_counts, train_x, train_y, train_w;
   DevBuf mlp_theta, mlp_m, mlp_v, mlp_grad;
+  DevBuf eval_out;  // splat_trainer_evaluate: loss, SSIM, PSNR per view
   int64_t rec_n = 0;
   bool rec_valid = false;
   bool mlp_ready = false;
@@ -907,7 +908,7 @@ SPLAT_API int splat_trainer_destroy(splat_trainer* t) {
     for (DevBuf* b : {&t->pgrad, &t->stats, &t->pred_grad, &t->loss_out, &t->normals, &t->init, &t->bf16}) b->release();
     for (DevBuf* b : {&t->birth, &t->birth_next, &t->origin, &t->origin_next, &t->feat, &t->feat_scratch, &t->policy,
                       &t->rec_x, &t->rec_action, &t->alive, &t->useful, &t->rec_csum, &t->labels, &t->label_counts,
-                      &t->train_x,
+                      &t->train_x, &t->eval_out,
                       &t->train_y, &t->train_w, &t->mlp_theta, &t->mlp_m, &t->mlp_v, &t->mlp_grad})
       b->release();
     t->vb.release();
@@ -1121,6 +1122,59 @@ SPLAT_API int splat_trainer_render(splat_trainer* t, const splat_camera* cam, fl
                     "download image");
   if (s.good()) s = cuda_status(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
   return s.good() ? SPLAT_OK : tfail(t, s);
+}
+
+// evaluate (train.rs:309-321) on the device: every training view rendered with the current
+// model at the trainer's SH degree and background, and scored by the loss kernel (loss,
+// SSIM and PSNR per view, PSNR as loss.rs:175-190). All views are queued without a host
+// wait (device-driven binning); if any view's binning overflowed, all are redone with more
+// room.
+SPLAT_API int splat_trainer_evaluate(splat_trainer* t, float* per_view3_host, double* mean_psnr) {
+  if (!t || !mean_psnr) return SPLAT_ERR_INVALID;
+  *mean_psnr = NAN;
+  const size_t nv = t->views.size();
+  if (nv == 0) return SPLAT_OK;  // the reference returns NaN for no views
+  TEnter e(t);
+  Ctx* c = t->c;
+  const float bgv = t->cfg.white_background ? 1.0f : 0.0f;
+  const float bg[3] = {bgv, bgv, bgv};
+  splat_proj_opts opts;
+  opts.near_plane = t->cfg.near_plane;
+  opts.eps2d = 0.3f;
+  opts.antialias = t->cfg.antialias;
+  opts.sh_degree = t->sh_degree;
+  opts.fp64_conic = t->cfg.fp64_conic;
+  Status s = initial_capacity(t);
+  size_t most_pix = 0;
+  for (const View* v : t->views) most_pix = std::max(most_pix, (size_t)v->cam.width * v->cam.height);
+  if (s.good()) s = t->pred_grad.ensure(most_pix * 12);
+  if (s.good()) s = t->eval_out.ensure(nv * 12);
+  for (int attempt = 0; s.good(); attempt++) {
+    for (size_t k = 0; k < nv && s.good(); k++) {
+      const View& v = *t->views[k];
+      arena_reset(c);  // the previous view's scratch is consumed on this stream first
+      s = render_view_dev(c, t->cur.params.as<float>(), t->n, t->cur.cap, v.cam, opts, bg, t->vb, nullptr,
+                          bf16_copy(t));
+      if (s.good())
+        s = launch_loss(c, t->vb.image.as<float>(), v.rgb.ptr, 1, v.cam.width, v.cam.height, t->cfg.lambda_dssim,
+                        t->pred_grad.as<float>(), t->eval_out.as<float>() + 3 * k);
+    }
+    uint32_t w[4] = {0, 0, 0, 0};
+    if (s.good()) s = cuda_status(cudaMemcpyAsync(w, t->vb.counters.ptr, 16, cudaMemcpyDeviceToHost, c->stream),
+                                  "read binning counters");
+    if (s.good()) s = cuda_status(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
+    if (!s.good() || w[2] == 0) break;
+    s = grow_entries(t, (uint64_t)w[0] | ((uint64_t)w[1] << 32));
+  }
+  std::vector<float> res(nv * 3);
+  if (s.good())
+    s = cuda_status(cudaMemcpy(res.data(), t->eval_out.ptr, nv * 12, cudaMemcpyDeviceToHost), "read evaluation");
+  if (!s.good()) return tfail(t, s);
+  double tot = 0.0;
+  for (size_t k = 0; k < nv; k++) tot += res[3 * k + 2];
+  *mean_psnr = tot / (double)nv;
+  if (per_view3_host) std::memcpy(per_view3_host, res.data(), nv * 12);
+  return SPLAT_OK;
 }
 
 }  // extern "C"

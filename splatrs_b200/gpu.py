@@ -461,10 +461,12 @@ class Trainer:
         ctx._adopt(self)
         p = np.ascontiguousarray(init_params, np.float32).reshape(-1, 59)
         check(self.lib.splat_trainer_set_model(self.h, p.ctypes.data_as(C.c_void_p), p.shape[0]), ctx.h)
+        self._nviews = 0
         for cam, rgb in views:
             c = cam if isinstance(cam, Camera) else Camera.from_record(cam)
             r = np.ascontiguousarray(rgb, np.uint8)
             check(self.lib.splat_trainer_add_view(self.h, C.byref(c), r.ctypes.data_as(C.c_void_p)), ctx.h)
+            self._nviews += 1
         check(self.lib.splat_trainer_start(self.h), ctx.h)
 
     def step(self) -> dict:
@@ -490,6 +492,18 @@ class Trainer:
         keys = ("events", "records", "label_keep", "label_densify", "label_prune", "adam_steps", "heldout_net",
                 "heldout_rule", "heldout_records")
         return dict(zip(keys, [int(v) for v in out]))
+
+    def evaluate(self) -> dict:
+        """evaluate (src/train.rs:309-321) on the device over the training views: mean PSNR,
+        and loss, SSIM and PSNR per view."""
+        import numpy as np
+        nv = self._nviews
+        per = np.zeros((max(nv, 1), 3), np.float32)
+        mean = C.c_double()
+        check(self.lib.splat_trainer_evaluate(self.h, per.ctypes.data_as(C.c_void_p), C.byref(mean)), self.ctx.h)
+        per = per[:nv]
+        return {"psnr": float(mean.value), "ssim": float(per[:, 1].mean()) if nv else float("nan"),
+                "per_view": per}
 
     def tuning(self) -> dict:
         """The autotuner's last timings (ms per render pass per configuration), the

@@ -548,3 +548,23 @@ def test_learned_densification_contribution_labels_prune(ctx):
           f"learned {res[1][0]} Gaussians {res[1][1]:.2f} dB")
     assert res[1][0] < res[0][0]
     assert res[1][1] > res[0][1] - 1.5
+
+
+def test_trainer_evaluate_matches_host_evaluation(ctx):
+    """splat_trainer_evaluate (evaluate, src/train.rs:309-321) on the device: per-view PSNR
+    equals the oracle's psnr of the downloaded render (to float rounding of the summed
+    error), the mean is their mean, and a batched trainer evaluates the same way."""
+    views, extent, init = _views_and_init(120, 40, 6, 64, 48, [0.0, 0.0, 0.0])
+    for batch in (1, 3):
+        cfg = dict(iterations=100, densify=0, sh_degree=1, sh_degree_interval=50, position_lr_max_steps=100, seed=1,
+                   batch_views=batch)
+        t = G.Trainer(ctx, init, extent, views, **cfg)
+        t.run(60)
+        ev = t.evaluate()
+        host = [O.psnr(t.render(cam), rgb.astype(np.float32) / np.float32(255.0)) for cam, rgb in views]
+        assert ev["per_view"].shape == (len(views), 3)
+        assert np.abs(ev["per_view"][:, 2] - np.array(host)).max() < 1e-3
+        assert abs(ev["psnr"] - float(np.mean(host))) < 1e-3
+        assert 0.0 < ev["ssim"] <= 1.0
+        print(f"\nbatch {batch}: device evaluation {ev['psnr']:.3f} dB, host {np.mean(host):.3f} dB")
+        t.close()
