@@ -680,8 +680,11 @@ def main():
         import torch
         import torch.distributed as dist
         from datetime import timedelta
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+        gpu = torch.cuda.is_available()
+        if gpu:
+            torch.cuda.set_device(local)
+        # NCCL on the GPU box; gloo where there is no GPU (the CPU reference arm).
+        dist.init_process_group("nccl" if gpu else "gloo", timeout=timedelta(seconds=300))
     if args.profile_small:
         args.n = 200_000
         args.steps = 1

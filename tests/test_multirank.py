@@ -1,4 +1,5 @@
-"""The N > 1 host logic of bench.py (replicas, max over ranks) on two gloo ranks on CPU."""
+"""The N > 1 host logic of bench.py (replicas, max over ranks, the reference arm under
+torchrun) on two gloo ranks on CPU."""
 import os
 import socket
 import subprocess
@@ -47,3 +48,27 @@ def test_max_over_ranks_with_two_gloo_ranks():
         outs.append(out)
         assert p.returncode == 0, out
     assert all("ok" in o for o in outs)
+
+
+def test_reference_arm_under_two_ranks():
+    """`bench.py --impl reference` launched as two ranks: rank 0 alone times the CPU path
+    and prints one JSON line with impl "reference" and its e2e object; rank 1 prints
+    nothing and both exit 0."""
+    import json
+    port = free_port()
+    procs = []
+    for r in range(2):
+        env = dict(os.environ, RANK=str(r), WORLD_SIZE="2", LOCAL_RANK=str(r), MASTER_ADDR="127.0.0.1",
+                   MASTER_PORT=str(port), CUDA_VISIBLE_DEVICES="")
+        procs.append(subprocess.Popen([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference",
+                                       "--gpus", "2", "--steps", "1", "--warmup", "1", "--n", "20000"], env=env,
+                                      stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True))
+    outs = []
+    for p in procs:
+        out, err = p.communicate(timeout=300)
+        assert p.returncode == 0, err[-2000:]
+        outs.append([ln for ln in out.splitlines() if ln.startswith("{")])
+    assert len(outs[0]) == 1 and not outs[1]
+    line = json.loads(outs[0][0])
+    assert line["impl"] == "reference" and line["value"] > 0
+    assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["cpu_baseline"]["kind"] == "port"
