@@ -489,7 +489,7 @@ def run_train_cpu(init, views, extent, cfg, iterations):
     """The same run on the CPU oracle trainer (all host threads), for `iterations` steps."""
     from oracle import oracle as O
     from splatrs_b200 import scenes
-    ot = O.Trainer(init, extent, views, **{k: v for k, v in cfg.items() if k != "max_gaussians"})
+    ot = O.Trainer(init, extent, views, **{k: v for k, v in cfg.items() if k not in ("max_gaussians", "autotune")})
     tw = time.perf_counter()
     for _ in range(iterations):
         ot.step()

@@ -143,7 +143,7 @@ typedef struct splat_train_config {
   int32_t learned_densify;
   /* Not in the reference: 1 times the iteration's render stages (no optimiser step) under
    * every compositing configuration (splat_raster_candidates) before the first iteration
-   * and again whenever the Gaussian count has moved by more than a quarter since, and
+   * and again whenever the Gaussian count has doubled or halved since, and
    * keeps the fastest on the context; 0 uses the context's configuration as it is. */
   int32_t autotune;
   /* Not in the reference; learned densification only. learn_contribution > 0: hindsight

@@ -726,13 +726,13 @@ Status initial_capacity(splat_trainer* t) {
   return ensure_stats(t, t->cur.cap);
 }
 
-// Autotuning is due before the first iteration and whenever the Gaussian count has moved
-// by more than a quarter since the last tuning.
+// Autotuning is due before the first iteration and whenever the Gaussian count has doubled
+// or halved since the last tuning (a tuning costs about a hundred probe passes, so a growing
+// model is retuned a handful of times, not at every densification).
 bool tune_due(const splat_trainer* t) {
   if (!t->cfg.autotune) return false;
   if (t->tunes == 0) return true;
-  const int64_t d = t->n > t->tuned_n ? t->n - t->tuned_n : t->tuned_n - t->n;
-  return 4 * d > t->tuned_n;
+  return t->n >= 2 * t->tuned_n || 2 * t->n <= t->tuned_n;
 }
 
 // Times iteration p's render stages (a probe: everything but the optimiser step, so the

@@ -237,8 +237,8 @@ def test_trainer_autotune_trains_like_fixed_config(ctx, config):
 
 
 def test_trainer_autotune_retunes_as_the_count_grows(ctx, config):
-    """With densification the count grows past a quarter of the last tuning's, which
-    triggers new tunings; training still converges."""
+    """With densification the count doubles past the last tuning's, which triggers new
+    tunings; training still converges."""
     views, extent, init = _views(312, [(96, 72)] * 6)
     cfg = dict(iterations=400, densify=1, densify_from_iter=50, densify_until_iter=300, densification_interval=50,
                opacity_reset_interval=0, sh_degree=1, sh_degree_interval=100, position_lr_max_steps=400, seed=4,
@@ -249,7 +249,7 @@ def test_trainer_autotune_retunes_as_the_count_grows(ctx, config):
     info = t.tuning()
     p = _psnr(t, views)
     print(f"\n{n0} -> {t.count} Gaussians, {info['tunes']} tunings, picked {info['picked']}, {p:.2f} dB")
-    assert t.count > 1.25 * n0 and info["tunes"] >= 2
+    assert t.count > 2 * n0 and info["tunes"] >= 2
     assert p > 25.0
     t.close()
 
