@@ -276,3 +276,54 @@ def test_blend_weight_statistic_sums_to_coverage(ctx, config):
     ref = per[(16, 16, 256, 1)]
     for cfg, w in per.items():
         assert np.abs(w - ref).max() <= 1e-5 * ref.max(), cfg
+
+
+@pytest.mark.parametrize("cfg", [(8, 8, 32, 2), (16, 32, 64, 1), (16, 16, 128, 2)])
+def test_ragged_image_sizes_under_other_configs(ctx, cr_math, config, cfg):
+    """Image sizes that are no multiple of any tile edge (97x61, 1024x36): forward
+    bit-identical to the oracle, backward within the bar."""
+    for seed, n, size in [(51, 1500, (97, 61)), (52, 2500, (1024, 36))]:
+        rng = np.random.default_rng(seed)
+        g = scenes.random_gaussians(rng, n, -1.0, 1.0, -3.5, 0.5, 1.2)
+        cam = scenes.look_at(size[0], size[1], 0.9 * size[0], 0.9 * size[0], (0.4, -0.3, -3.2), (0, 0, 0))
+        p = O.project_all(g, cam, antialias=True, sh_degree=3)
+        bg = np.array((0.3, 0.6, 0.1), np.float32)
+        ob = O.bin(p, *size)
+        img, ft, nc, pairs = O.rasterize_forward(p, ob, size[0], size[1], bg)
+        dimage = rng.normal(0, 1, size[0] * size[1] * 3).astype(np.float32)
+        og, _, _ = O.rasterize_backward(p, ob, size[0], size[1], bg, ft, nc, dimage)
+        config(cfg)
+        proj = G.proj_from_reference(ctx, dev(p), *size)
+        b = G.bin(ctx, proj)
+        out = G.rasterize_forward(ctx, proj, b, bg)
+        assert (bits(out.image.cpu().numpy()) == bits(img)).all()
+        assert (bits(out.final_t.cpu().numpy()) == bits(ft)).all()
+        pg = G.rasterize_backward(ctx, proj, b, bg, out, dev(dimage))
+        gg, _ = G.pgrad_to_reference(pg, n)
+        err = (np.abs(gg.cpu().numpy() - og).max(0) / np.maximum(np.abs(og).max(0), 1e-30)).max()
+        assert err < 1e-3, (size, err)
+        config(DEFAULT)
+
+
+@pytest.mark.parametrize("cfg", [(16, 16, 256, 1), (8, 8, 64, 2), (16, 32, 256, 2)])
+def test_empty_and_fully_culled_under_every_shape(ctx, config, cfg):
+    """No Gaussian at all, and every Gaussian behind the camera: the image is the
+    background, final T is 1, contributor counts and gradients are zero."""
+    config(cfg)
+    bgv = [0.2, 0.3, 0.4]
+    cam_rec = scenes.look_at(80, 60, 70.0, 70.0, (0.0, 0.0, -3.0), (0, 0, 0))
+    cam, opts = Camera.from_record(cam_rec), ProjOpts.make(sh_degree=3)
+    rng = np.random.default_rng(60)
+    behind = scenes.random_gaussians(rng, 64, -1.0, 1.0, -3.5, 0.5, 1.0)
+    behind[:, 2] = -50.0
+    for g in (behind[:0], behind):
+        n = g.shape[0]
+        planes = G.params_to_planes(ctx, dev(g), max(n, 1))
+        proj = G.project_all(ctx, planes, n, max(n, 1), cam, opts)
+        b = G.bin(ctx, proj)
+        out = G.rasterize_forward(ctx, proj, b, bgv)
+        assert b.num_entries == 0
+        assert np.allclose(out.image.cpu().numpy().reshape(-1, 3), bgv)
+        assert (out.final_t.cpu().numpy() == 1.0).all() and (out.n_contrib.cpu().numpy() == 0).all()
+        pg = G.rasterize_backward(ctx, proj, b, bgv, out, torch.ones(80 * 60 * 3, device="cuda"), cap=max(n, 1))
+        assert (pg.cpu().numpy() == 0).all()
