@@ -403,8 +403,8 @@ __global__ void mlp_adam_kernel(float* __restrict__ theta, const float* __restri
   theta[i] -= lr * (m[i] / c1) / (sqrtf(v[i] / c2) + 1e-8f);
 }
 // ---------------------------------------------------------------------------------------
-// The forward on the 5th-generation tensor cores (tcgen05): one CTA of 4 warps per 128
-// Gaussians (M = 128, TMEM lane = row), operands in shared memory in the canonical
+// The forward on the 5th-generation tensor cores (tcgen05): CTAs of 4 warps over tiles of
+// 128 Gaussians (M = 128, TMEM lane = row), operands in shared memory in the canonical
 // K-major, no-swizzle layout (8-row x 16-byte core matrices; K-adjacent cores 128 bytes
 // apart, row groups SBO apart), accumulators in 64 TMEM columns that each layer reuses once
 // the previous epilogue has read them. One thread issues each layer's MMAs and
