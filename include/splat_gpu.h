@@ -318,6 +318,9 @@ SPLAT_API int splat_project_bwd_adam(splat_ctx* ctx, float* planes_dev, float* m
  *     for the tensor cores returns SPLAT_ERR_TIMEOUT.
  *   splat_mlp_grad: adds to grad_dev the gradient of the weighted mean cross-entropy
  *     sum_s w_s * -log p_s[y_s] / sum_s w_s (labels y in 0..2; scale = 1 / sum_s w_s).
+ *   splat_mlp_grad_tc: the same on tcgen05 (tensor-memory accumulators for the layer
+ *     outputs and the weight gradients, which are summed over each CTA's tiles; x_dev
+ *     16-byte aligned). Synchronises; SPLAT_ERR_TIMEOUT if a tensor-core wait ran out.
  *   splat_mlp_adam: one Adam step (beta 0.9 / 0.999, eps 1e-8) on the FP32 parameters.
  * -------------------------------------------------------------------------------------- */
 SPLAT_API int32_t splat_mlp_num_params(void);
@@ -326,6 +329,8 @@ SPLAT_API int splat_mlp_forward_tc(splat_ctx* ctx, const float* x_dev, int64_t n
                                   float* prob_dev);
 SPLAT_API int splat_mlp_grad(splat_ctx* ctx, const float* x_dev, const int32_t* y_dev, const float* w_dev, int64_t n,
                              float scale, const float* theta_dev, float* grad_dev);
+SPLAT_API int splat_mlp_grad_tc(splat_ctx* ctx, const float* x_dev, const int32_t* y_dev, const float* w_dev,
+                               int64_t n, float scale, const float* theta_dev, float* grad_dev);
 SPLAT_API int splat_mlp_adam(splat_ctx* ctx, float* theta_dev, const float* grad_dev, float* m_dev, float* v_dev,
                              uint64_t step, float lr);
 

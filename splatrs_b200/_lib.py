@@ -158,6 +158,7 @@ def _declare(L):
         "splat_mlp_forward": ([vp, vp, i64, vp, vp], C.c_int),
         "splat_mlp_forward_tc": ([vp, vp, i64, vp, vp], C.c_int),
         "splat_mlp_grad": ([vp, vp, vp, vp, i64, C.c_float, vp, vp], C.c_int),
+        "splat_mlp_grad_tc": ([vp, vp, vp, vp, i64, C.c_float, vp, vp], C.c_int),
         "splat_mlp_adam": ([vp, vp, vp, vp, vp, C.c_uint64, C.c_float], C.c_int),
         "splat_raster_candidates": ([P(C.c_uint32)], i32),
         "splat_set_raster_config": ([vp, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32], C.c_int),

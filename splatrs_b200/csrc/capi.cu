@@ -374,6 +374,20 @@ SPLAT_API int splat_mlp_grad(splat_ctx* ctx, const float* x_dev, const int32_t* 
   return finish(ctx, launch_mlp_grad(&ctx->c, x_dev, y_dev, w_dev, n, scale, theta_dev, grad_dev));
 }
 
+SPLAT_API int splat_mlp_grad_tc(splat_ctx* ctx, const float* x_dev, const int32_t* y_dev, const float* w_dev,
+                               int64_t n, float scale, const float* theta_dev, float* grad_dev) {
+  if (!ctx) return SPLAT_ERR_INVALID;
+  if (n < 0 || !theta_dev || !grad_dev || (n && (!x_dev || !y_dev || !w_dev)))
+    return invalid(ctx, "splat_mlp_grad_tc: bad buffers");
+  if (reinterpret_cast<uintptr_t>(x_dev) % 16) return invalid(ctx, "splat_mlp_grad_tc: x_dev not 16-byte aligned");
+  Enter e(ctx);
+  Status s = mlp_tc_error_clear(&ctx->c);
+  if (s.good()) s = launch_mlp_grad_tc(&ctx->c, x_dev, y_dev, w_dev, n, scale, theta_dev, grad_dev,
+                                       mlp_tc_error_word(&ctx->c));
+  if (s.good()) s = mlp_tc_error_check(&ctx->c);
+  return finish(ctx, s);
+}
+
 SPLAT_API int splat_mlp_adam(splat_ctx* ctx, float* theta_dev, const float* grad_dev, float* m_dev, float* v_dev,
                              uint64_t step, float lr) {
   if (!ctx) return SPLAT_ERR_INVALID;

@@ -105,6 +105,15 @@ constexpr int kTcErrWord = 1000;
 // Runs the tcgen05 forward with the error word cleared, synchronises and turns a reported
 // timeout into an error status.
 Status mlp_forward_tc_checked(Ctx* c, const float* x, int64_t n, const float* theta, float* prob);
+// The gradient of launch_mlp_grad on tcgen05 (tensor-memory accumulators; one CTA per SM),
+// added to grad. `err` as for launch_mlp_forward_tc.
+Status launch_mlp_grad_tc(Ctx* c, const float* x, const int32_t* y, const float* w, int64_t n, float scale,
+                          const float* theta, float* grad, uint32_t* err);
+// The error word of the tcgen05 network kernels: cleared on the host before a run of
+// launches, checked (after a synchronisation) once they are done.
+Status mlp_tc_error_clear(Ctx* c);
+uint32_t* mlp_tc_error_word(Ctx* c);
+Status mlp_tc_error_check(Ctx* c);
 Status launch_mlp_grad(Ctx* c, const float* x, const int32_t* y, const float* w, int64_t n, float scale,
                        const float* theta, float* grad);
 Status launch_mlp_adam(Ctx* c, float* theta, const float* grad, float* m, float* v, uint64_t step, float lr);

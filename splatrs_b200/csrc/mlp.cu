@@ -1,9 +1,10 @@
 // The learned-densification network (no reference counterpart; it proposes, per Gaussian,
 // one of {keep, clone/split, prune} beside the threshold rule of src/densify.rs:125-221):
 // 16 features -> 64 SiLU -> 64 SiLU -> 3 logits -> softmax, BF16 operands on the tensor
-// cores with FP32 accumulation: the inference forward on tcgen05 (accumulators in tensor
-// memory, further down), the training kernels on mma.sync m16n8k16 (their per-warp
-// transposed products want register fragments).
+// cores with FP32 accumulation, in two generations: mma.sync m16n8k16 kernels (forward and
+// gradient, register fragments, below) and tcgen05 kernels (forward and gradient,
+// accumulators in tensor memory, further down), which the trainer runs; both give the same
+// results up to summation order.
 //
 // Parameters are one FP32 vector (the optimiser's master copy): W1 [16][64], b1 [64],
 // W2 [64][64], b2 [64], W3 [64][3], b3 [3] with W[in][out]. Each block rounds them to BF16
@@ -647,6 +648,302 @@ __global__ void __launch_bounds__(kTcRows) mlp_forward_tc_kernel(const float* __
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
   }
 }
+// ---------------------------------------------------------------------------------------
+// The gradient on tcgen05: the forward of a 128-row tile as above with its layer outputs
+// z1, z2, z3 kept in tensor memory, then
+//   dh2 = dz3 W3^T and dh1 = dz2 W2^T     (M = the tile's rows, K-major operands), and
+//   [dW2^T ; dW1^T] = [dz2 | dz1]^T [h1 | x]   and   dW3^T = [. | dz3 | .]^T h2,
+// the weight gradients as two M = 128 products over the tile's rows (K), which read the
+// same shared-memory buffers as MN-major operands: a buffer laid out K-major for one
+// product is, core matrix for core matrix, the MN-major operand of the transposed one.
+// dW2^T and dW1^T are the diagonal blocks of one 128 x 80 product; dW3^T is rows 64-66 of a
+// 128 x 64 one whose A is the dz buffer while dz3 sits in its columns 64-79. Both
+// accumulate in tensor memory over all of the CTA's tiles and reach global memory once.
+// Bias gradients (unrounded dz) go through shared memory. Rounding points are those of the
+// mma.sync kernel and the oracle's bf16 mode.
+// ---------------------------------------------------------------------------------------
+constexpr uint32_t kGradTmemCols = 512;
+constexpr uint32_t kZ1 = 0, kZ2 = 64, kZ3 = 128, kDH = 160, kAcc3 = 224, kAccW = 288;
+constexpr int kXH = 80;   // columns of the [h1 | x] buffer
+constexpr int kDZ = 128;  // columns of the [dz2 | dz1] buffer (dz3 in 64-79 before dz1)
+
+struct TcGradSmem {
+  alignas(1024) unsigned char xh[kTcRows * kXH * 2];
+  alignas(1024) unsigned char h2[kTcRows * kHid * 2];
+  alignas(1024) unsigned char dz[kTcRows * kDZ * 2];
+  alignas(1024) unsigned char w1t[kHid * kIn * 2];   // B of layer 1: [out][in], K = in
+  alignas(1024) unsigned char w2t[kHid * kHid * 2];  // B of layer 2: [out][in]
+  alignas(1024) unsigned char w3t[16 * kHid * 2];    // B of layer 3: [out (16)][in]
+  alignas(1024) unsigned char w2n[kHid * kHid * 2];  // B of dh1 = dz2 W2^T: [in][out], K = out
+  alignas(1024) unsigned char w3n[kHid * 16 * 2];    // B of dh2 = dz3 W3^T: [in][out (16)]
+  float b1[kHid], b2[kHid], b3[16];
+  float gb[kHid + kHid + 16];  // bias gradients: b1, b2, b3
+  alignas(8) uint64_t mbar;
+  uint32_t tmem_base;
+};
+
+__host__ __device__ constexpr uint32_t idesc_bf16_major(uint32_t n, uint32_t a_mn, uint32_t b_mn) {
+  return idesc_bf16(n) | (a_mn << 15) | (b_mn << 16);
+}
+
+__device__ __forceinline__ uint64_t smem_desc_lbo(const void* p, uint32_t lbo, uint32_t sbo) {
+  const uint32_t a = (uint32_t)__cvta_generic_to_shared(p);
+  return (uint64_t)((a >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// Reads 64 accumulator columns from col0 of this thread's row, adds the bias and writes
+// SiLU of the sum, rounded to BF16, to columns 0..63 of a K-major buffer of kdim columns.
+__device__ __forceinline__ void silu_to(unsigned char* buf, int kdim, uint32_t tmem_row, uint32_t col0,
+                                        const float* bias, int row) {
+#pragma unroll
+  for (int c = 0; c < kHid; c += 16) {
+    float v[16];
+    tmem_ld16(tmem_row + col0 + c, v);
+#pragma unroll
+    for (int h = 0; h < 16; h += 8) {
+      uint32_t w[4];
+#pragma unroll
+      for (int i = 0; i < 4; i++)
+        w[i] = pack2(silu(v[h + 2 * i] + bias[c + h + 2 * i]), silu(v[h + 2 * i + 1] + bias[c + h + 2 * i + 1]));
+      *reinterpret_cast<uint4*>(buf + core_off(row, c + h, kdim)) = make_uint4(w[0], w[1], w[2], w[3]);
+    }
+  }
+}
+
+// dz = dh * SiLU'(z + bias) for 64 columns (dh at dh_col, z at z_col of this thread's row),
+// rounded to BF16 into columns col_out.. of the dz buffer; the unrounded dz added to gb.
+__device__ __forceinline__ void dz_to(TcGradSmem& s, uint32_t tmem_row, uint32_t dh_col, uint32_t z_col,
+                                      const float* bias, float* gb, int col_out, int row, bool live) {
+#pragma unroll
+  for (int c = 0; c < kHid; c += 16) {
+    float d[16], z[16];
+    tmem_ld16(tmem_row + dh_col + c, d);
+    tmem_ld16(tmem_row + z_col + c, z);
+#pragma unroll
+    for (int i = 0; i < 16; i++) d[i] *= silu_grad(z[i] + bias[c + i]);
+#pragma unroll
+    for (int h = 0; h < 16; h += 8) {
+      uint32_t w[4];
+#pragma unroll
+      for (int i = 0; i < 4; i++) w[i] = pack2(d[h + 2 * i], d[h + 2 * i + 1]);
+      *reinterpret_cast<uint4*>(s.dz + core_off(row, col_out + c + h, kDZ)) = make_uint4(w[0], w[1], w[2], w[3]);
+    }
+    if (live)
+#pragma unroll
+      for (int i = 0; i < 16; i++) atomicAdd(&gb[c + i], d[i]);
+  }
+}
+
+__global__ void __launch_bounds__(kTcRows) mlp_grad_tc_kernel(const float* __restrict__ x,
+                                                               const int32_t* __restrict__ y,
+                                                               const float* __restrict__ wgt, int64_t n, float scale,
+                                                               const float* __restrict__ th, float* __restrict__ grad,
+                                                               volatile uint32_t* __restrict__ err) {
+  extern __shared__ unsigned char tc_raw[];
+  TcGradSmem& s = *reinterpret_cast<TcGradSmem*>((reinterpret_cast<uintptr_t>(tc_raw) + 1023) & ~(uintptr_t)1023);
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int64_t tiles = (n + kTcRows - 1) / kTcRows;
+  if (tid == 0) {
+    const uint32_t a = (uint32_t)__cvta_generic_to_shared(&s.mbar);
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(a) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    const uint32_t a = (uint32_t)__cvta_generic_to_shared(&s.tmem_base);
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(a), "r"(kGradTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  for (int i = tid; i < kIn * kHid; i += kTcRows) {
+    const int in = i / kHid, out = i % kHid;
+    *reinterpret_cast<bf*>(s.w1t + core_off(out, in, kIn)) = __float2bfloat16_rn(th[kW1 + i]);
+  }
+  for (int i = tid; i < kHid * kHid; i += kTcRows) {
+    const int in = i / kHid, out = i % kHid;
+    const bf v = __float2bfloat16_rn(th[kW2 + i]);
+    *reinterpret_cast<bf*>(s.w2t + core_off(out, in, kHid)) = v;
+    *reinterpret_cast<bf*>(s.w2n + core_off(in, out, kHid)) = v;
+  }
+  for (int i = tid; i < 16 * kHid; i += kTcRows) {
+    const int out = i / kHid, in = i % kHid;
+    const bf v = __float2bfloat16_rn(out < kOut ? th[kW3 + in * kOut + out] : 0.0f);
+    *reinterpret_cast<bf*>(s.w3t + core_off(out, in, kHid)) = v;
+    *reinterpret_cast<bf*>(s.w3n + core_off(in, out, 16)) = v;
+  }
+  if (tid < kHid) {
+    s.b1[tid] = th[kB1 + tid];
+    s.b2[tid] = th[kB2 + tid];
+  }
+  if (tid < 16) s.b3[tid] = tid < kOut ? th[kB3 + tid] : 0.0f;
+  for (int i = tid; i < kHid + kHid + 16; i += kTcRows) s.gb[i] = 0.0f;
+  for (int i = tid; i < kTcRows * kDZ / 8; i += kTcRows) reinterpret_cast<uint4*>(s.dz)[i] = make_uint4(0, 0, 0, 0);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = s.tmem_base;
+  const uint32_t tmem_row = tmem + ((uint32_t)(32 * warp) << 16);
+  bool ok = true, first = true;
+  uint32_t phase = 0;
+  float4 xr[4];
+  int64_t tile = blockIdx.x;
+  if (tile < tiles) load_tile(x, tile, n, xr);
+  // One wait for the MMAs committed by thread 0; the whole block agrees on the outcome.
+#define SPLAT_TC_WAIT()                                          \
+  do {                                                           \
+    ok = !__syncthreads_or(!mbar_wait(&s.mbar, phase));          \
+    if (!ok) goto done;                                          \
+    phase ^= 1u;                                                 \
+    tc_fence_after();                                            \
+  } while (0)
+#define SPLAT_TC_HANDOFF()  \
+  do {                      \
+    async_proxy_fence();    \
+    tc_fence_before();      \
+    __syncthreads();        \
+    tc_fence_after();       \
+  } while (0)
+  for (; tile < tiles; tile += gridDim.x) {
+    const int64_t row_g = tile * kTcRows + tid;
+    const bool live = row_g < n;
+    const int yl = live ? y[row_g] : -1;
+    const float wl = live ? wgt[row_g] * scale : 0.0f;
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const int f = tid + kTcRows * q;
+      *reinterpret_cast<uint2*>(s.xh + core_off(f >> 2, kHid + (f & 3) * 4, kXH)) =
+          make_uint2(pack2(xr[q].x, xr[q].y), pack2(xr[q].z, xr[q].w));
+    }
+    SPLAT_TC_HANDOFF();
+    if (tid == 0) {  // z1 = x W1
+      tc_mma(tmem + kZ1, smem_desc_lbo(s.xh + 8 * 128, 128, kXH / 8 * 128), smem_desc(s.w1t, 256), idesc_bf16(kHid),
+             0u);
+      tc_commit(&s.mbar);
+    }
+    if (tile + gridDim.x < tiles) load_tile(x, tile + gridDim.x, n, xr);
+    SPLAT_TC_WAIT();
+    silu_to(s.xh, kXH, tmem_row, kZ1, s.b1, tid);  // h1 into columns 0-63
+    SPLAT_TC_HANDOFF();
+    if (tid == 0) {  // z2 = h1 W2
+#pragma unroll
+      for (int k = 0; k < 4; k++)
+        tc_mma(tmem + kZ2, smem_desc_lbo(s.xh + 256 * k, 128, kXH / 8 * 128), smem_desc(s.w2t + 256 * k, 1024),
+               idesc_bf16(kHid), k > 0 ? 1u : 0u);
+      tc_commit(&s.mbar);
+    }
+    SPLAT_TC_WAIT();
+    silu_to(s.h2, kHid, tmem_row, kZ2, s.b2, tid);
+    SPLAT_TC_HANDOFF();
+    if (tid == 0) {  // z3 = h2 W3
+#pragma unroll
+      for (int k = 0; k < 4; k++)
+        tc_mma(tmem + kZ3, smem_desc(s.h2 + 256 * k, 1024), smem_desc(s.w3t + 256 * k, 1024), idesc_bf16(16),
+               k > 0 ? 1u : 0u);
+      tc_commit(&s.mbar);
+    }
+    SPLAT_TC_WAIT();
+    {  // softmax and dz3 = (p - onehot(y)) w scale, into dz columns 64-79
+      float v[16];
+      tmem_ld16(tmem_row + kZ3, v);
+      const float z0 = v[0] + s.b3[0], z1 = v[1] + s.b3[1], z2 = v[2] + s.b3[2];
+      const float m = fmaxf(z0, fmaxf(z1, z2));
+      const float e0 = __expf(z0 - m), e1 = __expf(z1 - m), e2 = __expf(z2 - m);
+      const float inv = 1.0f / (e0 + e1 + e2);
+      const float d0 = (e0 * inv - (yl == 0 ? 1.0f : 0.0f)) * wl;
+      const float d1 = (e1 * inv - (yl == 1 ? 1.0f : 0.0f)) * wl;
+      const float d2 = (e2 * inv - (yl == 2 ? 1.0f : 0.0f)) * wl;
+      *reinterpret_cast<uint4*>(s.dz + core_off(tid, kHid, kDZ)) = make_uint4(pack2(d0, d1), pack2(d2, 0.0f), 0u, 0u);
+      *reinterpret_cast<uint4*>(s.dz + core_off(tid, kHid + 8, kDZ)) = make_uint4(0u, 0u, 0u, 0u);
+      if (live) {
+        atomicAdd(&s.gb[2 * kHid], d0);
+        atomicAdd(&s.gb[2 * kHid + 1], d1);
+        atomicAdd(&s.gb[2 * kHid + 2], d2);
+      }
+    }
+    SPLAT_TC_HANDOFF();
+    if (tid == 0) {
+      // dh2 = dz3 W3^T (K = 16 outputs, 3 used)
+      tc_mma(tmem + kDH, smem_desc_lbo(s.dz + 8 * 128, 128, kDZ / 8 * 128), smem_desc(s.w3n, 256), idesc_bf16(kHid),
+             0u);
+      // dW3^T += (dz columns)^T h2 over the tile's rows: A MN-major (M = 128 columns), B MN-major (N = 64)
+#pragma unroll
+      for (int k = 0; k < kTcRows / 16; k++)
+        tc_mma(tmem + kAcc3, smem_desc_lbo(s.dz + 2 * k * (kDZ / 8 * 128), kDZ / 8 * 128, 128),
+               smem_desc_lbo(s.h2 + 2 * k * 1024, 1024, 128), idesc_bf16_major(kHid, 1u, 1u),
+               (first && k == 0) ? 0u : 1u);
+      tc_commit(&s.mbar);
+    }
+    SPLAT_TC_WAIT();
+    dz_to(s, tmem_row, kDH, kZ2, s.b2, s.gb + kHid, 0, tid, live);  // dz2 into columns 0-63
+    SPLAT_TC_HANDOFF();
+    if (tid == 0) {  // dh1 = dz2 W2^T
+#pragma unroll
+      for (int k = 0; k < 4; k++)
+        tc_mma(tmem + kDH, smem_desc_lbo(s.dz + 256 * k, 128, kDZ / 8 * 128), smem_desc(s.w2n + 256 * k, 1024),
+               idesc_bf16(kHid), k > 0 ? 1u : 0u);
+      tc_commit(&s.mbar);
+    }
+    SPLAT_TC_WAIT();
+    dz_to(s, tmem_row, kDH, kZ1, s.b1, s.gb, kHid, tid, live);  // dz1 into columns 64-127
+    SPLAT_TC_HANDOFF();
+    if (tid == 0) {  // [dW2^T ; dW1^T] += [dz2 | dz1]^T [h1 | x]
+#pragma unroll
+      for (int k = 0; k < kTcRows / 16; k++)
+        tc_mma(tmem + kAccW, smem_desc_lbo(s.dz + 2 * k * (kDZ / 8 * 128), kDZ / 8 * 128, 128),
+               smem_desc_lbo(s.xh + 2 * k * (kXH / 8 * 128), kXH / 8 * 128, 128), idesc_bf16_major(kXH, 1u, 1u),
+               (first && k == 0) ? 0u : 1u);
+      tc_commit(&s.mbar);
+    }
+    SPLAT_TC_WAIT();  // the buffers are free for the next tile
+    first = false;
+  }
+  if (!first) {  // this CTA's accumulated weight gradients, once
+    if (warp == 2) {  // dW3^T rows 64-66: lanes 0-2
+#pragma unroll
+      for (int c = 0; c < kHid; c += 16) {
+        float v[16];
+        tmem_ld16(tmem_row + kAcc3 + c, v);
+        const int out = tid - 2 * 32;
+        if (out < kOut)
+#pragma unroll
+          for (int i = 0; i < 16; i++) atomicAdd(&grad[kW3 + (c + i) * kOut + out], v[i]);
+      }
+    }
+    if (warp < 2) {  // dW2^T rows 0-63, columns 0-63
+#pragma unroll
+      for (int c = 0; c < kHid; c += 16) {
+        float v[16];
+        tmem_ld16(tmem_row + kAccW + c, v);
+#pragma unroll
+        for (int i = 0; i < 16; i++) atomicAdd(&grad[kW2 + (c + i) * kHid + tid], v[i]);
+      }
+    } else {  // dW1^T rows 64-127, columns 64-79
+      float v[16];
+      tmem_ld16(tmem_row + kAccW + kHid, v);
+#pragma unroll
+      for (int i = 0; i < 16; i++) atomicAdd(&grad[kW1 + i * kHid + (tid - kHid)], v[i]);
+    }
+    __syncthreads();
+    for (int i = tid; i < kHid; i += kTcRows) {
+      atomicAdd(&grad[kB1 + i], s.gb[i]);
+      atomicAdd(&grad[kB2 + i], s.gb[kHid + i]);
+    }
+    if (tid < kOut) atomicAdd(&grad[kB3 + tid], s.gb[2 * kHid + tid]);
+  }
+done:
+  if (!ok) {
+    mbar_wait(&s.mbar, phase);  // the timed-out MMAs, before their TMEM is freed
+    if (tid == 0) *err = 1u;
+  }
+#undef SPLAT_TC_WAIT
+#undef SPLAT_TC_HANDOFF
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kGradTmemCols) : "memory");
+  }
+}
 }  // namespace
 
 int mlp_num_params() { return kParams; }
@@ -697,6 +994,38 @@ Status launch_mlp_grad(Ctx* c, const float* x, const int32_t* y, const float* w,
   mlp_grad_kernel<<<ceil_div(n, kRows), kThreads, smem, c->stream>>>(x, y, w, n, scale, theta, grad);
   c->launches.count++;
   SPLAT_LAUNCHED("mlp_grad_kernel");
+  return Status::ok();
+}
+
+Status launch_mlp_grad_tc(Ctx* c, const float* x, const int32_t* y, const float* w, int64_t n, float scale,
+                          const float* theta, float* grad, uint32_t* err) {
+  if (n == 0) return Status::ok();
+  const size_t smem = sizeof(TcGradSmem) + 1024;
+  SPLAT_CUDA(cudaFuncSetAttribute(mlp_grad_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int dev = 0, sms = 0;
+  SPLAT_CUDA(cudaGetDevice(&dev));
+  SPLAT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  // One CTA per SM: each holds all 512 tensor-memory columns.
+  const int64_t grid = std::min<int64_t>(ceil_div(n, kTcRows), (int64_t)sms);
+  mlp_grad_tc_kernel<<<(unsigned)grid, kTcRows, smem, c->stream>>>(x, y, w, n, scale, theta, grad, err);
+  c->launches.count++;
+  SPLAT_LAUNCHED("mlp_grad_tc_kernel");
+  return Status::ok();
+}
+
+Status mlp_tc_error_clear(Ctx* c) {
+  volatile uint32_t* h = reinterpret_cast<volatile uint32_t*>(c->host_small) + kTcErrWord;
+  *h = 0u;
+  std::atomic_thread_fence(std::memory_order_seq_cst);
+  return Status::ok();
+}
+
+uint32_t* mlp_tc_error_word(Ctx* c) { return reinterpret_cast<uint32_t*>(c->host_small_dev) + kTcErrWord; }
+
+Status mlp_tc_error_check(Ctx* c) {
+  SPLAT_CUDA(cudaStreamSynchronize(c->stream));
+  volatile uint32_t* h = reinterpret_cast<volatile uint32_t*>(c->host_small) + kTcErrWord;
+  if (*h != 0u) return Status::make(SPLAT_ERR_TIMEOUT, "tcgen05 network kernel: a wait for the tensor cores timed out");
   return Status::ok();
 }
 

@@ -597,13 +597,17 @@ Status learn_from_previous(splat_trainer* t) {
   SPLAT_TRY(launch_gather_training(c, t->rec_x.as<float>(), t->labels.as<int32_t>(), rn, first, stride, w,
                                    t->train_x.as<float>(), t->train_y.as<int32_t>(), t->train_w.as<float>(), m));
   const size_t np = (size_t)mlp_num_params();
+  // 40 Adam steps, the gradients on tcgen05; one check of its timeout word at the end.
+  SPLAT_TRY(mlp_tc_error_clear(c));
   for (int k = 0; k < 40; k++) {
     SPLAT_TRY(launch_fill_u32(c, t->mlp_grad.ptr, np, 0u));
-    SPLAT_TRY(launch_mlp_grad(c, t->train_x.as<float>(), t->train_y.as<int32_t>(), t->train_w.as<float>(), m,
-                              1.0f / (float)m, t->mlp_theta.as<float>(), t->mlp_grad.as<float>()));
+    SPLAT_TRY(launch_mlp_grad_tc(c, t->train_x.as<float>(), t->train_y.as<int32_t>(), t->train_w.as<float>(), m,
+                                 1.0f / (float)m, t->mlp_theta.as<float>(), t->mlp_grad.as<float>(),
+                                 mlp_tc_error_word(c)));
     SPLAT_TRY(launch_mlp_adam(c, t->mlp_theta.as<float>(), t->mlp_grad.as<float>(), t->mlp_m.as<float>(),
                               t->mlp_v.as<float>(), ++t->mlp_steps, 1e-3f));
   }
+  SPLAT_TRY(mlp_tc_error_check(c));
   t->learn_events++;
   t->learn_records += (uint64_t)m;
   for (int k = 0; k < 3; k++) t->label_hist[k] += cnt[k];

@@ -603,13 +603,15 @@ def mlp_forward(ctx: Context, x: torch.Tensor, theta: torch.Tensor, tcgen05: boo
     return prob
 
 
-def mlp_grad(ctx: Context, x, y, w, theta, grad=None):
-    """Gradient of the weighted mean cross-entropy (added into `grad` when given)."""
+def mlp_grad(ctx: Context, x, y, w, theta, grad=None, tcgen05: bool = False):
+    """Gradient of the weighted mean cross-entropy (added into `grad` when given); with
+    `tcgen05` on the 5th-generation tensor cores."""
     x = x.contiguous().float()
     y = y.contiguous().to(torch.int32)
     w = w.contiguous().float()
     if grad is None:
         grad = torch.zeros(int(ctx.lib.splat_mlp_num_params()), dtype=torch.float32, device=x.device)
     scale = 1.0 / float(w.sum().item())
-    check(ctx.lib.splat_mlp_grad(ctx.h, _ptr(x), _ptr(y), _ptr(w), x.shape[0], scale, _ptr(theta), _ptr(grad)), ctx.h)
+    fn = ctx.lib.splat_mlp_grad_tc if tcgen05 else ctx.lib.splat_mlp_grad
+    check(fn(ctx.h, _ptr(x), _ptr(y), _ptr(w), x.shape[0], scale, _ptr(theta), _ptr(grad)), ctx.h)
     return grad

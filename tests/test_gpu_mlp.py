@@ -90,6 +90,35 @@ def test_mlp_gradient_matches_oracle(ctx, n):
         o += k
 
 
+@pytest.mark.parametrize("n", [1, 100, 128, 129, 1000, 40_000])
+def test_mlp_gradient_tcgen05_matches_oracle(ctx, n):
+    """The tcgen05 gradient (layer outputs and weight gradients in tensor memory, the
+    weight gradients as stacked M = 128 products over the rows) against the bf16 oracle and
+    the mma.sync kernel: same rounding points, sums in another order."""
+    theta, x, y, w = _case(80 + n % 97, n)
+    tx, ty, tw, tth = _t(x), _t(y, torch.int32), _t(w), _t(theta)
+    got = G.mlp_grad(ctx, tx, ty, tw, tth, tcgen05=True).cpu().numpy().astype(np.float64)
+    ref = G.mlp_grad(ctx, tx, ty, tw, tth).cpu().numpy().astype(np.float64)
+    m = min(n, 4000)
+    want = M.backward(theta, x[:m], y[:m], w[:m], bf16_like=True) if n <= 4000 else None
+    o = 0
+    for name, shape in M.SIZES:
+        k = int(np.prod(shape))
+        a, r = got[o:o + k], ref[o:o + k]
+        assert np.isfinite(a).all(), name
+        scale = max(np.abs(r).max(), 1e-30)
+        rel_ref = np.abs(a - r).max() / scale
+        msg = f"{name}: rel. vs mma.sync {rel_ref:.2e}"
+        assert rel_ref < 2e-2, msg
+        if want is not None:
+            b = want[o:o + k]
+            rel = np.abs(a - b).max() / max(np.abs(b).max(), 1e-30)
+            msg += f", vs bf16 oracle {rel:.2e}"
+            assert rel < 2e-2, msg
+        print("\n" + msg)
+        o += k
+
+
 def test_mlp_adam_matches_oracle(ctx):
     rng = np.random.default_rng(30)
     theta = rng.normal(0, 1, M.NUM_PARAMS).astype(np.float32)
