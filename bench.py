@@ -634,6 +634,27 @@ def run_mlp(local, rows, reps=20):
         ms = e0.elapsed_time(e1) / reps
         out[name] = {"ms": round(ms, 4), "tflops": round(out["flop_per_row"] * rows / ms / 1e9, 2),
                      "gbs": round(out["bytes_per_row"] * rows / ms / 1e6, 1)}
+    # The gradient over the same rows (labels and weights drawn alike): forward and backward,
+    # 3 x the forward's multiply-adds per row.
+    yl = torch.from_numpy(rng.integers(0, 3, rows).astype(np.int32)).to(dev)
+    wl = torch.from_numpy(rng.uniform(0.2, 2.0, rows).astype(np.float32)).to(dev)
+    grad = torch.zeros(int(M.NUM_PARAMS), dtype=torch.float32, device=dev)
+    out["grad_flop_per_row"] = 3 * out["flop_per_row"]
+    for name, tc in (("grad_tcgen05", True), ("grad_mma_sync", False)):
+        fn = ctx.lib.splat_mlp_grad_tc if tc else ctx.lib.splat_mlp_grad
+        call = lambda: G.check(fn(ctx.h, G._ptr(x), G._ptr(yl), G._ptr(wl), rows, 1.0 / rows, G._ptr(th),
+                                  G._ptr(grad)), ctx.h)
+        for _ in range(3):
+            call()
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            call()
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        ms = e0.elapsed_time(e1) / reps
+        out[name] = {"ms": round(ms, 4), "tflops": round(out["grad_flop_per_row"] * rows / ms / 1e9, 2)}
     ctx.close()
     return out
 

@@ -678,6 +678,7 @@ struct TcGradSmem {
   alignas(1024) unsigned char w3n[kHid * 16 * 2];    // B of dh2 = dz3 W3^T: [in][out (16)]
   float b1[kHid], b2[kHid], b3[16];
   float gb[kHid + kHid + 16];  // bias gradients: b1, b2, b3
+  float f[kTcRows][kHid + 1];  // a tile's unrounded dz2 or dz1, for the column sums of the bias gradients
   alignas(8) uint64_t mbar;
   uint32_t tmem_base;
 };
@@ -712,9 +713,10 @@ __device__ __forceinline__ void silu_to(unsigned char* buf, int kdim, uint32_t t
 }
 
 // dz = dh * SiLU'(z + bias) for 64 columns (dh at dh_col, z at z_col of this thread's row),
-// rounded to BF16 into columns col_out.. of the dz buffer; the unrounded dz added to gb.
+// rounded to BF16 into columns col_out.. of the dz buffer; the unrounded dz into row `row`
+// of the staging tile f (a row past the batch has dz = 0: its weight is 0).
 __device__ __forceinline__ void dz_to(TcGradSmem& s, uint32_t tmem_row, uint32_t dh_col, uint32_t z_col,
-                                      const float* bias, float* gb, int col_out, int row, bool live) {
+                                      const float* bias, int col_out, int row) {
 #pragma unroll
   for (int c = 0; c < kHid; c += 16) {
     float d[16], z[16];
@@ -729,10 +731,19 @@ __device__ __forceinline__ void dz_to(TcGradSmem& s, uint32_t tmem_row, uint32_t
       for (int i = 0; i < 4; i++) w[i] = pack2(d[h + 2 * i], d[h + 2 * i + 1]);
       *reinterpret_cast<uint4*>(s.dz + core_off(row, col_out + c + h, kDZ)) = make_uint4(w[0], w[1], w[2], w[3]);
     }
-    if (live)
 #pragma unroll
-      for (int i = 0; i < 16; i++) atomicAdd(&gb[c + i], d[i]);
+    for (int i = 0; i < 16; i++) s.f[row][c + i] = d[i];
   }
+}
+
+// This thread's share of the staging tile's column sums: column tid % 64 over half of the
+// rows (conflict-free: the tile's rows are 65 floats apart).
+__device__ __forceinline__ float column_half_sum(const TcGradSmem& s, int tid) {
+  const int col = tid & (kHid - 1), r0 = (tid >> 6) * (kTcRows / 2);
+  float acc = 0.0f;
+#pragma unroll 8
+  for (int r = 0; r < kTcRows / 2; r++) acc += s.f[r0 + r][col];
+  return acc;
 }
 
 __global__ void __launch_bounds__(kTcRows) mlp_grad_tc_kernel(const float* __restrict__ x,
@@ -785,6 +796,7 @@ __global__ void __launch_bounds__(kTcRows) mlp_grad_tc_kernel(const float* __res
   const uint32_t tmem_row = tmem + ((uint32_t)(32 * warp) << 16);
   bool ok = true, first = true;
   uint32_t phase = 0;
+  float gacc1 = 0.0f, gacc2 = 0.0f;  // this thread's share of the b1 and b2 gradients
   float4 xr[4];
   int64_t tile = blockIdx.x;
   if (tile < tiles) load_tile(x, tile, n, xr);
@@ -854,10 +866,17 @@ __global__ void __launch_bounds__(kTcRows) mlp_grad_tc_kernel(const float* __res
       const float d2 = (e2 * inv - (yl == 2 ? 1.0f : 0.0f)) * wl;
       *reinterpret_cast<uint4*>(s.dz + core_off(tid, kHid, kDZ)) = make_uint4(pack2(d0, d1), pack2(d2, 0.0f), 0u, 0u);
       *reinterpret_cast<uint4*>(s.dz + core_off(tid, kHid + 8, kDZ)) = make_uint4(0u, 0u, 0u, 0u);
-      if (live) {
-        atomicAdd(&s.gb[2 * kHid], d0);
-        atomicAdd(&s.gb[2 * kHid + 1], d1);
-        atomicAdd(&s.gb[2 * kHid + 2], d2);
+      float r0 = d0, r1 = d1, r2 = d2;  // b3 gradient: the warp's sums, one atomic each
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        r0 += __shfl_xor_sync(0xffffffffu, r0, o);
+        r1 += __shfl_xor_sync(0xffffffffu, r1, o);
+        r2 += __shfl_xor_sync(0xffffffffu, r2, o);
+      }
+      if ((tid & 31) == 0) {
+        atomicAdd(&s.gb[2 * kHid], r0);
+        atomicAdd(&s.gb[2 * kHid + 1], r1);
+        atomicAdd(&s.gb[2 * kHid + 2], r2);
       }
     }
     SPLAT_TC_HANDOFF();
@@ -874,7 +893,7 @@ __global__ void __launch_bounds__(kTcRows) mlp_grad_tc_kernel(const float* __res
       tc_commit(&s.mbar);
     }
     SPLAT_TC_WAIT();
-    dz_to(s, tmem_row, kDH, kZ2, s.b2, s.gb + kHid, 0, tid, live);  // dz2 into columns 0-63
+    dz_to(s, tmem_row, kDH, kZ2, s.b2, 0, tid);  // dz2 into columns 0-63
     SPLAT_TC_HANDOFF();
     if (tid == 0) {  // dh1 = dz2 W2^T
 #pragma unroll
@@ -883,8 +902,9 @@ __global__ void __launch_bounds__(kTcRows) mlp_grad_tc_kernel(const float* __res
                idesc_bf16(kHid), k > 0 ? 1u : 0u);
       tc_commit(&s.mbar);
     }
+    gacc2 += column_half_sum(s, tid);  // while the MMAs run
     SPLAT_TC_WAIT();
-    dz_to(s, tmem_row, kDH, kZ1, s.b1, s.gb, kHid, tid, live);  // dz1 into columns 64-127
+    dz_to(s, tmem_row, kDH, kZ1, s.b1, kHid, tid);  // dz1 into columns 64-127
     SPLAT_TC_HANDOFF();
     if (tid == 0) {  // [dW2^T ; dW1^T] += [dz2 | dz1]^T [h1 | x]
 #pragma unroll
@@ -894,6 +914,7 @@ __global__ void __launch_bounds__(kTcRows) mlp_grad_tc_kernel(const float* __res
                (first && k == 0) ? 0u : 1u);
       tc_commit(&s.mbar);
     }
+    gacc1 += column_half_sum(s, tid);
     SPLAT_TC_WAIT();  // the buffers are free for the next tile
     first = false;
   }
@@ -923,6 +944,8 @@ __global__ void __launch_bounds__(kTcRows) mlp_grad_tc_kernel(const float* __res
 #pragma unroll
       for (int i = 0; i < 16; i++) atomicAdd(&grad[kW1 + i * kHid + (tid - kHid)], v[i]);
     }
+    atomicAdd(&s.gb[tid & (kHid - 1)], gacc1);
+    atomicAdd(&s.gb[kHid + (tid & (kHid - 1))], gacc2);
     __syncthreads();
     for (int i = tid; i < kHid; i += kTcRows) {
       atomicAdd(&grad[kB1 + i], s.gb[i]);
