@@ -170,6 +170,10 @@ SPLAT_API int splat_ctx_synchronize(splat_ctx* ctx);
 SPLAT_API const char* splat_last_error(const splat_ctx* ctx);
 SPLAT_API const char* splat_status_string(int status);
 SPLAT_API int splat_version(void);
+/* sizeof of the public structs, for bindings to check their layouts against: splat_camera,
+ * splat_proj_opts, splat_lr, splat_densify_config, splat_train_config,
+ * splat_densify_report, splat_step_info (7 values written to out; returns 7). */
+SPLAT_API int32_t splat_struct_sizes(uint64_t* out);
 /* Kernels launched through this context since creation (all stage entry points count). */
 SPLAT_API uint64_t splat_ctx_launch_count(const splat_ctx* ctx);
 

@@ -154,6 +154,7 @@ def _declare(L):
         "splat_bin_count_noalloc": ([vp, vp, i64, vp, P(i64)], C.c_int),
         "splat_bin_sort": ([vp, vp, vp, i64, i64, vp, u32, u32, vp, vp, vp], C.c_int),
         "splat_bin_count_device": ([vp, vp, i64, vp, vp], C.c_int),
+        "splat_struct_sizes": ([P(C.c_uint64)], i32),
         "splat_mlp_num_params": ([], i32),
         "splat_mlp_forward": ([vp, vp, i64, vp, vp], C.c_int),
         "splat_mlp_forward_tc": ([vp, vp, i64, vp, vp], C.c_int),

@@ -109,6 +109,16 @@ extern "C" {
 
 SPLAT_API int splat_version(void) { return 1; }
 
+SPLAT_API int32_t splat_struct_sizes(uint64_t* out) {
+  const uint64_t sizes[] = {sizeof(splat_camera),         sizeof(splat_proj_opts),      sizeof(splat_lr),
+                            sizeof(splat_densify_config), sizeof(splat_train_config),   sizeof(splat_densify_report),
+                            sizeof(splat_step_info)};
+  const int32_t k = (int32_t)(sizeof(sizes) / sizeof(sizes[0]));
+  if (out)
+    for (int32_t i = 0; i < k; i++) out[i] = sizes[i];
+  return k;
+}
+
 SPLAT_API const char* splat_status_string(int status) {
   switch (status) {
     case SPLAT_OK: return "ok";

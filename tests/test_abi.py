@@ -37,3 +37,16 @@ def test_context_creation_fails_cleanly_without_device():
     h = C.c_void_p()
     st = L.splat_ctx_create(0, None, C.byref(h))
     assert st == _lib.SPLAT_ERR_CUDA and not h.value
+
+
+def test_struct_layouts_match_the_library():
+    """The ctypes mirrors of the public structs have the sizes the library was compiled
+    with (a field added on one side only shows here)."""
+    L = _lib.lib()
+    out = (C.c_uint64 * 16)()
+    k = L.splat_struct_sizes(out)
+    mirrors = [_lib.Camera, _lib.ProjOpts, _lib.LearningRates, _lib.DensifyConfig, _lib.TrainConfig,
+               _lib.DensifyReport, _lib.StepInfo]
+    assert k == len(mirrors)
+    for i, m in enumerate(mirrors):
+        assert C.sizeof(m) == out[i], (m.__name__, C.sizeof(m), out[i])
