@@ -503,26 +503,49 @@ def run_train_cpu(init, views, extent, cfg, iterations):
 
 def cpu_reference_steps(args, steps):
     """The CPU oracle (the reference's hot path restated in C++, all host threads) on the
-    same workload: `steps` full forward+backward passes of the 1920x1080 view."""
+    same workload: `steps` full forward+backward passes of the 1920x1080 view. Returns the
+    mean seconds per step, the threads used and a per-stage breakdown (as the reference's
+    examples/profile.rs reports it) with the compositing cost in ns per pair per core, over
+    the pairs that pass the alpha threshold: the unit of the reference's published figures
+    (README.md:153: ~15 ns forward, ~25 ns backward)."""
     from oracle import oracle as O
     from splatrs_b200 import scenes
     s = scenes.config1(n=args.n)
     p, cam, dimage = s["params"], s["cam"], s["dimage"]
     bg = np.zeros(3, np.float32)
+    names = ("project", "bin", "raster_fwd", "raster_bwd", "project_bwd")
+    acc = dict.fromkeys(names, 0.0)
+    passed = [0, 0]
 
-    def one():
+    def one(record):
+        t = [time.perf_counter()]
         projs = O.project_all(p, cam, sh_degree=3)
+        t.append(time.perf_counter())
         b = O.bin(projs, WIDTH, HEIGHT)
+        t.append(time.perf_counter())
         img, ft, nc, _ = O.rasterize_forward(projs, b, WIDTH, HEIGHT, bg)
+        t.append(time.perf_counter())
         g, a, _ = O.rasterize_backward(projs, b, WIDTH, HEIGHT, bg, ft, nc, dimage)
+        t.append(time.perf_counter())
         O.project_backward_all(p, cam, g, sh_degree=3)
+        t.append(time.perf_counter())
+        if record:
+            for k, nm in enumerate(names):
+                acc[nm] += t[k + 1] - t[k]
+            passed[:] = O.last_passed_pairs()
 
-    one()  # warm caches and thread pool
-    t = time.perf_counter()
+    one(False)  # warm caches and thread pool
+    t0 = time.perf_counter()
     for _ in range(steps):
-        one()
-    dt = (time.perf_counter() - t) / steps
-    return dt, O.threads()
+        one(True)
+    dt = (time.perf_counter() - t0) / steps
+    cores = O.threads()
+    ms = {nm: round(acc[nm] / steps * 1e3, 2) for nm in names}
+    detail = {"stages_ms": ms, "passed_pairs": {"forward": passed[0], "backward": passed[1]},
+              "ns_per_pair_core": {"forward": round(ms["raster_fwd"] * 1e6 * cores / max(passed[0], 1), 2),
+                                   "backward": round(ms["raster_bwd"] * 1e6 * cores / max(passed[1], 1), 2),
+                                   "reference_published": {"forward": 15, "backward": 25}}}
+    return dt, cores, detail
 
 
 ADAM_BYTES = 4 * 240 + 3 * 240            # params, grads, m, v read; params, m, v written (60 floats padded)
@@ -715,7 +738,7 @@ def main():
     if args.impl == "reference":
         if rank == 0:
             steps = max(1, args.steps if args.steps <= 5 else 3)
-            dt, cores = cpu_reference_steps(args, steps)
+            dt, cores, detail = cpu_reference_steps(args, steps)
             v = WIDTH * HEIGHT / 1e6 / dt
             line = {"impl": "reference", "metric": METRIC, "value": round(v, 4), "unit": UNIT, "n_gpus": world,
                     "steps": steps, "warmup": 1, "ms_per_step": round(dt * 1e3, 2), "higher_is_better": True,
@@ -723,7 +746,7 @@ def main():
                     "data": "synthetic (seeded; config-1 distributions)",
                     "config": {"workload": WORKLOAD, "gaussians": args.n, "width": WIDTH, "height": HEIGHT},
                     "cpu_baseline": {"value": round(v, 4), "unit": UNIT, "cores": cores, "kind": "port",
-                                     "sample": f"{steps} full fwd+bwd steps of the workload"},
+                                     "sample": f"{steps} full fwd+bwd steps of the workload", **detail},
                     "e2e": {"value": round(v, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
             print(json.dumps(line), flush=True)
         if world > 1:
@@ -765,9 +788,10 @@ def main():
         if c0 is not None and not args.no_cpu_baseline and world == 1:
             line["train_c0"]["cpu"] = run_train_cpu(*c0, C0_TRAIN, C0_TRAIN["iterations"])
         if not args.no_cpu_baseline and world == 1:
-            dt, cores = cpu_reference_steps(args, args.cpu_steps)
+            dt, cores, detail = cpu_reference_steps(args, args.cpu_steps)
             line["cpu_baseline"] = {"value": round(WIDTH * HEIGHT / 1e6 / dt, 4), "unit": UNIT, "cores": cores,
-                                    "kind": "port", "sample": f"{args.cpu_steps} full fwd+bwd steps of the workload"}
+                                    "kind": "port", "sample": f"{args.cpu_steps} full fwd+bwd steps of the workload",
+                                    **detail}
         elif world > 1:
             line["cpu_baseline"] = None
         print(json.dumps(line), flush=True)

@@ -75,6 +75,8 @@ def _declare(L):
         f = getattr(L, f"ora_sigmoid_{s}"); f.argtypes = [R]; f.restype = R
         f = getattr(L, f"ora_inverse_sigmoid_{s}"); f.argtypes = [R]; f.restype = R
     L.ora_threads.restype = ci
+    L.ora_last_passed_pairs.argtypes = [vp]
+    L.ora_last_passed_pairs.restype = None
     L.ora_set_threads.argtypes = [ci]
     L.ora_set_cr_math.argtypes = [ci]
     for nm in ("ora_expf", "ora_logf", "ora_expf_cr", "ora_logf_cr"):
@@ -264,6 +266,15 @@ def rasterize_backward(projs, binning, width, height, background, final_t, n_con
         _p(p), n, binning.h, width, height, _p(_arr(background, dt)), _p(_arr(final_t, dt)),
         _p(np.ascontiguousarray(n_contrib, np.uint32)), _p(_arr(dimage, dt)), _p(g), _p(a), _p(pairs))
     return g, a, int(pairs[0])
+
+
+def last_passed_pairs():
+    """(forward, backward) pairs that passed the alpha threshold in the last
+    rasterize_forward / rasterize_backward call: the unit of the reference's published
+    per-core cost (README.md:153)."""
+    out = np.zeros(2, np.uint64)
+    lib().ora_last_passed_pairs(_p(out))
+    return int(out[0]), int(out[1])
 
 
 def naive_render(projs, width, height, background, dtype=np.float32):

@@ -363,6 +363,10 @@ template <class R> Binning* do_bin(const R* p15, int64_t n, uint32_t w, uint32_t
   return b;
 }
 
+// Pairs that passed the alpha threshold in the last forward and backward call (read by
+// ora_last_passed_pairs; calls are not expected to overlap).
+static std::atomic<uint64_t> g_last_passed[2];
+
 template <class R> void do_raster_fwd(const R* p15, int64_t n, const Binning* b, uint32_t w, uint32_t h, const R* bg,
                                       R* image, R* final_t, uint32_t* n_contrib, uint64_t* pairs) {
   std::vector<Proj<R>> projs = projs_from(p15, n);
@@ -374,6 +378,7 @@ template <class R> void do_raster_fwd(const R* p15, int64_t n, const Binning* b,
   std::memcpy(final_t, out.final_t.data(), out.final_t.size() * sizeof(R));
   std::memcpy(n_contrib, out.n_contrib.data(), out.n_contrib.size() * sizeof(uint32_t));
   if (pairs) *pairs = cnt.pairs_fwd.load();
+  g_last_passed[0] = cnt.passed_fwd.load();
 }
 
 template <class R> void do_raster_bwd(const R* p15, int64_t n, const Binning* b, uint32_t w, uint32_t h, const R* bg,
@@ -401,6 +406,7 @@ template <class R> void do_raster_bwd(const R* p15, int64_t n, const Binning* b,
     d[8] = g[i].color[2];
   }
   if (pairs) *pairs = cnt.pairs_bwd.load();
+  g_last_passed[1] = cnt.passed_bwd.load();
 }
 
 template <class R> int64_t do_densify(const R* params, const R* m, const R* v, int64_t n0, const R* grad_accum,
@@ -451,6 +457,10 @@ template <class R> int64_t do_densify(const R* params, const R* m, const R* v, i
 #define ORA_API extern "C" __attribute__((visibility("default")))
 
 ORA_API int ora_threads(void) { return num_threads(); }
+ORA_API void ora_last_passed_pairs(uint64_t* out2) {
+  out2[0] = g_last_passed[0].load();
+  out2[1] = g_last_passed[1].load();
+}
 ORA_API void ora_set_threads(int n) { set_num_threads(n); }
 ORA_API void ora_set_cr_math(int on) { Math::cr = on != 0; }
 ORA_API float ora_expf(float x) { return rexp(x); }

@@ -82,6 +82,17 @@ def test_render_golden_covers_edge_cases(render_golden):
     assert (d["n_contrib"] > 0).mean() > 0.5 and int(d["pairs"]) > 0 and int(d["bwd_pairs"]) > 0
 
 
+def test_passed_pair_counters(render_golden):
+    """The counters behind the CPU baseline's ns per pair per core: pairs passing the alpha
+    threshold are a subset of the evaluated ones; the backward walks only entries before a
+    pixel's last contributor, so it never passes more than the forward."""
+    inp = {k: render_golden[k] for k in RENDER_INPUTS}
+    MG.render_outputs(inp)
+    fwd, bwd = O.last_passed_pairs()
+    assert 0 < bwd <= fwd <= int(render_golden["pairs"])
+    assert bwd <= int(render_golden["bwd_pairs"])
+
+
 def test_oracle_reproduces_mlp_golden():
     """The network oracle (bf16 mode) on the fixture's rows: probabilities and gradient as
     stored, to float64 rounding (numpy's exp may differ by an ulp between CPUs)."""
