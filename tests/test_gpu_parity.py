@@ -131,6 +131,50 @@ def test_binning_large_single_view(ctx):
     assert (b.tile_range.cpu().numpy().view(np.uint32) == a["tile_range"]).all()
 
 
+def test_render_benchmark_workload_matches_oracle(ctx, cr_math):
+    """The render benchmark's workload at full size (1M Gaussians, 1920x1080, SH degree 3,
+    dL/dpix ~ N(0,1)), stage by stage against the correctly rounded oracle: projections
+    bit-identical; fed the oracle's projections, image, final T, contributor counts and
+    evaluated pairs bit-identical, screen-space gradients within 1e-3 of each quantity's
+    scale; fed the oracle's screen-space gradients, the 59 parameter gradients
+    bit-identical."""
+    s = scenes.config1(n=1_000_000)
+    g, cam, dimage = s["params"], s["cam"], s["dimage"]
+    w, h, n = 1920, 1080, g.shape[0]
+    bg = np.zeros(3, np.float32)
+    p = O.project_all(g, cam, sh_degree=3)
+    planes, gproj = gpu_project(ctx, g, cam, sh_degree=3)
+    mism = (bits(gproj.to_reference(ctx).cpu().numpy()) != bits(p)).any(1)
+    assert mism.sum() == 0, f"{mism.sum()} projections differ, first {np.nonzero(mism)[0][:5]}"
+    ob = O.bin(p, w, h)
+    img, ft, nc, pairs = O.rasterize_forward(p, ob, w, h, bg)
+    og, oa, bpairs = O.rasterize_backward(p, ob, w, h, bg, ft, nc, dimage)
+    proj = G.proj_from_reference(ctx, dev(p), w, h)
+    b = G.bin(ctx, proj)
+    assert b.num_entries == ob.num_entries
+    out = G.rasterize_forward(ctx, proj, b, bg)
+    assert (bits(out.image.cpu().numpy()) == bits(img)).all()
+    assert (bits(out.final_t.cpu().numpy()) == bits(ft)).all()
+    assert (out.n_contrib.cpu().numpy().view(np.uint32) == nc).all()
+    assert int(out.pairs.item()) == pairs
+    tp = torch.zeros(1, dtype=torch.int64, device="cuda")
+    pg = G.rasterize_backward(ctx, proj, b, bg, out, dev(dimage), pairs=tp)
+    gg, ga = G.pgrad_to_reference(pg, n)
+    gg, ga = gg.cpu().numpy(), ga.cpu().numpy()
+    assert int(tp.item()) == bpairs
+    err = grad_rel_error(gg, og)
+    assert err.max() < 1e-3, err
+    assert grad_rel_error(ga, oa).max() < 1e-3
+    gp = G.project_backward_all(ctx, planes, n, n, Camera.from_record(cam), ProjOpts.make(sh_degree=3), gproj,
+                                G.pgrad_from_reference(dev(og)))
+    got = G.planes_to_params(ctx, gp, n, n).cpu().numpy()
+    want = O.project_backward_all(g, cam, og, sh_degree=3)
+    mism = (bits(got) != bits(want)).any(1)
+    assert mism.sum() == 0, f"{mism.sum()} gradient records differ, first {np.nonzero(mism)[0][:5]}"
+    print(f"\n1M / 1080p: {ob.num_entries} entries, {pairs} forward and {bpairs} backward pairs, "
+          f"screen-space gradient error {err.max():.2e} of scale")
+
+
 @pytest.mark.parametrize("seed,size", [(8, (320, 240)), (9, (1024, 64)), (10, (1920, 1080))])
 def test_device_driven_binning_equals_host_driven(ctx, seed, size):
     """splat_bin_count_device + splat_bin_sort_device (no host read-back, capacity-sized
