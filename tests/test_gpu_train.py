@@ -41,10 +41,11 @@ def from_planes(ctx, planes, n, cap):
 
 
 @pytest.mark.parametrize("w,h,lam,u8", [(64, 48, 0.2, True), (97, 53, 0.2, False), (320, 240, 0.8, True),
-                                        (16, 12, 1.0, False)])
+                                        (16, 12, 1.0, False), (1297, 840, 0.2, True), (1600, 1200, 0.2, True)])
 def test_loss_matches_oracle(ctx, w, h, lam, u8):
     """photometric_loss: gradient bit-identical (same blur order, same formulas); loss and
-    PSNR to summation-order rounding."""
+    PSNR to summation-order rounding. The last two sizes are the training workloads' views
+    (1297x840; the largest mixed-size view, 1600x1200)."""
     rng = np.random.default_rng(w * h)
     pred = rng.uniform(-0.1, 1.1, w * h * 3).astype(np.float32)
     if u8:
@@ -75,10 +76,11 @@ def test_ssim_identity_on_device(ctx):
     assert np.abs(grad.cpu().numpy()).max() < 1e-3
 
 
-def test_adam_bit_exact(ctx):
-    """Adam::step over five steps: parameters and moments bit-identical to the oracle."""
+@pytest.mark.parametrize("n", [3000, 500_000])
+def test_adam_bit_exact(ctx, n):
+    """Adam::step over five steps: parameters and moments bit-identical to the oracle (500k:
+    the training workload's initial model size)."""
     rng = np.random.default_rng(7)
-    n = 3000
     p = rng.normal(0, 1, (n, 59)).astype(np.float32)
     p_o = p.copy()
     m_o = np.zeros_like(p)
