@@ -88,6 +88,7 @@ def _declare(L):
     L.ora_mean_nn_dist2.argtypes = [vp, i64, vp]
     L.ora_splitmix_next.argtypes = [vp]; L.ora_splitmix_next.restype = u64
     L.ora_splitmix_normal.argtypes = [vp]; L.ora_splitmix_normal.restype = cd
+    L.ora_splitmix_normals.argtypes = [vp, i64, vp]; L.ora_splitmix_normals.restype = None
     L.ora_train_config_fields.restype = C.c_char_p
     L.ora_trainer_new.argtypes = [vp, i64, cf, vp]; L.ora_trainer_new.restype = vp
     L.ora_trainer_add_view.argtypes = [vp, vp, vp]
@@ -266,6 +267,14 @@ def rasterize_backward(projs, binning, width, height, background, final_t, n_con
         _p(p), n, binning.h, width, height, _p(_arr(background, dt)), _p(_arr(final_t, dt)),
         _p(np.ascontiguousarray(n_contrib, np.uint32)), _p(_arr(dimage, dt)), _p(g), _p(a), _p(pairs))
     return g, a, int(pairs[0])
+
+
+def splitmix_normals(state, count):
+    """`count` normals of the shared SplitMix64 generator; `state` (np.uint64 array of
+    one) advances as by `count` single draws."""
+    out = np.zeros(count, np.float64)
+    lib().ora_splitmix_normals(_p(state), count, _p(out))
+    return out
 
 
 def last_passed_pairs():

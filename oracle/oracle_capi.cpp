@@ -623,6 +623,13 @@ ORA_API double ora_splitmix_normal(uint64_t* state) {
   *state = r.s;
   return v;
 }
+// `count` successive normals of the generator (the same values ora_splitmix_normal returns
+// one by one).
+ORA_API void ora_splitmix_normals(uint64_t* state, int64_t count, double* out) {
+  SplitMix64 r(*state);
+  for (int64_t i = 0; i < count; i++) out[i] = r.normal();
+  *state = r.s;
+}
 
 // ---------------------------------------------------------------------------------------
 // Trainer (float only). The config is passed field by field through an array of doubles

@@ -120,7 +120,16 @@ def test_densify_bit_exact(ctx, cr_math, opts):
     """densify_and_prune with the same generator state: counts, order and every
     parameter and moment bit-identical to the oracle (with the correctly rounded exp the
     kernels use for the scales); the generator advances identically."""
-    g, m, v, accum, denom, maxr = densify_case(5)
+    _densify_bit_exact(ctx, opts, 5, 4000)
+
+
+def test_densify_bit_exact_training_size(ctx, cr_math):
+    """The same at the training workload's initial model size (500k Gaussians)."""
+    _densify_bit_exact(ctx, {}, 15, 500_000)
+
+
+def _densify_bit_exact(ctx, opts, seed_case, n_case):
+    g, m, v, accum, denom, maxr = densify_case(seed_case, n_case)
     n = g.shape[0]
     extent = 4.4
     cfg = dict(grad_threshold=0.0002, percent_dense=0.01, min_opacity=0.005, prune_big_world=False,
@@ -135,7 +144,7 @@ def test_densify_bit_exact(ctx, cr_math, opts):
                                                        n, stats, DensifyConfig.make(**cfg), extent, seed)
     # The oracle draws from the same generator.
     state = np.array([seed], np.uint64)
-    normals = np.array([O.lib().ora_splitmix_normal(state.ctypes.data) for _ in range(6 * n)])
+    normals = O.splitmix_normals(state, 6 * n)
     op, om, ov, orep = O.densify_and_prune(g, m, v, accum, denom, maxr, extent, normals, **cfg)
     assert (rep.cloned, rep.split, rep.pruned) == orep[:3]
     assert rep.new_count == op.shape[0]
@@ -145,8 +154,7 @@ def test_densify_bit_exact(ctx, cr_math, opts):
     assert np.array_equal(from_planes(ctx, mo, k, cap_out), om)
     assert np.array_equal(from_planes(ctx, vo, k, cap_out), ov)
     s2 = np.array([seed], np.uint64)
-    for _ in range(orep[3]):
-        O.lib().ora_splitmix_normal(s2.ctypes.data)
+    O.splitmix_normals(s2, orep[3])
     assert st == int(s2[0])
 
 

@@ -163,3 +163,13 @@ def test_psnr_clamps_and_handles_identity():
     c = np.array([0.4, 1.0, 0.0], np.float32)
     mse = (np.float64(np.float32(0.5)) - np.float64(np.float32(0.4))) ** 2 / 3
     assert abs(O.psnr(a, c) - (-10 * math.log10(mse))) < 1e-4
+
+
+def test_splitmix_bulk_equals_single_draws():
+    """The bulk generator used by the densification parity tests draws the same normals,
+    and leaves the same state, as single draws."""
+    s1 = np.array([1234], np.uint64)
+    one = np.array([O.lib().ora_splitmix_normal(s1.ctypes.data) for _ in range(1000)])
+    s2 = np.array([1234], np.uint64)
+    bulk = O.splitmix_normals(s2, 1000)
+    assert np.array_equal(one, bulk) and s1[0] == s2[0]
