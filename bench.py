@@ -46,22 +46,22 @@ def parse():
     ap.add_argument("--raster", default="auto",
                     help="compositing configuration: 'auto' (autotune) or TWxTHxCHUNK[/PIXELS_PER_THREAD], "
                          "e.g. 16x16x256/2")
-    ap.add_argument("--no-train", action="store_true", help="skip the config-0 training run")
-    ap.add_argument("--train-c2", action="store_true",
+    ap.add_argument("--no-train", action="store_true", help="skip the small-scene training run (10k-Gaussian blobs, 256x256 views)")
+    ap.add_argument("--train-shells", action="store_true",
                     help="also run plain training on the clustered 500k-Gaussian multi-view scene")
-    ap.add_argument("--train-c2-iters", type=int, default=0, help="iterations of that run (default: all 30,000)")
-    ap.add_argument("--c2-cpu-iters", type=int, default=5, help="iterations of its CPU oracle sample")
-    ap.add_argument("--train-c3", action="store_true",
+    ap.add_argument("--train-shells-iters", type=int, default=0, help="iterations of that run (default: all 30,000)")
+    ap.add_argument("--shells-cpu-iters", type=int, default=5, help="iterations of its CPU oracle sample")
+    ap.add_argument("--train-batched", action="store_true",
                     help="batched mixed-size BF16 training on the same scene (8 views per step)")
-    ap.add_argument("--train-c3-iters", type=int, default=0, help="steps of that run (default: all 3,750)")
-    ap.add_argument("--train-c4", action="store_true",
+    ap.add_argument("--train-batched-iters", type=int, default=0, help="steps of that run (default: all 3,750)")
+    ap.add_argument("--train-learned", action="store_true",
                     help="learned densification: learn on scene seeds 2-5, compare with the rule on seed 6")
-    ap.add_argument("--c4-learn-iters", type=int, default=1875, help="steps of each learning run")
+    ap.add_argument("--learn-iters", type=int, default=1875, help="steps of each learning run")
     ap.add_argument("--profile-mlp", action="store_true",
                     help="only the densification network's forward (tcgen05) on 4M rows, for an ncu capture")
     ap.add_argument("--mlp-rows", type=int, default=4_000_000)
     ap.add_argument("--profile-train", action="store_true",
-                    help="only a short config-2 training run (20 views, 300 iterations) for an ncu launch list; "
+                    help="only a short shell-scene training run (20 views, 300 iterations) for an ncu launch list; "
                          "prints the launches before its last 100 iterations")
     ap.add_argument("--profile-small", action="store_true",
                     help="a reduced case for ncu captures (fewer Gaussians, one step)")
@@ -174,7 +174,7 @@ def run_ours(args, rank, world, local):
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     n = args.n
-    s = scenes.config1(n=n)
+    s = scenes.render_benchmark_scene(n=n)
     cam = Camera.from_record(s["cam"])
     opts = ProjOpts.make(sh_degree=3)
     bg = s["background"]
@@ -340,7 +340,7 @@ def run_ours(args, rank, world, local):
     line = {
         "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4), "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded; config-1 distributions)",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded; 1M Gaussians uniform in a 10 m cube)",
         "config": {"workload": WORKLOAD, "gaussians": n, "width": WIDTH, "height": HEIGHT,
                    "tile": [raster[0], raster[1]], "chunk": raster[2], "bwd_pixels_per_thread": raster[3],
                    "raster": "autotuned" if tuning else "fixed",
@@ -357,22 +357,22 @@ def run_ours(args, rank, world, local):
     return line
 
 
-# Plain training on the small scene (config 0): 2,000 iterations, densification every 100
+# Plain training on the small blob scene (10k ground-truth Gaussians, 16 views at 256x256): 2,000 iterations, densification every 100
 # from 500 to 1,500 (threshold 2e-4), lambda 0.2, SH degree 3 with the reference's ramp.
-C0_TRAIN = dict(iterations=2000, densify=1, densify_from_iter=500, densify_until_iter=1500, densification_interval=100,
+BLOB_TRAIN = dict(iterations=2000, densify=1, densify_from_iter=500, densify_until_iter=1500, densification_interval=100,
                 densify_grad_threshold=0.0002, lambda_dssim=0.2, sh_degree=3, position_lr_max_steps=2000, seed=0)
 
-# Plain training on the clustered multi-view scene (config 2): the reference's defaults
+# Plain training on the shell scene (500k ground-truth Gaussians on 40 shells, 200 views at 1297x840): the reference's defaults
 # (30,000 iterations, densification 500-15,000) with at most 3,000,000 Gaussians.
-C2_TRAIN = dict(iterations=30000, densify=1, densify_from_iter=500, densify_until_iter=15000,
+SHELL_TRAIN = dict(iterations=30000, densify=1, densify_from_iter=500, densify_until_iter=15000,
                 densification_interval=100, densify_grad_threshold=0.0002, lambda_dssim=0.2, sh_degree=3,
                 position_lr_max_steps=30000, seed=0, max_gaussians=3_000_000)
 
 
-# Batched mixed-precision training on the same scene (config 3): 8 views of mixed sizes per
+# Batched mixed-precision training on the same scene with mixed view sizes: 8 views of mixed sizes per
 # step, BF16 render copy, f64 conic re-solve, graph replay; as many views as the plain
 # run (3,750 steps of 8) with the plain schedule in views (every step-count divided by 8).
-C3_TRAIN = dict(iterations=3750, densify=1, densify_from_iter=63, densify_until_iter=1875, densification_interval=13,
+BATCHED_TRAIN = dict(iterations=3750, densify=1, densify_from_iter=63, densify_until_iter=1875, densification_interval=13,
                 opacity_reset_interval=375, densify_grad_threshold=0.0002, lambda_dssim=0.2, sh_degree=3,
                 sh_degree_interval=125, position_lr_max_steps=3750, seed=0, max_gaussians=3_000_000,
                 batch_views=8, bf16_storage=1, fp64_conic=1, autotune=1)
@@ -394,21 +394,21 @@ def gt_views_gpu(ctx, s):
 # Learned densification's labels and policy: a kept Gaussian whose descendants blended
 # less than 10 pixel-equivalents over a densification window (13 steps of 8 views) is
 # labelled prune, and applying prunes at a prune probability of 0.95.
-C4_LEARN = dict(learn_contribution=10.0, learn_prune_confidence=0.95)
+LEARN_SETTINGS = dict(learn_contribution=10.0, learn_prune_confidence=0.95)
 
 
-def run_c4(local, learn_iters, learn=None, plain=True):
-    """Learned densification on the clustered scene in config-3 precision: the network
+def run_learned_densify(local, learn_iters, learn=None, plain=True):
+    """Learned densification on the shell scene with mixed view sizes, BF16 storage and f64 conics: the network
     learns online from plain runs on scene seeds 2-5 (the densification window of each),
     then plain and learned densification train scene seed 6 for the same number of steps."""
-    learn_cfg = dict(C4_LEARN if learn is None else learn)
+    learn_cfg = dict(LEARN_SETTINGS if learn is None else learn)
     import torch
     from splatrs_b200 import gpu as G
     from splatrs_b200 import scenes
     ctx = G.Context(local, torch.cuda.current_stream(local))
 
     def setup(seed):
-        s = scenes.config3(seed_gt=seed, seed_init=seed + 100)
+        s = scenes.shell_scene_mixed_sizes(seed_gt=seed, seed_init=seed + 100)
         views = gt_views_gpu(ctx, s)
         ip = G.init_from_points(ctx, s["init_points"], s["init_rgb"])
         n0 = len(s["init_points"])
@@ -418,7 +418,7 @@ def run_c4(local, learn_iters, learn=None, plain=True):
     theta, learn_log = None, []
     for seed in (2, 3, 4, 5):
         init, views, ext = setup(seed)
-        t = G.Trainer(ctx, init, ext, views, **dict(C3_TRAIN, learned_densify=1, **learn_cfg))
+        t = G.Trainer(ctx, init, ext, views, **dict(BATCHED_TRAIN, learned_densify=1, **learn_cfg))
         if theta is not None:
             t.set_mlp(theta)
         tw = time.perf_counter()
@@ -435,16 +435,16 @@ def run_c4(local, learn_iters, learn=None, plain=True):
     init, views, ext = setup(6)
     ev = {}
     for name, mode in ((("plain", 0),) if plain else ()) + (("learned", 2),):
-        t = G.Trainer(ctx, init, ext, views, **dict(C3_TRAIN, learned_densify=mode, **(learn_cfg if mode else {})))
+        t = G.Trainer(ctx, init, ext, views, **dict(BATCHED_TRAIN, learned_densify=mode, **(learn_cfg if mode else {})))
         if mode == 2:
             t.set_mlp(theta)
         torch.cuda.synchronize(local)
         tw = time.perf_counter()
-        t.run(C3_TRAIN["iterations"])
+        t.run(BATCHED_TRAIN["iterations"])
         torch.cuda.synchronize(local)
         wall = time.perf_counter() - tw
         sc = t.evaluate()  # splat_trainer_evaluate: every view scored on the device
-        ev[name] = {"steps": C3_TRAIN["iterations"], "wall_s": round(wall, 3), "psnr_train_views": round(sc["psnr"], 2),
+        ev[name] = {"steps": BATCHED_TRAIN["iterations"], "wall_s": round(wall, 3), "psnr_train_views": round(sc["psnr"], 2),
                     "ssim_train_views": round(sc["ssim"], 4), "gaussians": t.count}
         t.close()
     ctx.close()
@@ -510,7 +510,7 @@ def cpu_reference_steps(args, steps):
     (README.md:153: ~15 ns forward, ~25 ns backward)."""
     from oracle import oracle as O
     from splatrs_b200 import scenes
-    s = scenes.config1(n=args.n)
+    s = scenes.render_benchmark_scene(n=args.n)
     p, cam, dimage = s["params"], s["cam"], s["dimage"]
     bg = np.zeros(3, np.float32)
     names = ("project", "bin", "raster_fwd", "raster_bwd", "project_bwd")
@@ -599,7 +599,7 @@ def run_stages(local, reps=20):
                               "fp32_frac_nominal": round(LOSS_FLOP_PER_PIXEL * px / ms / 1e9 / fp32_nominal, 4)}
     del pred, tgt, grad
     n = 1_000_000
-    sc = scenes.config1(n=n)
+    sc = scenes.render_benchmark_scene(n=n)
     planes = G.params_to_planes(ctx, torch.from_numpy(sc["params"]).to(dev))
     grads = torch.randn_like(planes) * 1e-3
     m, v = torch.zeros_like(planes), torch.zeros_like(planes)
@@ -689,14 +689,14 @@ def run_profile_train(local):
     import torch
     from splatrs_b200 import gpu as G
     from splatrs_b200 import scenes
-    s = scenes.config2()
+    s = scenes.shell_scene()
     s["cams"] = s["cams"][:20]
     ctx = G.Context(local, torch.cuda.current_stream(local))
     views = gt_views_gpu(ctx, s)
     init_planes = G.init_from_points(ctx, s["init_points"], s["init_rgb"])
     n0 = len(s["init_points"])
     init = G.planes_to_params(ctx, init_planes, n0, n0).cpu().numpy()
-    cfg = dict(C2_TRAIN, iterations=300, densify_from_iter=100, densify_until_iter=250, densification_interval=50,
+    cfg = dict(SHELL_TRAIN, iterations=300, densify_from_iter=100, densify_until_iter=250, densification_interval=50,
                position_lr_max_steps=300)
     t = G.Trainer(ctx, init, scenes.scene_extent(s["cams"]), views, **cfg)
     t.run(200)
@@ -743,7 +743,7 @@ def main():
             line = {"impl": "reference", "metric": METRIC, "value": round(v, 4), "unit": UNIT, "n_gpus": world,
                     "steps": steps, "warmup": 1, "ms_per_step": round(dt * 1e3, 2), "higher_is_better": True,
                     "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-                    "data": "synthetic (seeded; config-1 distributions)",
+                    "data": "synthetic (seeded; 1M Gaussians uniform in a 10 m cube)",
                     "config": {"workload": WORKLOAD, "gaussians": args.n, "width": WIDTH, "height": HEIGHT},
                     "cpu_baseline": {"value": round(v, 4), "unit": UNIT, "cores": cores, "kind": "port",
                                      "sample": f"{steps} full fwd+bwd steps of the workload", **detail},
@@ -759,34 +759,34 @@ def main():
     if not args.profile_small:
         line["mlp"] = run_mlp(local, args.mlp_rows)
         line["stages"] = run_stages(local)
-    c0 = None
+    blobs = None
     if not args.profile_small and not args.no_train:
         from splatrs_b200 import scenes
-        gpu_c0, init, views, extent = run_train_gpu(local, scenes.config0(), C0_TRAIN, C0_TRAIN["iterations"])
-        line["train_c0"] = {"gpu": gpu_c0}
-        c0 = (init, views, extent)
-    if args.train_c2 and not args.profile_small:
+        gpu_blobs, init, views, extent = run_train_gpu(local, scenes.blob_scene(), BLOB_TRAIN, BLOB_TRAIN["iterations"])
+        line["train_blobs"] = {"gpu": gpu_blobs}
+        blobs = (init, views, extent)
+    if args.train_shells and not args.profile_small:
         from splatrs_b200 import scenes
-        iters = args.train_c2_iters or C2_TRAIN["iterations"]
-        gpu_c2, init2, views2, extent2 = run_train_gpu(local, scenes.config2(), C2_TRAIN, iters)
-        line["train_c2"] = {"gpu": gpu_c2}
-        if rank == 0 and world == 1 and args.c2_cpu_iters > 0:
-            line["train_c2"]["cpu"] = run_train_cpu(init2, views2, extent2, C2_TRAIN, args.c2_cpu_iters)
-            line["train_c2"]["cpu"]["sample"] = (f"first {args.c2_cpu_iters} iterations from the same initial "
+        iters = args.train_shells_iters or SHELL_TRAIN["iterations"]
+        gpu_shells, init2, views2, extent2 = run_train_gpu(local, scenes.shell_scene(), SHELL_TRAIN, iters)
+        line["train_shells"] = {"gpu": gpu_shells}
+        if rank == 0 and world == 1 and args.shells_cpu_iters > 0:
+            line["train_shells"]["cpu"] = run_train_cpu(init2, views2, extent2, SHELL_TRAIN, args.shells_cpu_iters)
+            line["train_shells"]["cpu"]["sample"] = (f"first {args.shells_cpu_iters} iterations from the same initial "
                                                  "model (no densification yet)")
         del views2
-    if args.train_c3 and not args.profile_small:
+    if args.train_batched and not args.profile_small:
         from splatrs_b200 import scenes
-        iters = args.train_c3_iters or C3_TRAIN["iterations"]
-        gpu_c3, _, views3, _ = run_train_gpu(local, scenes.config3(), C3_TRAIN, iters)
-        line["train_c3"] = {"gpu": gpu_c3, "views_per_step": C3_TRAIN["batch_views"],
+        iters = args.train_batched_iters or BATCHED_TRAIN["iterations"]
+        gpu_batched, _, views3, _ = run_train_gpu(local, scenes.shell_scene_mixed_sizes(), BATCHED_TRAIN, iters)
+        line["train_batched"] = {"gpu": gpu_batched, "views_per_step": BATCHED_TRAIN["batch_views"],
                             "sizes": "uniform over 640x480, 1024x768, 1297x840, 1600x1200 per view"}
         del views3
-    if args.train_c4 and not args.profile_small:
-        line["train_c4"] = run_c4(local, args.c4_learn_iters)
+    if args.train_learned and not args.profile_small:
+        line["train_learned"] = run_learned_densify(local, args.learn_iters)
     if rank == 0:
-        if c0 is not None and not args.no_cpu_baseline and world == 1:
-            line["train_c0"]["cpu"] = run_train_cpu(*c0, C0_TRAIN, C0_TRAIN["iterations"])
+        if blobs is not None and not args.no_cpu_baseline and world == 1:
+            line["train_blobs"]["cpu"] = run_train_cpu(*blobs, BLOB_TRAIN, BLOB_TRAIN["iterations"])
         if not args.no_cpu_baseline and world == 1:
             dt, cores, detail = cpu_reference_steps(args, args.cpu_steps)
             line["cpu_baseline"] = {"value": round(WIDTH * HEIGHT / 1e6 / dt, 4), "unit": UNIT, "cores": cores,

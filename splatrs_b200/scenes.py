@@ -61,7 +61,7 @@ def fibonacci_sphere(n, radius):
     return np.array(pts)
 
 
-def config0(seed_gt=0, seed_init=1, n_gt=10000, n_cams=16, size=256, f=300.0, n_init=5000):
+def blob_scene(seed_gt=0, seed_init=1, n_gt=10000, n_cams=16, size=256, f=300.0, n_init=5000):
     """Plain method on a small scene: 10k ground-truth Gaussians in [-1,1]^3, log-scales
     N(-4,0.3), opacity logits N(0,1), SH degree 3 (DC N(0.5,0.2), rest N(0,0.05)); 16
     cameras on a radius-4 sphere looking at the origin at 256x256, f=300, c=128; 5k
@@ -76,10 +76,10 @@ def config0(seed_gt=0, seed_init=1, n_gt=10000, n_cams=16, size=256, f=300.0, n_
     return dict(gt=gt, cams=cams, init_points=pts, init_rgb=rgb, sh_degree=3, background=(0.0, 0.0, 0.0))
 
 
-def config1(seed=0, n=1_000_000, width=1920, height=1080, f=1500.0, distance=12.0):
+def render_benchmark_scene(seed=0, n=1_000_000, width=1920, height=1080, f=1500.0, distance=12.0):
     """Render-only kernel benchmark: 1M Gaussians with means uniform in a 10x10x10 box
     centred at the origin, camera at distance 12 looking at the centre, f=1500, 1920x1080,
-    log-scales N(-4.5,0.5), opacity logits N(0,1.5), SH degree 3 as in config 0, and an
+    log-scales N(-4.5,0.5), opacity logits N(0,1.5), SH degree 3 as in blob_scene, and an
     upstream dL/dpixel drawn N(0,1) per channel."""
     rng = np.random.default_rng(seed)
     g = random_gaussians(rng, n, -5.0, 5.0, -4.5, 0.5, 1.5)
@@ -102,13 +102,13 @@ def hemisphere_cameras(n, radius, width, height, f):
     return np.stack(cams)
 
 
-def config2(seed_gt=0, seed_init=1, n_gt=500_000, n_shells=40, n_cams=200, width=1297, height=840, f=1150.0,
+def shell_scene(seed_gt=0, seed_init=1, n_gt=500_000, n_shells=40, n_cams=200, width=1297, height=840, f=1150.0,
             n_init=100_000, cube=6.0):
     """Clustered multi-view scene: n_gt Gaussians on n_shells shells inside a cube of side
     `cube` centred at the origin, half of them spheres and half planar discs, radius
     U(0.2, 2), each point jittered N(0, 0.01) per axis; points split over the shells in
     proportion to their area. Log-scales N(-4.5, 0.3), opacity logits N(0, 1), SH degree 3
-    as in config 0. n_cams cameras on a radius-8 hemisphere at width x height, f = 1150.
+    as in blob_scene. n_cams cameras on a radius-8 hemisphere at width x height, f = 1150.
     n_init initial points = ground-truth means + N(0, 0.02), colours from the ground-truth
     DC band."""
     rng = np.random.default_rng(seed_gt)
@@ -145,18 +145,18 @@ def config2(seed_gt=0, seed_init=1, n_gt=500_000, n_shells=40, n_cams=200, width
     return dict(gt=gt, cams=cams, init_points=ip, init_rgb=rgb, sh_degree=3, background=(0.0, 0.0, 0.0))
 
 
-C3_SIZES = ((640, 480), (1024, 768), (1297, 840), (1600, 1200))
+MIXED_VIEW_SIZES = ((640, 480), (1024, 768), (1297, 840), (1600, 1200))
 
 
-def config3(seed_sizes=7, **kw):
-    """The config-2 scene with every camera at a resolution drawn uniformly from C3_SIZES
+def shell_scene_mixed_sizes(seed_sizes=7, **kw):
+    """shell_scene with every camera at a resolution drawn uniformly from MIXED_VIEW_SIZES
     (seeded), its focal length scaled with the width (f = 1150 at 1297 pixels)."""
-    s = config2(**kw)
+    s = shell_scene(**kw)
     rng = np.random.default_rng(seed_sizes)
-    pick = rng.integers(0, len(C3_SIZES), len(s["cams"]))
+    pick = rng.integers(0, len(MIXED_VIEW_SIZES), len(s["cams"]))
     cams = []
     for cam, k in zip(s["cams"], pick):
-        w, h = C3_SIZES[k]
+        w, h = MIXED_VIEW_SIZES[k]
         c = cam.copy()
         f = 1150.0 * w / 1297.0
         c[0:6] = [w, h, f, f, w / 2.0, h / 2.0]

@@ -120,7 +120,7 @@ def test_binning_bit_exact_from_oracle_projections(ctx, seed, size):
 
 def test_binning_large_single_view(ctx):
     """bin on a 1M-Gaussian full-HD view (the render benchmark's scene): identical lists."""
-    s = scenes.config1(n=1_000_000)
+    s = scenes.render_benchmark_scene(n=1_000_000)
     want_p = O.project_all(s["params"], s["cam"], sh_degree=3)
     proj = G.proj_from_reference(ctx, dev(want_p), 1920, 1080)
     b = G.bin(ctx, proj)
@@ -138,7 +138,7 @@ def test_render_benchmark_workload_matches_oracle(ctx, cr_math):
     evaluated pairs bit-identical, screen-space gradients within 1e-3 of each quantity's
     scale; fed the oracle's screen-space gradients, the 59 parameter gradients
     bit-identical."""
-    s = scenes.config1(n=1_000_000)
+    s = scenes.render_benchmark_scene(n=1_000_000)
     g, cam, dimage = s["params"], s["cam"], s["dimage"]
     w, h, n = 1920, 1080, g.shape[0]
     bg = np.zeros(3, np.float32)

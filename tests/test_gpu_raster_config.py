@@ -150,7 +150,7 @@ def test_device_projection_path_identical_across_configs(ctx, config, cfg):
 
 
 def test_autotune_render_times_every_candidate(ctx, config):
-    s = scenes.config1(n=100_000, width=1280, height=720, f=1000.0)
+    s = scenes.render_benchmark_scene(n=100_000, width=1280, height=720, f=1000.0)
     n = s["params"].shape[0]
     planes = G.params_to_planes(ctx, dev(s["params"]))
     cam, opts = Camera.from_record(s["cam"]), ProjOpts.make(sh_degree=3)

@@ -463,7 +463,7 @@ def test_batched_densification_statistics_are_per_view(ctx):
 
 def _c0_like(seed):
     from splatrs_b200 import scenes as S
-    s = S.config0(seed_gt=seed, seed_init=seed + 100, n_gt=3000, n_cams=8, size=128, f=150.0, n_init=1500)
+    s = S.blob_scene(seed_gt=seed, seed_init=seed + 100, n_gt=3000, n_cams=8, size=128, f=150.0, n_init=1500)
     r = G.Renderer(ctx_holder[0])
     r.set_model(s["gt"], 3)
     from splatrs_b200._lib import Camera, ProjOpts
@@ -524,7 +524,7 @@ def test_learned_densification_contribution_labels_prune(ctx):
     many pixel-equivalents over the window is labelled prune: learning sees more prune
     labels than with opacity-only labels, and applying the network it trained removes
     Gaussians the rule keeps (at a quality cost this 64x48 scene bounds loosely; the quality
-    bar is measured on the config-3 scene)."""
+    bar is measured on the shell scene with mixed view sizes)."""
     ctx_holder[:] = [ctx]
     cfg = dict(iterations=900, densify=1, densify_from_iter=100, densify_until_iter=800, densification_interval=50,
                opacity_reset_interval=0, densify_grad_threshold=0.0002, sh_degree=1, sh_degree_interval=300,
