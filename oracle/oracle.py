@@ -24,10 +24,23 @@ PROJ_FIELDS = 15
 CAM_FIELDS = 18
 
 
-def build(force: bool = False) -> str:
-    """Compile the oracle with its Makefile (gcc, -ffp-contract=off)."""
-    if force or not os.path.exists(LIB_PATH):
-        subprocess.run(["make", "-s", "-C", HERE], check=True)
+SOURCES = ("oracle_capi.cpp", "splat_oracle.hpp", "splat_oracle_train.hpp", "Makefile",
+           os.path.join("..", "splatrs_b200", "csrc", "crmath.h"))
+
+
+def stale() -> bool:
+    """The library is missing or older than one of its sources."""
+    if not os.path.exists(LIB_PATH):
+        return True
+    t = os.path.getmtime(LIB_PATH)
+    return any(os.path.getmtime(os.path.join(HERE, f)) > t for f in SOURCES)
+
+
+def build(force: bool = False, if_stale: bool = False) -> str:
+    """Compile the oracle with its Makefile (gcc, -ffp-contract=off): always with `force`,
+    when out of date with `if_stale`, else only when the library is missing."""
+    if force or not os.path.exists(LIB_PATH) or (if_stale and stale()):
+        subprocess.run(["make", "-s", "-C", HERE] + (["-B"] if force else []), check=True)
     return LIB_PATH
 
 
