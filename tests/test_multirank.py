@@ -72,3 +72,13 @@ def test_reference_arm_under_two_ranks():
     line = json.loads(outs[0][0])
     assert line["impl"] == "reference" and line["value"] > 0
     assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["cpu_baseline"]["kind"] == "port"
+    for k in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better", "scaling",
+              "vs_baseline", "dtype", "data", "config", "cpu_baseline", "e2e"):
+        assert k in line, k
+    assert line["n_gpus"] == 2 and line["higher_is_better"] is True and "workload" in line["config"]
+    cb = line["cpu_baseline"]
+    assert cb["value"] == line["value"] and cb["unit"] == line["unit"] and cb["cores"] >= 1 and cb["sample"]
+    assert set(cb["stages_ms"]) == {"project", "bin", "raster_fwd", "raster_bwd", "project_bwd"}
+    assert cb["passed_pairs"]["forward"] >= cb["passed_pairs"]["backward"] > 0
+    assert cb["ns_per_pair_core"]["forward"] > 0 and cb["ns_per_pair_core"]["backward"] > 0
+    assert line["e2e"]["value"] == line["value"] and line["e2e"]["d2h_bytes_per_step"] == 0
