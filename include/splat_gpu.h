@@ -297,6 +297,13 @@ SPLAT_API int splat_project_bwd(splat_ctx* ctx, const float* planes_dev, int64_t
  * (negative != 0 selects -|x|). Synchronises. */
 SPLAT_API int splat_diag_fast_exp_error(splat_ctx* ctx, float lo, float hi, int32_t negative, float* max_rel_error);
 
+/* Diagnostic of the bounded waits of the tensor-core kernels: one block waits on an
+ * mbarrier with `limit` tries (1..4194304; the kernels use 4194304), through the same wait
+ * and error word as those kernels. With arrive == 0 nothing arrives: the wait runs out and
+ * the call returns SPLAT_ERR_TIMEOUT. With arrive != 0 the phase completes first and it
+ * returns SPLAT_OK. The context stays usable either way. Synchronises. */
+SPLAT_API int splat_diag_mbarrier_wait(splat_ctx* ctx, uint32_t limit, int32_t arrive);
+
 /* project_backward_all fused with Adam::step (reference src/project.rs:477-493,
  * src/adam.rs:77-161): the parameter gradients stay in registers and update planes_dev in
  * place together with the moments m_dev and v_dev (parameter-plane layout, capacity cap);

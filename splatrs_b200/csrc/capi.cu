@@ -195,6 +195,13 @@ SPLAT_API int splat_diag_fast_exp_error(splat_ctx* ctx, float lo, float hi, int3
   return finish(ctx, launch_diag_fast_exp(&ctx->c, lo, hi, negative, max_rel_error));
 }
 
+SPLAT_API int splat_diag_mbarrier_wait(splat_ctx* ctx, uint32_t limit, int32_t arrive) {
+  if (!ctx) return SPLAT_ERR_INVALID;
+  if (limit == 0 || limit > (1u << 22)) return invalid(ctx, "splat_diag_mbarrier_wait: limit must be in 1..4194304");
+  Enter e(ctx);
+  return finish(ctx, diag_mbar_wait(&ctx->c, limit, arrive));
+}
+
 SPLAT_API int splat_zero(splat_ctx* ctx, void* dev, size_t bytes) {
   if (!ctx || (!dev && bytes)) return invalid(ctx, "splat_zero: null pointer");
   Enter e(ctx);

@@ -114,6 +114,9 @@ Status launch_mlp_grad_tc(Ctx* c, const float* x, const int32_t* y, const float*
 Status mlp_tc_error_clear(Ctx* c);
 uint32_t* mlp_tc_error_word(Ctx* c);
 Status mlp_tc_error_check(Ctx* c);
+// Runs one bounded mbarrier wait of `limit` tries that times out unless `arrive`, through
+// the error word; SPLAT_ERR_TIMEOUT when it ran out. Synchronises.
+Status diag_mbar_wait(Ctx* c, uint32_t limit, int arrive);
 Status launch_mlp_grad(Ctx* c, const float* x, const int32_t* y, const float* w, int64_t n, float scale,
                        const float* theta, float* grad);
 Status launch_mlp_adam(Ctx* c, float* theta, const float* grad, float* m, float* v, uint64_t step, float lr);

@@ -456,9 +456,9 @@ __device__ __forceinline__ void tc_commit(uint64_t* bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(a) : "memory");
 }
 
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase) {
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase, uint32_t limit = 1u << 22) {
   const uint32_t a = (uint32_t)__cvta_generic_to_shared(bar);
-  for (uint32_t it = 0; it < (1u << 22); it++) {
+  for (uint32_t it = 0; it < limit; it++) {
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
@@ -1034,6 +1034,40 @@ Status launch_mlp_grad_tc(Ctx* c, const float* x, const int32_t* y, const float*
   c->launches.count++;
   SPLAT_LAUNCHED("mlp_grad_tc_kernel");
   return Status::ok();
+}
+
+// Diagnostic of the bounded wait and of the error word the tensor-core kernels report in:
+// one block waits, with `limit` tries, on an mbarrier that nothing arrives on (arrive == 0),
+// or that one thread has completed first (arrive != 0). When the wait runs out the block
+// reports it exactly as the tensor-core kernels do, completes the phase itself and
+// invalidates the barrier before it exits.
+__global__ void diag_mbar_wait_kernel(uint32_t limit, int arrive, uint32_t* err) {
+  __shared__ __align__(8) uint64_t bar;
+  const uint32_t a = (uint32_t)__cvta_generic_to_shared(&bar);
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(a) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (arrive && threadIdx.x == 0)
+    asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}" ::"r"(a) : "memory");
+  const bool ok = !__syncthreads_or(!mbar_wait(&bar, 0u, limit));
+  if (threadIdx.x == 0) {
+    if (!ok) {
+      *err = 1u;
+      asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}" ::"r"(a) : "memory");
+    }
+    asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(a) : "memory");
+  }
+}
+
+Status diag_mbar_wait(Ctx* c, uint32_t limit, int arrive) {
+  SPLAT_TRY(mlp_tc_error_clear(c));
+  diag_mbar_wait_kernel<<<1, 32, 0, c->stream>>>(limit, arrive, mlp_tc_error_word(c));
+  c->launches.count++;
+  SPLAT_LAUNCHED("diag_mbar_wait_kernel");
+  SPLAT_CUDA(cudaGetLastError());
+  return mlp_tc_error_check(c);
 }
 
 Status mlp_tc_error_clear(Ctx* c) {

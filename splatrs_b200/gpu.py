@@ -593,6 +593,13 @@ def init_from_points(ctx: Context, points, rgb, cap: int | None = None) -> torch
     return planes
 
 
+def diag_mbarrier_wait(ctx: Context, limit: int, arrive: bool) -> None:
+    """splat_diag_mbarrier_wait: one bounded mbarrier wait of `limit` tries through the
+    tensor-core kernels' wait and error word; raises SplatError with SPLAT_ERR_TIMEOUT when
+    it ran out (nothing arrived)."""
+    check(ctx.lib.splat_diag_mbarrier_wait(ctx.h, int(limit), int(bool(arrive))), ctx.h)
+
+
 def mlp_forward(ctx: Context, x: torch.Tensor, theta: torch.Tensor, tcgen05: bool = False) -> torch.Tensor:
     """Learned-densification network: probabilities (n, 3) of feature rows (n, 16); with
     `tcgen05` on the 5th-generation tensor cores (accumulators in tensor memory)."""

@@ -64,6 +64,23 @@ def test_mlp_forward_tcgen05_matches_oracle(ctx, n):
           f"vs mma.sync {np.abs(got - ref).max():.2e}, equal rows {np.mean(np.all(got == ref, 1)):.3f}")
 
 
+def test_bounded_wait_times_out_and_context_stays_usable(ctx):
+    """The tensor-core kernels' bounded mbarrier wait, run out on purpose (nothing arrives;
+    4096 tries): SPLAT_ERR_TIMEOUT through the kernels' error word. The same wait with the
+    phase completed first succeeds, and the context keeps working: the tcgen05 forward still
+    matches the oracle afterwards."""
+    from splatrs_b200._lib import SplatError
+    G.diag_mbarrier_wait(ctx, 4096, True)
+    with pytest.raises(SplatError) as e:
+        G.diag_mbarrier_wait(ctx, 4096, False)
+    assert e.value.status == 4
+    G.diag_mbarrier_wait(ctx, 4096, True)
+    theta, x, _, _ = _case(90, 300)
+    got = G.mlp_forward(ctx, _t(x), _t(theta), tcgen05=True).cpu().numpy()
+    want, _ = M.forward(theta, x, bf16_like=True)
+    assert np.abs(got - want).max() < 5e-3
+
+
 def test_mlp_forward_tcgen05_empty_and_repeated(ctx):
     theta, x, _, _ = _case(70, 300)
     empty = G.mlp_forward(ctx, _t(x[:0]), _t(theta), tcgen05=True)
