@@ -160,7 +160,10 @@ typedef struct splat_train_config {
 typedef struct splat_ctx splat_ctx;
 
 /* ----------------------------------------------------------------------------------------
- * Context: device, stream, scratch arena, error message.
+ * Context: device, stream, scratch arena, error message. No counterpart in the reference,
+ * whose functions run on the caller's thread and the global rayon pool and panic on
+ * violated invariants (e.g. src/rasterize.rs:65-74, :466-469); here every entry point
+ * returns a status and leaves the message in the context.
  * -------------------------------------------------------------------------------------- */
 /* `stream` is a cudaStream_t (NULL for the legacy default stream). */
 SPLAT_API int splat_ctx_create(int device, void* stream, splat_ctx** out);
@@ -178,7 +181,9 @@ SPLAT_API int32_t splat_struct_sizes(uint64_t* out);
 SPLAT_API uint64_t splat_ctx_launch_count(const splat_ctx* ctx);
 
 /* ----------------------------------------------------------------------------------------
- * Parameter layout conversion (reference Gaussian records <-> planes).
+ * Parameter layout conversion: the reference's Gaussian records (59 floats in field order,
+ * reference src/model.rs:16-28; the caller's &[Gaussian]) to and from the device
+ * parameter planes.
  * -------------------------------------------------------------------------------------- */
 SPLAT_API int splat_params_from_aos(splat_ctx* ctx, const float* aos59_dev, int64_t n, float* planes_dev,
                                     int64_t cap);
@@ -371,7 +376,8 @@ SPLAT_API int splat_autotune_render(splat_ctx* ctx, const float* planes_dev, int
                                     const splat_camera* cam, const splat_proj_opts* opts, const float* background,
                                     const float* dimage_dev, int32_t reps, float* ms_out, uint32_t* picked);
 
-/* Fill `bytes` bytes of device memory with zeros on the context stream. */
+/* Fill `bytes` bytes of device memory with zeros on the context stream (no reference
+ * counterpart: host vectors there are zeroed on allocation). */
 SPLAT_API int splat_zero(splat_ctx* ctx, void* dev, size_t bytes);
 
 /* ----------------------------------------------------------------------------------------
