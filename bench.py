@@ -65,6 +65,9 @@ def parse():
                          "prints the launches before its last 100 iterations")
     ap.add_argument("--profile-small", action="store_true",
                     help="a reduced case for ncu captures (fewer Gaussians, one step)")
+    ap.add_argument("--profile-stages", action="store_true",
+                    help="only the HBM-bound stages, twice each, for an ncu capture: projection forward and backward "
+                         "and Adam over 1M Gaussians, the SSIM + L1 loss on one 1297x840 view")
     return ap.parse_args()
 
 
@@ -148,6 +151,20 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
+def unit_peaks(ctx, local):
+    """FP32 (FMA) and special-function-unit (ex2) throughput measured on this GPU by the
+    library's microbenchmark (splat_diag_peak), best of three, with the SM clock sampled
+    while it runs: the denominators of the compositing stages' roofline."""
+    sampler = ClockSampler(local)
+    sampler.start()
+    fp32 = max(ctx.peak("fp32")["ops_per_s"] for _ in range(3))
+    mufu = max(ctx.peak("mufu")["ops_per_s"] for _ in range(3))
+    clocks = sampler.stop()
+    return {"fp32_tflops": round(fp32 / 1e12, 2), "mufu_gops": round(mufu / 1e9, 1),
+            "source": "measured (splat_diag_peak: FMA and ex2 chains on every SM, CUDA events)",
+            "clocks": clocks}
+
+
 # Algorithmic work per unit (fixed constants): bytes for the HBM-bound stages.
 PROJ_FWD_BYTES = 236 + 64          # parameters read + projection record written, per Gaussian
 PROJ_BWD_BYTES = 236 + 36 + 236    # parameters + screen gradients read, parameter gradients written
@@ -163,6 +180,42 @@ NCU_DRAM_BYTES_1M = {("raster_bwd", 16, 16, 256, 1): int((197.05 + 17.84) * 1e6)
                      ("raster_fwd", 16, 16, 256, 2): int((83.13 + 20.63) * 1e6)}
 RASTER_FWD_FLOP_PER_PAIR = 20
 RASTER_BWD_FLOP_PER_PAIR = 50
+RASTER_FWD_SFU_PER_PAIR = 1        # one exp
+RASTER_BWD_SFU_PER_PAIR = 2        # one exp, one reciprocal (the transmittance division)
+BIN_BYTES_PER_ENTRY = 40 + 24      # key emission (key 8 + value 4 + entry Gaussian 4, Proj read) + sort (24)
+
+
+def stage_rooflines(stage_ms, n, entries, pairs_fwd, pairs_bwd, pixels, hbm_gbs, fp32_tflops, mufu_gops):
+    """Per stage: the algorithmic work, the time each unit's peak needs for it, the bound
+    (the unit needing the longest) and the fraction of that bound achieved."""
+    work = {
+        "project_fwd": {"bytes": PROJ_FWD_BYTES * n},
+        "bin": {"bytes": BIN_BYTES_PER_ENTRY * entries},
+        "raster_fwd": {"bytes": RASTER_FWD_BYTES_PER_PIXEL * pixels + RASTER_BYTES_PER_ENTRY * entries,
+                       "flop": RASTER_FWD_FLOP_PER_PAIR * pairs_fwd, "sfu": RASTER_FWD_SFU_PER_PAIR * pairs_fwd},
+        "raster_bwd": {"bytes": RASTER_BWD_BYTES_PER_PIXEL * pixels + RASTER_BYTES_PER_ENTRY * entries,
+                       "flop": RASTER_BWD_FLOP_PER_PAIR * pairs_bwd, "sfu": RASTER_BWD_SFU_PER_PAIR * pairs_bwd},
+        "project_bwd": {"bytes": PROJ_BWD_BYTES * n},
+    }
+    out = {}
+    for k, w in work.items():
+        t = {"hbm": w["bytes"] / (hbm_gbs * 1e9) * 1e3}
+        if "flop" in w:
+            t["fp32"] = w["flop"] / (fp32_tflops * 1e12) * 1e3
+            t["mufu"] = w["sfu"] / (mufu_gops * 1e9) * 1e3
+        bound = max(t, key=t.get)
+        out[k] = {**w, "ms": round(stage_ms[k], 4), "roofline_ms": round(t[bound], 4), "bound": bound,
+                  "frac": round(t[bound] / stage_ms[k], 4), "unit_ms": {u: round(v, 4) for u, v in t.items()}}
+    return out
+
+
+REF_MAX_STEPS, REF_MAX_WARMUP = 200, 20
+
+
+def workload_config(n, world):
+    """The workload's `config`, the same in both arms."""
+    return {"workload": WORKLOAD, "gaussians": n, "width": WIDTH, "height": HEIGHT,
+            "l2": "inputs larger than L2 (240 MB parameter planes), no flush", "parallelism": f"replicas x{world}"}
 
 
 def run_ours(args, rank, world, local):
@@ -186,6 +239,8 @@ def run_ours(args, rank, world, local):
     dimage = torch.from_numpy(s["dimage"]).to(dev)
     pgrad = torch.zeros((3, n, 4), dtype=torch.float32, device=dev)
     del params
+
+    peaks = unit_peaks(ctx, local)
 
     # Compositing configuration: every candidate timed on this workload, the fastest kept.
     tuning = None
@@ -306,26 +361,31 @@ def run_ours(args, rank, world, local):
            "synchronous_ms_per_step": round(sync_ms, 3),
            "pcie_gbs": round((dimage_h[0].nbytes + img_h[0].nbytes + grads_h[0].nbytes) / e2e_ms / 1e6, 1)}
 
-    # Roofline of the dominant kernel.
+    # Roofline per stage: max(bytes / HBM, FLOP / FP32, exp+rcp / special-function unit),
+    # the HBM peak from the driver's copy measurement, FP32 and the special-function unit
+    # from the microbenchmark above; the dominant kernel's goes into `roofline`.
     hbm_peak, peak_kind = measured_peaks()
+    rl = stage_rooflines(stage_ms, n, entries, pairs_fwd, pairs_bwd, WIDTH * HEIGHT, hbm_peak,
+                         peaks["fp32_tflops"], peaks["mufu_gops"])
     dom = max(stage_ms, key=stage_ms.get)
-    sort_passes = None
-    if dom in ("raster_fwd", "raster_bwd"):
-        byts = (RASTER_FWD_BYTES_PER_PIXEL if dom == "raster_fwd" else RASTER_BWD_BYTES_PER_PIXEL) * WIDTH * HEIGHT \
-               + RASTER_BYTES_PER_ENTRY * entries
-    elif dom == "project_fwd":
-        byts = PROJ_FWD_BYTES * n
-    elif dom == "project_bwd":
-        byts = PROJ_BWD_BYTES * n
+    d = rl[dom]
+    sec = stage_ms[dom] / 1e3
+    if d["bound"] == "fp32":
+        achieved, peak, unit, src = d["flop"] / sec / 1e12, peaks["fp32_tflops"], "TFLOP/s", "measured (microbenchmark)"
+    elif d["bound"] == "mufu":
+        achieved, peak, unit, src = d["sfu"] / sec / 1e9, peaks["mufu_gops"], "Gop/s", "measured (microbenchmark)"
     else:
-        byts = (EMIT_BYTES_PER_ENTRY + SORT_BYTES_PER_KEY_PASS) * entries
-    achieved = byts / (stage_ms[dom] / 1e3) / 1e9
-    # DRAM bytes per launch from one ncu capture of this workload (1M Gaussians, 1080p):
-    # profiles/raster_dram_traffic_1M_1080p_ncu.md. Other sizes have no capture.
+        achieved, peak, unit, src = d["bytes"] / sec / 1e9, hbm_peak, "GB/s", peak_kind
+    # DRAM bytes per launch from one ncu capture of this workload (1M Gaussians, 1080p,
+    # dram__bytes_read.sum + dram__bytes_write.sum). Other sizes have no capture.
     traffic = NCU_DRAM_BYTES_1M.get((dom,) + tuple(raster)) if n == 1_000_000 else None
-    roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
-                "frac": round(achieved / hbm_peak, 4), "traffic": traffic, "peak_source": peak_kind,
-                "algorithmic_bytes_per_launch": int(byts)}
+    roofline = {"bound": d["bound"], "kernel": dom, "achieved": round(achieved, 3), "peak": peak, "unit": unit,
+                "frac": round(achieved / peak, 4), "traffic": traffic, "peak_source": src,
+                "algorithmic_bytes_per_launch": int(d["bytes"]),
+                "algorithmic_flop_per_launch": int(d.get("flop", 0)),
+                "algorithmic_sfu_ops_per_launch": int(d.get("sfu", 0)),
+                "hbm_frac": round(d["bytes"] / sec / 1e9 / hbm_peak, 4)}
+    step_roofline_ms = sum(v["roofline_ms"] for v in rl.values())
     flops = {"raster_fwd": RASTER_FWD_FLOP_PER_PAIR * pairs_fwd, "raster_bwd": RASTER_BWD_FLOP_PER_PAIR * pairs_bwd}
     compute = {k: {"pairs": p, "flop": flops[k], "ms": round(stage_ms[k], 4),
                    "tflops": round(flops[k] / (stage_ms[k] / 1e3) / 1e12, 3),
@@ -341,16 +401,17 @@ def run_ours(args, rank, world, local):
         "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded; 1M Gaussians uniform in a 10 m cube)",
-        "config": {"workload": WORKLOAD, "gaussians": n, "width": WIDTH, "height": HEIGHT,
-                   "tile": [raster[0], raster[1]], "chunk": raster[2], "bwd_pixels_per_thread": raster[3],
-                   "raster": "autotuned" if tuning else "fixed",
-                   "l2": "inputs larger than L2 (240 MB parameter planes), no flush", "parallelism": f"replicas x{world}"},
+        "config": workload_config(n, world),
+        "raster_config": {"tile": [raster[0], raster[1]], "chunk": raster[2], "bwd_pixels_per_thread": raster[3],
+                          "chosen": "autotuned" if tuning else "fixed"},
         "autotune": tuning,
         "iters_per_s": round(1e3 / ms_per_step, 3),
         "stages_ms": {k: round(v, 4) for k, v in stage_ms.items()},
         "entries": entries, "visible": visible, "sort_keys_per_s": round(entries / (stage_ms["bin"] / 1e3), 1),
         "pairs": {"fwd": pairs_fwd, "bwd": pairs_bwd},
-        "e2e": e2e, "gpu_launches": int(launches), "roofline": roofline, "compute": compute, "hbm_stages": stage_hbm,
+        "e2e": e2e, "gpu_launches": int(launches), "roofline": roofline,
+        "step_roofline_frac": round(step_roofline_ms / ms_per_step, 4), "step_roofline_ms": round(step_roofline_ms, 4),
+        "stage_roofline": rl, "peaks": peaks, "compute": compute, "hbm_stages": stage_hbm,
         "clocks": clocks,
     }
     ctx.close()
@@ -501,7 +562,7 @@ def run_train_cpu(init, views, extent, cfg, iterations):
     return out
 
 
-def cpu_reference_steps(args, steps):
+def cpu_reference_steps(args, steps, warmup=1):
     """The CPU oracle (the reference's hot path restated in C++, all host threads) on the
     same workload: `steps` full forward+backward passes of the 1920x1080 view. Returns the
     mean seconds per step, the threads used and a per-stage breakdown (as the reference's
@@ -534,7 +595,8 @@ def cpu_reference_steps(args, steps):
                 acc[nm] += t[k + 1] - t[k]
             passed[:] = O.last_passed_pairs()
 
-    one(False)  # warm caches and thread pool
+    for _ in range(max(1, warmup)):
+        one(False)  # warm caches and thread pool
     t0 = time.perf_counter()
     for _ in range(steps):
         one(True)
@@ -567,7 +629,7 @@ def run_stages(local, reps=20):
     stream = torch.cuda.current_stream(dev)
     ctx = G.Context(local, stream)
     hbm, kind = measured_peaks()
-    fp32_nominal = 148 * 128 * 2 * 1.965e9 / 1e12  # TFLOP/s at the maximum SM clock
+    fp32_peak = max(ctx.peak("fp32")["ops_per_s"] for _ in range(3)) / 1e12  # measured, TFLOP/s
 
     def timed(fn):
         for _ in range(3):
@@ -581,7 +643,7 @@ def run_stages(local, reps=20):
         torch.cuda.synchronize(dev)
         return e0.elapsed_time(e1) / reps
 
-    out = {"peak_hbm_gbs": hbm, "peak_source": kind, "fp32_tflops_nominal": round(fp32_nominal, 1)}
+    out = {"peak_hbm_gbs": hbm, "peak_source": kind, "fp32_tflops_measured": round(fp32_peak, 1)}
     w, h = 1297, 840
     rng = np.random.default_rng(3)
     pred = torch.from_numpy(rng.uniform(0, 1, w * h * 3).astype(np.float32)).to(dev)
@@ -596,7 +658,7 @@ def run_stages(local, reps=20):
                               "hbm_frac": round(LOSS_BYTES_PER_PIXEL * px / ms / 1e6 / hbm, 4),
                               "flop_per_pixel": LOSS_FLOP_PER_PIXEL,
                               "tflops": round(LOSS_FLOP_PER_PIXEL * px / ms / 1e9, 2),
-                              "fp32_frac_nominal": round(LOSS_FLOP_PER_PIXEL * px / ms / 1e9 / fp32_nominal, 4)}
+                              "fp32_frac": round(LOSS_FLOP_PER_PIXEL * px / ms / 1e9 / fp32_peak, 4)}
     del pred, tgt, grad
     n = 1_000_000
     sc = scenes.render_benchmark_scene(n=n)
@@ -682,6 +744,42 @@ def run_mlp(local, rows, reps=20):
     return out
 
 
+def run_profile_stages(local):
+    """The HBM-bound stages for an ncu capture, each run twice (skip the first of each):
+    projection forward, projection backward and Adam over the render benchmark's 1M
+    Gaussians, and the fused SSIM + L1 loss forward and backward on one 1297x840 view
+    (u8 target). About 1.5 GB on the device."""
+    import torch
+    from splatrs_b200 import gpu as G
+    from splatrs_b200 import scenes
+    from splatrs_b200._lib import Camera, LearningRates, ProjOpts
+    dev = torch.device("cuda", local)
+    ctx = G.Context(local, torch.cuda.current_stream(dev))
+    n = 1_000_000
+    sc = scenes.render_benchmark_scene(n=n)
+    planes = G.params_to_planes(ctx, torch.from_numpy(sc["params"]).to(dev))
+    cam, opts = Camera.from_record(sc["cam"]), ProjOpts.make(sh_degree=3)
+    pgrad = torch.randn((3, n, 4), dtype=torch.float32, device=dev) * 1e-3
+    grads = torch.randn_like(planes) * 1e-3
+    m, v = torch.zeros_like(planes), torch.zeros_like(planes)
+    lr = LearningRates(mean=1.6e-4, log_scale=0.005, quat=0.001, opacity=0.025, sh_dc=0.0025, sh_rest=0.000125)
+    w, h = 1297, 840
+    rng = np.random.default_rng(3)
+    pred = torch.from_numpy(rng.uniform(0, 1, w * h * 3).astype(np.float32)).to(dev)
+    tgt = torch.from_numpy(rng.integers(0, 256, w * h * 3).astype(np.uint8)).to(dev)
+    lgrad = torch.empty_like(pred)
+    lo = torch.empty(3, dtype=torch.float32, device=dev)
+    for rep in range(2):
+        proj = G.project_all(ctx, planes, n, n, cam, opts)
+        G.project_backward_all(ctx, planes, n, n, cam, opts, proj, pgrad)
+        G.adam_step(ctx, planes, grads, m, v, n, n, rep + 1, lr)
+        G.check(ctx.lib.splat_loss_fwd_bwd(ctx.h, G._ptr(pred), G._ptr(tgt), 1, w, h, 0.2, G._ptr(lgrad), G._ptr(lo)),
+                ctx.h)
+    torch.cuda.synchronize(dev)
+    ctx.close()
+    return {"profile_stages": {"gaussians": n, "loss_view": [w, h], "reps": 2}}
+
+
 def run_profile_train(local):
     """Config-2 training for an ncu launch list: the scene's first 20 cameras, 300 plain
     iterations (densification from 100 every 50). Prints how many kernel launches come
@@ -719,6 +817,9 @@ def main():
     if args.profile_mlp:
         print(json.dumps({"mlp": run_mlp(0, args.mlp_rows, reps=3)}), flush=True)
         return
+    if args.profile_stages:
+        print(json.dumps(run_profile_stages(0)), flush=True)
+        return
     rank, world, local = dist_info()
     if world > 1:
         import torch
@@ -737,17 +838,22 @@ def main():
 
     if args.impl == "reference":
         if rank == 0:
-            steps = max(1, args.steps if args.steps <= 5 else 3)
-            dt, cores, detail = cpu_reference_steps(args, steps)
+            # Each CPU step takes about 0.6 s on 16 host threads: up to 200 steps and 20
+            # warm-up steps keep the run within a few minutes; more are capped (and said so).
+            steps, warmup = max(1, min(args.steps, REF_MAX_STEPS)), max(1, min(args.warmup, REF_MAX_WARMUP))
+            dt, cores, detail = cpu_reference_steps(args, steps, warmup)
             v = WIDTH * HEIGHT / 1e6 / dt
             line = {"impl": "reference", "metric": METRIC, "value": round(v, 4), "unit": UNIT, "n_gpus": world,
-                    "steps": steps, "warmup": 1, "ms_per_step": round(dt * 1e3, 2), "higher_is_better": True,
+                    "steps": steps, "warmup": warmup, "ms_per_step": round(dt * 1e3, 2), "higher_is_better": True,
                     "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                     "data": "synthetic (seeded; 1M Gaussians uniform in a 10 m cube)",
-                    "config": {"workload": WORKLOAD, "gaussians": args.n, "width": WIDTH, "height": HEIGHT},
+                    "config": workload_config(args.n, world),
                     "cpu_baseline": {"value": round(v, 4), "unit": UNIT, "cores": cores, "kind": "port",
                                      "sample": f"{steps} full fwd+bwd steps of the workload", **detail},
                     "e2e": {"value": round(v, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            if steps != args.steps or warmup != args.warmup:
+                line["capped"] = (f"--steps {args.steps} --warmup {args.warmup} capped to {steps}/{warmup} "
+                                  f"(about 0.6 s per CPU step)")
             print(json.dumps(line), flush=True)
         if world > 1:
             import torch.distributed as dist

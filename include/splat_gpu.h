@@ -179,6 +179,10 @@ SPLAT_API int splat_version(void);
 SPLAT_API int32_t splat_struct_sizes(uint64_t* out);
 /* Kernels launched through this context since creation (all stage entry points count). */
 SPLAT_API uint64_t splat_ctx_launch_count(const splat_ctx* ctx);
+/* The context's scratch arena: out2[0] = bytes it holds on the device, out2[1] = a counter
+ * that changes whenever it allocates or frees (no counterpart in the reference; lets a
+ * caller check that an entry point allocated nothing). */
+SPLAT_API int splat_ctx_scratch_info(const splat_ctx* ctx, uint64_t* out2);
 
 /* ----------------------------------------------------------------------------------------
  * Parameter layout conversion: the reference's Gaussian records (59 floats in field order,
@@ -240,8 +244,9 @@ SPLAT_API int splat_bin_count(splat_ctx* ctx, const uint32_t* num_tiles_dev, int
  * splat_bin_count, but its scratch is a fixed 32 KiB array in device memory held by every
  * GPU that loads the library, so n may be at most 16,777,216 (larger n returns
  * SPLAT_ERR_CAPACITY). The first call on each device looks the array's address up; make
- * it before any stream capture. All calls share the array: calls that overlap on the GPU
- * race. Allocates nothing; synchronises to return the count. */
+ * it before any stream capture; the address is cached for the process and does not
+ * survive cudaDeviceReset. All calls share the array: calls that overlap on the GPU race.
+ * Allocates nothing; synchronises to return the count. */
 SPLAT_API int splat_bin_count_noalloc(splat_ctx* ctx, const uint32_t* num_tiles_dev, int64_t n,
                                       uint32_t* entry_offset_dev, int64_t* num_entries);
 SPLAT_API int splat_bin_sort(splat_ctx* ctx, const float* proj_dev, const uint32_t* entry_offset_dev, int64_t n,
@@ -308,6 +313,13 @@ SPLAT_API int splat_diag_fast_exp_error(splat_ctx* ctx, float lo, float hi, int3
  * the call returns SPLAT_ERR_TIMEOUT. With arrive != 0 the phase completes first and it
  * returns SPLAT_OK. The context stays usable either way. Synchronises. */
 SPLAT_API int splat_diag_mbarrier_wait(splat_ctx* ctx, uint32_t limit, int32_t arrive);
+
+/* Diagnostic: throughput of the units that bound the compositing kernels, measured on the
+ * context's device (no counterpart in the reference). unit 0: FP32 fused multiply-adds,
+ * *ops_per_s in FLOP/s (2 per FMA); unit 1: special-function unit ex2 (the fast exp),
+ * operations/s. One timed launch of about 2 ms (*ms) after an untimed one, CUDA events on
+ * the context's stream, at the current SM clock. Synchronises. */
+SPLAT_API int splat_diag_peak(splat_ctx* ctx, int32_t unit, double* ops_per_s, float* ms);
 
 /* project_backward_all fused with Adam::step (reference src/project.rs:477-493,
  * src/adam.rs:77-161): the parameter gradients stay in registers and update planes_dev in

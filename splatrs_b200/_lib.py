@@ -146,6 +146,8 @@ def _declare(L):
         "splat_zero": ([vp, vp, sz], C.c_int),
         "splat_diag_fast_exp_error": ([vp, C.c_float, C.c_float, i32, P(C.c_float)], C.c_int),
         "splat_diag_mbarrier_wait": ([vp, u32, i32], C.c_int),
+        "splat_diag_peak": ([vp, i32, P(C.c_double), P(C.c_float)], C.c_int),
+        "splat_ctx_scratch_info": ([vp, P(C.c_uint64)], C.c_int),
         "splat_params_from_aos": ([vp, vp, i64, vp, i64], C.c_int),
         "splat_params_to_aos": ([vp, vp, i64, i64, vp], C.c_int),
         "splat_project_fwd": ([vp, vp, i64, i64, P(Camera), P(ProjOpts), vp, vp, vp], C.c_int),

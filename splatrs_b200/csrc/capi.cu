@@ -195,6 +195,22 @@ SPLAT_API int splat_diag_fast_exp_error(splat_ctx* ctx, float lo, float hi, int3
   return finish(ctx, launch_diag_fast_exp(&ctx->c, lo, hi, negative, max_rel_error));
 }
 
+SPLAT_API int splat_diag_peak(splat_ctx* ctx, int32_t unit, double* ops_per_s, float* ms) {
+  if (!ctx) return SPLAT_ERR_INVALID;
+  if ((unit != 0 && unit != 1) || !ops_per_s || !ms) return invalid(ctx, "splat_diag_peak: unit must be 0 or 1");
+  Enter e(ctx);
+  return finish(ctx, launch_diag_peak(&ctx->c, unit, ops_per_s, ms));
+}
+
+SPLAT_API int splat_ctx_scratch_info(const splat_ctx* ctx, uint64_t* out2) {
+  if (!ctx || !out2) return SPLAT_ERR_INVALID;
+  uint64_t bytes = 0;
+  for (const auto& ch : ctx->c.arena.chunks) bytes += ch.size;
+  out2[0] = bytes;
+  out2[1] = ctx->c.arena.generation;
+  return SPLAT_OK;
+}
+
 SPLAT_API int splat_diag_mbarrier_wait(splat_ctx* ctx, uint32_t limit, int32_t arrive) {
   if (!ctx) return SPLAT_ERR_INVALID;
   if (limit == 0 || limit > (1u << 22)) return invalid(ctx, "splat_diag_mbarrier_wait: limit must be in 1..4194304");

@@ -182,6 +182,8 @@ Status launch_raster_bwd(Ctx* c, const float* proj, const uint32_t* gauss, const
                          const BatchTable* bt = nullptr, uint32_t tiles_cap = 0);
 
 Status launch_diag_fast_exp(Ctx* c, float magnitude_lo, float magnitude_hi, int negative, float* out_host);
+// Throughput of one unit (0: FP32 FMA, in FLOP/s; 1: MUFU ex2, in operations/s), peaks.cu.
+Status launch_diag_peak(Ctx* c, int unit, double* ops_per_s, float* ms_out);
 
 Status launch_loss(Ctx* c, const float* pred, const void* target, int target_u8, uint32_t width, uint32_t height,
                    float lambda, float* grad, float* out3, const StepParams* sp = nullptr,

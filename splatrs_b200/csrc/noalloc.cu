@@ -15,7 +15,10 @@
 // kNoAllocMaxGaussians (16,777,216) counts per call. Every GPU that loads the library holds
 // it until the process exits. Host code cannot use the array's name as a device address,
 // so the first call on each device resolves the address with cudaGetSymbolAddress (with
-// that device current) and caches it; make that first call before any stream capture.
+// that device current) and caches it; make that first call before any stream capture. The
+// cached address belongs to the device's primary context: after cudaDeviceReset (which
+// destroys that context) it is stale, so do not call this entry point again in a process
+// that has reset the device.
 // All calls share the array and it keeps the last call's contents; each call overwrites
 // every word it reads, so nothing has to start at zero. Calls whose kernels overlap on the
 // GPU (different streams, or different host threads) race on the array.
@@ -76,7 +79,15 @@ extern "C" SPLAT_API int splat_bin_count_noalloc(splat_ctx* ctx, const uint32_t*
     cudaGetLastError();
     prev = -1;
   }
-  if (prev != c->device) cudaSetDevice(c->device);
+  if (prev != c->device) {
+    const cudaError_t e = cudaSetDevice(c->device);
+    if (e != cudaSuccess) {
+      // Resolving (and caching) the scratch address now would do it on the wrong device.
+      cudaGetLastError();
+      c->last_error = std::string("splat_bin_count_noalloc: cudaSetDevice: ") + cudaGetErrorString(e);
+      return SPLAT_ERR_CUDA;
+    }
+  }
   uint64_t* scratch = nullptr;
   Status s = scratch_address(c->device, &scratch);
   if (s.good()) s = launch_scan_u32_into(c, num_tiles_dev, n, entry_offset_dev, 1, scratch,

@@ -53,6 +53,20 @@ class Context:
     def launches(self) -> int:
         return int(self.lib.splat_ctx_launch_count(self.h))
 
+    @property
+    def scratch_info(self) -> tuple:
+        """(bytes the scratch arena holds on the device, its allocation counter)."""
+        out = (C.c_uint64 * 2)()
+        check(self.lib.splat_ctx_scratch_info(self.h, out), self.h)
+        return int(out[0]), int(out[1])
+
+    def peak(self, unit: str) -> dict:
+        """Measured throughput of 'fp32' (FMA, FLOP/s) or 'mufu' (ex2, operations/s) on this
+        context's device (splat_diag_peak)."""
+        ops, ms = C.c_double(), C.c_float()
+        check(self.lib.splat_diag_peak(self.h, {"fp32": 0, "mufu": 1}[unit], C.byref(ops), C.byref(ms)), self.h)
+        return {"ops_per_s": float(ops.value), "ms": float(ms.value)}
+
     @staticmethod
     def raster_candidates() -> list:
         """The supported compositing configurations (tile_w, tile_h, chunk depth, backward

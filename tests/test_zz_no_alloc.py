@@ -53,6 +53,37 @@ def test_bin_count_noalloc_matches_bin_count_on_two_calls():
     ctx.close()
 
 
+def test_bin_count_noalloc_allocates_nothing_at_its_largest_size():
+    """n = 16,777,216, the largest size the fixed scratch accepts (its 4,096 partial sums
+    and the total fill the array to its last word), on a fresh context: the result equals
+    the allocating entry point's, and neither the context's scratch arena nor the device's
+    free memory changes around the call."""
+    n = 16_777_216
+    torch.manual_seed(5)
+    nt = torch.randint(0, 4, (n,), dtype=torch.int32, device="cuda")
+    off = torch.full((n + 1,), -7, dtype=torch.int32, device="cuda")
+    torch.cuda.synchronize()
+    ctx = G.Context(0)
+    L = ctx.lib
+    # A first call resolves the scratch address once (no allocation either way).
+    e = C.c_int64(-1)
+    _lib.check(L.splat_bin_count_noalloc(ctx.h, C.c_void_p(nt.data_ptr()), 16, C.c_void_p(off.data_ptr()),
+                                         C.byref(e)), ctx.h)
+    torch.cuda.synchronize()
+    arena0 = ctx.scratch_info
+    free0 = torch.cuda.mem_get_info()[0]
+    _lib.check(L.splat_bin_count_noalloc(ctx.h, C.c_void_p(nt.data_ptr()), n, C.c_void_p(off.data_ptr()),
+                                         C.byref(e)), ctx.h)
+    torch.cuda.synchronize()
+    assert ctx.scratch_info == arena0 == (0, 0)
+    assert torch.cuda.mem_get_info()[0] == free0
+    got_off, got_e = off.cpu().numpy().copy(), int(e.value)
+    want_off, want_e = _count(ctx, L.splat_bin_count, nt)
+    assert got_e == want_e == int(nt.sum().item())
+    assert np.array_equal(got_off, want_off)
+    ctx.close()
+
+
 def test_bin_count_noalloc_rejects_sizes_beyond_its_scratch():
     """More counts than the fixed scratch covers: SPLAT_ERR_CAPACITY before any device work."""
     ctx = G.Context(0)
