@@ -155,6 +155,13 @@ typedef struct splat_train_config {
    * 0.9). */
   float learn_contribution;
   float learn_prune_confidence;
+  /* Not in the reference's config, but its arithmetic: 1 takes every iteration's compositing
+   * backward through splat_rasterize_bwd_deterministic's reduction (the reference's per-entry
+   * slots and ordered per-Gaussian sums), so the whole run equals the reference's CPU
+   * trainer (with correctly rounded exp/log) bit for bit; 0 (default) sums with float
+   * atomics, whose order is unspecified. Needs one view per iteration, 16x16 tiles, no
+   * autotuning, no BF16 copy and no f64 conics. */
+  int32_t deterministic;
 } splat_train_config;
 
 typedef struct splat_ctx splat_ctx;
@@ -289,6 +296,22 @@ SPLAT_API int splat_rasterize_bwd(splat_ctx* ctx, const float* proj_dev, const u
                                   const float background[3], const float* final_t_dev,
                                   const uint32_t* n_contrib_dev, const float* dimage_dev, float* pgrad_dev,
                                   int64_t cap, uint64_t* pairs_dev);
+
+/* The compositing backward with the reference's own reduction, bit for bit
+ * (src/rasterize.rs:341-505): every entry's 11 gradient slots (and the blending weight) are
+ * summed over its pixel rectangle in row-major order, in the reference's unfused f32
+ * arithmetic with the correctly rounded exp, stored per entry in emission order
+ * (rasterize.rs:449-454), then summed per Gaussian over its contiguous entries in order
+ * (:480-503). WRITES pgrad_dev (3 planes, stride cap), it does not accumulate. Needs the
+ * reference's 16x16 tiles (splat_set_raster_config) and entry_offset_dev / num_entries from
+ * splat_bin_count. Slower than splat_rasterize_bwd, whose float atomics sum in an
+ * unspecified order; for bit-exact comparison with the reference's CPU path. */
+SPLAT_API int splat_rasterize_bwd_deterministic(splat_ctx* ctx, const float* proj_dev, const uint32_t* gauss_dev,
+                                                const uint32_t* tile_range_dev, const uint32_t* entry_offset_dev,
+                                                int64_t n, int64_t num_entries, uint32_t width, uint32_t height,
+                                                const float background[3], const float* final_t_dev,
+                                                const uint32_t* n_contrib_dev, const float* dimage_dev,
+                                                float* pgrad_dev, int64_t cap);
 
 /* ----------------------------------------------------------------------------------------
  * Projection backward: project_backward_all (reference src/project.rs:477-493,

@@ -488,6 +488,27 @@ SPLAT_API int splat_rasterize_bwd(splat_ctx* ctx, const float* proj_dev, const u
                                        final_t_dev, n_contrib_dev, dimage_dev, pgrad_dev, cap, pairs_dev));
 }
 
+SPLAT_API int splat_rasterize_bwd_deterministic(splat_ctx* ctx, const float* proj_dev, const uint32_t* gauss_dev,
+                                                const uint32_t* tile_range_dev, const uint32_t* entry_offset_dev,
+                                                int64_t n, int64_t num_entries, uint32_t width, uint32_t height,
+                                                const float background[3], const float* final_t_dev,
+                                                const uint32_t* n_contrib_dev, const float* dimage_dev,
+                                                float* pgrad_dev, int64_t cap) {
+  if (!ctx) return SPLAT_ERR_INVALID;
+  if (width == 0 || height == 0 || width > 65535 || height > 65535)
+    return invalid(ctx, "splat_rasterize_bwd_deterministic: image size must be in 1..65535");
+  if (n < 0 || cap < n || num_entries < 0 || !background || !tile_range_dev || !final_t_dev || !n_contrib_dev ||
+      !dimage_dev || (n && (!entry_offset_dev || !pgrad_dev || !proj_dev)) || (num_entries && !gauss_dev))
+    return invalid(ctx, "splat_rasterize_bwd_deterministic: bad buffers");
+  Enter e(ctx);
+  float* eslot = nullptr;
+  Status s = arena_reserve(&ctx->c, (size_t)std::max<int64_t>(num_entries, 1) * 48, (void**)&eslot);
+  if (s.good())
+    s = launch_raster_bwd_det(&ctx->c, proj_dev, gauss_dev, tile_range_dev, entry_offset_dev, n, num_entries, width,
+                              height, background, final_t_dev, n_contrib_dev, dimage_dev, eslot, pgrad_dev, cap);
+  return finish(ctx, s);
+}
+
 SPLAT_API int splat_project_bwd(splat_ctx* ctx, const float* planes_dev, int64_t n, int64_t cap,
                                 const splat_camera* cam, const splat_proj_opts* opts, const float* proj_dev,
                                 const float* pgrad_dev, float* grad_planes_dev, void* stats_dev, int32_t absgrad) {

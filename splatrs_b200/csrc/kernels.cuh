@@ -180,6 +180,13 @@ Status launch_raster_bwd(Ctx* c, const float* proj, const uint32_t* gauss, const
                          uint32_t height, const float bg[3], const float* final_t, const uint32_t* n_contrib,
                          const float* dimage, float* pgrad, int64_t cap, uint64_t* pairs,
                          const BatchTable* bt = nullptr, uint32_t tiles_cap = 0);
+// The deterministic backward (16x16 tiles only): per-entry slot sums in the reference's
+// pixel order into eslot (12 floats per entry, e_cap entries, indexed by emission order),
+// then per-Gaussian sums in entry order written into pgrad (3 planes, stride cap).
+Status launch_raster_bwd_det(Ctx* c, const float* proj, const uint32_t* gauss, const uint32_t* ranges,
+                             const uint32_t* entry_offset, int64_t n, int64_t e_cap, uint32_t width, uint32_t height,
+                             const float bg[3], const float* final_t, const uint32_t* n_contrib, const float* dimage,
+                             float* eslot, float* pgrad, int64_t cap);
 
 Status launch_diag_fast_exp(Ctx* c, float magnitude_lo, float magnitude_hi, int negative, float* out_host);
 // Throughput of one unit (0: FP32 FMA, in FLOP/s; 1: MUFU ex2, in operations/s), peaks.cu.

@@ -70,6 +70,22 @@ __device__ __forceinline__ bool evaluate(float px, float py, float mx, float my,
   return true;
 }
 
+// evaluate (rasterize.rs:231-244) with the general correctly rounded exp: same values and
+// decisions as evaluate() (the narrow-range table form equals it on the whole argument range).
+__device__ __forceinline__ bool evaluate_ref(float px, float py, float mx, float my, float A, float B, float C,
+                                             float opacity, float sigma_max, float* gauss_out, float* alpha_out) {
+  const float dx = px - mx;
+  const float dy = py - my;
+  const float sigma = 0.5f * (A * dx * dx + C * dy * dy) + B * dx * dy;
+  if (sigma < 0.0f || sigma > sigma_max) return false;
+  const float gauss = crm::expf_cr(-sigma);
+  const float og = opacity * gauss;
+  if (og < SPLAT_ALPHA_MIN) return false;
+  *gauss_out = gauss;
+  *alpha_out = fminf(og, SPLAT_ALPHA_MAX);
+  return true;
+}
+
 // evaluate for the backward pass. The decisions must be the forward's, which were taken on
 // the correctly rounded exp; the value may carry a few ulps. A fast exp (MUFU ex2) decides
 // whenever the product opacity * gauss lies outside a relative band of kExpBand around the
@@ -563,6 +579,234 @@ __global__ void __launch_bounds__(TW * TH / PPL, (PPL == 1 ? 1024 : 768) / (TW *
     for (int o = 16; o > 0; o >>= 1) np += __shfl_xor_sync(0xffffffffu, np, o);
     if (lane == 0 && np) atomicAdd(pairs, np);
   }
+}
+
+// ---------------------------------------------------------------------------------------
+// Deterministic backward (16x16 tiles): the reference's own reduction, bit for bit.
+//
+// backward_tile (rasterize.rs:394-454) sums each entry's 11 slots over the pixels of its
+// rectangle in row-major order, in unfused f32 arithmetic, and stores them per entry;
+// rasterize_backward (:480-503) then sums every Gaussian's entries in entry order. Here a
+// block walks its tile's list in reverse like the atomic kernel, but every pixel writes its
+// per-entry contribution to shared memory (kDetGroup entries at a time) and one thread per
+// (entry, slot) adds the contributions of the rectangle's pixels in row-major order; the
+// per-entry sums go to a slot array indexed by the entry's emission index (Gaussian-major,
+// rasterize.rs:76-97), which entry_slots_reduce_kernel sums per Gaussian. Pixels that do not
+// contribute add +0.0, which leaves a sum unchanged (a sum that starts at +0.0 is never -0.0),
+// so the totals equal the reference's, which skips them. The arithmetic per pixel is the
+// reference's operation for operation: the correctly rounded exp of the forward, true
+// divisions, no contraction (the file is compiled with --fmad=false), and dalpha built from
+// 0.0 as the reference builds it.
+// ---------------------------------------------------------------------------------------
+constexpr int kDetGroup = 8;
+constexpr int kDetChunk = 64;
+constexpr size_t kDetSmemBytes = (size_t)kDetGroup * kSlots * 256 * sizeof(float);
+
+// Emission index of the entry of Gaussian g in tile (tx, ty): its entries are emitted row by
+// row over its tile rectangle (rasterize.rs:87-96).
+__device__ __forceinline__ uint32_t entry_index(const float4* __restrict__ rec,
+                                                const uint32_t* __restrict__ entry_offset, uint32_t g, uint32_t tx,
+                                                uint32_t ty) {
+  const float4 r3 = rec[4 * (size_t)g + 3];
+  const uint32_t tmin = fbits(r3.z), tmax = fbits(r3.w);
+  const uint32_t tx0 = tmin & 0xffffu, ty0 = tmin >> 16, w = (tmax & 0xffffu) - tx0;
+  return entry_offset[g] + (ty - ty0) * w + (tx - tx0);
+}
+
+__global__ void __launch_bounds__(256) raster_bwd_det_kernel(
+    const float4* __restrict__ rec, const uint32_t* __restrict__ gauss, const uint2* __restrict__ ranges,
+    const uint32_t* __restrict__ entry_offset, int64_t e_cap, uint32_t width, uint32_t height, uint32_t tiles_x,
+    float bg0, float bg1, float bg2, const float* __restrict__ final_t, const uint32_t* __restrict__ n_contrib,
+    const float* __restrict__ dimage, float* __restrict__ eslot) {
+  extern __shared__ float cbuf[];  // [kDetGroup][kSlots][256], pixel index row-major in the tile
+  __shared__ float4 s0[kDetChunk], s1[kDetChunk];
+  __shared__ float2 s2[kDetChunk];
+  __shared__ uint32_t srect[kDetChunk];
+  __shared__ uint32_t sent[kDetChunk];
+  __shared__ uint32_t s_max_last;
+  const uint32_t tile = blockIdx.x;
+  const uint32_t tx = tile % tiles_x, ty = tile / tiles_x;
+  const uint32_t ox = tx * 16u, oy = ty * 16u;
+  const uint32_t lx = threadIdx.x & 15u, ly = threadIdx.x >> 4;
+  const uint32_t x = ox + lx, y = oy + ly;
+  const bool inside = x < width && y < height;
+  const float px = (float)x + 0.5f, py = (float)y + 0.5f;
+  const uint2 range = ranges[tile];
+  const uint32_t list_len = range.y - range.x;
+  // Clipped extent of the tile (tile_geom, rasterize.rs:203-215).
+  const uint32_t gw = min(width - ox, 16u), gh = min(height - oy, 16u);
+
+  uint32_t last = 0;
+  float T = 1.0f, t_fin = 1.0f, d0 = 0.0f, d1 = 0.0f, d2 = 0.0f, bg_dot = 0.0f;
+  if (inside) {
+    const size_t pix = (size_t)y * width + x;
+    last = min(n_contrib[pix], list_len);
+    T = final_t[pix];
+    t_fin = T;
+    d0 = dimage[3 * pix];
+    d1 = dimage[3 * pix + 1];
+    d2 = dimage[3 * pix + 2];
+    bg_dot = bg0 * d0 + bg1 * d1 + bg2 * d2;
+  }
+  float acc_r = 0.0f, acc_g = 0.0f, acc_b = 0.0f, last_alpha = 0.0f, lc_r = 0.0f, lc_g = 0.0f, lc_b = 0.0f;
+  if (threadIdx.x == 0) s_max_last = 0;
+  __syncthreads();
+  const uint32_t wmax = __reduce_max_sync(0xffffffffu, last);
+  if ((threadIdx.x & 31u) == 0) atomicMax(&s_max_last, wmax);
+  __syncthreads();
+  const uint32_t max_last = s_max_last;
+  // Entries no pixel reaches keep zero slots.
+  for (uint32_t k = max_last + threadIdx.x; k < list_len; k += 256) {
+    const uint32_t e = entry_index(rec, entry_offset, gauss[range.x + k], tx, ty);
+    if (e < e_cap) {
+#pragma unroll
+      for (int q = 0; q < kSlots; q++) eslot[(size_t)e * kSlots + q] = 0.0f;
+    }
+  }
+
+  for (uint32_t cend = max_last; cend > 0;) {
+    const uint32_t cstart = cend > (uint32_t)kDetChunk ? cend - kDetChunk : 0u;
+    const uint32_t cnt = cend - cstart;
+    for (uint32_t e = threadIdx.x; e < cnt; e += 256) {
+      const uint32_t g = gauss[range.x + cstart + e];
+      s0[e] = rec[4 * (size_t)g];
+      s1[e] = rec[4 * (size_t)g + 1];
+      const float4 e2 = rec[4 * (size_t)g + 2];
+      s2[e] = make_float2(e2.x, e2.y);
+      srect[e] = tile_rect_masks<16, 16>(fbits(e2.z), fbits(e2.w), ox, oy);
+      sent[e] = entry_index(rec, entry_offset, g, tx, ty);
+    }
+    __syncthreads();
+    for (uint32_t gend = cnt; gend > 0;) {
+      const uint32_t gstart = gend > (uint32_t)kDetGroup ? gend - kDetGroup : 0u;
+      // Each pixel's contributions to the group's entries, in reverse depth order.
+      for (uint32_t kk = gend; kk-- > gstart;) {
+        const uint32_t j = gend - 1u - kk;
+        const uint32_t rm = srect[kk];
+        if (!inside || !((rm >> lx) & 1u) || !((rm >> (16u + ly)) & 1u)) continue;  // outside the rectangle
+        float c[kSlots];
+#pragma unroll
+        for (int q = 0; q < kSlots; q++) c[q] = 0.0f;
+        const uint32_t k = cstart + kk;
+        const float4 e0 = s0[kk], e1 = s1[kk];
+        const float2 e2 = s2[kk];
+        float gval, alpha;
+        if (k < last && evaluate_ref(px, py, e0.x, e0.y, e0.z, e0.w, e1.x, e1.y, e1.z, &gval, &alpha)) {
+          const float col_r = e1.w, col_g = e2.x, col_b = e2.y;
+          T = T / (1.0f - alpha);
+          const float t = T;
+          float dalpha = 0.0f;
+          acc_r = last_alpha * lc_r + (1.0f - last_alpha) * acc_r;
+          dalpha += (col_r - acc_r) * d0;
+          c[6] = alpha * t * d0;
+          acc_g = last_alpha * lc_g + (1.0f - last_alpha) * acc_g;
+          dalpha += (col_g - acc_g) * d1;
+          c[7] = alpha * t * d1;
+          acc_b = last_alpha * lc_b + (1.0f - last_alpha) * acc_b;
+          dalpha += (col_b - acc_b) * d2;
+          c[8] = alpha * t * d2;
+          dalpha *= t;
+          lc_r = col_r;
+          lc_g = col_g;
+          lc_b = col_b;
+          last_alpha = alpha;
+          dalpha += -t_fin / (1.0f - alpha) * bg_dot;
+          c[11] = alpha * t;
+          const float opacity = e1.y;
+          if (opacity * gval < SPLAT_ALPHA_MAX) {
+            c[5] = gval * dalpha;
+            const float dgauss = opacity * dalpha;
+            const float dsigma = -dgauss * gval;
+            const float dx = px - e0.x;
+            const float dy = py - e0.y;
+            const float ddx = dsigma * (e0.z * dx + e0.w * dy);
+            const float ddy = dsigma * (e0.w * dx + e1.x * dy);
+            c[0] = -ddx;
+            c[1] = -ddy;
+            c[2] = dsigma * 0.5f * dx * dx;
+            c[3] = dsigma * dx * dy;
+            c[4] = dsigma * 0.5f * dy * dy;
+            c[9] = fabsf(ddx);
+            c[10] = fabsf(ddy);
+          }
+        }
+#pragma unroll
+        for (int q = 0; q < kSlots; q++) cbuf[((size_t)j * kSlots + q) * 256 + threadIdx.x] = c[q];
+      }
+      __syncthreads();
+      // One thread per (entry, slot): the rectangle's pixels in row-major order.
+      if (threadIdx.x < (gend - gstart) * (uint32_t)kSlots) {
+        const uint32_t j = threadIdx.x / kSlots, q = threadIdx.x % kSlots;
+        const uint32_t kk = gend - 1u - j;
+        const uint32_t rm = srect[kk];
+        const uint32_t cols = rm & 0xffffu, rows = rm >> 16;
+        float a = 0.0f;
+        if (cols && rows) {
+          const uint32_t x0 = __ffs(cols) - 1u, x1 = min(32u - __clz(cols), gw);
+          const uint32_t y0 = __ffs(rows) - 1u, y1 = min(32u - __clz(rows), gh);
+          const float* b = cbuf + ((size_t)j * kSlots + q) * 256;
+          for (uint32_t yy = y0; yy < y1; yy++)
+            for (uint32_t xx = x0; xx < x1; xx++) a += b[yy * 16u + xx];
+        }
+        const uint32_t e = sent[kk];
+        if (e < e_cap) eslot[(size_t)e * kSlots + q] = a;
+      }
+      __syncthreads();
+      gend = gstart;
+    }
+    cend = cstart;
+  }
+}
+
+// The per-Gaussian sum of rasterize_backward (rasterize.rs:480-503): entries in emission
+// order from 0.0, into the screen-space gradient planes (written, not accumulated).
+__global__ void __launch_bounds__(256) entry_slots_reduce_kernel(const uint32_t* __restrict__ entry_offset,
+                                                                 int64_t n, const float4* __restrict__ eslot,
+                                                                 int64_t e_cap, float4* __restrict__ pgrad,
+                                                                 int64_t cap) {
+  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= n) return;
+  const int64_t s = entry_offset[g], e = min((int64_t)entry_offset[g + 1], e_cap);
+  float4 a = make_float4(0.0f, 0.0f, 0.0f, 0.0f), b = a, c = a;
+  for (int64_t i = s; i < e; i++) {
+    const float4 u = eslot[3 * i], v = eslot[3 * i + 1], w = eslot[3 * i + 2];
+    a.x += u.x; a.y += u.y; a.z += u.z; a.w += u.w;
+    b.x += v.x; b.y += v.y; b.z += v.z; b.w += v.w;
+    c.x += w.x; c.y += w.y; c.z += w.z; c.w += w.w;
+  }
+  pgrad[g] = a;
+  pgrad[cap + g] = b;
+  pgrad[2 * cap + g] = c;
+}
+
+Status launch_raster_bwd_det(Ctx* c, const float* proj, const uint32_t* gauss, const uint32_t* ranges,
+                             const uint32_t* entry_offset, int64_t n, int64_t e_cap, uint32_t width, uint32_t height,
+                             const float bg[3], const float* final_t, const uint32_t* n_contrib, const float* dimage,
+                             float* eslot, float* pgrad, int64_t cap) {
+  if (!c->raster.reference_tiles())
+    return Status::make(SPLAT_ERR_INVALID, "the deterministic backward needs the reference's 16x16 tiles");
+  static bool attr_set[64] = {};
+  if (c->device >= 0 && c->device < 64 && !attr_set[c->device]) {
+    SPLAT_CUDA(cudaFuncSetAttribute(raster_bwd_det_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)kDetSmemBytes));
+    attr_set[c->device] = true;
+  }
+  const uint32_t tiles_x = c->raster.tiles_x(width);
+  const uint32_t blocks = c->raster.tiles(width, height);
+  if (blocks > 0 && e_cap > 0) {
+    raster_bwd_det_kernel<<<blocks, 256, kDetSmemBytes, c->stream>>>(
+        reinterpret_cast<const float4*>(proj), gauss, reinterpret_cast<const uint2*>(ranges), entry_offset, e_cap,
+        width, height, tiles_x, bg[0], bg[1], bg[2], final_t, n_contrib, dimage, eslot);
+    c->launches.count++;
+    SPLAT_LAUNCHED("raster_bwd_det_kernel");
+  }
+  if (n > 0) {
+    entry_slots_reduce_kernel<<<ceil_div(n, 256), 256, 0, c->stream>>>(
+        entry_offset, n, reinterpret_cast<const float4*>(eslot), e_cap, reinterpret_cast<float4*>(pgrad), cap);
+    c->launches.count++;
+    SPLAT_LAUNCHED("entry_slots_reduce_kernel");
+  }
+  return Status::ok();
 }
 
 // Expands CALL(TW, TH, CH) for the configuration rc; an unsupported one is an error.

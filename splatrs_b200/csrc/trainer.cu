@@ -122,6 +122,7 @@ struct splat_trainer {
   DevBuf rec_x, rec_action, alive, useful, rec_csum, labels, label_counts, train_x, train_y, train_w;
   DevBuf mlp_theta, mlp_m, mlp_v, mlp_grad;
   DevBuf eval_out;  // splat_trainer_evaluate: loss, SSIM, PSNR per view
+  DevBuf eslot;     // cfg.deterministic: 12 gradient slots per tile entry (emission order)
   int64_t rec_n = 0;
   bool rec_valid = false;
   bool mlp_ready = false;
@@ -150,13 +151,15 @@ struct TEnter {
   }
 };
 
-// train.rs:132-137 (host f32 with the platform libm, as the reference).
+// train.rs:132-137 in host f32 with the correctly rounded exp and log the kernels use (the
+// platform's expf/logf misround some inputs; one of the 2,000 rates of a 2,000-iteration
+// run differs by an ulp).
 float position_lr(const splat_train_config& c, uint32_t iteration, float extent) {
   float t = (float)iteration / (float)std::max<uint32_t>(c.position_lr_max_steps, 1u);
   t = t < 0.0f ? 0.0f : (t > 1.0f ? 1.0f : t);
   const float init = c.position_lr_init * extent;
   const float fin = c.position_lr_final * extent;
-  return expf(logf(init) * (1.0f - t) + logf(fin) * t);
+  return crm::expf_cr(crm::logf_cr(init) * (1.0f - t) + crm::logf_cr(fin) * t);
 }
 
 // The statistics are three arrays of `cap` words (grad_accum, denom, max_radii) laid out
@@ -249,7 +252,7 @@ std::vector<uint64_t> graph_key(splat_trainer* t, const IterPlan& p) {
                              (uint64_t)p.densify_window, w, h, t->c->arena.generation, (uint64_t)t->stats_cap,
                              (uint64_t)t->batch, t->tiles_cap, t->pix_cap, t->c->raster.tile_w,
                              t->c->raster.tile_h, t->c->raster.chunk, t->c->raster.ppl};
-  for (const DevBuf* b : {&t->cur.params, &t->cur.m, &t->cur.v, &t->bf16, &t->stats, &t->pgrad, &t->pred_grad, &t->loss_out,
+  for (const DevBuf* b : {&t->cur.params, &t->cur.m, &t->cur.v, &t->bf16, &t->stats, &t->pgrad, &t->eslot, &t->pred_grad, &t->loss_out,
                           &t->params_dev, &t->batch_dev, &t->vb.proj, &t->vb.num_tiles, &t->vb.entry_offset, &t->vb.depth_range,
                           &t->vb.tile_range, &t->vb.gauss, &t->vb.image, &t->vb.final_t, &t->vb.n_contrib,
                           &t->vb.sort_scratch, &t->vb.scan_partial, &t->vb.counters})
@@ -294,10 +297,21 @@ Status body(splat_trainer* t, const IterPlan& p, int slot, bool probe = false) {
   SPLAT_TRY(launch_loss(c, t->vb.image.as<float>(), view.rgb.ptr, 1, cam.width, cam.height, cfg.lambda_dssim,
                         t->pred_grad.as<float>(), t->loss_out.as<float>(), sp));
   SPLAT_TRY(t->pgrad.ensure((size_t)cap * 48));
-  SPLAT_TRY(launch_fill_u32(c, t->pgrad.ptr, (size_t)cap * 12, 0u));
-  SPLAT_TRY(launch_raster_bwd(c, t->vb.proj.as<float>(), t->vb.gauss.as<uint32_t>(), t->vb.tile_range.as<uint32_t>(),
-                              cam.width, cam.height, bg, t->vb.final_t.as<float>(), t->vb.n_contrib.as<uint32_t>(),
-                              t->pred_grad.as<float>(), t->pgrad.as<float>(), cap, nullptr));
+  if (cfg.deterministic) {
+    // The reference's reduction (per-entry slots, ordered per-Gaussian sums); writes pgrad.
+    SPLAT_TRY(t->eslot.ensure((size_t)std::max<int64_t>(t->vb.e_cap, 1) * 48));
+    SPLAT_TRY(launch_raster_bwd_det(c, t->vb.proj.as<float>(), t->vb.gauss.as<uint32_t>(),
+                                    t->vb.tile_range.as<uint32_t>(), t->vb.entry_offset.as<uint32_t>(), n, t->vb.e_cap,
+                                    cam.width, cam.height, bg, t->vb.final_t.as<float>(),
+                                    t->vb.n_contrib.as<uint32_t>(), t->pred_grad.as<float>(), t->eslot.as<float>(),
+                                    t->pgrad.as<float>(), cap));
+  } else {
+    SPLAT_TRY(launch_fill_u32(c, t->pgrad.ptr, (size_t)cap * 12, 0u));
+    SPLAT_TRY(launch_raster_bwd(c, t->vb.proj.as<float>(), t->vb.gauss.as<uint32_t>(),
+                                t->vb.tile_range.as<uint32_t>(), cam.width, cam.height, bg, t->vb.final_t.as<float>(),
+                                t->vb.n_contrib.as<uint32_t>(), t->pred_grad.as<float>(), t->pgrad.as<float>(), cap,
+                                nullptr));
+  }
   // Optimiser step (train.rs:238-246), fused into the projection backward: the 59
   // gradients per Gaussian go from registers straight into Adam. A probe (autotuning)
   // leaves the model as it is.
@@ -629,7 +643,7 @@ Status density_control(splat_trainer* t, const IterPlan& p, splat_step_info* inf
     dp.cfg.max_screen_size = cfg.max_screen_size;
     dp.cfg.split_children = 2;
     dp.extent = t->extent;
-    dp.shrink = logf(0.8f * (float)dp.cfg.split_children);
+    dp.shrink = crm::logf_cr(0.8f * (float)dp.cfg.split_children);
     float* accum = t->stats.as<float>();
     uint32_t* denom = reinterpret_cast<uint32_t*>(accum + t->stats_cap);
     uint32_t* maxr = denom + t->stats_cap;
@@ -705,7 +719,7 @@ Status density_control(splat_trainer* t, const IterPlan& p, splat_step_info* inf
   }
   if (p.reset_now) {
     const float x = 0.01f;
-    const float limit = logf(x / (1.0f - x));  // inverse_sigmoid (math.rs:454)
+    const float limit = crm::logf_cr(x / (1.0f - x));  // inverse_sigmoid (math.rs:454)
     SPLAT_TRY(launch_reset_opacity(c, t->cur.params.as<float>(), t->cur.m.as<float>(), t->cur.v.as<float>(), t->n,
                                    limit));
     info->reset = 1;
@@ -863,6 +877,13 @@ SPLAT_API int splat_trainer_create(splat_ctx* ctx, const splat_train_config* cfg
     splat_ctx_impl(ctx)->last_error = "batch_views exceeds the maximum of 8";
     return SPLAT_ERR_INVALID;
   }
+  if (cfg->deterministic && (cfg->batch_views > 1 || cfg->autotune || cfg->bf16_storage || cfg->fp64_conic ||
+                             cfg->learned_densify || !splat_ctx_impl(ctx)->raster.reference_tiles())) {
+    splat_ctx_impl(ctx)->last_error =
+        "deterministic needs one view per iteration, the 16x16 tiles and no autotune, BF16 copy, f64 conics or "
+        "learned densification";
+    return SPLAT_ERR_INVALID;
+  }
   splat_trainer* t = new (std::nothrow) splat_trainer();
   if (!t) return SPLAT_ERR_INVALID;
   t->ctx = ctx;
@@ -909,7 +930,8 @@ SPLAT_API int splat_trainer_destroy(splat_trainer* t) {
     cudaStreamSynchronize(t->c->stream);
     t->cur.release();
     t->next.release();
-    for (DevBuf* b : {&t->pgrad, &t->stats, &t->pred_grad, &t->loss_out, &t->normals, &t->init, &t->bf16}) b->release();
+    for (DevBuf* b : {&t->pgrad, &t->stats, &t->pred_grad, &t->loss_out, &t->normals, &t->init, &t->bf16, &t->eslot})
+      b->release();
     for (DevBuf* b : {&t->birth, &t->birth_next, &t->origin, &t->origin_next, &t->feat, &t->feat_scratch, &t->policy,
                       &t->rec_x, &t->rec_action, &t->alive, &t->useful, &t->rec_csum, &t->labels, &t->label_counts,
                       &t->train_x, &t->eval_out,

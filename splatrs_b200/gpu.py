@@ -281,6 +281,24 @@ def rasterize_backward(ctx: Context, proj: Projection, b: Binning, background, o
     return pgrad
 
 
+def rasterize_backward_deterministic(ctx: Context, proj: Projection, b: Binning, background, out: RasterOutput,
+                                     dimage: torch.Tensor, pgrad: torch.Tensor | None = None,
+                                     cap: int | None = None) -> torch.Tensor:
+    """rasterize_backward (src/rasterize.rs:459-505) with the reference's own reduction
+    (per-entry slots in pixel order, ordered per-Gaussian sums): the screen-space gradient
+    planes (3, cap, 4), written (not accumulated), bit for bit the reference's."""
+    dev = proj.rec.device
+    cap = proj.n if cap is None else cap
+    if pgrad is None:
+        pgrad = torch.empty((3, cap, 4), dtype=torch.float32, device=dev)
+    bgp, keep = _bg(background)
+    check(ctx.lib.splat_rasterize_bwd_deterministic(
+        ctx.h, _ptr(proj.rec), _ptr(b.gauss), _ptr(b.tile_range), _ptr(b.entry_offset), proj.n, b.num_entries,
+        proj.width, proj.height, bgp, _ptr(out.final_t), _ptr(out.n_contrib), _ptr(dimage.contiguous()),
+        _ptr(pgrad), cap), ctx.h)
+    return pgrad
+
+
 def pgrad_to_reference(pgrad: torch.Tensor, n: int):
     """Screen-space gradient planes -> (ProjGrad (n, 9), abs (n, 2)) in the reference layout."""
     g0, g1, g2 = pgrad[0, :n], pgrad[1, :n], pgrad[2, :n]
