@@ -546,6 +546,46 @@ def run_train_gpu(local, s, cfg, iterations):
     return out, init, views, extent
 
 
+def run_blob_seeds(local, seeds=(0, 1, 2, 3, 4)):
+    """The small blob scene trained with the default backward (float atomics: sums in no
+    fixed order) and with the deterministic one (the reference's reduction; bit-identical to
+    the oracle trainer with correctly rounded exp/log, which the GPU tests check), for
+    trainer seeds 0-4 (view order and split draws): the PSNR gap atomic - deterministic per
+    seed, its mean and spread, and both modes' iterations per second."""
+    import torch
+    from splatrs_b200 import gpu as G
+    from splatrs_b200 import scenes
+    ctx = G.Context(local, torch.cuda.current_stream(local))
+    s = scenes.blob_scene()
+    views = gt_views_gpu(ctx, s)
+    ip = G.init_from_points(ctx, s["init_points"], s["init_rgb"])
+    n0 = len(s["init_points"])
+    init = G.planes_to_params(ctx, ip, n0, n0).cpu().numpy()
+    del ip
+    extent = scenes.scene_extent(s["cams"])
+    rows = []
+    for seed in seeds:
+        row = {"seed": seed}
+        for name, det in (("atomic", 0), ("deterministic", 1)):
+            t = G.Trainer(ctx, init, extent, views, **dict(BLOB_TRAIN, seed=seed, deterministic=det))
+            torch.cuda.synchronize(local)
+            tw = time.perf_counter()
+            t.run(BLOB_TRAIN["iterations"])
+            torch.cuda.synchronize(local)
+            wall = time.perf_counter() - tw
+            row[name] = {"psnr": round(t.evaluate()["psnr"], 3), "gaussians": t.count,
+                         "iters_per_s": round(BLOB_TRAIN["iterations"] / wall, 1)}
+            t.close()
+        row["gap_db"] = round(row["atomic"]["psnr"] - row["deterministic"]["psnr"], 3)
+        rows.append(row)
+    ctx.close()
+    gaps = np.array([r["gap_db"] for r in rows])
+    return {"seeds": rows, "mean_gap_db": round(float(gaps.mean()), 3), "std_gap_db": round(float(gaps.std(ddof=1)), 3),
+            "max_abs_gap_db": round(float(np.abs(gaps).max()), 3),
+            "note": "deterministic = the reference's reduction order, bit-identical to the correctly rounded "
+                    "oracle trainer (tests/test_gpu_deterministic.py); atomic = the default float-atomic backward"}
+
+
 def run_train_cpu(init, views, extent, cfg, iterations):
     """The same run on the CPU oracle trainer (all host threads), for `iterations` steps."""
     from oracle import oracle as O
@@ -871,6 +911,7 @@ def main():
         gpu_blobs, init, views, extent = run_train_gpu(local, scenes.blob_scene(), BLOB_TRAIN, BLOB_TRAIN["iterations"])
         line["train_blobs"] = {"gpu": gpu_blobs}
         blobs = (init, views, extent)
+        line["train_blobs"]["atomic_vs_deterministic"] = run_blob_seeds(local)
     if args.train_shells and not args.profile_small:
         from splatrs_b200 import scenes
         iters = args.train_shells_iters or SHELL_TRAIN["iterations"]

@@ -394,13 +394,15 @@ SPLAT_API int splat_mlp_adam(splat_ctx* ctx, float* theta_dev, const float* grad
  * rectangle is first narrowed to its 16-pixel tile rectangle). Chunk depth: entries
  * staged in shared memory per round, 32, 64, 128 or 256. Pixels per thread of the
  * backward: 1 or 2 (a warp then covers 8x8 pixels). Default 16x16, 256, 1.
- *   splat_raster_candidates: writes the 24 supported (tile_w, tile_h, chunk,
- *     pixels_per_thread) quadruples to out (96 values) and returns 24.
+ *   splat_raster_candidates: writes the supported (tile_w, tile_h, chunk,
+ *     pixels_per_thread) quadruples to out (4 values each; out may be NULL) and returns
+ *     how many (24).
  *   splat_set_raster_config: SPLAT_ERR_INVALID for an unsupported quadruple.
  *   splat_autotune_render: times projection + binning + forward + backward compositing of
  *     one view (dimage_dev: dL/dimage, H*W*3) under every candidate, `reps` timed passes
  *     each after an untimed one, sets the fastest on the context and writes the mean
- *     milliseconds per pass of every candidate to ms_out (24) and the pick to picked (4).
+ *     milliseconds per pass of every candidate to ms_out (one per candidate) and the pick
+ *     to picked (4).
  *     Synchronises; changes no caller buffer.
  * -------------------------------------------------------------------------------------- */
 SPLAT_API int32_t splat_raster_candidates(uint32_t* out);
@@ -565,12 +567,15 @@ SPLAT_API int splat_trainer_get_mlp(splat_trainer* t, float* theta_host);
 SPLAT_API int splat_trainer_set_mlp(splat_trainer* t, const float* theta_host);
 SPLAT_API int splat_trainer_mlp_stats(const splat_trainer* t, uint64_t out[9]);
 /* Autotuning (splat_train_config.autotune): the last tuning's milliseconds per render pass
- * of every candidate (ms_out, 24, in splat_raster_candidates order; 0 before any), the
+ * of every candidate (ms_out, one per candidate, in splat_raster_candidates order; 0 before any), the
  * configuration in use (picked, 4) and how many tunings ran. Any pointer may be NULL. */
 SPLAT_API int splat_trainer_tuning(const splat_trainer* t, float* ms_out, uint32_t* picked, uint32_t* tunes);
 SPLAT_API int32_t splat_trainer_sh_degree(const splat_trainer* t);
 SPLAT_API uint32_t splat_trainer_iteration(const splat_trainer* t);
 SPLAT_API int splat_trainer_get_model(splat_trainer* t, float* aos59_host);
+/* The optimiser's state: Adam's first and second moments (reference Adam::m / Adam::v,
+ * src/adam.rs:28-41), one 59-float record per Gaussian in the model's order. */
+SPLAT_API int splat_trainer_get_moments(splat_trainer* t, float* m_aos59_host, float* v_aos59_host);
 /* render::render of the current model at the active SH degree and the config's background. */
 SPLAT_API int splat_trainer_render(splat_trainer* t, const splat_camera* cam, float* image_host);
 /* evaluate (train.rs:309-321) on the device: renders every training view with the current

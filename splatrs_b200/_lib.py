@@ -219,6 +219,7 @@ def _declare(L):
         "splat_trainer_sh_degree": ([vp], i32),
         "splat_trainer_iteration": ([vp], u32),
         "splat_trainer_get_model": ([vp, vp], C.c_int),
+        "splat_trainer_get_moments": ([vp, vp, vp], C.c_int),
         "splat_trainer_render": ([vp, P(Camera), vp], C.c_int),
     })
     optional = {}

@@ -1127,6 +1127,26 @@ SPLAT_API int splat_trainer_get_model(splat_trainer* t, float* aos59_host) {
   return s.good() ? SPLAT_OK : tfail(t, s);
 }
 
+// Adam's first and second moments (Adam::m, Adam::v, reference src/adam.rs:28-41) in the
+// 59-float record layout, like splat_trainer_get_model.
+SPLAT_API int splat_trainer_get_moments(splat_trainer* t, float* m_aos59_host, float* v_aos59_host) {
+  if (!t || (t->n && (!m_aos59_host || !v_aos59_host))) return SPLAT_ERR_INVALID;
+  TEnter e(t);
+  Ctx* c = t->c;
+  DevBuf tmp;
+  Status s = tmp.ensure((size_t)std::max<int64_t>(t->n, 1) * 59 * 4);
+  for (int k = 0; k < 2 && s.good(); k++) {
+    s = launch_params_to_aos(c, (k ? t->cur.v : t->cur.m).as<float>(), t->n, t->cur.cap, tmp.as<float>());
+    if (s.good() && t->n)
+      s = cuda_status(cudaMemcpyAsync(k ? v_aos59_host : m_aos59_host, tmp.ptr, (size_t)t->n * 59 * 4,
+                                      cudaMemcpyDeviceToHost, c->stream),
+                      "download moments");
+    if (s.good()) s = cuda_status(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
+  }
+  tmp.release();
+  return s.good() ? SPLAT_OK : tfail(t, s);
+}
+
 // render::render of the current model at the trainer's active SH degree and background.
 SPLAT_API int splat_trainer_render(splat_trainer* t, const splat_camera* cam, float* image_host) {
   if (!t || !cam || !image_host || cam->width == 0 || cam->height == 0 || cam->width > 65535 || cam->height > 65535)

@@ -72,7 +72,7 @@ class Context:
         """The supported compositing configurations (tile_w, tile_h, chunk depth, backward
         pixels per thread)."""
         lib = L.lib()
-        out = (C.c_uint32 * 96)()
+        out = (C.c_uint32 * (4 * int(lib.splat_raster_candidates(None))))()
         k = int(lib.splat_raster_candidates(out))
         return [tuple(int(v) for v in out[4 * i:4 * i + 4]) for i in range(k)]
 
@@ -94,7 +94,7 @@ class Context:
     def autotune_render(self, planes, n, cap, cam, opts, background, dimage, reps: int = 3) -> dict:
         """Times one view's render + backward under every configuration and keeps the
         fastest; returns {config: ms per pass} and the pick."""
-        ms = (C.c_float * 24)()
+        ms = (C.c_float * int(self.lib.splat_raster_candidates(None)))()
         picked = (C.c_uint32 * 4)()
         bgp, _keep = _bg(background)
         check(self.lib.splat_autotune_render(self.h, _ptr(planes), n, cap, C.byref(cam), C.byref(opts), bgp,
@@ -540,7 +540,7 @@ class Trainer:
     def tuning(self) -> dict:
         """The autotuner's last timings (ms per render pass per configuration), the
         configuration in use and how many tunings ran."""
-        ms = (C.c_float * 24)()
+        ms = (C.c_float * int(self.lib.splat_raster_candidates(None)))()
         picked = (C.c_uint32 * 4)()
         tunes = C.c_uint32()
         check(self.lib.splat_trainer_tuning(self.h, ms, picked, C.byref(tunes)), self.ctx.h)
@@ -567,6 +567,15 @@ class Trainer:
         out = np.empty((self.count, 59), np.float32)
         check(self.lib.splat_trainer_get_model(self.h, out.ctypes.data_as(C.c_void_p)), self.ctx.h)
         return out
+
+    def moments(self):
+        """Adam's first and second moments, (count, 59) each (numpy float32)."""
+        import numpy as np
+        m = np.empty((self.count, 59), np.float32)
+        v = np.empty((self.count, 59), np.float32)
+        check(self.lib.splat_trainer_get_moments(self.h, m.ctypes.data_as(C.c_void_p), v.ctypes.data_as(C.c_void_p)),
+              self.ctx.h)
+        return m, v
 
     def render(self, cam):
         import numpy as np
