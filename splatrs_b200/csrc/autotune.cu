@@ -70,6 +70,7 @@ Status tune_render(Ctx* c, const float* planes, int64_t n, int64_t cap, const sp
       SPLAT_CUDA(cudaMemcpyAsync(w, v.counters.ptr, 16, cudaMemcpyDeviceToHost, c->stream));
       SPLAT_CUDA(cudaStreamSynchronize(c->stream));
       if (w[2] == 0) return Status::ok();
+      if (w[2] & 2u) return Status::make(SPLAT_ERR_TIMEOUT, "radix sort: a tile's look-back wait ran out");
       const uint64_t entries = (uint64_t)w[0] | ((uint64_t)w[1] << 32);
       v.e_cap = std::max<int64_t>(2 * v.e_cap, (int64_t)(entries + entries / 4 + 4096));
       if (v.e_cap >= 0xffffffffLL) return Status::make(SPLAT_ERR_CAPACITY, "too many tile entries for 32-bit offsets");

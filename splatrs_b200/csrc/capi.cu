@@ -154,6 +154,7 @@ SPLAT_API int splat_ctx_create(int device, void* stream, splat_ctx** out) {
     delete ctx;
     return SPLAT_ERR_CUDA;
   }
+  std::memset(ctx->c.host_small, 0, 4096);
   cudaSetDevice(prev);
   *out = ctx;
   return SPLAT_OK;
@@ -181,7 +182,9 @@ SPLAT_API int splat_ctx_set_stream(splat_ctx* ctx, void* stream) {
 SPLAT_API int splat_ctx_synchronize(splat_ctx* ctx) {
   if (!ctx) return SPLAT_ERR_INVALID;
   Enter e(ctx);
-  return finish(ctx, cuda_status(cudaStreamSynchronize(ctx->c.stream), "cudaStreamSynchronize"));
+  Status s = cuda_status(cudaStreamSynchronize(ctx->c.stream), "cudaStreamSynchronize");
+  if (s.good()) s = take_sort_error(&ctx->c);
+  return finish(ctx, s);
 }
 
 SPLAT_API const char* splat_last_error(const splat_ctx* ctx) { return ctx ? ctx->c.last_error.c_str() : "no context"; }
@@ -303,6 +306,7 @@ SPLAT_API int splat_bin_count(splat_ctx* ctx, const uint32_t* num_tiles_dev, int
   uint64_t* h = reinterpret_cast<uint64_t*>(ctx->c.host_small);
   if (s.good()) s = cuda_status(cudaMemcpyAsync(h, total, 8, cudaMemcpyDeviceToHost, ctx->c.stream), "read entry count");
   if (s.good()) s = cuda_status(cudaStreamSynchronize(ctx->c.stream), "cudaStreamSynchronize");
+  if (s.good()) s = take_sort_error(&ctx->c);
   if (!s.good()) return fail(ctx, s);
   if (h[0] >= 0xffffffffull) return fail(ctx, Status::make(SPLAT_ERR_CAPACITY, "too many tile entries for 32-bit offsets"));
   *num_entries = (int64_t)h[0];
@@ -322,6 +326,7 @@ SPLAT_API int splat_bin_sort(splat_ctx* ctx, const float* proj_dev, const uint32
   uint32_t* h = reinterpret_cast<uint32_t*>(ctx->c.host_small);
   Status s = cuda_status(cudaMemcpyAsync(h, depth_range_dev, 8, cudaMemcpyDeviceToHost, ctx->c.stream), "read depth range");
   if (s.good()) s = cuda_status(cudaStreamSynchronize(ctx->c.stream), "cudaStreamSynchronize");
+  if (s.good()) s = take_sort_error(&ctx->c);  // of an earlier sort on this context
   if (!s.good()) return fail(ctx, s);
   const uint32_t dmin = h[0], dmax = h[1];
   if (num_entries > 0 && dmin > dmax) return invalid(ctx, "splat_bin_sort: depth range is empty but entries exist");

@@ -102,6 +102,12 @@ Status launch_mlp_forward_tc(Ctx* c, const float* x, int64_t n, const float* the
 // Word of the context's mapped host page (c->host_small) that the tcgen05 kernels report
 // timeouts in.
 constexpr int kTcErrWord = 1000;
+// Word of the context's mapped host memory where a radix sort records a look-back wait that
+// ran out (bit 2); read and cleared by take_sort_error at the context's next synchronising
+// entry point.
+constexpr int kSortErrWord = 1001;
+constexpr size_t kAsyncErrorWordOffset = (size_t)kSortErrWord * 4;
+Status take_sort_error(Ctx* c);
 // Runs the tcgen05 forward with the error word cleared, synchronises and turns a reported
 // timeout into an error status.
 Status mlp_forward_tc_checked(Ctx* c, const float* x, int64_t n, const float* theta, float* prob);

@@ -112,6 +112,7 @@ Status render_view(Ctx* c, const float* planes, int64_t n, int64_t cap, const sp
   // on a copy engine (a renderer step's downloads overlap the next step).
   SPLAT_TRY(launch_publish_u32(c, reinterpret_cast<const uint32_t*>(total), 2, dr, 2));
   SPLAT_CUDA(cudaStreamSynchronize(c->stream));
+  SPLAT_TRY(take_sort_error(c));
   const volatile uint64_t* h = reinterpret_cast<const volatile uint64_t*>(c->host_small);
   const uint64_t E = h[0];
   if (E >= 0xffffffffull) return Status::make(SPLAT_ERR_CAPACITY, "too many tile entries for 32-bit offsets");

@@ -180,6 +180,13 @@ Status launch_publish_u32_to(Ctx* c, const uint32_t* a, int na, const uint32_t* 
   return Status::ok();
 }
 
+Status take_sort_error(Ctx* c) {
+  volatile uint32_t* w = reinterpret_cast<volatile uint32_t*>(c->host_small) + kSortErrWord;
+  if (*w == 0) return Status::ok();
+  *w = 0;
+  return Status::make(SPLAT_ERR_TIMEOUT, "radix sort: a tile's look-back wait ran out; that sort's output is invalid");
+}
+
 Status launch_scan_u32(Ctx* c, const uint32_t* in, int64_t n, uint32_t* out, int write_total, uint64_t* total_dev) {
   const uint32_t blocks = ceil_div((uint64_t)std::max<int64_t>(n, 1), kScanTile);
   uint64_t* partial = nullptr;
@@ -272,63 +279,128 @@ __global__ void __launch_bounds__(256) emit_keys_kernel(const float4* __restrict
 }
 
 // ---------------------------------------------------------------------------------------
-// Stable LSD radix sort, 8-bit digits, reduce-then-scan per pass.
-// A block sorts 4096 keys: 8 warps, each owning 512 consecutive keys that it ranks in
-// 16 rounds of 32 (position order), with match-any peer groups and per-warp digit
-// counters; a per-digit prefix over the warps then gives block-local stable ranks.
+// Stable LSD radix sort, 8-bit digits, one kernel per pass (onesweep).
+// One histogram kernel counts every pass's digits in a single read of the keys. Each pass
+// kernel then takes tiles of 4096 keys in ticket order (an atomic counter, so a tile only
+// ever waits for tiles whose blocks already run): 8 warps each rank 512 consecutive keys in
+// 16 rounds of 32 (position order) with match-any peer groups and per-warp digit counters;
+// a per-digit prefix over the warps gives block-local stable ranks. The tile's global
+// offset per digit is the digit's start (a prefix over the pass's histogram) plus the
+// counts of that digit in all earlier tiles, found by decoupled look-back: every tile
+// publishes its count per digit as soon as it has it (AGGREGATE), then its inclusive
+// prefix (PREFIX); a tile walks back over its predecessors' words, adding aggregates until
+// it meets a prefix. Every wait on a predecessor is bounded: past kLookbackSpins polls the
+// tile sets the error bit 2 in *err, sets the abort word so no other tile waits any longer,
+// and writes nothing (callers treat the sort as failed).
 // ---------------------------------------------------------------------------------------
 constexpr int kSortThreads = 256;
 constexpr int kSortWarps = kSortThreads / 32;
 constexpr int kSortRounds = 16;
 constexpr int kSortTile = kSortThreads * kSortRounds;  // 4096
+constexpr int kMaxPasses = 8;
+constexpr uint64_t kLbAggregate = 1ull << 62, kLbPrefix = 2ull << 62, kLbCount = (1ull << 62) - 1ull;
+constexpr uint32_t kLookbackSpins = 1u << 22;
+constexpr int kLbWindow = 16;
 
+// Control words of one sort (zeroed before it): the digit histogram of every pass, one
+// ticket counter per pass, the abort word, and per pass one look-back word per tile and digit.
+struct SortCtl {
+  uint32_t* hist;     // [kMaxPasses][256]
+  uint32_t* ticket;   // [kMaxPasses]
+  uint32_t* abort;    // [1]
+  uint64_t* status;   // [kMaxPasses][tiles][256]
+};
+inline size_t sort_ctl_bytes(uint64_t tiles) {
+  return (size_t)kMaxPasses * 256 * 4 + kMaxPasses * 4 + 8 + (size_t)kMaxPasses * tiles * 256 * 8 + 64;
+}
+inline SortCtl carve_sort_ctl(void* base, uint64_t tiles) {
+  SortCtl ctl;
+  char* b = static_cast<char*>(base);
+  ctl.status = reinterpret_cast<uint64_t*>(b);
+  b += (size_t)kMaxPasses * tiles * 256 * 8;
+  ctl.hist = reinterpret_cast<uint32_t*>(b);
+  b += (size_t)kMaxPasses * 256 * 4;
+  ctl.ticket = reinterpret_cast<uint32_t*>(b);
+  b += kMaxPasses * 4;
+  ctl.abort = reinterpret_cast<uint32_t*>(b);
+  return ctl;
+}
+
+// Digit histograms of `passes` passes over keys[0, n): per-block counters in shared memory
+// (native integer atomics), added to the global ones once per block.
 template <typename K>
-__device__ __forceinline__ void upsweep_body(const K* __restrict__ keys, int64_t n, int shift,
-                                             uint32_t* __restrict__ hist, uint32_t nblocks, uint32_t* cnt) {
-  cnt[threadIdx.x] = 0;
+__device__ __forceinline__ void hist_body(const K* __restrict__ keys, int64_t n, int passes,
+                                          uint32_t* __restrict__ hist, uint32_t (*cnt)[256]) {
+  for (int i = threadIdx.x; i < kMaxPasses * 256; i += blockDim.x) cnt[i >> 8][i & 255] = 0;
   __syncthreads();
-  const int64_t base = (int64_t)blockIdx.x * kSortTile;
-#pragma unroll 4
-  for (int r = 0; r < kSortRounds; r++) {
-    const int64_t idx = base + (int64_t)r * kSortThreads + threadIdx.x;
-    if (idx < n) {
-      const uint32_t d = (uint32_t)(keys[idx] >> shift) & 0xffu;
-      // Aggregate equal digits within the warp before the shared-memory atomic.
-      const uint32_t peers = __match_any_sync(__activemask(), d);
-      if ((threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&cnt[d], (uint32_t)__popc(peers));
-    }
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const K k = keys[i];
+    for (int p = 0; p < passes; p++) atomicAdd(&cnt[p][(uint32_t)(k >> (8 * p)) & 0xffu], 1u);
   }
   __syncthreads();
-  hist[(int64_t)threadIdx.x * nblocks + blockIdx.x] = cnt[threadIdx.x];
+  for (int i = threadIdx.x; i < passes * 256; i += blockDim.x) {
+    const uint32_t v = cnt[i >> 8][i & 255];
+    if (v) atomicAdd(&hist[i], v);
+  }
 }
 
 template <typename K>
-__global__ void __launch_bounds__(kSortThreads) radix_upsweep_kernel(const K* __restrict__ keys, int64_t n, int shift,
-                                                                     uint32_t* __restrict__ hist, uint32_t nblocks) {
-  __shared__ uint32_t cnt[256];
-  upsweep_body<K>(keys, n, shift, hist, nblocks, cnt);
+__global__ void __launch_bounds__(kSortThreads) radix_hist_kernel(const K* __restrict__ keys, int64_t n, int passes,
+                                                                  uint32_t* __restrict__ hist) {
+  __shared__ uint32_t cnt[kMaxPasses][256];
+  hist_body<K>(keys, n, passes, hist, cnt);
 }
 
-// Dynamic shared memory of the downsweep: the block's keys and values reordered by digit,
-// the per-warp digit counters and the block's digit starts.
-template <typename K> constexpr size_t downsweep_smem() {
-  return (size_t)kSortTile * (sizeof(K) + 4) + (size_t)kSortWarps * 256 * 4 + 256 * 4 + 64;
+// Dynamic shared memory of a pass: the tile's keys and values reordered by digit, the
+// per-warp digit counters, the digits' block starts and output offsets, scan scratch.
+template <typename K> constexpr size_t onesweep_smem() {
+  return (size_t)kSortTile * (sizeof(K) + 4) + (size_t)kSortWarps * 256 * 4 + 2 * 256 * 4 + 64;
 }
 
+// Exclusive prefix over the 256 digits of v (thread d holds digit d's value); `wsum` holds
+// kSortWarps words. Returns thread d's prefix.
+__device__ __forceinline__ uint32_t digit_exclusive(uint32_t v, uint32_t* wsum) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t incl = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  __syncthreads();
+  if (lane == 31) wsum[warp] = incl;
+  __syncthreads();
+  uint32_t wprefix = 0;
+  for (int w = 0; w < warp; w++) wprefix += wsum[w];
+  return wprefix + incl - v;
+}
+
+// One pass over keys_in[0, n) (digit at `shift`): `hist` is this pass's 256 global counts,
+// `status` its look-back words, `ticket` its tile counter.
 template <typename K>
-__device__ __forceinline__ void downsweep_body(const K* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
-                                               int64_t n, int shift, const uint32_t* __restrict__ offsets,
-                                               uint32_t nblocks, K* __restrict__ keys_out,
-                                               uint32_t* __restrict__ vals_out, unsigned char* dsm) {
+__device__ __forceinline__ void onesweep_body(const K* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
+                                              int64_t n, int shift, const uint32_t* __restrict__ hist,
+                                              uint64_t* __restrict__ status, uint32_t* __restrict__ ticket,
+                                              uint32_t* __restrict__ abort_word, uint32_t* __restrict__ err,
+                                              K* __restrict__ keys_out, uint32_t* __restrict__ vals_out,
+                                              unsigned char* dsm) {
   K* sk = reinterpret_cast<K*>(dsm);
   uint32_t* sv = reinterpret_cast<uint32_t*>(sk + kSortTile);
   uint32_t(*wcnt)[256] = reinterpret_cast<uint32_t(*)[256]>(sv + kSortTile);
   uint32_t* dstart = reinterpret_cast<uint32_t*>(wcnt) + kSortWarps * 256;
-  uint32_t* wsum = dstart + 256;
+  uint32_t* doff = dstart + 256;
+  uint32_t* wsum = doff + 256;  // kSortWarps words, then the tile number and the failure word
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t tiles = (n + kSortTile - 1) / kSortTile;
+  if (threadIdx.x == 0) {
+    wsum[kSortWarps] = atomicAdd(ticket, 1u);
+    wsum[kSortWarps + 1] = 0;
+  }
   for (int d = lane; d < 256; d += 32) wcnt[warp][d] = 0;
-  __syncwarp();
-  const int64_t bbase = (int64_t)blockIdx.x * kSortTile;
+  __syncthreads();
+  const uint32_t tile = wsum[kSortWarps];
+  if ((int64_t)tile >= tiles) return;
+  const int64_t bbase = (int64_t)tile * kSortTile;
   const int64_t wbase = bbase + (int64_t)warp * (32 * kSortRounds);
   K k[kSortRounds];
   uint32_t v[kSortRounds];
@@ -349,7 +421,7 @@ __device__ __forceinline__ void downsweep_body(const K* __restrict__ keys_in, co
     __syncwarp();
   }
   __syncthreads();
-  // Per digit (thread d): exclusive prefix over the warps and the block total.
+  // Per digit (thread d): exclusive prefix over the warps and the tile's count.
   const int d = threadIdx.x;
   uint32_t total = 0;
 #pragma unroll
@@ -358,20 +430,62 @@ __device__ __forceinline__ void downsweep_body(const K* __restrict__ keys_in, co
     wcnt[w][d] = total;
     total += c;
   }
-  // Block-wide exclusive scan of the totals over the digits.
-  uint32_t incl = total;
+  // Publish the tile's count of digit d at once; tile 0's is already its prefix.
+  volatile uint64_t* my_word = status + (size_t)tile * 256 + d;
+  *my_word = (tile == 0 ? kLbPrefix : kLbAggregate) | (uint64_t)total;
+  // Look back over the earlier tiles, kLbWindow words at a time (independent loads), nearest
+  // first: add aggregates until a prefix; a word not yet published is polled alone (bounded).
+  uint64_t excl = 0;
+  bool failed = false;
+  int64_t t = (int64_t)tile - 1;
+  while (t >= 0) {
+    uint64_t w[kLbWindow];
 #pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
-    if (lane >= o) incl += y;
+    for (int i = 0; i < kLbWindow; i++)
+      w[i] = t - i >= 0 ? *(const volatile uint64_t*)(status + (size_t)(t - i) * 256 + d) : kLbPrefix;
+    int i = 0;
+    bool done = false;
+#pragma unroll
+    for (int q = 0; q < kLbWindow; q++) {
+      if (done || i < q) continue;  // stopped at a prefix or an unpublished word before q
+      const uint64_t sq = w[q];
+      if ((sq >> 62) == 0) continue;
+      excl += sq & kLbCount;
+      i = q + 1;
+      if ((sq >> 62) == 2) done = true;
+    }
+    if (done) break;
+    t -= i;
+    if (i == kLbWindow) continue;
+    // Word t is not published yet: wait for it.
+    const volatile uint64_t* wp = status + (size_t)t * 256 + d;
+    uint32_t spins = 0;
+    while ((*wp >> 62) == 0) {
+      if (++spins >= kLookbackSpins || *(volatile uint32_t*)abort_word) {
+        failed = true;
+        break;
+      }
+      __nanosleep(32);
+    }
+    if (failed) break;
   }
-  if (lane == 31) wsum[warp] = incl;
+  if (failed) {
+    atomicOr(abort_word, 1u);
+    // A plain store: err may be mapped host memory. Racing writers all set the same bit.
+    volatile uint32_t* e = err;
+    *e = *e | 2u;
+    wsum[kSortWarps + 1] = 1;
+  } else if (tile > 0) {
+    *my_word = kLbPrefix | (excl + total);
+  }
+  // Block starts of the digits and the pass's global digit starts.
+  const uint32_t start = digit_exclusive(total, wsum);
+  dstart[d] = start;
+  const uint32_t gstart = digit_exclusive(hist[d], wsum);
+  doff[d] = gstart + (uint32_t)excl - start;  // output index = doff[digit] + block-sorted index
   __syncthreads();
-  uint32_t wprefix = 0;
-  for (int w = 0; w < warp; w++) wprefix += wsum[w];
-  dstart[d] = wprefix + incl - total;
-  __syncthreads();
-  // Reorder the block's keys by digit in shared memory (stable).
+  if (wsum[kSortWarps + 1]) return;
+  // Reorder the tile's keys by digit in shared memory (stable).
 #pragma unroll
   for (int r = 0; r < kSortRounds; r++) {
     const int64_t idx = wbase + r * 32 + lane;
@@ -388,20 +502,24 @@ __device__ __forceinline__ void downsweep_body(const K* __restrict__ keys_in, co
   for (int i = threadIdx.x; i < nb; i += kSortThreads) {
     const K key = sk[i];
     const uint32_t dg = (uint32_t)(key >> shift) & 0xffu;
-    const uint32_t pos = offsets[(int64_t)dg * nblocks + blockIdx.x] + (uint32_t)i - dstart[dg];
-    keys_out[pos] = key;
-    vals_out[pos] = sv[i];
+    const uint32_t pos = doff[dg] + (uint32_t)i;
+    if (pos < (uint64_t)n) {
+      keys_out[pos] = key;
+      vals_out[pos] = sv[i];
+    }
   }
 }
 
 template <typename K>
-__global__ void __launch_bounds__(kSortThreads) radix_downsweep_kernel(const K* __restrict__ keys_in,
-                                                                       const uint32_t* __restrict__ vals_in, int64_t n,
-                                                                       int shift, const uint32_t* __restrict__ offsets,
-                                                                       uint32_t nblocks, K* __restrict__ keys_out,
-                                                                       uint32_t* __restrict__ vals_out) {
+__global__ void __launch_bounds__(kSortThreads) radix_onesweep_kernel(const K* __restrict__ keys_in,
+                                                                      const uint32_t* __restrict__ vals_in, int64_t n,
+                                                                      int pass, SortCtl ctl, uint32_t* __restrict__ err,
+                                                                      K* __restrict__ keys_out,
+                                                                      uint32_t* __restrict__ vals_out) {
   extern __shared__ __align__(16) unsigned char dsm[];
-  downsweep_body<K>(keys_in, vals_in, n, shift, offsets, nblocks, keys_out, vals_out, dsm);
+  const uint64_t tiles = (uint64_t)((n + kSortTile - 1) / kSortTile);
+  onesweep_body<K>(keys_in, vals_in, n, 8 * pass, ctl.hist + 256 * pass, ctl.status + (size_t)pass * tiles * 256,
+                   ctl.ticket + pass, ctl.abort, err, keys_out, vals_out, dsm);
 }
 
 // Tile ranges (rasterize.rs:108-119) and, optionally, the reference 64-bit keys.
@@ -426,14 +544,19 @@ template <typename K>
 static Status sort_and_range(Ctx* c, const float* proj, const uint32_t* entry_offset, int64_t n, int64_t E,
                              const uint32_t* depth_range, int dbits, int total_bits, uint32_t tiles_x,
                              uint32_t num_tiles, uint32_t* gauss_out, uint64_t* keys_out, uint32_t* ranges) {
-  const int passes = (total_bits + 7) / 8;
-  SPLAT_CUDA(cudaFuncSetAttribute(radix_downsweep_kernel<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)downsweep_smem<K>()));
+  const int passes = std::max(1, (total_bits + 7) / 8);
+  SPLAT_CUDA(cudaFuncSetAttribute(radix_onesweep_kernel<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)onesweep_smem<K>()));
   K *ka = nullptr, *kb = nullptr;
   uint32_t* vb = nullptr;
   SPLAT_TRY(arena_reserve(c, (size_t)E * sizeof(K), (void**)&ka));
   SPLAT_TRY(arena_reserve(c, (size_t)E * sizeof(K), (void**)&kb));
   SPLAT_TRY(arena_reserve(c, (size_t)E * 4, (void**)&vb));
+  const uint64_t tiles = ceil_div(E, kSortTile);
+  void* ctl_base = nullptr;
+  SPLAT_TRY(arena_reserve(c, sort_ctl_bytes(tiles), &ctl_base));
+  const SortCtl ctl = carve_sort_ctl(ctl_base, tiles);
+  SPLAT_TRY(launch_fill_u32(c, ctl_base, sort_ctl_bytes(tiles) / 4, 0u));
   // Ping-pong so that the last pass writes the caller's buffer.
   uint32_t* va = (passes % 2 == 0) ? gauss_out : vb;
   uint32_t* vo = (passes % 2 == 0) ? vb : gauss_out;
@@ -442,25 +565,20 @@ static Status sort_and_range(Ctx* c, const float* proj, const uint32_t* entry_of
       reinterpret_cast<const float4*>(proj), entry_offset, n, tiles_x, depth_range, dbits, ka, va);
   c->launches.count++;
   SPLAT_LAUNCHED("emit_keys_kernel");
-  const uint32_t nblocks = ceil_div(E, kSortTile);
-  uint32_t* hist = nullptr;
-  uint32_t* offs = nullptr;
-  uint64_t* tot = nullptr;
-  SPLAT_TRY(arena_reserve(c, (size_t)nblocks * 256 * 4, (void**)&hist));
-  SPLAT_TRY(arena_reserve(c, (size_t)nblocks * 256 * 4, (void**)&offs));
-  SPLAT_TRY(arena_reserve(c, 8, (void**)&tot));
+  radix_hist_kernel<K><<<std::min<uint64_t>(tiles, (uint64_t)c->sm_count * 4), kSortThreads, 0, c->stream>>>(
+      ka, E, passes, ctl.hist);
+  c->launches.count++;
+  SPLAT_LAUNCHED("radix_hist_kernel");
+  uint32_t* err = reinterpret_cast<uint32_t*>(static_cast<char*>(c->host_small_dev) + kAsyncErrorWordOffset);
   K* kin = ka;
   K* kout = kb;
   uint32_t* vin = va;
   uint32_t* vout = vo;
   for (int p = 0; p < passes; p++) {
-    const int shift = 8 * p;
-    radix_upsweep_kernel<K><<<nblocks, kSortThreads, 0, c->stream>>>(kin, E, shift, hist, nblocks);
-    SPLAT_TRY(launch_scan_u32(c, hist, (int64_t)nblocks * 256, offs, 0, tot));
-    radix_downsweep_kernel<K><<<nblocks, kSortThreads, downsweep_smem<K>(), c->stream>>>(kin, vin, E, shift, offs,
-                                                                                         nblocks, kout, vout);
-    c->launches.count += 2;
-    SPLAT_LAUNCHED("radix sort pass");
+    radix_onesweep_kernel<K><<<(uint32_t)tiles, kSortThreads, onesweep_smem<K>(), c->stream>>>(kin, vin, E, p, ctl,
+                                                                                              err, kout, vout);
+    c->launches.count++;
+    SPLAT_LAUNCHED("radix_onesweep_kernel");
     std::swap(kin, kout);
     std::swap(vin, vout);
   }
@@ -530,29 +648,27 @@ __global__ void __launch_bounds__(256) emit_keys_dev_kernel(const float4* __rest
   emit_keys_body<uint64_t>(rec, entry_offset, n, tiles_x, depth_range, p.dbits, E_cap, keys, vals, bt, n_view);
 }
 
-__global__ void __launch_bounds__(kSortThreads) radix_upsweep_dev_kernel(const uint64_t* __restrict__ ka,
-                                                                         const uint64_t* __restrict__ kb,
-                                                                         const uint64_t* __restrict__ E_dev,
-                                                                         int64_t E_cap,
-                                                                         const uint32_t* __restrict__ dr, int tbits,
-                                                                         int pass, uint32_t* __restrict__ hist,
-                                                                         uint32_t nblocks) {
-  __shared__ uint32_t cnt[256];
+__global__ void __launch_bounds__(kSortThreads) radix_hist_dev_kernel(const uint64_t* __restrict__ keys,
+                                                                      const uint64_t* __restrict__ E_dev,
+                                                                      int64_t E_cap, const uint32_t* __restrict__ dr,
+                                                                      int tbits, uint32_t* __restrict__ hist) {
+  __shared__ uint32_t cnt[kMaxPasses][256];
   const DevSortPlan p = dev_sort_plan(E_dev, E_cap, dr, tbits);
-  if (pass >= p.passes) return;
-  upsweep_body<uint64_t>((pass & 1) ? kb : ka, p.E, 8 * pass, hist, nblocks, cnt);
+  hist_body<uint64_t>(keys, p.E, p.passes, hist, cnt);
 }
 
-__global__ void __launch_bounds__(kSortThreads) radix_downsweep_dev_kernel(
+__global__ void __launch_bounds__(kSortThreads) radix_onesweep_dev_kernel(
     uint64_t* __restrict__ ka, uint64_t* __restrict__ kb, uint32_t* __restrict__ va, uint32_t* __restrict__ vb,
     const uint64_t* __restrict__ E_dev, int64_t E_cap, const uint32_t* __restrict__ dr, int tbits, int pass,
-    const uint32_t* __restrict__ offsets, uint32_t nblocks, uint32_t* __restrict__ vals_final) {
+    SortCtl ctl, uint64_t tiles_cap, uint32_t* __restrict__ err, uint32_t* __restrict__ vals_final) {
   extern __shared__ __align__(16) unsigned char dsm[];
   const DevSortPlan p = dev_sort_plan(E_dev, E_cap, dr, tbits);
   if (pass >= p.passes) return;
   const bool odd = pass & 1;
   uint32_t* vout = pass == p.passes - 1 ? vals_final : (odd ? va : vb);
-  downsweep_body<uint64_t>(odd ? kb : ka, odd ? vb : va, p.E, 8 * pass, offsets, nblocks, odd ? ka : kb, vout, dsm);
+  onesweep_body<uint64_t>(odd ? kb : ka, odd ? vb : va, p.E, 8 * pass, ctl.hist + 256 * pass,
+                          ctl.status + (size_t)pass * tiles_cap * 256, ctl.ticket + pass, ctl.abort, err,
+                          odd ? ka : kb, vout, dsm);
 }
 
 __global__ void tile_ranges_dev_kernel(const uint64_t* __restrict__ ka, const uint64_t* __restrict__ kb,
@@ -569,9 +685,8 @@ __global__ void tile_ranges_dev_kernel(const uint64_t* __restrict__ ka, const ui
 
 size_t dev_sort_scratch_bytes(int64_t E_cap) {
   const uint64_t cap = (uint64_t)std::max<int64_t>(E_cap, 1);
-  const uint64_t nblocks = ceil_div(cap, kSortTile);
-  const uint64_t scan_blocks = ceil_div(nblocks * 256, kScanTile);
-  return 2 * cap * 8 + 2 * cap * 4 + 2 * nblocks * 256 * 4 + scan_blocks * 8 + 8 + 8 * 256;  // 8 pieces, 256-aligned
+  const uint64_t tiles = ceil_div(cap, kSortTile);
+  return 2 * cap * 8 + 2 * cap * 4 + sort_ctl_bytes(tiles) + 6 * 256;  // 5 pieces, 256-aligned
 }
 
 Status launch_bin_sort_dev(Ctx* c, const float* proj, const uint32_t* entry_offset, int64_t n, const uint64_t* E_dev,
@@ -583,8 +698,7 @@ Status launch_bin_sort_dev(Ctx* c, const float* proj, const uint32_t* entry_offs
   const int tbits = num_tiles <= 1 ? 0 : 32 - __builtin_clz(num_tiles - 1);
   const int max_passes = (tbits + 32 + 7) / 8;
   const uint64_t cap = (uint64_t)std::max<int64_t>(E_cap, 1);
-  const uint32_t nblocks = ceil_div(cap, kSortTile);
-  const uint64_t scan_blocks = ceil_div((uint64_t)nblocks * 256, kScanTile);
+  const uint64_t tiles = ceil_div(cap, kSortTile);
   // Carve the scratch (256-byte aligned pieces).
   auto carve = [&](size_t bytes) {
     void* p = scratch;
@@ -595,21 +709,22 @@ Status launch_bin_sort_dev(Ctx* c, const float* proj, const uint32_t* entry_offs
   uint64_t* kb = static_cast<uint64_t*>(carve(cap * 8));
   uint32_t* va = static_cast<uint32_t*>(carve(cap * 4));
   uint32_t* vb = static_cast<uint32_t*>(carve(cap * 4));
-  uint32_t* hist = static_cast<uint32_t*>(carve((size_t)nblocks * 256 * 4));
-  uint32_t* offs = static_cast<uint32_t*>(carve((size_t)nblocks * 256 * 4));
-  uint64_t* partial = static_cast<uint64_t*>(carve(scan_blocks * 8));
-  uint64_t* tot = static_cast<uint64_t*>(carve(8));
+  void* ctl_base = carve(sort_ctl_bytes(tiles));
+  const SortCtl ctl = carve_sort_ctl(ctl_base, tiles);
   // Once per device (and never inside a stream capture after the first call).
   static std::atomic<uint64_t> attr_done{0};
   if (c->device < 64 && !(attr_done.load() & (1ull << c->device))) {
-    SPLAT_CUDA(cudaFuncSetAttribute(radix_downsweep_dev_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)downsweep_smem<uint64_t>()));
+    SPLAT_CUDA(cudaFuncSetAttribute(radix_onesweep_dev_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)onesweep_smem<uint64_t>()));
     attr_done.fetch_or(1ull << c->device);
   } else if (c->device >= 64) {
-    SPLAT_CUDA(cudaFuncSetAttribute(radix_downsweep_dev_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)downsweep_smem<uint64_t>()));
+    SPLAT_CUDA(cudaFuncSetAttribute(radix_onesweep_dev_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)onesweep_smem<uint64_t>()));
   }
   SPLAT_TRY(launch_fill_u32(c, ranges, (size_t)num_tiles * 2, 0u));
+  // Only the passes these keys can need have look-back words to clear.
+  SPLAT_TRY(launch_fill_u32(c, ctl.status, (size_t)max_passes * tiles * 256 * 2, 0u));
+  SPLAT_TRY(launch_fill_u32(c, ctl.hist, (size_t)(kMaxPasses * 256 + kMaxPasses + 2), 0u));
   if (n > 0) {
     const uint32_t warps = ceil_div(n, 32);
     emit_keys_dev_kernel<<<ceil_div((uint64_t)warps * 32, 256), 256, 0, c->stream>>>(
@@ -618,14 +733,15 @@ Status launch_bin_sort_dev(Ctx* c, const float* proj, const uint32_t* entry_offs
     c->launches.count++;
     SPLAT_LAUNCHED("emit_keys_dev_kernel");
   }
+  radix_hist_dev_kernel<<<(uint32_t)std::min<uint64_t>(tiles, (uint64_t)c->sm_count * 4), kSortThreads, 0,
+                          c->stream>>>(ka, E_dev, E_cap, depth_range_dev, tbits, ctl.hist);
+  c->launches.count++;
+  SPLAT_LAUNCHED("radix_hist_dev_kernel");
   for (int pass = 0; pass < max_passes; pass++) {
-    radix_upsweep_dev_kernel<<<nblocks, kSortThreads, 0, c->stream>>>(ka, kb, E_dev, E_cap, depth_range_dev, tbits,
-                                                                       pass, hist, nblocks);
-    SPLAT_TRY(launch_scan_u32_into(c, hist, (int64_t)nblocks * 256, offs, 0, partial, tot));
-    radix_downsweep_dev_kernel<<<nblocks, kSortThreads, downsweep_smem<uint64_t>(), c->stream>>>(
-        ka, kb, va, vb, E_dev, E_cap, depth_range_dev, tbits, pass, offs, nblocks, gauss_out);
-    c->launches.count += 2;
-    SPLAT_LAUNCHED("radix sort pass (device-driven)");
+    radix_onesweep_dev_kernel<<<(uint32_t)tiles, kSortThreads, onesweep_smem<uint64_t>(), c->stream>>>(
+        ka, kb, va, vb, E_dev, E_cap, depth_range_dev, tbits, pass, ctl, tiles, overflow, gauss_out);
+    c->launches.count++;
+    SPLAT_LAUNCHED("radix_onesweep_dev_kernel");
   }
   tile_ranges_dev_kernel<<<ceil_div(cap, 256), 256, 0, c->stream>>>(ka, kb, E_dev, E_cap, depth_range_dev, tbits,
                                                                      ranges);

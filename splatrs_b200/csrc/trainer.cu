@@ -510,7 +510,8 @@ Status enqueue(splat_trainer* t, const IterPlan& p, int slot) {
 struct SlotResult {
   float loss, psnr;
   uint64_t entries;
-  bool overflow;
+  bool overflow;  // the binning overflowed its capacity (bit 1) or its sort failed (bit 2)
+  bool timeout;   // the sort's look-back wait ran out (bit 2): an error, not a capacity matter
 };
 
 SlotResult read_slot(splat_trainer* t, int slot) {
@@ -530,11 +531,15 @@ SlotResult read_slot(splat_trainer* t, int slot) {
   r.psnr = (float)(psnr / nv);
   r.entries = (uint64_t)w[3 * nv] | ((uint64_t)w[3 * nv + 1] << 32);
   r.overflow = w[3 * nv + 2] != 0;
+  r.timeout = (w[3 * nv + 2] & 2u) != 0;
   return r;
 }
 
-// After an overflow: room for the view that overflowed with a margin, the flag cleared.
-Status grow_entries(splat_trainer* t, uint64_t entries) {
+// After an overflow: room for the view that overflowed with a margin, the flag cleared. A
+// failed sort is an error instead.
+Status grow_entries(splat_trainer* t, const SlotResult& r) {
+  if (r.timeout) return Status::make(SPLAT_ERR_TIMEOUT, "radix sort: a tile's look-back wait ran out");
+  const uint64_t entries = r.entries;
   t->vb.e_cap = std::max<int64_t>(t->vb.e_cap * 2, (int64_t)(entries + entries / 4 + 4096));
   if (t->vb.e_cap >= 0xffffffffLL) return Status::make(SPLAT_ERR_CAPACITY, "too many tile entries for 32-bit offsets");
   return launch_fill_u32(t->c, t->vb.overflow_flag(), 1, 0u);
@@ -770,7 +775,7 @@ Status autotune(splat_trainer* t, const IterPlan& p) {
       SPLAT_CUDA(cudaStreamSynchronize(c->stream));
       const SlotResult r = read_slot(t, 0);
       if (!r.overflow) return Status::ok();
-      SPLAT_TRY(grow_entries(t, r.entries));
+      SPLAT_TRY(grow_entries(t, r));
       arena_reset(c);
     }
   };
@@ -789,7 +794,7 @@ Status run_one(splat_trainer* t, const IterPlan& p, int slot, SlotResult* out) {
     SPLAT_CUDA(cudaEventSynchronize(t->slot_done[slot]));
     *out = read_slot(t, slot);
     if (!out->overflow) return Status::ok();
-    SPLAT_TRY(grow_entries(t, out->entries));
+    SPLAT_TRY(grow_entries(t, *out));
   }
 }
 
@@ -832,7 +837,7 @@ Status run(splat_trainer* t, uint32_t count, splat_step_info* info) {
       const SlotResult pr = read_slot(t, pending_slot);
       if (pr.overflow) {
         SPLAT_CUDA(cudaEventSynchronize(t->slot_done[slot]));
-        SPLAT_TRY(grow_entries(t, pr.entries));
+        SPLAT_TRY(grow_entries(t, pr));
         SlotResult tmp;
         SPLAT_TRY(run_one(t, pending, pending_slot, &tmp));
         SPLAT_TRY(run_one(t, p, slot, &tmp));
@@ -843,7 +848,7 @@ Status run(splat_trainer* t, uint32_t count, splat_step_info* info) {
       SPLAT_CUDA(cudaEventSynchronize(t->slot_done[slot]));
       r = read_slot(t, slot);
       if (r.overflow) {
-        SPLAT_TRY(grow_entries(t, r.entries));
+        SPLAT_TRY(grow_entries(t, r));
         SPLAT_TRY(run_one(t, p, slot, &r));
       }
       SPLAT_TRY(density_control(t, p, info));
@@ -1210,7 +1215,11 @@ SPLAT_API int splat_trainer_evaluate(splat_trainer* t, float* per_view3_host, do
                                   "read binning counters");
     if (s.good()) s = cuda_status(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
     if (!s.good() || w[2] == 0) break;
-    s = grow_entries(t, (uint64_t)w[0] | ((uint64_t)w[1] << 32));
+    SlotResult gr{};
+    gr.entries = (uint64_t)w[0] | ((uint64_t)w[1] << 32);
+    gr.overflow = true;
+    gr.timeout = (w[2] & 2u) != 0;
+    s = grow_entries(t, gr);
   }
   std::vector<float> res(nv * 3);
   if (s.good())
