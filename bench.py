@@ -17,6 +17,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import subprocess
 import sys
@@ -47,16 +48,21 @@ def parse():
                     help="compositing configuration: 'auto' (autotune) or TWxTHxCHUNK[/PIXELS_PER_THREAD], "
                          "e.g. 16x16x256/2")
     ap.add_argument("--no-train", action="store_true", help="skip the small-scene training run (10k-Gaussian blobs, 256x256 views)")
-    ap.add_argument("--train-shells", action="store_true",
-                    help="also run plain training on the clustered 500k-Gaussian multi-view scene")
+    ap.add_argument("--no-train-shells", action="store_true",
+                    help="skip plain training on the clustered 500k-Gaussian multi-view scene (30,000 iterations) "
+                         "and its CPU samples")
     ap.add_argument("--train-shells-iters", type=int, default=0, help="iterations of that run (default: all 30,000)")
-    ap.add_argument("--shells-cpu-iters", type=int, default=5, help="iterations of its CPU oracle sample")
+    ap.add_argument("--shells-cpu-iters", type=int, default=3,
+                    help="timed CPU oracle iterations at each sampled model state of that run")
     ap.add_argument("--train-batched", action="store_true",
                     help="batched mixed-size BF16 training on the same scene (8 views per step)")
     ap.add_argument("--train-batched-iters", type=int, default=0, help="steps of that run (default: all 3,750)")
     ap.add_argument("--train-learned", action="store_true",
                     help="learned densification: learn on scene seeds 2-5, compare with the rule on seed 6")
     ap.add_argument("--learn-iters", type=int, default=1875, help="steps of each learning run")
+    ap.add_argument("--no-train-target", action="store_true",
+                    help="skip the training-target comparison (plain one-view trainer vs the batched, coarse-to-fine, "
+                         "learned-densification trainer on the clustered scene)")
     ap.add_argument("--profile-mlp", action="store_true",
                     help="only the densification network's forward (tcgen05) on 4M rows, for an ncu capture")
     ap.add_argument("--mlp-rows", type=int, default=4_000_000)
@@ -103,6 +109,19 @@ class ClockSampler:
     def _read(self):
         for line in self.proc.stdout:
             self.lines.append(line.strip())
+
+    def wait_first(self, timeout=2.0):
+        """Until the first sample arrives (or `timeout` s)."""
+        t0 = time.time()
+        while self.proc is not None and not self.lines and time.time() - t0 < timeout:
+            time.sleep(0.01)
+
+    def wait_next(self, timeout=2.0):
+        """Until one more sample arrives after this call (so the window closes after the
+        region it brackets)."""
+        n, t0 = len(self.lines), time.time()
+        while self.proc is not None and len(self.lines) <= n and time.time() - t0 < timeout:
+            time.sleep(0.01)
 
     def stop(self):
         if self.proc is None:
@@ -282,6 +301,11 @@ def run_ours(args, rank, world, local):
     visible = int((proj.num_tiles > 0).sum().item())
     torch.cuda.synchronize(dev)
 
+    # nvidia-smi samples every 100 ms, longer than the timed steps take: the sampler runs
+    # from before the warm-up to after the timed region, and waits for its first sample.
+    sampler = ClockSampler(local)
+    sampler.start()
+    sampler.wait_first()
     for _ in range(args.warmup):
         full_step()
     torch.cuda.synchronize(dev)
@@ -290,8 +314,6 @@ def run_ours(args, rank, world, local):
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize(dev)
-    sampler = ClockSampler(local)
-    sampler.start()
     launches0 = ctx.launches
     ev = [[torch.cuda.Event(enable_timing=True) for _ in range(6)] for _ in range(args.steps)]
     t0 = torch.cuda.Event(enable_timing=True)
@@ -302,6 +324,7 @@ def run_ours(args, rank, world, local):
     t1.record(stream)
     torch.cuda.synchronize(dev)
     launches = ctx.launches - launches0
+    sampler.wait_next()
     clocks = sampler.stop()
     elapsed_ms = max_over_ranks(t0.elapsed_time(t1), world, dev)
     if world > 1:
@@ -512,10 +535,105 @@ def run_learned_densify(local, learn_iters, learn=None, plain=True):
     return {"labels": learn_cfg, "learn": learn_log, "seed6": ev}
 
 
-def run_train_gpu(local, s, cfg, iterations):
+def target_config(batch, coarse_frac=2.0 / 3.0, views_total=30000, threshold=0.0002):
+    """The batched, coarse-to-fine trainer's schedule: the plain trainer's 30,000-view schedule
+    in steps of `batch` views (every step count divided by the batch), learning rates scaled
+    by sqrt(batch) (Adam's step does not grow with the summed gradient), and the first
+    `coarse_frac` of the steps on the views box-filtered by 2."""
+    it = views_total // batch
+    sc = math.sqrt(batch)
+    return dict(iterations=it, densify=1, densify_from_iter=500 // batch, densify_until_iter=15000 // batch,
+                densification_interval=max(1, 100 // batch), opacity_reset_interval=3000 // batch,
+                densify_grad_threshold=threshold, lambda_dssim=0.2, sh_degree=3,
+                sh_degree_interval=max(1, 1000 // batch), position_lr_max_steps=it, seed=0, max_gaussians=3_000_000,
+                batch_views=batch, position_lr_init=0.00016 * sc, position_lr_final=0.0000016 * sc,
+                feature_lr=0.0025 * sc, opacity_lr=0.025 * sc, scaling_lr=0.005 * sc, rotation_lr=0.001 * sc,
+                coarse_until=int(it * coarse_frac), coarse_factor=2)
+
+
+# The training target's trainer: batches of TARGET_BATCH views, coarse-to-fine, learned
+# densification (learned on scene seeds 2-5, applied on seed 6), graph-replayed.
+TARGET_BATCH = 2
+TARGET_THRESHOLD = 0.0002
+TARGET_LEARN = dict(learn_contribution=10.0, learn_prune_confidence=0.95)
+
+
+def run_train_target(local):
+    """The training target on the clustered 500k-Gaussian scene (seed 6), all 200 views at
+    1297x840: the plain one-view trainer (30,000 iterations, the reference's schedule)
+    against the batched, graph-replayed, coarse-to-fine trainer with learned densification
+    (the same 30,000 views), whose network first learns on four other scenes (seeds 2-5) with
+    the same schedule up to the end of densification. Reports each run's wall time, PSNR
+    over the 200 views at full resolution and Gaussian count, and the three ratios the
+    target sets bars on: PSNR within 0.1 dB of plain's, at least 1.5x less wall time, at
+    most 0.8x the Gaussians."""
+    import torch
+    from splatrs_b200 import gpu as G
+    from splatrs_b200 import scenes
+    ctx = G.Context(local, torch.cuda.current_stream(local))
+
+    def setup(seed):
+        sc = scenes.shell_scene(seed_gt=seed, seed_init=seed + 100)
+        views = gt_views_gpu(ctx, sc)
+        ip = G.init_from_points(ctx, sc["init_points"], sc["init_rgb"])
+        n0 = len(sc["init_points"])
+        init = G.planes_to_params(ctx, ip, n0, n0).cpu().numpy()
+        return init, views, scenes.scene_extent(sc["cams"])
+
+    def train(init, views, ext, cfg, theta=None, iterations=None):
+        t = G.Trainer(ctx, init, ext, views, **cfg)
+        if theta is not None:
+            t.set_mlp(theta)
+        torch.cuda.synchronize(local)
+        tw = time.perf_counter()
+        t.run(iterations or cfg["iterations"])
+        torch.cuda.synchronize(local)
+        wall = time.perf_counter() - tw
+        return t, wall
+
+    tcfg = target_config(TARGET_BATCH, threshold=TARGET_THRESHOLD)
+    theta, learn_log = None, []
+    for seed in (2, 3, 4, 5):
+        init, views, ext = setup(seed)
+        steps = tcfg["densify_until_iter"] + 2 * tcfg["densification_interval"]
+        t, wall = train(init, views, ext, dict(tcfg, learned_densify=1, **TARGET_LEARN), theta, steps)
+        st = t.mlp_stats()
+        theta = t.get_mlp()
+        learn_log.append({"seed": seed, "steps": steps, "wall_s": round(wall, 2), "records": st["records"],
+                          "heldout_accuracy_network": round(st["heldout_net"] / max(st["heldout_records"], 1), 4),
+                          "heldout_accuracy_rule": round(st["heldout_rule"] / max(st["heldout_records"], 1), 4)})
+        t.close()
+        del views
+    init, views, ext = setup(6)
+    res = {}
+    for name, cfg, th in (("plain", SHELL_TRAIN, None), ("target", dict(tcfg, learned_densify=2, **TARGET_LEARN), theta)):
+        t, wall = train(init, views, ext, cfg, th)
+        ev = t.evaluate()
+        res[name] = {"views_per_step": int(cfg.get("batch_views", 1) or 1), "steps": cfg["iterations"],
+                     "wall_s": round(wall, 2), "psnr": round(ev["psnr"], 3), "ssim": round(ev["ssim"], 4),
+                     "gaussians": t.count}
+        t.close()
+    ctx.close()
+    p, q = res["plain"], res["target"]
+    out = {"scene": "500k Gaussians on 40 shells, seed 6; 200 views at 1297x840",
+           "plain": p, "target": q, "learn": learn_log,
+           "target_settings": {"batch_views": TARGET_BATCH, "coarse": "first 2/3 of the steps at half resolution",
+                               "lr_scale": round(math.sqrt(TARGET_BATCH), 3), "densify_grad_threshold": TARGET_THRESHOLD,
+                               "learned_densify": "apply", **TARGET_LEARN},
+           "psnr_diff_db": round(q["psnr"] - p["psnr"], 3), "wall_time_ratio": round(p["wall_s"] / q["wall_s"], 3),
+           "gaussian_ratio": round(q["gaussians"] / max(p["gaussians"], 1), 3)}
+    out["bars_met"] = {"psnr_within_0.1db_or_above": out["psnr_diff_db"] >= -0.1,
+                       "wall_time_ratio_at_least_1.5": out["wall_time_ratio"] >= 1.5,
+                       "gaussian_ratio_at_most_0.8": out["gaussian_ratio"] <= 0.8}
+    return out
+
+
+def run_train_gpu(local, s, cfg, iterations, snapshots=()):
     """A plain training run on the device trainer: wall time, iterations/s, PSNR over the
     training views, final Gaussian count. Targets and initial model are built on the
-    device before the clock starts."""
+    device before the clock starts. `snapshots`: iteration numbers at which the model is
+    copied out (the run pauses there; the copy is outside the clock), returned with the
+    result as out["snapshots"] = [(iteration, model)], the initial model first."""
     import torch
     from splatrs_b200 import gpu as G
     from splatrs_b200 import scenes
@@ -527,11 +645,17 @@ def run_train_gpu(local, s, cfg, iterations):
     del init_planes
     extent = scenes.scene_extent(s["cams"])
     t = G.Trainer(ctx, init, extent, views, **cfg)
-    torch.cuda.synchronize(local)
-    tw = time.perf_counter()
-    t.run(iterations)  # splat_trainer_run: the whole run in one call, queued ahead of the device
-    torch.cuda.synchronize(local)
-    wall = time.perf_counter() - tw
+    snaps = [(0, init)] if snapshots else []
+    wall, done = 0.0, 0
+    for stop in sorted(set(int(x) for x in snapshots if 0 < x < iterations)) + [iterations]:
+        torch.cuda.synchronize(local)
+        tw = time.perf_counter()
+        t.run(stop - done)  # splat_trainer_run: the segment in one call, queued ahead of the device
+        torch.cuda.synchronize(local)
+        wall += time.perf_counter() - tw
+        done = stop
+        if snapshots:
+            snaps.append((stop, t.model()))
     ev = t.evaluate()  # splat_trainer_evaluate: every view scored on the device
     bv = max(1, int(cfg.get("batch_views", 1)))
     out = {"iterations": iterations, "wall_s": round(wall, 3), "iters_per_s": round(iterations / wall, 1),
@@ -541,9 +665,40 @@ def run_train_gpu(local, s, cfg, iterations):
         tu = t.tuning()
         out["autotune"] = {"tunes": tu["tunes"], "picked": list(tu["picked"]),
                            "ms_per_pass": {f"{a}x{b}x{c}/{d}": round(v, 4) for (a, b, c, d), v in tu["ms"].items()}}
+    if snapshots:
+        out["snapshots"] = snaps
     t.close()
     ctx.close()
     return out, init, views, extent
+
+
+def run_train_cpu_states(snaps, views, extent, cfg, iters, total_iters):
+    """CPU oracle time per iteration at several model states of a GPU run (the model copied
+    out at those iterations; fresh Adam moments, no densification, the SH degree ramped to
+    its final value over 3 untimed iterations, then `iters` timed ones), and the run's CPU
+    time extrapolated from them by the trapezoid rule over the iterations between states."""
+    from oracle import oracle as O
+    ccfg = {k: v for k, v in cfg.items() if k not in ("max_gaussians", "autotune")}
+    ccfg.update(densify=0, sh_degree_interval=1)
+    rows = []
+    for it, model in snaps:
+        ot = O.Trainer(model, extent, views, **ccfg)
+        for _ in range(3):
+            ot.step()
+        tw = time.perf_counter()
+        for _ in range(iters):
+            ot.step()
+        rows.append({"iteration": it, "gaussians": int(model.shape[0]),
+                     "s_per_iter": round((time.perf_counter() - tw) / iters, 4)})
+        del ot
+    est = 0.0
+    for a, b in zip(rows[:-1], rows[1:]):
+        est += 0.5 * (a["s_per_iter"] + b["s_per_iter"]) * (b["iteration"] - a["iteration"])
+    return {"states": rows, "extrapolated_s": round(est, 1), "iterations": total_iters,
+            "extrapolated_iters_per_s": round(total_iters / est, 4) if est > 0 else None, "cores": O.threads(),
+            "kind": "port",
+            "sample": (f"{iters} timed iterations (after 3 untimed) at each model state of the GPU run; the "
+                       f"{total_iters}-iteration CPU time is EXTRAPOLATED by the trapezoid rule between states")}
 
 
 def run_blob_seeds(local, seeds=(0, 1, 2, 3, 4)):
@@ -902,38 +1057,67 @@ def main():
         return
 
     line = run_ours(args, rank, world, local)
+
+    def leg(name, fn):
+        """Runs one optional leg; a failure is recorded in the line instead of losing it."""
+        try:
+            return fn()
+        except Exception as e:  # noqa: BLE001 - the headline line must survive any leg
+            import traceback
+            traceback.print_exc()
+            line.setdefault("leg_errors", {})[name] = f"{type(e).__name__}: {e}"
+            return None
+
     if not args.profile_small:
-        line["mlp"] = run_mlp(local, args.mlp_rows)
-        line["stages"] = run_stages(local)
+        line["mlp"] = leg("mlp", lambda: run_mlp(local, args.mlp_rows))
+        line["stages"] = leg("stages", lambda: run_stages(local))
     blobs = None
-    if not args.profile_small and not args.no_train:
+    train_legs = not args.profile_small and not args.no_train and world == 1
+    if train_legs:
         from splatrs_b200 import scenes
-        gpu_blobs, init, views, extent = run_train_gpu(local, scenes.blob_scene(), BLOB_TRAIN, BLOB_TRAIN["iterations"])
-        line["train_blobs"] = {"gpu": gpu_blobs}
-        blobs = (init, views, extent)
-        line["train_blobs"]["atomic_vs_deterministic"] = run_blob_seeds(local)
-    if args.train_shells and not args.profile_small:
+
+        def blob_leg():
+            gpu_blobs, init, views, extent = run_train_gpu(local, scenes.blob_scene(), BLOB_TRAIN,
+                                                           BLOB_TRAIN["iterations"])
+            return {"gpu": gpu_blobs}, (init, views, extent)
+        r = leg("train_blobs", blob_leg)
+        if r is not None:
+            line["train_blobs"], blobs = r
+            line["train_blobs"]["atomic_vs_deterministic"] = leg("atomic_vs_deterministic",
+                                                                 lambda: run_blob_seeds(local))
+    if train_legs and not args.no_train_shells:
         from splatrs_b200 import scenes
-        iters = args.train_shells_iters or SHELL_TRAIN["iterations"]
-        gpu_shells, init2, views2, extent2 = run_train_gpu(local, scenes.shell_scene(), SHELL_TRAIN, iters)
-        line["train_shells"] = {"gpu": gpu_shells}
-        if rank == 0 and world == 1 and args.shells_cpu_iters > 0:
-            line["train_shells"]["cpu"] = run_train_cpu(init2, views2, extent2, SHELL_TRAIN, args.shells_cpu_iters)
-            line["train_shells"]["cpu"]["sample"] = (f"first {args.shells_cpu_iters} iterations from the same initial "
-                                                 "model (no densification yet)")
-        del views2
-    if args.train_batched and not args.profile_small:
+
+        def shells_leg():
+            iters = args.train_shells_iters or SHELL_TRAIN["iterations"]
+            marks = [m for m in (7000, 15000) if m < iters]
+            gpu_shells, init2, views2, extent2 = run_train_gpu(local, scenes.shell_scene(), SHELL_TRAIN, iters, marks)
+            snaps = gpu_shells.pop("snapshots", [])
+            out = {"gpu": gpu_shells}
+            if rank == 0 and args.shells_cpu_iters > 0 and not args.no_cpu_baseline:
+                cpu = run_train_cpu_states(snaps, views2, extent2, SHELL_TRAIN, args.shells_cpu_iters, iters)
+                out["cpu"] = cpu
+                if cpu["extrapolated_s"]:
+                    out["gpu_over_cpu_extrapolated"] = round(cpu["extrapolated_s"] / gpu_shells["wall_s"], 1)
+            return out
+        line["train_shells"] = leg("train_shells", shells_leg)
+    if train_legs and args.train_batched:
         from splatrs_b200 import scenes
-        iters = args.train_batched_iters or BATCHED_TRAIN["iterations"]
-        gpu_batched, _, views3, _ = run_train_gpu(local, scenes.shell_scene_mixed_sizes(), BATCHED_TRAIN, iters)
-        line["train_batched"] = {"gpu": gpu_batched, "views_per_step": BATCHED_TRAIN["batch_views"],
-                            "sizes": "uniform over 640x480, 1024x768, 1297x840, 1600x1200 per view"}
-        del views3
-    if args.train_learned and not args.profile_small:
-        line["train_learned"] = run_learned_densify(local, args.learn_iters)
+
+        def batched_leg():
+            iters = args.train_batched_iters or BATCHED_TRAIN["iterations"]
+            gpu_batched, _, _, _ = run_train_gpu(local, scenes.shell_scene_mixed_sizes(), BATCHED_TRAIN, iters)
+            return {"gpu": gpu_batched, "views_per_step": BATCHED_TRAIN["batch_views"],
+                    "sizes": "uniform over 640x480, 1024x768, 1297x840, 1600x1200 per view"}
+        line["train_batched"] = leg("train_batched", batched_leg)
+    if train_legs and args.train_learned:
+        line["train_learned"] = leg("train_learned", lambda: run_learned_densify(local, args.learn_iters))
+    if train_legs and not args.no_train_target:
+        line["train_target"] = leg("train_target", lambda: run_train_target(local))
     if rank == 0:
         if blobs is not None and not args.no_cpu_baseline and world == 1:
-            line["train_blobs"]["cpu"] = run_train_cpu(*blobs, BLOB_TRAIN, BLOB_TRAIN["iterations"])
+            line["train_blobs"]["cpu"] = leg("train_blobs_cpu",
+                                             lambda: run_train_cpu(*blobs, BLOB_TRAIN, BLOB_TRAIN["iterations"]))
         if not args.no_cpu_baseline and world == 1:
             dt, cores, detail = cpu_reference_steps(args, args.cpu_steps)
             line["cpu_baseline"] = {"value": round(WIDTH * HEIGHT / 1e6 / dt, 4), "unit": UNIT, "cores": cores,

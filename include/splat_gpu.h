@@ -162,6 +162,13 @@ typedef struct splat_train_config {
    * atomics, whose order is unspecified. Needs one view per iteration, 16x16 tiles, no
    * autotuning, no BF16 copy and no f64 conics. */
   int32_t deterministic;
+  /* Not in the reference: coarse-to-fine training. Iterations 1..coarse_until train on
+   * every view box-filtered by coarse_factor (2 or 4; the camera's size, focal lengths and
+   * principal point divided by it, rows and columns past the last whole block dropped), the
+   * rest on the views as given. 0 (default) is off. Evaluation always uses the views as
+   * given. Not with `deterministic`. */
+  uint32_t coarse_until;
+  uint32_t coarse_factor;
 } splat_train_config;
 
 typedef struct splat_ctx splat_ctx;

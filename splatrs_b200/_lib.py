@@ -86,7 +86,8 @@ class TrainConfig(C.Structure):
                 ("near_plane", C.c_float), ("seed", C.c_uint64), ("max_gaussians", C.c_uint64),
                 ("entry_capacity", C.c_uint64), ("bf16_storage", C.c_int32), ("fp64_conic", C.c_int32),
                 ("batch_views", C.c_uint32), ("learned_densify", C.c_int32), ("autotune", C.c_int32),
-                ("learn_contribution", C.c_float), ("learn_prune_confidence", C.c_float), ("deterministic", C.c_int32)]
+                ("learn_contribution", C.c_float), ("learn_prune_confidence", C.c_float), ("deterministic", C.c_int32),
+                ("coarse_until", C.c_uint32), ("coarse_factor", C.c_uint32)]
 
     DEFAULTS = dict(iterations=30000, position_lr_init=0.00016, position_lr_final=0.0000016,
                     position_lr_max_steps=30000, feature_lr=0.0025, opacity_lr=0.025, scaling_lr=0.005,
@@ -96,7 +97,7 @@ class TrainConfig(C.Structure):
                     white_background=0, sh_degree=3, sh_degree_interval=1000, near_plane=0.2, seed=0,
                     max_gaussians=0, entry_capacity=0, bf16_storage=0, fp64_conic=0,
                     batch_views=0, learned_densify=0, autotune=0, learn_contribution=0.0,
-                    learn_prune_confidence=0.0, deterministic=0)
+                    learn_prune_confidence=0.0, deterministic=0, coarse_until=0, coarse_factor=2)
 
     @classmethod
     def make(cls, **kw):

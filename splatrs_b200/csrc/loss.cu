@@ -21,6 +21,8 @@ constexpr int kLT = 32;            // output tile edge
 constexpr int kHalo = 5;           // SSIM_WINDOW / 2
 constexpr int kLE = kLT + 2 * kHalo;
 constexpr int kLossThreads = 256;
+constexpr int kRB = 2;             // consecutive outputs per thread in each blur pass
+static_assert(kLT % kRB == 0, "blocks of kRB outputs tile the output rows and columns");
 
 struct LossKernel {
   float w[11];
@@ -74,70 +76,84 @@ __global__ void __launch_bounds__(kLossThreads) ssim_fwd_kernel(const float* __r
       sy[r][c] = vy;
     }
     __syncthreads();
-    // Horizontal pass (loss.rs:42-56) for every halo row and every output column.
-    for (int i = tid; i < kLE * kLT; i += kLossThreads) {
-      const int r = i / kLT, c = i % kLT;
-      const int gx = ox0 + c;
-      float a0 = 0.0f, a1 = 0.0f, a2 = 0.0f, a3 = 0.0f, a4 = 0.0f;
+    // Horizontal pass (loss.rs:42-56) for every halo row: a thread takes kRB consecutive
+    // output columns of a row from kRB + 10 inputs. Taps outside the image read the tile's
+    // zero padding and add +0.0, which leaves every sum as the reference's (it skips them).
+    for (int item = tid; item < kLE * (kLT / kRB); item += kLossThreads) {
+      const int r = item / (kLT / kRB), c0 = (item % (kLT / kRB)) * kRB;
+      float vx[kRB + 10], vy[kRB + 10];
 #pragma unroll
-      for (int k = 0; k < 11; k++) {
-        const int xs = gx + k - kHalo;
-        if (xs >= 0 && xs < (int)width) {
-          const float vx = sx[r][c + k], vy = sy[r][c + k];
-          a0 += K.w[k] * vx;
-          a1 += K.w[k] * vy;
-          a2 += K.w[k] * (vx * vx);
-          a3 += K.w[k] * (vy * vy);
-          a4 += K.w[k] * (vx * vy);
-        }
+      for (int q = 0; q < kRB + 10; q++) {
+        vx[q] = sx[r][c0 + q];
+        vy[q] = sy[r][c0 + q];
       }
-      h[0][r][c] = a0;
-      h[1][r][c] = a1;
-      h[2][r][c] = a2;
-      h[3][r][c] = a3;
-      h[4][r][c] = a4;
+#pragma unroll
+      for (int o = 0; o < kRB; o++) {
+        float a0 = 0.0f, a1 = 0.0f, a2 = 0.0f, a3 = 0.0f, a4 = 0.0f;
+#pragma unroll
+        for (int k = 0; k < 11; k++) {
+          const float x = vx[o + k], y = vy[o + k];
+          a0 += K.w[k] * x;
+          a1 += K.w[k] * y;
+          a2 += K.w[k] * (x * x);
+          a3 += K.w[k] * (y * y);
+          a4 += K.w[k] * (x * y);
+        }
+        h[0][r][c0 + o] = a0;
+        h[1][r][c0 + o] = a1;
+        h[2][r][c0 + o] = a2;
+        h[3][r][c0 + o] = a3;
+        h[4][r][c0 + o] = a4;
+      }
     }
     __syncthreads();
-    // Vertical pass (loss.rs:58-70) and per-pixel SSIM (loss.rs:101-119).
-    for (int i = tid; i < kLT * kLT; i += kLossThreads) {
-      const int r = i / kLT, c = i % kLT;
-      const int gy = oy0 + r, gx = ox0 + c;
-      if (gx >= (int)width || gy >= (int)height) continue;
-      float mx = 0.0f, my = 0.0f, exx = 0.0f, eyy = 0.0f, exy = 0.0f;
+    // Vertical pass (loss.rs:58-70) and per-pixel SSIM (loss.rs:101-119): a thread takes kRB
+    // consecutive rows of a column.
+    for (int item = tid; item < kLT * (kLT / kRB); item += kLossThreads) {
+      const int c = item % kLT, r0 = (item / kLT) * kRB;
+      float col[5][kRB + 10];
 #pragma unroll
-      for (int k = 0; k < 11; k++) {
-        const int ys = gy + k - kHalo;
-        if (ys >= 0 && ys < (int)height) {
+      for (int m = 0; m < 5; m++)
+#pragma unroll
+        for (int q = 0; q < kRB + 10; q++) col[m][q] = h[m][r0 + q][c];
+#pragma unroll
+      for (int o = 0; o < kRB; o++) {
+        const int r = r0 + o;
+        const int gy = oy0 + r, gx = ox0 + c;
+        float mx = 0.0f, my = 0.0f, exx = 0.0f, eyy = 0.0f, exy = 0.0f;
+#pragma unroll
+        for (int k = 0; k < 11; k++) {
           const float kv = K.w[k];
-          mx += kv * h[0][r + k][c];
-          my += kv * h[1][r + k][c];
-          exx += kv * h[2][r + k][c];
-          eyy += kv * h[3][r + k][c];
-          exy += kv * h[4][r + k][c];
+          mx += kv * col[0][o + k];
+          my += kv * col[1][o + k];
+          exx += kv * col[2][o + k];
+          eyy += kv * col[3][o + k];
+          exy += kv * col[4][o + k];
         }
+        if (gx >= (int)width || gy >= (int)height) continue;
+        const float sx2 = exx - mx * mx;
+        const float sy2 = eyy - my * my;
+        const float sxy = exy - mx * my;
+        const float n1 = 2.0f * mx * my + c1;
+        const float n2 = 2.0f * sxy + c2;
+        const float d1 = mx * mx + my * my + c1;
+        const float d2 = sx2 + sy2 + c2;
+        const float num = n1 * n2;
+        const float den = d1 * d2;
+        const float sv = num / den;
+        const float dn_dmx = 2.0f * my * n2 - 2.0f * my * n1;
+        const float dd_dmx = 2.0f * mx * d2 - 2.0f * mx * d1;
+        const size_t idx = ((size_t)gy * width + gx) * 3 + ch;
+        const size_t npix3 = (size_t)width * height * 3;
+        dmaps[idx] = (dn_dmx * den - num * dd_dmx) / (den * den);
+        dmaps[npix3 + idx] = -num * d1 / (den * den);
+        dmaps[2 * npix3 + idx] = 2.0f * n1 / den;
+        const float x = sx[r + kHalo][c + kHalo], y = sy[r + kHalo][c + kHalo];
+        s_ssim += (double)sv;
+        s_l1 += (double)fabsf(x - y);
+        const double e = (double)fminf(fmaxf(x, 0.0f), 1.0f) - (double)fminf(fmaxf(y, 0.0f), 1.0f);
+        s_se += e * e;
       }
-      const float sx2 = exx - mx * mx;
-      const float sy2 = eyy - my * my;
-      const float sxy = exy - mx * my;
-      const float n1 = 2.0f * mx * my + c1;
-      const float n2 = 2.0f * sxy + c2;
-      const float d1 = mx * mx + my * my + c1;
-      const float d2 = sx2 + sy2 + c2;
-      const float num = n1 * n2;
-      const float den = d1 * d2;
-      const float s = num / den;
-      const float dn_dmx = 2.0f * my * n2 - 2.0f * my * n1;
-      const float dd_dmx = 2.0f * mx * d2 - 2.0f * mx * d1;
-      const size_t idx = ((size_t)gy * width + gx) * 3 + ch;
-      const size_t npix3 = (size_t)width * height * 3;
-      dmaps[idx] = (dn_dmx * den - num * dd_dmx) / (den * den);
-      dmaps[npix3 + idx] = -num * d1 / (den * den);
-      dmaps[2 * npix3 + idx] = 2.0f * n1 / den;
-      const float x = sx[r + kHalo][c + kHalo], y = sy[r + kHalo][c + kHalo];
-      s_ssim += (double)s;
-      s_l1 += (double)fabsf(x - y);
-      const double e = (double)fminf(fmaxf(x, 0.0f), 1.0f) - (double)fminf(fmaxf(y, 0.0f), 1.0f);
-      s_se += e * e;
     }
     __syncthreads();
   }
@@ -209,46 +225,52 @@ __global__ void __launch_bounds__(kLossThreads) ssim_bwd_kernel(const float* __r
       sm[2][r][c] = e;
     }
     __syncthreads();
-    for (int i = tid; i < kLE * kLT; i += kLossThreads) {
-      const int r = i / kLT, c = i % kLT;
-      const int gx = ox0 + c;
-      float a0 = 0.0f, a1 = 0.0f, a2 = 0.0f;
+    // The blur of the three partial maps (loss.rs:124-127), blocked as in ssim_fwd_kernel;
+    // zero-padded taps add +0.0 (the sums start at +0.0 and never become -0.0).
+    for (int item = tid; item < kLE * (kLT / kRB); item += kLossThreads) {
+      const int r = item / (kLT / kRB), c0 = (item % (kLT / kRB)) * kRB;
 #pragma unroll
-      for (int k = 0; k < 11; k++) {
-        const int xs = gx + k - kHalo;
-        if (xs >= 0 && xs < (int)width) {
-          a0 += K.w[k] * sm[0][r][c + k];
-          a1 += K.w[k] * sm[1][r][c + k];
-          a2 += K.w[k] * sm[2][r][c + k];
+      for (int m = 0; m < 3; m++) {
+        float v[kRB + 10];
+#pragma unroll
+        for (int q = 0; q < kRB + 10; q++) v[q] = sm[m][r][c0 + q];
+#pragma unroll
+        for (int o = 0; o < kRB; o++) {
+          float a = 0.0f;
+#pragma unroll
+          for (int k = 0; k < 11; k++) a += K.w[k] * v[o + k];
+          h[m][r][c0 + o] = a;
         }
       }
-      h[0][r][c] = a0;
-      h[1][r][c] = a1;
-      h[2][r][c] = a2;
     }
     __syncthreads();
-    for (int i = tid; i < kLT * kLT; i += kLossThreads) {
-      const int r = i / kLT, c = i % kLT;
-      const int gy = oy0 + r, gx = ox0 + c;
-      if (gx >= (int)width || gy >= (int)height) continue;
-      float bmu = 0.0f, bexx = 0.0f, bexy = 0.0f;
+    for (int item = tid; item < kLT * (kLT / kRB); item += kLossThreads) {
+      const int c = item % kLT, r0 = (item / kLT) * kRB;
+      float col[3][kRB + 10];
 #pragma unroll
-      for (int k = 0; k < 11; k++) {
-        const int ys = gy + k - kHalo;
-        if (ys >= 0 && ys < (int)height) {
+      for (int m = 0; m < 3; m++)
+#pragma unroll
+        for (int q = 0; q < kRB + 10; q++) col[m][q] = h[m][r0 + q][c];
+#pragma unroll
+      for (int o = 0; o < kRB; o++) {
+        const int gy = oy0 + r0 + o, gx = ox0 + c;
+        float bmu = 0.0f, bexx = 0.0f, bexy = 0.0f;
+#pragma unroll
+        for (int k = 0; k < 11; k++) {
           const float kv = K.w[k];
-          bmu += kv * h[0][r + k][c];
-          bexx += kv * h[1][r + k][c];
-          bexy += kv * h[2][r + k][c];
+          bmu += kv * col[0][o + k];
+          bexx += kv * col[1][o + k];
+          bexy += kv * col[2][o + k];
         }
+        if (gx >= (int)width || gy >= (int)height) continue;
+        const size_t idx = ((size_t)gy * width + gx) * 3 + ch;
+        const float x = pred[idx];
+        const float y = load_target(target, target_u8, idx);
+        const float dssim = (bmu + 2.0f * x * bexx + y * bexy) * inv_n;
+        const float d = x - y;
+        const float sign = d > 0.0f ? 1.0f : (d < 0.0f ? -1.0f : 0.0f);
+        grad[idx] = (w1 * sign - lambda * dssim) * scale;
       }
-      const size_t idx = ((size_t)gy * width + gx) * 3 + ch;
-      const float x = pred[idx];
-      const float y = load_target(target, target_u8, idx);
-      const float dssim = (bmu + 2.0f * x * bexx + y * bexy) * inv_n;
-      const float d = x - y;
-      const float sign = d > 0.0f ? 1.0f : (d < 0.0f ? -1.0f : 0.0f);
-      grad[idx] = (w1 * sign - lambda * dssim) * scale;
     }
     __syncthreads();
   }

@@ -40,7 +40,37 @@ struct SplitMix64 {
 struct View {
   splat_camera cam;
   DevBuf rgb;  // H*W*3 uint8
+  // Coarse copy for the first cfg.coarse_until iterations (not in the reference): the view
+  // box-filtered by cfg.coarse_factor, with the camera scaled to match.
+  splat_camera coarse_cam;
+  DevBuf coarse_rgb;
 };
+
+// Box filter of an 8-bit RGB image by an integer factor f (output pixel (x, y) averages the
+// f x f input pixels from (f x, f y), rounded to nearest; rows and columns past the last
+// whole block are dropped).
+__global__ void box_downscale_u8_kernel(const uint8_t* __restrict__ in, uint32_t w, uint32_t h, uint32_t f,
+                                        uint8_t* __restrict__ out, uint32_t w2, uint32_t h2) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (uint64_t)w2 * h2 * 3) return;
+  const uint32_t ch = (uint32_t)(i % 3), px = (uint32_t)((i / 3) % w2), py = (uint32_t)(i / 3 / w2);
+  uint32_t sum = 0;
+  for (uint32_t dy = 0; dy < f; dy++)
+    for (uint32_t dx = 0; dx < f; dx++) sum += in[((size_t)(f * py + dy) * w + f * px + dx) * 3 + ch];
+  out[i] = (uint8_t)((sum + f * f / 2) / (f * f));
+}
+
+// The camera of a view downscaled by f: pixel centres (i + 0.5) / f of the original.
+splat_camera scaled_camera(const splat_camera& c, uint32_t f) {
+  splat_camera s = c;
+  s.width = c.width / f;
+  s.height = c.height / f;
+  s.fx = c.fx / (float)f;
+  s.fy = c.fy / (float)f;
+  s.cx = c.cx / (float)f;
+  s.cy = c.cy / (float)f;
+  return s;
+}
 
 // The model and its optimiser state, in parameter-plane layout with capacity `cap`.
 struct ModelBufs {
@@ -202,7 +232,12 @@ struct IterPlan {
   splat_lr lr{};
   uint64_t adam_step = 0;
   bool densify_window = false, densify_now = false, reset_now = false;
+  bool coarse = false;  // the iteration trains on the views' coarse copies
 };
+
+// The camera and target of view v for iteration p (its coarse copy while p.coarse).
+const splat_camera& plan_cam(const IterPlan& p, const View& v) { return p.coarse ? v.coarse_cam : v.cam; }
+const void* plan_rgb(const IterPlan& p, const View& v) { return p.coarse ? v.coarse_rgb.ptr : v.rgb.ptr; }
 
 IterPlan schedule(splat_trainer* t) {
   const splat_train_config& cfg = t->cfg;
@@ -241,11 +276,12 @@ IterPlan schedule(splat_trainer* t) {
   p.densify_now = p.densify_window && p.it > cfg.densify_from_iter && p.it % cfg.densification_interval == 0;
   p.reset_now = p.densify_window && cfg.opacity_reset_interval > 0 &&
                 (p.it % cfg.opacity_reset_interval == 0 || (cfg.white_background && p.it == cfg.densify_from_iter));
+  p.coarse = cfg.coarse_until > 0 && p.it <= cfg.coarse_until;
   return p;
 }
 
 std::vector<uint64_t> graph_key(splat_trainer* t, const IterPlan& p) {
-  const splat_camera& cam = t->views[p.view]->cam;
+  const splat_camera& cam = plan_cam(p, *t->views[p.view]);
   // A batch's launches are sized by the capacities, not by its views' sizes.
   const uint64_t w = t->batch > 1 ? 0 : cam.width, h = t->batch > 1 ? 0 : cam.height;
   std::vector<uint64_t> k = {(uint64_t)t->n, (uint64_t)t->cur.cap, (uint64_t)t->vb.e_cap, (uint64_t)p.sh_degree,
@@ -277,7 +313,7 @@ Status body(splat_trainer* t, const IterPlan& p, int slot, bool probe = false) {
   Ctx* c = t->c;
   const splat_train_config& cfg = t->cfg;
   View& view = *t->views[p.view];
-  const splat_camera& cam = view.cam;
+  const splat_camera& cam = plan_cam(p, view);
   const float bgv = cfg.white_background ? 1.0f : 0.0f;
   const float bg[3] = {bgv, bgv, bgv};
   splat_proj_opts opts;
@@ -294,7 +330,7 @@ Status body(splat_trainer* t, const IterPlan& p, int slot, bool probe = false) {
   const size_t npix = (size_t)cam.width * cam.height;
   SPLAT_TRY(t->pred_grad.ensure(npix * 12));
   SPLAT_TRY(t->loss_out.ensure(16));
-  SPLAT_TRY(launch_loss(c, t->vb.image.as<float>(), view.rgb.ptr, 1, cam.width, cam.height, cfg.lambda_dssim,
+  SPLAT_TRY(launch_loss(c, t->vb.image.as<float>(), plan_rgb(p, view), 1, cam.width, cam.height, cfg.lambda_dssim,
                         t->pred_grad.as<float>(), t->loss_out.as<float>(), sp));
   SPLAT_TRY(t->pgrad.ensure((size_t)cap * 48));
   if (cfg.deterministic) {
@@ -339,7 +375,7 @@ Status body_batch(splat_trainer* t, const IterPlan& p, int slot, bool probe = fa
   opts.sh_degree = p.sh_degree;
   opts.fp64_conic = cfg.fp64_conic;
   const int64_t n = t->n, cap = t->cur.cap, records = (int64_t)t->batch * n, pcap = (int64_t)t->batch * cap;
-  const splat_camera& cam0 = t->views[p.views[0]]->cam;  // launch arguments only; the table rules
+  const splat_camera& cam0 = plan_cam(p, *t->views[p.views[0]]);  // launch arguments only; the table rules
   const BatchTable* bt = t->batch_dev.as<BatchTable>();
   ViewBuffers& v = t->vb;
   SPLAT_TRY(launch_load_words(c, static_cast<const char*>(t->batch_host_dev) + slot * sizeof(BatchTable),
@@ -392,15 +428,16 @@ void fill_batch_table(splat_trainer* t, const IterPlan& p, BatchTable& b) {
   b.adam = make_adam_args(p.adam_step, p.lr);
   for (int k = 0; k < p.nviews; k++) {
     const View& v = *t->views[p.views[k]];
-    const uint32_t tx = t->c->raster.tiles_x(v.cam.width), ty = t->c->raster.tiles_y(v.cam.height);
-    const uint32_t lx = (v.cam.width + 31) / 32, ly = (v.cam.height + 31) / 32;
-    b.cam[k] = v.cam;
-    b.target[k] = v.rgb.ptr;
+    const splat_camera& vc = plan_cam(p, v);
+    const uint32_t tx = t->c->raster.tiles_x(vc.width), ty = t->c->raster.tiles_y(vc.height);
+    const uint32_t lx = (vc.width + 31) / 32, ly = (vc.height + 31) / 32;
+    b.cam[k] = vc;
+    b.target[k] = plan_rgb(p, v);
     b.tiles_x[k] = tx;
     b.tile_start[k + 1] = b.tile_start[k] + tx * ty;
     b.loss_blocks_x[k] = lx;
     b.loss_start[k + 1] = b.loss_start[k] + lx * ly;
-    b.pix_start[k + 1] = b.pix_start[k] + (uint64_t)v.cam.width * v.cam.height;
+    b.pix_start[k + 1] = b.pix_start[k] + (uint64_t)vc.width * vc.height;
   }
 }
 
@@ -412,9 +449,9 @@ Status prepare(splat_trainer* t, const IterPlan& p, int slot) {
   } else {
     View& view = *t->views[p.view];
     StepParams& hp = t->params_host[slot];
-    hp.cam = view.cam;
+    hp.cam = plan_cam(p, view);
     hp.adam = make_adam_args(p.adam_step, p.lr);
-    hp.target = view.rgb.ptr;
+    hp.target = plan_rgb(p, view);
   }
   return t->params_dev.ensure(sizeof(StepParams));
 }
@@ -882,11 +919,16 @@ SPLAT_API int splat_trainer_create(splat_ctx* ctx, const splat_train_config* cfg
     splat_ctx_impl(ctx)->last_error = "batch_views exceeds the maximum of 8";
     return SPLAT_ERR_INVALID;
   }
+  if (cfg->coarse_until > 0 && cfg->coarse_factor != 2 && cfg->coarse_factor != 4) {
+    splat_ctx_impl(ctx)->last_error = "coarse_factor must be 2 or 4";
+    return SPLAT_ERR_INVALID;
+  }
   if (cfg->deterministic && (cfg->batch_views > 1 || cfg->autotune || cfg->bf16_storage || cfg->fp64_conic ||
-                             cfg->learned_densify || !splat_ctx_impl(ctx)->raster.reference_tiles())) {
+                             cfg->learned_densify || cfg->coarse_until ||
+                             !splat_ctx_impl(ctx)->raster.reference_tiles())) {
     splat_ctx_impl(ctx)->last_error =
-        "deterministic needs one view per iteration, the 16x16 tiles and no autotune, BF16 copy, f64 conics or "
-        "learned densification";
+        "deterministic needs one view per iteration, the 16x16 tiles and no autotune, BF16 copy, f64 conics, "
+        "learned densification or coarse views";
     return SPLAT_ERR_INVALID;
   }
   splat_trainer* t = new (std::nothrow) splat_trainer();
@@ -945,6 +987,7 @@ SPLAT_API int splat_trainer_destroy(splat_trainer* t) {
     t->vb.release();
     for (View* v : t->views) {
       v->rgb.release();
+      v->coarse_rgb.release();
       delete v;
     }
     t->views.clear();
@@ -1034,6 +1077,27 @@ SPLAT_API int splat_trainer_start(splat_trainer* t) {
   if (s.good()) s = launch_fill_u32(c, t->birth.ptr, t->birth.bytes / 4, 0u);
   t->rec_n = 0;
   t->rec_valid = false;
+  // Coarse copies of the views for the first coarse_until iterations.
+  if (t->cfg.coarse_until > 0) {
+    const uint32_t f = t->cfg.coarse_factor;
+    for (View* v : t->views) {
+      if (!s.good()) break;
+      v->coarse_cam = scaled_camera(v->cam, f);
+      if (v->coarse_cam.width == 0 || v->coarse_cam.height == 0) {
+        s = Status::make(SPLAT_ERR_INVALID, "a view is smaller than coarse_factor");
+        break;
+      }
+      const uint64_t outs = (uint64_t)v->coarse_cam.width * v->coarse_cam.height * 3;
+      s = v->coarse_rgb.ensure(outs);
+      if (s.good()) {
+        box_downscale_u8_kernel<<<ceil_div(outs, 256), 256, 0, c->stream>>>(
+            static_cast<const uint8_t*>(v->rgb.ptr), v->cam.width, v->cam.height, f,
+            static_cast<uint8_t*>(v->coarse_rgb.ptr), v->coarse_cam.width, v->coarse_cam.height);
+        c->launches.count++;
+        s = cuda_status(cudaGetLastError(), "box_downscale_u8_kernel");
+      }
+    }
+  }
   if (s.good()) s = cuda_status(cudaStreamSynchronize(c->stream), "cudaStreamSynchronize");
   return s.good() ? SPLAT_OK : tfail(t, s);
 }
