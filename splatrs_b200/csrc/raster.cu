@@ -104,8 +104,8 @@ __device__ __forceinline__ bool evaluate_bwd(float px, float py, float mx, float
   if (sigma < 0.0f || sigma > sigma_max) return false;
   float gauss = __expf(-sigma);
   float og = opacity * gauss;
-  const bool near_min = og < SPLAT_ALPHA_MIN * (1.0f + kExpBand) && og > SPLAT_ALPHA_MIN * (1.0f - kExpBand);
-  const bool near_max = og < SPLAT_ALPHA_MAX * (1.0f + kExpBand) && og > SPLAT_ALPHA_MAX * (1.0f - kExpBand);
+  const bool near_min = fabsf(og - SPLAT_ALPHA_MIN) < SPLAT_ALPHA_MIN * kExpBand;
+  const bool near_max = fabsf(og - SPLAT_ALPHA_MAX) < SPLAT_ALPHA_MAX * kExpBand;
   if (near_min || near_max) {
     gauss = crm::expf_cr(-sigma);
     og = opacity * gauss;
@@ -380,12 +380,14 @@ __device__ __forceinline__ float warp_transpose_reduce12(const float v[12]) {
   return z;
 }
 
-// 1 / x for x in [0.01, 1]: the MUFU approximation refined by one Newton step (values only;
-// used to recover transmittance, never for a decision).
-__device__ __forceinline__ float rcp_refined(float x) {
+// 1 / x for x in [0.01, 1] by the special-function unit alone (relative error within a few
+// ulps; values only, never a decision). Over a pixel's reverse walk the recovered
+// transmittance then carries at most about one ulp per entry walked, far inside the
+// gradients' 1e-3 bar.
+__device__ __forceinline__ float rcp_fast(float x) {
   float r;
   asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
-  return __fmaf_rn(r, __fmaf_rn(-x, r, 1.0f), r);
+  return r;
 }
 
 // PPL pixels per thread (1 or 2): a warp owns an 8 x (4 PPL) sub-block, lane L the pixels
@@ -434,24 +436,25 @@ __global__ void __launch_bounds__(TW * TH / PPL, (PPL == 1 ? 1024 : 768) / (TW *
   // Per pixel: contributor count, transmittance, dL/dpixel and the running sums of the
   // reverse walk (rasterize.rs:347-455).
   uint32_t last[PPL];
-  float T[PPL], t_fin[PPL], d0[PPL], d1[PPL], d2[PPL], bg_dot[PPL];
+  // nbg = -T_final (bg . dL/dpixel): the background's share of dL/dalpha is nbg / (1 - alpha).
+  float T[PPL], nbg[PPL], d0[PPL], d1[PPL], d2[PPL], py[PPL];
   float acc_r[PPL], acc_g[PPL], acc_b[PPL], last_alpha[PPL], lc_r[PPL], lc_g[PPL], lc_b[PPL];
   uint32_t lane_last = 0;
 #pragma unroll
   for (int q = 0; q < PPL; q++) {
     const uint32_t y = oy + ly0 + 4u * q, x = ox + lx;
+    py[q] = (float)y + 0.5f;
     last[q] = 0;
-    T[q] = t_fin[q] = 1.0f;
-    d0[q] = d1[q] = d2[q] = bg_dot[q] = 0.0f;
+    T[q] = 1.0f;
+    d0[q] = d1[q] = d2[q] = nbg[q] = 0.0f;
     if (x < width && y < height) {
       const size_t pix = pix0 + (size_t)y * width + x;
       last[q] = min(n_contrib[pix], list_len);  // n_contrib never exceeds its tile's list
       T[q] = final_t[pix];
-      t_fin[q] = T[q];
       d0[q] = dimage[3 * pix];
       d1[q] = dimage[3 * pix + 1];
       d2[q] = dimage[3 * pix + 2];
-      bg_dot[q] = bg0 * d0[q] + bg1 * d1[q] + bg2 * d2[q];
+      nbg[q] = -T[q] * (bg0 * d0[q] + bg1 * d1[q] + bg2 * d2[q]);
     }
     acc_r[q] = acc_g[q] = acc_b[q] = 0.0f;  // accum (rasterize.rs:347)
     last_alpha[q] = lc_r[q] = lc_g[q] = lc_b[q] = 0.0f;
@@ -503,15 +506,14 @@ __global__ void __launch_bounds__(TW * TH / PPL, (PPL == 1 ? 1024 : 768) / (TW *
         const float2 e2 = s2[kk];
         npairs++;
         const float4 e0 = s0[kk], e1 = s1[kk];
-        const float py = (float)(oy + ly0 + 4u * q) + 0.5f;
         float gval, alpha;
         bool unclamped;
-        if (!evaluate_bwd(px, py, e0.x, e0.y, e0.z, e0.w, e1.x, e1.y, e1.z, &gval, &alpha, &unclamped)) continue;
+        if (!evaluate_bwd(px, py[q], e0.x, e0.y, e0.z, e0.w, e1.x, e1.y, e1.z, &gval, &alpha, &unclamped)) continue;
         active = true;
         // Values only from here on: the arithmetic is fused and the divisions are
         // reciprocals; every decision was taken above exactly as in the forward pass.
         const float col_r = e1.w, col_g = e2.x, col_b = e2.y;
-        const float inv = rcp_refined(1.0f - alpha);
+        const float inv = rcp_fast(1.0f - alpha);
         T[q] = T[q] * inv;
         const float t = T[q];
         const float keep = 1.0f - last_alpha[q];
@@ -530,13 +532,13 @@ __global__ void __launch_bounds__(TW * TH / PPL, (PPL == 1 ? 1024 : 768) / (TW *
         lc_g[q] = col_g;
         lc_b[q] = col_b;
         last_alpha[q] = alpha;
-        dalpha = __fmaf_rn(dalpha, t, -t_fin[q] * inv * bg_dot[q]);
+        dalpha = __fmaf_rn(dalpha, t, nbg[q] * inv);
         if (unclamped) {
           const float opacity = e1.y;
           c[5] = __fmaf_rn(gval, dalpha, c[5]);
           const float dsigma = -(opacity * dalpha) * gval;
           const float dx = px - e0.x;
-          const float dy = py - e0.y;
+          const float dy = py[q] - e0.y;
           const float ddx = dsigma * __fmaf_rn(e0.z, dx, e0.w * dy);
           const float ddy = dsigma * __fmaf_rn(e0.w, dx, e1.x * dy);
           c[0] -= ddx;
