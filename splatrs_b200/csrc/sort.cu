@@ -137,6 +137,31 @@ __global__ void fill_u32_kernel(uint32_t* __restrict__ dst, size_t words, uint32
   for (size_t i = quads * 4 + (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < words; i += stride) dst[i] = value;
 }
 
+// Zeroes up to three regions of 32-bit words in one launch.
+__global__ void zero3_u32_kernel(uint32_t* __restrict__ a, size_t na, uint32_t* __restrict__ b, size_t nb,
+                                 uint32_t* __restrict__ c3, size_t nc) {
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < na + nb + nc; i += stride) {
+    if (i < na)
+      a[i] = 0u;
+    else if (i < na + nb)
+      b[i - na] = 0u;
+    else
+      c3[i - na - nb] = 0u;
+  }
+}
+
+Status launch_zero3_u32(Ctx* c, void* a, size_t na, void* b, size_t nb, void* c3, size_t nc) {
+  const size_t words = na + nb + nc;
+  if (words == 0) return Status::ok();
+  const uint32_t grid = (uint32_t)std::min<size_t>((words + 255) / 256, (size_t)c->sm_count * 8);
+  zero3_u32_kernel<<<grid, 256, 0, c->stream>>>(static_cast<uint32_t*>(a), na, static_cast<uint32_t*>(b), nb,
+                                                static_cast<uint32_t*>(c3), nc);
+  c->launches.count++;
+  SPLAT_LAUNCHED("zero3_u32_kernel");
+  return Status::ok();
+}
+
 Status launch_fill_u32(Ctx* c, void* dst, size_t words, uint32_t value) {
   if (words == 0) return Status::ok();
   const int vector = (reinterpret_cast<uintptr_t>(dst) & 15u) == 0;
@@ -295,8 +320,13 @@ __global__ void __launch_bounds__(256) emit_keys_kernel(const float4* __restrict
 // ---------------------------------------------------------------------------------------
 constexpr int kSortThreads = 256;
 constexpr int kSortWarps = kSortThreads / 32;
+// A pass block ranks ROUNDS rounds of 256 keys: 16 (4,096-key tiles) for large sorts, 4
+// (1,024-key tiles) when there are at most kSmallSortKeys keys, so that a small sort still
+// spreads over many SMs.
 constexpr int kSortRounds = 16;
-constexpr int kSortTile = kSortThreads * kSortRounds;  // 4096
+constexpr int kSortRoundsSmall = 4;
+constexpr int64_t kSmallSortKeys = 1 << 20;
+inline int sort_rounds_for(int64_t keys) { return keys <= kSmallSortKeys ? kSortRoundsSmall : kSortRounds; }
 constexpr int kMaxPasses = 8;
 constexpr uint64_t kLbAggregate = 1ull << 62, kLbPrefix = 2ull << 62, kLbCount = (1ull << 62) - 1ull;
 constexpr uint32_t kLookbackSpins = 1u << 22;
@@ -353,8 +383,8 @@ __global__ void __launch_bounds__(kSortThreads) radix_hist_kernel(const K* __res
 
 // Dynamic shared memory of a pass: the tile's keys and values reordered by digit, the
 // per-warp digit counters, the digits' block starts and output offsets, scan scratch.
-template <typename K> constexpr size_t onesweep_smem() {
-  return (size_t)kSortTile * (sizeof(K) + 4) + (size_t)kSortWarps * 256 * 4 + 2 * 256 * 4 + 64;
+template <typename K, int ROUNDS> constexpr size_t onesweep_smem() {
+  return (size_t)kSortThreads * ROUNDS * (sizeof(K) + 4) + (size_t)kSortWarps * 256 * 4 + 2 * 256 * 4 + 64;
 }
 
 // Exclusive prefix over the 256 digits of v (thread d holds digit d's value); `wsum` holds
@@ -377,21 +407,22 @@ __device__ __forceinline__ uint32_t digit_exclusive(uint32_t v, uint32_t* wsum) 
 
 // One pass over keys_in[0, n) (digit at `shift`): `hist` is this pass's 256 global counts,
 // `status` its look-back words, `ticket` its tile counter.
-template <typename K>
+template <typename K, int ROUNDS>
 __device__ __forceinline__ void onesweep_body(const K* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
                                               int64_t n, int shift, const uint32_t* __restrict__ hist,
                                               uint64_t* __restrict__ status, uint32_t* __restrict__ ticket,
                                               uint32_t* __restrict__ abort_word, uint32_t* __restrict__ err,
                                               K* __restrict__ keys_out, uint32_t* __restrict__ vals_out,
                                               unsigned char* dsm) {
+  constexpr int TILE = kSortThreads * ROUNDS;
   K* sk = reinterpret_cast<K*>(dsm);
-  uint32_t* sv = reinterpret_cast<uint32_t*>(sk + kSortTile);
-  uint32_t(*wcnt)[256] = reinterpret_cast<uint32_t(*)[256]>(sv + kSortTile);
+  uint32_t* sv = reinterpret_cast<uint32_t*>(sk + TILE);
+  uint32_t(*wcnt)[256] = reinterpret_cast<uint32_t(*)[256]>(sv + TILE);
   uint32_t* dstart = reinterpret_cast<uint32_t*>(wcnt) + kSortWarps * 256;
   uint32_t* doff = dstart + 256;
   uint32_t* wsum = doff + 256;  // kSortWarps words, then the tile number and the failure word
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int64_t tiles = (n + kSortTile - 1) / kSortTile;
+  const int64_t tiles = (n + TILE - 1) / TILE;
   if (threadIdx.x == 0) {
     wsum[kSortWarps] = atomicAdd(ticket, 1u);
     wsum[kSortWarps + 1] = 0;
@@ -400,14 +431,14 @@ __device__ __forceinline__ void onesweep_body(const K* __restrict__ keys_in, con
   __syncthreads();
   const uint32_t tile = wsum[kSortWarps];
   if ((int64_t)tile >= tiles) return;
-  const int64_t bbase = (int64_t)tile * kSortTile;
-  const int64_t wbase = bbase + (int64_t)warp * (32 * kSortRounds);
-  K k[kSortRounds];
-  uint32_t v[kSortRounds];
-  uint32_t rank[kSortRounds];
+  const int64_t bbase = (int64_t)tile * TILE;
+  const int64_t wbase = bbase + (int64_t)warp * (32 * ROUNDS);
+  K k[ROUNDS];
+  uint32_t v[ROUNDS];
+  uint32_t rank[ROUNDS];
   const uint32_t lt = (1u << lane) - 1u;
 #pragma unroll
-  for (int r = 0; r < kSortRounds; r++) {
+  for (int r = 0; r < ROUNDS; r++) {
     const int64_t idx = wbase + r * 32 + lane;
     const bool valid = idx < n;
     k[r] = valid ? keys_in[idx] : (K)0;
@@ -487,7 +518,7 @@ __device__ __forceinline__ void onesweep_body(const K* __restrict__ keys_in, con
   if (wsum[kSortWarps + 1]) return;
   // Reorder the tile's keys by digit in shared memory (stable).
 #pragma unroll
-  for (int r = 0; r < kSortRounds; r++) {
+  for (int r = 0; r < ROUNDS; r++) {
     const int64_t idx = wbase + r * 32 + lane;
     if (idx < n) {
       const uint32_t dg = (uint32_t)(k[r] >> shift) & 0xffu;
@@ -498,7 +529,7 @@ __device__ __forceinline__ void onesweep_body(const K* __restrict__ keys_in, con
   }
   __syncthreads();
   // Write out runs of equal digits contiguously.
-  const int64_t nb = n - bbase < kSortTile ? n - bbase : kSortTile;
+  const int64_t nb = n - bbase < TILE ? n - bbase : TILE;
   for (int i = threadIdx.x; i < nb; i += kSortThreads) {
     const K key = sk[i];
     const uint32_t dg = (uint32_t)(key >> shift) & 0xffu;
@@ -510,15 +541,15 @@ __device__ __forceinline__ void onesweep_body(const K* __restrict__ keys_in, con
   }
 }
 
-template <typename K>
+template <typename K, int ROUNDS>
 __global__ void __launch_bounds__(kSortThreads) radix_onesweep_kernel(const K* __restrict__ keys_in,
                                                                       const uint32_t* __restrict__ vals_in, int64_t n,
                                                                       int pass, SortCtl ctl, uint32_t* __restrict__ err,
                                                                       K* __restrict__ keys_out,
                                                                       uint32_t* __restrict__ vals_out) {
   extern __shared__ __align__(16) unsigned char dsm[];
-  const uint64_t tiles = (uint64_t)((n + kSortTile - 1) / kSortTile);
-  onesweep_body<K>(keys_in, vals_in, n, 8 * pass, ctl.hist + 256 * pass, ctl.status + (size_t)pass * tiles * 256,
+  const uint64_t tiles = (uint64_t)((n + kSortThreads * ROUNDS - 1) / (kSortThreads * ROUNDS));
+  onesweep_body<K, ROUNDS>(keys_in, vals_in, n, 8 * pass, ctl.hist + 256 * pass, ctl.status + (size_t)pass * tiles * 256,
                    ctl.ticket + pass, ctl.abort, err, keys_out, vals_out, dsm);
 }
 
@@ -540,19 +571,37 @@ __global__ void tile_ranges_kernel(const K* __restrict__ keys, int64_t n, int db
   }
 }
 
+// One pass of the sort over E keys with tiles of ROUNDS rounds (the kernel's shared memory
+// attribute set on first use).
+template <typename K, int ROUNDS>
+static Status launch_onesweep(Ctx* c, const K* kin, const uint32_t* vin, int64_t E, int pass, const SortCtl& ctl,
+                              uint32_t* err, K* kout, uint32_t* vout) {
+  static std::atomic<uint64_t> attr_done{0};
+  if (c->device >= 64 || !(attr_done.load() & (1ull << c->device))) {
+    SPLAT_CUDA(cudaFuncSetAttribute(radix_onesweep_kernel<K, ROUNDS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)onesweep_smem<K, ROUNDS>()));
+    if (c->device < 64) attr_done.fetch_or(1ull << c->device);
+  }
+  const uint64_t tiles = ceil_div(E, (uint64_t)kSortThreads * ROUNDS);
+  radix_onesweep_kernel<K, ROUNDS><<<(uint32_t)tiles, kSortThreads, onesweep_smem<K, ROUNDS>(), c->stream>>>(
+      kin, vin, E, pass, ctl, err, kout, vout);
+  c->launches.count++;
+  SPLAT_LAUNCHED("radix_onesweep_kernel");
+  return Status::ok();
+}
+
 template <typename K>
 static Status sort_and_range(Ctx* c, const float* proj, const uint32_t* entry_offset, int64_t n, int64_t E,
                              const uint32_t* depth_range, int dbits, int total_bits, uint32_t tiles_x,
                              uint32_t num_tiles, uint32_t* gauss_out, uint64_t* keys_out, uint32_t* ranges) {
   const int passes = std::max(1, (total_bits + 7) / 8);
-  SPLAT_CUDA(cudaFuncSetAttribute(radix_onesweep_kernel<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)onesweep_smem<K>()));
+  const int rounds = sort_rounds_for(E);
   K *ka = nullptr, *kb = nullptr;
   uint32_t* vb = nullptr;
   SPLAT_TRY(arena_reserve(c, (size_t)E * sizeof(K), (void**)&ka));
   SPLAT_TRY(arena_reserve(c, (size_t)E * sizeof(K), (void**)&kb));
   SPLAT_TRY(arena_reserve(c, (size_t)E * 4, (void**)&vb));
-  const uint64_t tiles = ceil_div(E, kSortTile);
+  const uint64_t tiles = ceil_div(E, (uint64_t)kSortThreads * rounds);
   void* ctl_base = nullptr;
   SPLAT_TRY(arena_reserve(c, sort_ctl_bytes(tiles), &ctl_base));
   const SortCtl ctl = carve_sort_ctl(ctl_base, tiles);
@@ -575,10 +624,10 @@ static Status sort_and_range(Ctx* c, const float* proj, const uint32_t* entry_of
   uint32_t* vin = va;
   uint32_t* vout = vo;
   for (int p = 0; p < passes; p++) {
-    radix_onesweep_kernel<K><<<(uint32_t)tiles, kSortThreads, onesweep_smem<K>(), c->stream>>>(kin, vin, E, p, ctl,
-                                                                                              err, kout, vout);
-    c->launches.count++;
-    SPLAT_LAUNCHED("radix_onesweep_kernel");
+    if (rounds == kSortRoundsSmall)
+      SPLAT_TRY((launch_onesweep<K, kSortRoundsSmall>(c, kin, vin, E, p, ctl, err, kout, vout)));
+    else
+      SPLAT_TRY((launch_onesweep<K, kSortRounds>(c, kin, vin, E, p, ctl, err, kout, vout)));
     std::swap(kin, kout);
     std::swap(vin, vout);
   }
@@ -657,6 +706,7 @@ __global__ void __launch_bounds__(kSortThreads) radix_hist_dev_kernel(const uint
   hist_body<uint64_t>(keys, p.E, p.passes, hist, cnt);
 }
 
+template <int ROUNDS>
 __global__ void __launch_bounds__(kSortThreads) radix_onesweep_dev_kernel(
     uint64_t* __restrict__ ka, uint64_t* __restrict__ kb, uint32_t* __restrict__ va, uint32_t* __restrict__ vb,
     const uint64_t* __restrict__ E_dev, int64_t E_cap, const uint32_t* __restrict__ dr, int tbits, int pass,
@@ -666,7 +716,7 @@ __global__ void __launch_bounds__(kSortThreads) radix_onesweep_dev_kernel(
   if (pass >= p.passes) return;
   const bool odd = pass & 1;
   uint32_t* vout = pass == p.passes - 1 ? vals_final : (odd ? va : vb);
-  onesweep_body<uint64_t>(odd ? kb : ka, odd ? vb : va, p.E, 8 * pass, ctl.hist + 256 * pass,
+  onesweep_body<uint64_t, ROUNDS>(odd ? kb : ka, odd ? vb : va, p.E, 8 * pass, ctl.hist + 256 * pass,
                           ctl.status + (size_t)pass * tiles_cap * 256, ctl.ticket + pass, ctl.abort, err,
                           odd ? ka : kb, vout, dsm);
 }
@@ -685,8 +735,25 @@ __global__ void tile_ranges_dev_kernel(const uint64_t* __restrict__ ka, const ui
 
 size_t dev_sort_scratch_bytes(int64_t E_cap) {
   const uint64_t cap = (uint64_t)std::max<int64_t>(E_cap, 1);
-  const uint64_t tiles = ceil_div(cap, kSortTile);
+  const uint64_t tiles = ceil_div(cap, (uint64_t)kSortThreads * sort_rounds_for((int64_t)cap));
   return 2 * cap * 8 + 2 * cap * 4 + sort_ctl_bytes(tiles) + 6 * 256;  // 5 pieces, 256-aligned
+}
+
+template <int ROUNDS>
+static Status launch_onesweep_dev(Ctx* c, uint64_t* ka, uint64_t* kb, uint32_t* va, uint32_t* vb,
+                                  const uint64_t* E_dev, int64_t E_cap, const uint32_t* dr, int tbits, int pass,
+                                  const SortCtl& ctl, uint64_t tiles, uint32_t* overflow, uint32_t* gauss_out) {
+  static std::atomic<uint64_t> attr_done{0};
+  if (c->device >= 64 || !(attr_done.load() & (1ull << c->device))) {
+    SPLAT_CUDA(cudaFuncSetAttribute(radix_onesweep_dev_kernel<ROUNDS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)onesweep_smem<uint64_t, ROUNDS>()));
+    if (c->device < 64) attr_done.fetch_or(1ull << c->device);
+  }
+  radix_onesweep_dev_kernel<ROUNDS><<<(uint32_t)tiles, kSortThreads, onesweep_smem<uint64_t, ROUNDS>(), c->stream>>>(
+      ka, kb, va, vb, E_dev, E_cap, dr, tbits, pass, ctl, tiles, overflow, gauss_out);
+  c->launches.count++;
+  SPLAT_LAUNCHED("radix_onesweep_dev_kernel");
+  return Status::ok();
 }
 
 Status launch_bin_sort_dev(Ctx* c, const float* proj, const uint32_t* entry_offset, int64_t n, const uint64_t* E_dev,
@@ -698,7 +765,8 @@ Status launch_bin_sort_dev(Ctx* c, const float* proj, const uint32_t* entry_offs
   const int tbits = num_tiles <= 1 ? 0 : 32 - __builtin_clz(num_tiles - 1);
   const int max_passes = (tbits + 32 + 7) / 8;
   const uint64_t cap = (uint64_t)std::max<int64_t>(E_cap, 1);
-  const uint64_t tiles = ceil_div(cap, kSortTile);
+  const int rounds = sort_rounds_for((int64_t)cap);
+  const uint64_t tiles = ceil_div(cap, (uint64_t)kSortThreads * rounds);
   // Carve the scratch (256-byte aligned pieces).
   auto carve = [&](size_t bytes) {
     void* p = scratch;
@@ -711,20 +779,10 @@ Status launch_bin_sort_dev(Ctx* c, const float* proj, const uint32_t* entry_offs
   uint32_t* vb = static_cast<uint32_t*>(carve(cap * 4));
   void* ctl_base = carve(sort_ctl_bytes(tiles));
   const SortCtl ctl = carve_sort_ctl(ctl_base, tiles);
-  // Once per device (and never inside a stream capture after the first call).
-  static std::atomic<uint64_t> attr_done{0};
-  if (c->device < 64 && !(attr_done.load() & (1ull << c->device))) {
-    SPLAT_CUDA(cudaFuncSetAttribute(radix_onesweep_dev_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)onesweep_smem<uint64_t>()));
-    attr_done.fetch_or(1ull << c->device);
-  } else if (c->device >= 64) {
-    SPLAT_CUDA(cudaFuncSetAttribute(radix_onesweep_dev_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)onesweep_smem<uint64_t>()));
-  }
-  SPLAT_TRY(launch_fill_u32(c, ranges, (size_t)num_tiles * 2, 0u));
-  // Only the passes these keys can need have look-back words to clear.
-  SPLAT_TRY(launch_fill_u32(c, ctl.status, (size_t)max_passes * tiles * 256 * 2, 0u));
-  SPLAT_TRY(launch_fill_u32(c, ctl.hist, (size_t)(kMaxPasses * 256 + kMaxPasses + 2), 0u));
+  // One launch clears the tile ranges, the look-back words of the passes these keys can need,
+  // and the histograms, tickets and abort word.
+  SPLAT_TRY(launch_zero3_u32(c, ranges, (size_t)num_tiles * 2, ctl.status, (size_t)max_passes * tiles * 256 * 2,
+                             ctl.hist, (size_t)(kMaxPasses * 256 + kMaxPasses + 2)));
   if (n > 0) {
     const uint32_t warps = ceil_div(n, 32);
     emit_keys_dev_kernel<<<ceil_div((uint64_t)warps * 32, 256), 256, 0, c->stream>>>(
@@ -738,10 +796,12 @@ Status launch_bin_sort_dev(Ctx* c, const float* proj, const uint32_t* entry_offs
   c->launches.count++;
   SPLAT_LAUNCHED("radix_hist_dev_kernel");
   for (int pass = 0; pass < max_passes; pass++) {
-    radix_onesweep_dev_kernel<<<(uint32_t)tiles, kSortThreads, onesweep_smem<uint64_t>(), c->stream>>>(
-        ka, kb, va, vb, E_dev, E_cap, depth_range_dev, tbits, pass, ctl, tiles, overflow, gauss_out);
-    c->launches.count++;
-    SPLAT_LAUNCHED("radix_onesweep_dev_kernel");
+    if (rounds == kSortRoundsSmall)
+      SPLAT_TRY(launch_onesweep_dev<kSortRoundsSmall>(c, ka, kb, va, vb, E_dev, E_cap, depth_range_dev, tbits, pass,
+                                                      ctl, tiles, overflow, gauss_out));
+    else
+      SPLAT_TRY(launch_onesweep_dev<kSortRounds>(c, ka, kb, va, vb, E_dev, E_cap, depth_range_dev, tbits, pass, ctl,
+                                                 tiles, overflow, gauss_out));
   }
   tile_ranges_dev_kernel<<<ceil_div(cap, 256), 256, 0, c->stream>>>(ka, kb, E_dev, E_cap, depth_range_dev, tbits,
                                                                      ranges);
