@@ -1,0 +1,46 @@
+// Paired single precision: two f32 values in one 64-bit register pair, operated on by the
+// sm_100 instructions add/sub/mul/fma.rn.f32x2. Each rounds both halves to nearest exactly
+// as the scalar instruction does, so a paired result is bit-identical to two scalar ones,
+// but it takes one issue slot for two operations (the FMA pipe is busy for two cycles; a
+// kernel bound by instruction issue rather than by that pipe gains the slot).
+#pragma once
+#include <cstdint>
+
+namespace splat {
+
+struct f2 {
+  unsigned long long v;
+};
+
+__device__ __forceinline__ f2 f2_make(float lo, float hi) {
+  f2 r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r.v) : "f"(lo), "f"(hi));
+  return r;
+}
+__device__ __forceinline__ f2 f2_splat(float x) { return f2_make(x, x); }
+__device__ __forceinline__ void f2_split(f2 a, float& lo, float& hi) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(a.v));
+}
+__device__ __forceinline__ f2 f2_add(f2 a, f2 b) {
+  f2 r;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
+  return r;
+}
+__device__ __forceinline__ f2 f2_sub(f2 a, f2 b) {
+  f2 r;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
+  return r;
+}
+__device__ __forceinline__ f2 f2_mul(f2 a, f2 b) {
+  f2 r;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v));
+  return r;
+}
+// a * b + c with one rounding per half.
+__device__ __forceinline__ f2 f2_fma(f2 a, f2 b, f2 c) {
+  f2 r;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r.v) : "l"(a.v), "l"(b.v), "l"(c.v));
+  return r;
+}
+
+}  // namespace splat

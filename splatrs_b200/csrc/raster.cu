@@ -13,6 +13,7 @@
 
 #include "common.cuh"
 #include "kernels.cuh"
+#include "pair.cuh"
 
 namespace splat {
 
@@ -95,6 +96,19 @@ __device__ __forceinline__ bool evaluate_ref(float px, float py, float mx, float
 // splat_diag_fast_exp_error). *unclamped is the reference's `opacity * gauss < 0.99`.
 constexpr float kExpBand = 3e-5f;
 
+// exp(x) through the special-function unit: 2^(x log2 e), the product rounded to nearest,
+// then ex2.approx (flush-to-zero). Relative error of the product's rounding is 2^-24 of an
+// exponent below 9 in magnitude on the range used, and ex2.approx's own is about 2^-22;
+// splat_diag_fast_exp_error measures the sum on every float of the range.
+constexpr float kLog2e = 1.44269504088896341f;
+
+__device__ __forceinline__ float ex2_approx(float x) {
+  float r;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+__device__ __forceinline__ float fast_exp(float x) { return ex2_approx(__fmul_rn(x, kLog2e)); }
+
 __device__ __forceinline__ bool evaluate_bwd(float px, float py, float mx, float my, float A, float B, float C,
                                              float opacity, float sigma_max, float* gauss_out, float* alpha_out,
                                              bool* unclamped) {
@@ -102,7 +116,7 @@ __device__ __forceinline__ bool evaluate_bwd(float px, float py, float mx, float
   const float dy = py - my;
   const float sigma = 0.5f * (A * dx * dx + C * dy * dy) + B * dx * dy;
   if (sigma < 0.0f || sigma > sigma_max) return false;
-  float gauss = __expf(-sigma);
+  float gauss = fast_exp(-sigma);
   float og = opacity * gauss;
   const bool near_min = fabsf(og - SPLAT_ALPHA_MIN) < SPLAT_ALPHA_MIN * kExpBand;
   const bool near_max = fabsf(og - SPLAT_ALPHA_MAX) < SPLAT_ALPHA_MAX * kExpBand;
@@ -125,7 +139,7 @@ __global__ void diag_fast_exp_kernel(uint32_t lo_bits, uint32_t count, int negat
     const uint32_t b = lo_bits + k;
     const float x = negative ? -__uint_as_float(b) : __uint_as_float(b);
     const float e = crm::expf_cr(x);
-    const float f = __expf(x);
+    const float f = fast_exp(x);
     if (e > 0.0f) worst = fmaxf(worst, fabsf(f - e) / e);
   }
   for (int o = 16; o > 0; o >>= 1) worst = fmaxf(worst, __shfl_xor_sync(0xffffffffu, worst, o));
@@ -583,6 +597,267 @@ __global__ void __launch_bounds__(TW * TH / PPL, (PPL == 1 ? 1024 : 768) / (TW *
   }
 }
 
+// Backward decisions without the exp. The reference skips a pixel when sigma < 0, sigma >
+// sigma_max or fl(opacity * exp(-sigma)) < 1/255 (rasterize.rs:231-244), with sigma_max =
+// ln(opacity * 255) (both correctly rounded). fl(opacity * exp(-sigma)) does not increase
+// with sigma, and for sigma <= sigma_max - kSigmaEdge it is at least
+// (1/255) e^(kSigmaEdge - 7.2e-7) (1 - 2^-23) > 1/255 (the roundings of the quotient, the
+// logarithm, the difference, the exp and the product, with ln(255 opacity) <= ln 255), so
+// such a pixel passes the alpha test whatever the exp's value: the decision needs sigma
+// only. Pixels within kSigmaEdge of sigma_max take the correctly rounded exp. Likewise
+// fl(opacity * exp(-sigma)) <= opacity, so an entry with opacity < 0.99 never clamps.
+constexpr float kSigmaEdge = 1e-4f;
+
+// The backward with two pixels per thread computed as pairs. Lane L owns the pixels
+// (L % 8, L / 8) and (L % 8, L / 8 + 4) of its warp's 8x8 sub-block; every per-pixel value of
+// backward_tile (rasterize.rs:394-454) is a pair, computed with the paired instructions of
+// pair.cuh, and an entry's record is staged in shared memory with each scalar duplicated
+// into both halves so that it is an operand as it stands. Decisions are taken on the
+// halves: sigma (bit-identical to the scalar sigma) against the entry's range, as above.
+// A pixel the entry does not reach (outside the rectangle, at or past n_contrib, skipped by
+// a decision) runs the arithmetic with sigma = +inf, so gauss = alpha = 0: its
+// transmittance is multiplied by rcp(1) = 1 exactly, its colour accumulator by 0 + 1, and
+// all its contributions are exactly zero; both pixels of a pair always run together and
+// still leave the scalar kernel's state and sums. The colour accumulator is advanced right
+// after its use (accum + alpha (c - accum)) instead of on the pixel's next entry, which
+// needs the same operands and so leaves neither last_alpha nor last_color to carry. A
+// lane's two contributions to each slot are added before the warp reduction. kCount adds
+// the evaluated-pair counter (untimed diagnostics only).
+template <int TW, int TH, int CH, bool kCount>
+__global__ void __launch_bounds__(TW * TH / 2, 768 / (TW * TH / 2)) raster_bwd_x2_kernel(
+    const float4* __restrict__ rec, const uint32_t* __restrict__ gauss, const uint2* __restrict__ ranges,
+    uint32_t width, uint32_t height, uint32_t tiles_x, float bg0, float bg1, float bg2,
+    const float* __restrict__ final_t, const uint32_t* __restrict__ n_contrib, const float* __restrict__ dimage,
+    float4* __restrict__ pgrad, int64_t cap, unsigned long long* __restrict__ pairs,
+    const BatchTable* __restrict__ bt) {
+  typedef TileGeo<TW, TH> Geo;
+  typedef typename Geo::Mask Mask;
+  constexpr int NT = TW * TH / 2, NW = NT / 32, WX = TW / 8, SBH = 8;
+  typedef typename std::conditional<(NW > 8), uint16_t, uint8_t>::type WarpMask;
+  if (bt && blockIdx.x >= bt->tile_start[bt->views]) return;  // past the batch's tiles
+  // Per entry, duplicated: (mx, mx, my, my), (A, A, B, B), (C, C, opacity, opacity),
+  // (r, r, g, g), (b, b); and (sigma_max, sigma_max - kSigmaEdge).
+  __shared__ float4 sxy[CH], sab[CH], sco[CH], srg[CH];
+  __shared__ float2 sb[CH], ssig[CH];
+  __shared__ Mask srect[CH];
+  __shared__ uint32_t sg[CH];
+  __shared__ float acc[CH * kSlots];
+  __shared__ WarpMask smask[CH];
+  __shared__ uint8_t slist[NW][CH];
+  __shared__ uint32_t s_max_last;
+  uint32_t tile = blockIdx.x;
+  size_t pix0 = 0;
+  if (bt) {
+    const int v = batch_view_of(bt->tile_start, bt->views, blockIdx.x);
+    tile = blockIdx.x - bt->tile_start[v];
+    width = bt->cam[v].width;
+    height = bt->cam[v].height;
+    tiles_x = bt->tiles_x[v];
+    pix0 = bt->pix_start[v];
+  }
+  const uint32_t ox = (tile % tiles_x) * TW, oy = (tile / tiles_x) * TH;
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t lx = (warp % WX) * 8u + (lane & 7u);
+  const uint32_t ly0 = (warp / WX) * (uint32_t)SBH + (lane >> 3);
+  // A pixel is in an entry's rectangle when both its column and its row bit are set.
+  const Mask bits0 = ((Mask)1 << lx) | ((Mask)1 << (ly0 + Geo::kRowShift));
+  const Mask bits1 = ((Mask)1 << lx) | ((Mask)1 << (ly0 + 4u + Geo::kRowShift));
+  const uint2 range = ranges[blockIdx.x];
+  uint8_t* list = slist[warp];
+  const uint32_t list_len = range.y - range.x;
+
+  // Per pixel pair: pixel centres, contributor counts, transmittance, dL/dpixel, the
+  // background's share of dL/dalpha (times 1 - alpha) and the colour accumulator.
+  const float pxf = (float)(ox + lx) + 0.5f;
+  const f2 px = f2_splat(pxf);
+  const f2 py = f2_make((float)(oy + ly0) + 0.5f, (float)(oy + ly0 + 4u) + 0.5f);
+  uint32_t last[2];
+  float Tq[2], nbgq[2], d0q[2], d1q[2], d2q[2];
+#pragma unroll
+  for (int q = 0; q < 2; q++) {
+    const uint32_t y = oy + ly0 + 4u * q, x = ox + lx;
+    last[q] = 0;
+    Tq[q] = 1.0f;
+    d0q[q] = d1q[q] = d2q[q] = nbgq[q] = 0.0f;
+    if (x < width && y < height) {
+      const size_t pix = pix0 + (size_t)y * width + x;
+      last[q] = min(n_contrib[pix], list_len);
+      Tq[q] = final_t[pix];
+      d0q[q] = dimage[3 * pix];
+      d1q[q] = dimage[3 * pix + 1];
+      d2q[q] = dimage[3 * pix + 2];
+      nbgq[q] = -Tq[q] * (bg0 * d0q[q] + bg1 * d1q[q] + bg2 * d2q[q]);
+    }
+  }
+  f2 T = f2_make(Tq[0], Tq[1]);
+  const f2 nbg = f2_make(nbgq[0], nbgq[1]);
+  const f2 d0 = f2_make(d0q[0], d0q[1]), d1 = f2_make(d1q[0], d1q[1]), d2 = f2_make(d2q[0], d2q[1]);
+  f2 acc_r = f2_splat(0.0f), acc_g = acc_r, acc_b = acc_r;
+  const f2 half = f2_splat(0.5f), one = f2_splat(1.0f), nlog2e = f2_splat(-kLog2e);
+  const uint32_t lane_last = max(last[0], last[1]);
+
+  if (threadIdx.x == 0) s_max_last = 0;
+  for (int i = threadIdx.x; i < CH * kSlots; i += NT) acc[i] = 0.0f;
+  __syncthreads();
+  const uint32_t warp_max_last = __reduce_max_sync(0xffffffffu, lane_last);
+  if (lane == 0) atomicMax(&s_max_last, warp_max_last);
+  __syncthreads();
+  const uint32_t max_last = s_max_last;
+  uint32_t npairs = 0;
+
+  for (uint32_t cend = max_last; cend > 0;) {
+    const uint32_t cstart = cend > (uint32_t)CH ? cend - CH : 0u;
+    const uint32_t cnt = cend - cstart;
+#pragma unroll
+    for (uint32_t e = threadIdx.x; e < (uint32_t)CH; e += NT) {
+      uint32_t m = 0;
+      if (e < cnt) {
+        const uint32_t g = gauss[range.x + cstart + e];
+        sg[e] = g;
+        const float4 r0 = rec[4 * (size_t)g], r1 = rec[4 * (size_t)g + 1], r2 = rec[4 * (size_t)g + 2];
+        sxy[e] = make_float4(r0.x, r0.x, r0.y, r0.y);
+        sab[e] = make_float4(r0.z, r0.z, r0.w, r0.w);
+        sco[e] = make_float4(r1.x, r1.x, r1.y, r1.y);
+        srg[e] = make_float4(r1.w, r1.w, r2.x, r2.x);
+        sb[e] = make_float2(r2.y, r2.y);
+        ssig[e] = make_float2(r1.z, r1.z - kSigmaEdge);
+        srect[e] = tile_rect_masks<TW, TH>(fbits(r2.z), fbits(r2.w), ox, oy);
+        m = subblock_mask<TW, TH, SBH>(fbits(r2.z), fbits(r2.w), ox, oy);
+      }
+      smask[e] = (WarpMask)m;
+    }
+    __syncthreads();
+    const uint32_t limit = warp_max_last > cstart ? warp_max_last - cstart : 0u;
+    const uint32_t nl = build_warp_list(smask, cnt, limit, list);
+    for (int i = (int)nl - 1; i >= 0; i--) {
+      const uint32_t kk = list[i];
+      const uint32_t k = cstart + kk;
+      const Mask rm = srect[kk];
+      const bool cov0 = (rm & bits0) == bits0 && k < last[0];
+      const bool cov1 = (rm & bits1) == bits1 && k < last[1];
+      if (kCount) npairs += (uint32_t)cov0 + (uint32_t)cov1;
+      const float4 exy = sxy[kk], eab = sab[kk], eco = sco[kk], erg = srg[kk];
+      const float2 eb = sb[kk], esig = ssig[kk];
+      const f2 mx = f2_make(exy.x, exy.y), my = f2_make(exy.z, exy.w);
+      const f2 A = f2_make(eab.x, eab.y), B = f2_make(eab.z, eab.w);
+      const f2 Cc = f2_make(eco.x, eco.y), op = f2_make(eco.z, eco.w);
+      // sigma = 0.5 (A dx dx + C dy dy) + B dx dy, operation for operation (rasterize.rs:236).
+      const f2 dx = f2_sub(px, mx), dy = f2_sub(py, my);
+      const f2 adx = f2_mul(A, dx), cdy = f2_mul(Cc, dy), bdx = f2_mul(B, dx);
+      const f2 sigma = f2_add(f2_mul(half, f2_add(f2_mul(adx, dx), f2_mul(cdy, dy))), f2_mul(bdx, dy));
+      float s0, s1;
+      f2_split(sigma, s0, s1);
+      // The reference's range test (false for NaN, as there), then the alpha test by sigma.
+      const bool in0 = cov0 && !(s0 < 0.0f) && !(s0 > esig.x);
+      const bool in1 = cov1 && !(s1 < 0.0f) && !(s1 > esig.x);
+      bool v0 = in0 && s0 <= esig.y, v1 = in1 && s1 <= esig.y;
+      const bool edge0 = in0 && !v0, edge1 = in1 && !v1;
+      if (__any_sync(0xffffffffu, edge0 || edge1)) {  // rare: the correctly rounded exp decides
+        if (edge0) v0 = !(eco.z * crm::expf_cr(-s0) < SPLAT_ALPHA_MIN);
+        if (edge1) v1 = !(eco.w * crm::expf_cr(-s1) < SPLAT_ALPHA_MIN);
+      }
+      // No pixel of the warp takes the entry: every update below would be an identity.
+      if (!__any_sync(0xffffffffu, v0 || v1)) continue;
+      const float inf = __int_as_float(0x7f800000);
+      float g0, g1;
+      f2_split(f2_mul(f2_make(v0 ? s0 : inf, v1 ? s1 : inf), nlog2e), g0, g1);
+      f2 gv = f2_make(ex2_approx(g0), ex2_approx(g1));  // gauss (fast exp), 0 where skipped
+      f2 alpha = f2_mul(op, gv);
+      if (!(eco.z < SPLAT_ALPHA_MAX)) {
+        // Opacity >= 0.99 (uniform over the warp): alpha clamps at 0.99 and the gradients
+        // through sigma and opacity vanish there (rasterize.rs:414-432). Products within a
+        // relative band of the clamp are decided with the correctly rounded exp.
+        float a0, a1, q0, q1;
+        f2_split(alpha, a0, a1);
+        f2_split(gv, q0, q1);
+        if (fabsf(a0 - SPLAT_ALPHA_MAX) < SPLAT_ALPHA_MAX * kExpBand) {
+          q0 = crm::expf_cr(-s0);
+          a0 = eco.z * q0;
+        }
+        if (fabsf(a1 - SPLAT_ALPHA_MAX) < SPLAT_ALPHA_MAX * kExpBand) {
+          q1 = crm::expf_cr(-s1);
+          a1 = eco.w * q1;
+        }
+        gv = f2_make(a0 < SPLAT_ALPHA_MAX ? q0 : 0.0f, a1 < SPLAT_ALPHA_MAX ? q1 : 0.0f);
+        alpha = f2_make(fminf(a0, SPLAT_ALPHA_MAX), fminf(a1, SPLAT_ALPHA_MAX));
+      }
+      // Values only from here on (fused, reciprocal for division).
+      float o0, o1;
+      f2_split(f2_sub(one, alpha), o0, o1);
+      const f2 inv = f2_make(rcp_fast(o0), rcp_fast(o1));
+      T = f2_mul(T, inv);
+      const f2 dr = f2_sub(f2_make(erg.x, erg.y), acc_r);
+      const f2 dg = f2_sub(f2_make(erg.z, erg.w), acc_g);
+      const f2 db = f2_sub(f2_make(eb.x, eb.y), acc_b);
+      f2 dalpha = f2_fma(db, d2, f2_fma(dg, d1, f2_mul(dr, d0)));
+      const f2 at = f2_mul(alpha, T);
+      acc_r = f2_fma(alpha, dr, acc_r);
+      acc_g = f2_fma(alpha, dg, acc_g);
+      acc_b = f2_fma(alpha, db, acc_b);
+      dalpha = f2_fma(dalpha, T, f2_mul(nbg, inv));
+      const f2 c5 = f2_mul(gv, dalpha);
+      // nds = opacity dalpha gauss = -dsigma; the signs are applied in the lane sums below.
+      const f2 nds = f2_mul(f2_mul(op, dalpha), gv);
+      const f2 ndx = f2_mul(nds, f2_fma(B, dy, adx));  // -ddx = -dsigma (A dx + B dy)
+      const f2 ndy = f2_mul(nds, f2_add(bdx, cdy));    // -ddy = -dsigma (B dx + C dy)
+      const f2 hs = f2_mul(half, nds);
+      const f2 c2 = f2_mul(f2_mul(hs, dx), dx);
+      const f2 c3 = f2_mul(f2_mul(nds, dx), dy);
+      const f2 c4 = f2_mul(f2_mul(hs, dy), dy);
+      const f2 c6 = f2_mul(at, d0), c7 = f2_mul(at, d1), c8 = f2_mul(at, d2);
+      float c[kSlots], lo, hi;
+      f2_split(ndx, lo, hi);
+      c[0] = lo + hi;
+      c[9] = fabsf(lo) + fabsf(hi);
+      f2_split(ndy, lo, hi);
+      c[1] = lo + hi;
+      c[10] = fabsf(lo) + fabsf(hi);
+      f2_split(c2, lo, hi);
+      c[2] = -lo - hi;
+      f2_split(c3, lo, hi);
+      c[3] = -lo - hi;
+      f2_split(c4, lo, hi);
+      c[4] = -lo - hi;
+      f2_split(c5, lo, hi);
+      c[5] = lo + hi;
+      f2_split(c6, lo, hi);
+      c[6] = lo + hi;
+      f2_split(c7, lo, hi);
+      c[7] = lo + hi;
+      f2_split(c8, lo, hi);
+      c[8] = lo + hi;
+      f2_split(at, lo, hi);
+      c[11] = lo + hi;
+      const float tot = warp_transpose_reduce12(c);
+      const uint32_t local = (lane >> 1) & 3u;
+      const uint32_t slot = 6u * ((lane >> 4) & 1u) + 3u * ((lane >> 3) & 1u) + local;
+      if (!(lane & 1u) && local < 3u) atomicAdd(&acc[kk * kSlots + slot], tot);
+    }
+    __syncthreads();
+#pragma unroll
+    for (uint32_t e = threadIdx.x; e < (uint32_t)CH; e += NT) {
+      if (e >= cnt) break;
+      float* a = &acc[e * kSlots];
+      const size_t g = sg[e];
+      const float4 v0 = make_float4(a[0], a[1], a[2], a[3]);
+      const float4 v1 = make_float4(a[4], a[5], a[6], a[7]);
+      const float4 v2 = make_float4(a[8], a[9], a[10], a[11]);
+      if (v0.x != 0.0f || v0.y != 0.0f || v0.z != 0.0f || v0.w != 0.0f) atomicAdd(&pgrad[g], v0);
+      if (v1.x != 0.0f || v1.y != 0.0f || v1.z != 0.0f || v1.w != 0.0f) atomicAdd(&pgrad[cap + g], v1);
+      if (v2.x != 0.0f || v2.y != 0.0f || v2.z != 0.0f || v2.w != 0.0f) atomicAdd(&pgrad[2 * cap + g], v2);
+#pragma unroll
+      for (int q = 0; q < kSlots; q++) a[q] = 0.0f;
+    }
+    __syncthreads();
+    cend = cstart;
+  }
+  if (kCount) {
+    unsigned long long np = npairs;
+    for (int o = 16; o > 0; o >>= 1) np += __shfl_xor_sync(0xffffffffu, np, o);
+    if (lane == 0 && np) atomicAdd(pairs, np);
+  }
+}
+
 // ---------------------------------------------------------------------------------------
 // Deterministic backward (16x16 tiles): the reference's own reduction, bit for bit.
 //
@@ -862,12 +1137,22 @@ Status launch_raster_bwd(Ctx* c, const float* proj, const uint32_t* gauss, const
       bg[0], bg[1], bg[2], final_t, n_contrib, dimage, reinterpret_cast<float4*>(pgrad), cap,                     \
       reinterpret_cast<unsigned long long*>(pairs), bt)
 #define SPLAT_BWD1(TW, TH, CH) SPLAT_BWD(TW, TH, CH, 1)
-#define SPLAT_BWD2(TW, TH, CH) SPLAT_BWD(TW, TH, CH, 2)
-  if (rc.ppl == 2)
+#define SPLAT_BWD2X(TW, TH, CH, K)                                                                                \
+  raster_bwd_x2_kernel<TW, TH, CH, K><<<blocks, TW * TH / 2, 0, c->stream>>>(                                    \
+      reinterpret_cast<const float4*>(proj), gauss, reinterpret_cast<const uint2*>(ranges), width, height, tiles_x, \
+      bg[0], bg[1], bg[2], final_t, n_contrib, dimage, reinterpret_cast<float4*>(pgrad), cap,                     \
+      reinterpret_cast<unsigned long long*>(pairs), bt)
+#define SPLAT_BWD2(TW, TH, CH) SPLAT_BWD2X(TW, TH, CH, false)
+#define SPLAT_BWD2C(TW, TH, CH) SPLAT_BWD2X(TW, TH, CH, true)
+  if (rc.ppl == 2 && pairs)
+    SPLAT_RASTER_DISPATCH(rc, SPLAT_BWD2C);
+  else if (rc.ppl == 2)
     SPLAT_RASTER_DISPATCH(rc, SPLAT_BWD2);
   else
     SPLAT_RASTER_DISPATCH(rc, SPLAT_BWD1);
+#undef SPLAT_BWD2C
 #undef SPLAT_BWD2
+#undef SPLAT_BWD2X
 #undef SPLAT_BWD1
 #undef SPLAT_BWD
   c->launches.count++;
