@@ -337,6 +337,12 @@ SPLAT_API int splat_project_bwd(splat_ctx* ctx, const float* planes_dev, int64_t
  * (negative != 0 selects -|x|). Synchronises. */
 SPLAT_API int splat_diag_fast_exp_error(splat_ctx* ctx, float lo, float hi, int32_t negative, float* max_rel_error);
 
+/* Diagnostic: the paired (f32x2) arithmetic of the compositing backward and the SSIM loss
+ * against scalar arithmetic with one rounding per operation, on n seeded inputs:
+ * mismatches2[0] counts sigma values (rasterize.rs:236) that differ, mismatches2[1] blur
+ * accumulation steps (loss.rs:42-70). Both must be 0. Synchronises. */
+SPLAT_API int splat_diag_pair_exact(splat_ctx* ctx, uint32_t n, uint32_t* mismatches2);
+
 /* Diagnostic of the bounded waits of the tensor-core kernels: one block waits on an
  * mbarrier with `limit` tries (1..4194304; the kernels use 4194304), through the same wait
  * and error word as those kernels. With arrive == 0 nothing arrives: the wait runs out and

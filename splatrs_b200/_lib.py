@@ -146,6 +146,7 @@ def _declare(L):
         "splat_ctx_launch_count": ([vp], C.c_uint64),
         "splat_zero": ([vp, vp, sz], C.c_int),
         "splat_diag_fast_exp_error": ([vp, C.c_float, C.c_float, i32, P(C.c_float)], C.c_int),
+        "splat_diag_pair_exact": ([vp, C.c_uint32, P(C.c_uint32)], C.c_int),
         "splat_diag_mbarrier_wait": ([vp, u32, i32], C.c_int),
         "splat_diag_peak": ([vp, i32, P(C.c_double), P(C.c_float)], C.c_int),
         "splat_ctx_scratch_info": ([vp, P(C.c_uint64)], C.c_int),

@@ -19,7 +19,7 @@ BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libsplatrs_b200.so")
 
 SOURCES = ["capi.cu", "project.cu", "sort.cu", "raster.cu", "renderer.cu", "loss.cu", "optim.cu", "trainer.cu", "noalloc.cu", "peaks.cu", "ply.cu", "init.cu", "mlp.cu", "densify_learn.cu", "autotune.cu"]
-HEADERS = ["common.cuh", "kernels.cuh", "renderer.cuh", "crmath.h", "adam.cuh"]
+HEADERS = ["common.cuh", "kernels.cuh", "renderer.cuh", "crmath.h", "adam.cuh", "pair.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

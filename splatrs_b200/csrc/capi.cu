@@ -191,6 +191,13 @@ SPLAT_API const char* splat_last_error(const splat_ctx* ctx) { return ctx ? ctx-
 
 SPLAT_API uint64_t splat_ctx_launch_count(const splat_ctx* ctx) { return ctx ? ctx->c.launches.count : 0; }
 
+SPLAT_API int splat_diag_pair_exact(splat_ctx* ctx, uint32_t n, uint32_t* mismatches2) {
+  if (!ctx) return SPLAT_ERR_INVALID;
+  if (!mismatches2) return invalid(ctx, "splat_diag_pair_exact: null output");
+  Enter e(ctx);
+  return finish(ctx, launch_diag_pair_exact(&ctx->c, n, mismatches2));
+}
+
 SPLAT_API int splat_diag_fast_exp_error(splat_ctx* ctx, float lo, float hi, int32_t negative, float* max_rel_error) {
   if (!ctx) return SPLAT_ERR_INVALID;
   if (!max_rel_error || !(lo >= 0.0f) || !(hi >= lo) || !(hi < 1e30f)) return invalid(ctx, "splat_diag_fast_exp_error: bad range");

@@ -195,6 +195,7 @@ Status launch_raster_bwd_det(Ctx* c, const float* proj, const uint32_t* gauss, c
                              float* eslot, float* pgrad, int64_t cap);
 
 Status launch_diag_fast_exp(Ctx* c, float magnitude_lo, float magnitude_hi, int negative, float* out_host);
+Status launch_diag_pair_exact(Ctx* c, uint32_t n, uint32_t* out_host);
 // Throughput of one unit (0: FP32 FMA, in FLOP/s; 1: MUFU ex2, in operations/s), peaks.cu.
 Status launch_diag_peak(Ctx* c, int unit, double* ops_per_s, float* ms_out);
 

@@ -11,9 +11,12 @@
 // (reference src/dataset.rs:23-25), or floats. Blur sums run over the window in the
 // reference's order and skip out-of-image taps, so the blurred maps, the partial maps and
 // the gradient are bit-identical to the reference's; only the three scalar sums depend on
-// summation order (accumulated in double here).
+// summation order (accumulated in double here). Blurs of two maps run together as f32x2
+// pairs (pair.cuh: each half rounded as the scalar operation), so a tap of (x, y) or of
+// (x^2, y^2) is one paired multiply and one paired add.
 #include "common.cuh"
 #include "kernels.cuh"
+#include "pair.cuh"
 
 namespace splat {
 
@@ -55,12 +58,16 @@ __global__ void __launch_bounds__(kLossThreads) ssim_fwd_kernel(const float* __r
     dmaps += 9 * bt->pix_start[v];
     sums += 3 * v;
   }
-  __shared__ float sx[kLE][kLE], sy[kLE][kLE];
-  __shared__ float h[5][kLE][kLT];
+  __shared__ float2 xy_tile[kLE][kLE];             // (prediction, target)
+  __shared__ float2 h01[kLE][kLT], h23[kLE][kLT];  // horizontal blurs of (x, y) and (x^2, y^2)
+  __shared__ float h4[kLE][kLT];                   // and of x y
   __shared__ double red[3][kLossThreads / 32];
   const int ox0 = bxi * kLT, oy0 = byi * kLT;
   const int tid = threadIdx.x;
   const float c1 = 0.01f * 0.01f, c2 = 0.03f * 0.03f;
+  f2 wp[11];
+#pragma unroll
+  for (int k = 0; k < 11; k++) wp[k] = f2_splat(K.w[k]);
   double s_ssim = 0.0, s_l1 = 0.0, s_se = 0.0;
   for (int ch = 0; ch < 3; ch++) {
     for (int i = tid; i < kLE * kLE; i += kLossThreads) {
@@ -72,65 +79,81 @@ __global__ void __launch_bounds__(kLossThreads) ssim_fwd_kernel(const float* __r
         vx = pred[idx];
         vy = load_target(target, target_u8, idx);
       }
-      sx[r][c] = vx;
-      sy[r][c] = vy;
+      xy_tile[r][c] = make_float2(vx, vy);
     }
     __syncthreads();
     // Horizontal pass (loss.rs:42-56) for every halo row: a thread takes kRB consecutive
-    // output columns of a row from kRB + 10 inputs. Taps outside the image read the tile's
-    // zero padding and add +0.0, which leaves every sum as the reference's (it skips them).
+    // output columns of a row and streams their kRB + 10 inputs once, each tap added in
+    // window order. Taps outside the image read the tile's zero padding and add +0.0,
+    // which leaves every sum as the reference's (it skips them).
     for (int item = tid; item < kLE * (kLT / kRB); item += kLossThreads) {
       const int r = item / (kLT / kRB), c0 = (item % (kLT / kRB)) * kRB;
-      float vx[kRB + 10], vy[kRB + 10];
+      f2 a01[kRB], a23[kRB];
+      float a4[kRB];
+#pragma unroll
+      for (int o = 0; o < kRB; o++) {
+        a01[o] = a23[o] = f2_splat(0.0f);
+        a4[o] = 0.0f;
+      }
 #pragma unroll
       for (int q = 0; q < kRB + 10; q++) {
-        vx[q] = sx[r][c0 + q];
-        vy[q] = sy[r][c0 + q];
+        const float2 t = xy_tile[r][c0 + q];
+        const f2 v = f2_make(t.x, t.y), sq = f2_mul(v, v);
+        const float xy = t.x * t.y;
+#pragma unroll
+        for (int o = 0; o < kRB; o++) {
+          const int k = q - o;
+          if (k < 0 || k > 10) continue;
+          a01[o] = f2_add(a01[o], f2_mul(wp[k], v));
+          a23[o] = f2_add(a23[o], f2_mul(wp[k], sq));
+          a4[o] += K.w[k] * xy;
+        }
       }
 #pragma unroll
       for (int o = 0; o < kRB; o++) {
-        float a0 = 0.0f, a1 = 0.0f, a2 = 0.0f, a3 = 0.0f, a4 = 0.0f;
-#pragma unroll
-        for (int k = 0; k < 11; k++) {
-          const float x = vx[o + k], y = vy[o + k];
-          a0 += K.w[k] * x;
-          a1 += K.w[k] * y;
-          a2 += K.w[k] * (x * x);
-          a3 += K.w[k] * (y * y);
-          a4 += K.w[k] * (x * y);
-        }
-        h[0][r][c0 + o] = a0;
-        h[1][r][c0 + o] = a1;
-        h[2][r][c0 + o] = a2;
-        h[3][r][c0 + o] = a3;
-        h[4][r][c0 + o] = a4;
+        float lo, hi;
+        f2_split(a01[o], lo, hi);
+        h01[r][c0 + o] = make_float2(lo, hi);
+        f2_split(a23[o], lo, hi);
+        h23[r][c0 + o] = make_float2(lo, hi);
+        h4[r][c0 + o] = a4[o];
       }
     }
     __syncthreads();
     // Vertical pass (loss.rs:58-70) and per-pixel SSIM (loss.rs:101-119): a thread takes kRB
-    // consecutive rows of a column.
+    // consecutive rows of a column, streamed the same way.
     for (int item = tid; item < kLT * (kLT / kRB); item += kLossThreads) {
       const int c = item % kLT, r0 = (item / kLT) * kRB;
-      float col[5][kRB + 10];
+      f2 m01[kRB], e23[kRB];
+      float exy_[kRB];
 #pragma unroll
-      for (int m = 0; m < 5; m++)
+      for (int o = 0; o < kRB; o++) {
+        m01[o] = e23[o] = f2_splat(0.0f);
+        exy_[o] = 0.0f;
+      }
 #pragma unroll
-        for (int q = 0; q < kRB + 10; q++) col[m][q] = h[m][r0 + q][c];
+      for (int q = 0; q < kRB + 10; q++) {
+        const float2 t01 = h01[r0 + q][c], t23 = h23[r0 + q][c];
+        const float t4 = h4[r0 + q][c];
+        const f2 v01 = f2_make(t01.x, t01.y), v23 = f2_make(t23.x, t23.y);
+#pragma unroll
+        for (int o = 0; o < kRB; o++) {
+          const int k = q - o;
+          if (k < 0 || k > 10) continue;
+          m01[o] = f2_add(m01[o], f2_mul(wp[k], v01));
+          e23[o] = f2_add(e23[o], f2_mul(wp[k], v23));
+          exy_[o] += K.w[k] * t4;
+        }
+      }
 #pragma unroll
       for (int o = 0; o < kRB; o++) {
         const int r = r0 + o;
         const int gy = oy0 + r, gx = ox0 + c;
-        float mx = 0.0f, my = 0.0f, exx = 0.0f, eyy = 0.0f, exy = 0.0f;
-#pragma unroll
-        for (int k = 0; k < 11; k++) {
-          const float kv = K.w[k];
-          mx += kv * col[0][o + k];
-          my += kv * col[1][o + k];
-          exx += kv * col[2][o + k];
-          eyy += kv * col[3][o + k];
-          exy += kv * col[4][o + k];
-        }
         if (gx >= (int)width || gy >= (int)height) continue;
+        float mx, my, exx, eyy;
+        f2_split(m01[o], mx, my);
+        f2_split(e23[o], exx, eyy);
+        const float exy = exy_[o];
         const float sx2 = exx - mx * mx;
         const float sy2 = eyy - my * my;
         const float sxy = exy - mx * my;
@@ -148,7 +171,8 @@ __global__ void __launch_bounds__(kLossThreads) ssim_fwd_kernel(const float* __r
         dmaps[idx] = (dn_dmx * den - num * dd_dmx) / (den * den);
         dmaps[npix3 + idx] = -num * d1 / (den * den);
         dmaps[2 * npix3 + idx] = 2.0f * n1 / den;
-        const float x = sx[r + kHalo][c + kHalo], y = sy[r + kHalo][c + kHalo];
+        const float2 xy = xy_tile[r + kHalo][c + kHalo];
+        const float x = xy.x, y = xy.y;
         s_ssim += (double)sv;
         s_l1 += (double)fabsf(x - y);
         const double e = (double)fminf(fmaxf(x, 0.0f), 1.0f) - (double)fminf(fmaxf(y, 0.0f), 1.0f);
@@ -202,13 +226,18 @@ __global__ void __launch_bounds__(kLossThreads) ssim_bwd_kernel(const float* __r
     grad += 3 * bt->pix_start[v];
     scale = bt->inv_views;
   }
-  __shared__ float sm[3][kLE][kLE];
-  __shared__ float h[3][kLE][kLT];
+  __shared__ float2 sm01[kLE][kLE];  // partial maps w.r.t. mu_x and E[x^2]
+  __shared__ float sm2[kLE][kLE];    // and w.r.t. E[xy]
+  __shared__ float2 h01[kLE][kLT];
+  __shared__ float h2[kLE][kLT];
   const int ox0 = bxi * kLT, oy0 = byi * kLT;
   const int tid = threadIdx.x;
   const size_t npix3 = (size_t)width * height * 3;
   const float inv_n = 1.0f / (float)npix3;
   const float w1 = (1.0f - lambda) * inv_n;
+  f2 wp[11];
+#pragma unroll
+  for (int k = 0; k < 11; k++) wp[k] = f2_splat(K.w[k]);
   for (int ch = 0; ch < 3; ch++) {
     for (int i = tid; i < kLE * kLE; i += kLossThreads) {
       const int r = i / kLE, c = i % kLE;
@@ -220,49 +249,73 @@ __global__ void __launch_bounds__(kLossThreads) ssim_bwd_kernel(const float* __r
         b = dmaps[npix3 + idx];
         e = dmaps[2 * npix3 + idx];
       }
-      sm[0][r][c] = a;
-      sm[1][r][c] = b;
-      sm[2][r][c] = e;
+      sm01[r][c] = make_float2(a, b);
+      sm2[r][c] = e;
     }
     __syncthreads();
-    // The blur of the three partial maps (loss.rs:124-127), blocked as in ssim_fwd_kernel;
-    // zero-padded taps add +0.0 (the sums start at +0.0 and never become -0.0).
+    // The blur of the three partial maps (loss.rs:124-127), blocked and streamed as in
+    // ssim_fwd_kernel; zero-padded taps add +0.0 (the sums start at +0.0 and never become
+    // -0.0).
     for (int item = tid; item < kLE * (kLT / kRB); item += kLossThreads) {
       const int r = item / (kLT / kRB), c0 = (item % (kLT / kRB)) * kRB;
+      f2 a01[kRB];
+      float a2[kRB];
 #pragma unroll
-      for (int m = 0; m < 3; m++) {
-        float v[kRB + 10];
+      for (int o = 0; o < kRB; o++) {
+        a01[o] = f2_splat(0.0f);
+        a2[o] = 0.0f;
+      }
 #pragma unroll
-        for (int q = 0; q < kRB + 10; q++) v[q] = sm[m][r][c0 + q];
+      for (int q = 0; q < kRB + 10; q++) {
+        const float2 t = sm01[r][c0 + q];
+        const f2 v = f2_make(t.x, t.y);
+        const float e = sm2[r][c0 + q];
 #pragma unroll
         for (int o = 0; o < kRB; o++) {
-          float a = 0.0f;
-#pragma unroll
-          for (int k = 0; k < 11; k++) a += K.w[k] * v[o + k];
-          h[m][r][c0 + o] = a;
+          const int k = q - o;
+          if (k < 0 || k > 10) continue;
+          a01[o] = f2_add(a01[o], f2_mul(wp[k], v));
+          a2[o] += K.w[k] * e;
         }
+      }
+#pragma unroll
+      for (int o = 0; o < kRB; o++) {
+        float lo, hi;
+        f2_split(a01[o], lo, hi);
+        h01[r][c0 + o] = make_float2(lo, hi);
+        h2[r][c0 + o] = a2[o];
       }
     }
     __syncthreads();
     for (int item = tid; item < kLT * (kLT / kRB); item += kLossThreads) {
       const int c = item % kLT, r0 = (item / kLT) * kRB;
-      float col[3][kRB + 10];
+      f2 b01[kRB];
+      float b2[kRB];
 #pragma unroll
-      for (int m = 0; m < 3; m++)
+      for (int o = 0; o < kRB; o++) {
+        b01[o] = f2_splat(0.0f);
+        b2[o] = 0.0f;
+      }
 #pragma unroll
-        for (int q = 0; q < kRB + 10; q++) col[m][q] = h[m][r0 + q][c];
+      for (int q = 0; q < kRB + 10; q++) {
+        const float2 t = h01[r0 + q][c];
+        const f2 v = f2_make(t.x, t.y);
+        const float e = h2[r0 + q][c];
+#pragma unroll
+        for (int o = 0; o < kRB; o++) {
+          const int k = q - o;
+          if (k < 0 || k > 10) continue;
+          b01[o] = f2_add(b01[o], f2_mul(wp[k], v));
+          b2[o] += K.w[k] * e;
+        }
+      }
 #pragma unroll
       for (int o = 0; o < kRB; o++) {
         const int gy = oy0 + r0 + o, gx = ox0 + c;
-        float bmu = 0.0f, bexx = 0.0f, bexy = 0.0f;
-#pragma unroll
-        for (int k = 0; k < 11; k++) {
-          const float kv = K.w[k];
-          bmu += kv * col[0][o + k];
-          bexx += kv * col[1][o + k];
-          bexy += kv * col[2][o + k];
-        }
         if (gx >= (int)width || gy >= (int)height) continue;
+        float bmu, bexx;
+        f2_split(b01[o], bmu, bexx);
+        const float bexy = b2[o];
         const size_t idx = ((size_t)gy * width + gx) * 3 + ch;
         const float x = pred[idx];
         const float y = load_target(target, target_u8, idx);

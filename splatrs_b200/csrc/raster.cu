@@ -109,6 +109,17 @@ __device__ __forceinline__ float ex2_approx(float x) {
 }
 __device__ __forceinline__ float fast_exp(float x) { return ex2_approx(__fmul_rn(x, kLog2e)); }
 
+// sigma = 0.5 (A dx dx + C dy dy) + B dx dy for a pair of pixels, operation for operation as
+// the reference (rasterize.rs:236), one rounding per operation (f2_mul is never contracted).
+// Also returns A dx, C dy and B dx for the gradients. A zero product may carry the other
+// sign than the scalar one; no decision on sigma depends on the sign of a zero.
+__device__ __forceinline__ f2 paired_sigma(f2 A, f2 B, f2 C, f2 dx, f2 dy, f2* adx, f2* cdy, f2* bdx) {
+  *adx = f2_mul(A, dx);
+  *cdy = f2_mul(C, dy);
+  *bdx = f2_mul(B, dx);
+  return f2_add(f2_mul(f2_splat(0.5f), f2_add(f2_mul(*adx, dx), f2_mul(*cdy, dy))), f2_mul(*bdx, dy));
+}
+
 __device__ __forceinline__ bool evaluate_bwd(float px, float py, float mx, float my, float A, float B, float C,
                                              float opacity, float sigma_max, float* gauss_out, float* alpha_out,
                                              bool* unclamped) {
@@ -158,6 +169,66 @@ Status launch_diag_fast_exp(Ctx* c, float magnitude_lo, float magnitude_hi, int 
   SPLAT_CUDA(cudaMemcpyAsync(&h, d, 4, cudaMemcpyDeviceToHost, c->stream));
   SPLAT_CUDA(cudaStreamSynchronize(c->stream));
   *out_host = bitsf(h);
+  return Status::ok();
+}
+
+// Paired arithmetic against scalar unfused arithmetic on seeded inputs: [0] counts pixels
+// whose paired_sigma differs from the scalar sigma of rasterize.rs:236, [1] blur steps
+// acc + w x (the SSIM loss's accumulation) that differ. Both must be zero.
+__device__ __forceinline__ float diag_uniform(uint32_t i, uint32_t salt, float lo, float hi) {
+  uint32_t h = i * 0x9e3779b9u ^ salt;
+  h ^= h >> 16;
+  h *= 0x7feb352du;
+  h ^= h >> 15;
+  h *= 0x846ca68bu;
+  h ^= h >> 16;
+  return lo + (hi - lo) * (float)(h >> 8) * (1.0f / 16777216.0f);
+}
+
+__global__ void diag_pair_exact_kernel(uint32_t n, unsigned int* __restrict__ mism) {
+  unsigned int bad_sigma = 0, bad_blur = 0;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const float A = diag_uniform(i, 1u, 0.0f, 3.4f), B = diag_uniform(i, 2u, -1.7f, 1.7f);
+    const float C = diag_uniform(i, 3u, 0.0f, 3.4f), dx = diag_uniform(i, 4u, -48.0f, 48.0f);
+    const float dy0 = diag_uniform(i, 5u, -48.0f, 48.0f), dy1 = diag_uniform(i, 6u, -48.0f, 48.0f);
+    f2 adx, cdy, bdx;
+    float p0, p1;
+    f2_split(paired_sigma(f2_splat(A), f2_splat(B), f2_splat(C), f2_splat(dx), f2_make(dy0, dy1), &adx, &cdy, &bdx),
+             p0, p1);
+    const float dys[2] = {dy0, dy1}, ps[2] = {p0, p1};
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+      const float dy = dys[q];
+      const float s = __fadd_rn(__fmul_rn(0.5f, __fadd_rn(__fmul_rn(__fmul_rn(A, dx), dx), __fmul_rn(__fmul_rn(C, dy), dy))),
+                                __fmul_rn(__fmul_rn(B, dx), dy));
+      bad_sigma += !(ps[q] == s);
+    }
+    const float w = diag_uniform(i, 7u, 0.0f, 0.3f), acc0 = diag_uniform(i, 8u, -2.0f, 2.0f);
+    const float acc1 = diag_uniform(i, 9u, 0.0f, 1.5f), x0 = diag_uniform(i, 10u, -0.2f, 1.2f);
+    const float x1 = diag_uniform(i, 11u, 0.0f, 1.0f);
+    float b0, b1;
+    f2_split(f2_add(f2_make(acc0, acc1), f2_mul(f2_splat(w), f2_make(x0, x1))), b0, b1);
+    bad_blur += !(b0 == __fadd_rn(acc0, __fmul_rn(w, x0))) + !(b1 == __fadd_rn(acc1, __fmul_rn(w, x1)));
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    bad_sigma += __shfl_xor_sync(0xffffffffu, bad_sigma, o);
+    bad_blur += __shfl_xor_sync(0xffffffffu, bad_blur, o);
+  }
+  if ((threadIdx.x & 31) == 0 && (bad_sigma | bad_blur)) {
+    atomicAdd(&mism[0], bad_sigma);
+    atomicAdd(&mism[1], bad_blur);
+  }
+}
+
+Status launch_diag_pair_exact(Ctx* c, uint32_t n, uint32_t* out_host) {
+  unsigned int* d = nullptr;
+  SPLAT_TRY(arena_reserve(c, 8, (void**)&d));
+  SPLAT_CUDA(cudaMemsetAsync(d, 0, 8, c->stream));
+  diag_pair_exact_kernel<<<c->sm_count * 8, 256, 0, c->stream>>>(n, d);
+  c->launches.count++;
+  SPLAT_LAUNCHED("diag_pair_exact_kernel");
+  SPLAT_CUDA(cudaMemcpyAsync(out_host, d, 8, cudaMemcpyDeviceToHost, c->stream));
+  SPLAT_CUDA(cudaStreamSynchronize(c->stream));
   return Status::ok();
 }
 
@@ -741,10 +812,9 @@ __global__ void __launch_bounds__(TW * TH / 2, 768 / (TW * TH / 2)) raster_bwd_x
       const f2 mx = f2_make(exy.x, exy.y), my = f2_make(exy.z, exy.w);
       const f2 A = f2_make(eab.x, eab.y), B = f2_make(eab.z, eab.w);
       const f2 Cc = f2_make(eco.x, eco.y), op = f2_make(eco.z, eco.w);
-      // sigma = 0.5 (A dx dx + C dy dy) + B dx dy, operation for operation (rasterize.rs:236).
       const f2 dx = f2_sub(px, mx), dy = f2_sub(py, my);
-      const f2 adx = f2_mul(A, dx), cdy = f2_mul(Cc, dy), bdx = f2_mul(B, dx);
-      const f2 sigma = f2_add(f2_mul(half, f2_add(f2_mul(adx, dx), f2_mul(cdy, dy))), f2_mul(bdx, dy));
+      f2 adx, cdy, bdx;
+      const f2 sigma = paired_sigma(A, B, Cc, dx, dy, &adx, &cdy, &bdx);
       float s0, s1;
       f2_split(sigma, s0, s1);
       // The reference's range test (false for NaN, as there), then the alpha test by sigma.

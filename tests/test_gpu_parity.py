@@ -422,6 +422,16 @@ def test_fast_exp_bound_behind_backward_screening(ctx):
     assert 0.0 < out.value < 3e-6
 
 
+def test_paired_arithmetic_keeps_one_rounding_per_operation(ctx):
+    """The compositing backward computes sigma, and the SSIM loss its blur sums, on f32x2
+    pairs; the code generator would fuse a paired multiply into a following add. Over 4M
+    seeded inputs the paired sigma and blur steps equal the scalar unfused values."""
+    import ctypes as C
+    out = (C.c_uint32 * 2)()
+    G.check(ctx.lib.splat_diag_pair_exact(ctx.h, 1 << 22, out), ctx.h)
+    assert (out[0], out[1]) == (0, 0), (out[0], out[1])
+
+
 def _bf16_round_params(g):
     """Reference records with quaternion, log-scales and SH rounded to bf16 (nearest even),
     the values the BF16 render copy holds; means and opacity stay f32."""
