@@ -198,10 +198,12 @@ RASTER_BYTES_PER_ENTRY = 52        # sorted index (4) + record gather (48)
 # dram__bytes_read.sum + dram__bytes_write.sum per launch, ncu, default workload.
 NCU_DRAM_BYTES_1M = {("raster_bwd", 16, 16, 256, 1): int((197.05 + 17.84) * 1e6),
                      ("raster_fwd", 16, 16, 256, 1): int((82.84 + 20.76) * 1e6),
-                     ("raster_bwd", 16, 16, 256, 2): int((196.78 + 16.71) * 1e6),
-                     ("raster_fwd", 16, 16, 256, 2): int((83.03 + 20.03) * 1e6),
-                     ("raster_bwd", 16, 32, 256, 2): int((186.21 + 13.99) * 1e6),
-                     ("raster_fwd", 16, 32, 256, 2): int((74.59 + 16.94) * 1e6)}
+                     ("raster_bwd", 16, 16, 128, 2): int((196.84 + 17.58) * 1e6),
+                     ("raster_fwd", 16, 16, 128, 2): int((82.91 + 21.21) * 1e6),
+                     ("raster_bwd", 16, 16, 256, 2): int((196.72 + 16.80) * 1e6),
+                     ("raster_fwd", 16, 16, 256, 2): int((82.95 + 22.06) * 1e6),
+                     ("raster_bwd", 16, 32, 256, 2): int((185.54 + 13.20) * 1e6),
+                     ("raster_fwd", 16, 32, 256, 2): int((74.59 + 16.79) * 1e6)}
 RASTER_FWD_FLOP_PER_PAIR = 20
 RASTER_BWD_FLOP_PER_PAIR = 50
 RASTER_FWD_SFU_PER_PAIR = 1        # one exp

@@ -71,7 +71,7 @@ struct LaunchCounter {
 // rectangle to its 16-pixel tile rectangle first), so images match the 16x16 path.
 struct RasterConfig {
   uint32_t tile_w = kTile, tile_h = kTile, chunk = 256;
-  uint32_t ppl = 1;  // pixels per thread of the compositing backward (1 or 2)
+  uint32_t ppl = 2;  // pixels per thread of the compositing backward (1 or 2)
   bool operator==(const RasterConfig& o) const {
     return tile_w == o.tile_w && tile_h == o.tile_h && chunk == o.chunk && ppl == o.ppl;
   }

@@ -26,7 +26,7 @@ pytestmark = pytest.mark.gpu
 SHAPES = [(16, 16, 256), (16, 16, 128), (16, 16, 64), (16, 16, 32), (8, 8, 256), (8, 8, 128), (8, 8, 64),
           (8, 8, 32), (16, 32, 256), (16, 32, 128), (16, 32, 64), (16, 32, 32)]
 CANDS = [s + (1,) for s in SHAPES] + [s + (2,) for s in SHAPES]
-DEFAULT = (16, 16, 256, 1)
+DEFAULT = (16, 16, 256, 2)
 SIZE = (640, 480)
 
 
