@@ -405,7 +405,8 @@ SPLAT_API int splat_mlp_adam(splat_ctx* ctx, float* theta_dev, const float* grad
  * reference's and give its tile lists; 8x8 and 16x32 give other lists but identical
  * images, final transmittances and, up to summation order, gradients (each entry's pixel
  * rectangle is first narrowed to its 16-pixel tile rectangle). Chunk depth: entries
- * staged in shared memory per round, 32, 64, 128 or 256. Pixels per thread of the
+ * staged in shared memory per round, 32, 64, 128 or 256 (with 16-pixel-wide tiles it sets
+ * the backward's; their forward always stages 256). Pixels per thread of the
  * backward: 1 or 2 (a warp then covers 8x8 pixels). Default 16x16, 256, 2.
  *   splat_raster_candidates: writes the supported (tile_w, tile_h, chunk,
  *     pixels_per_thread) quadruples to out (4 values each; out may be NULL) and returns
