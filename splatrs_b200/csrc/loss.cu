@@ -166,11 +166,12 @@ __global__ void __launch_bounds__(kLossThreads) ssim_fwd_kernel(const float* __r
         const float sv = num / den;
         const float dn_dmx = 2.0f * my * n2 - 2.0f * my * n1;
         const float dd_dmx = 2.0f * mx * d2 - 2.0f * mx * d1;
-        const size_t idx = ((size_t)gy * width + gx) * 3 + ch;
-        const size_t npix3 = (size_t)width * height * 3;
-        dmaps[idx] = (dn_dmx * den - num * dd_dmx) / (den * den);
-        dmaps[npix3 + idx] = -num * d1 / (den * den);
-        dmaps[2 * npix3 + idx] = 2.0f * n1 / den;
+        // The partial maps are planar (map, channel, pixel), so that the backward's per-channel
+        // tile loads are contiguous.
+        const size_t pix = (size_t)gy * width + gx, npix = (size_t)width * height;
+        dmaps[(size_t)ch * npix + pix] = (dn_dmx * den - num * dd_dmx) / (den * den);
+        dmaps[(size_t)(3 + ch) * npix + pix] = -num * d1 / (den * den);
+        dmaps[(size_t)(6 + ch) * npix + pix] = 2.0f * n1 / den;
         const float2 xy = xy_tile[r + kHalo][c + kHalo];
         const float x = xy.x, y = xy.y;
         s_ssim += (double)sv;
@@ -244,10 +245,10 @@ __global__ void __launch_bounds__(kLossThreads) ssim_bwd_kernel(const float* __r
       const int gy = oy0 - kHalo + r, gx = ox0 - kHalo + c;
       float a = 0.0f, b = 0.0f, e = 0.0f;
       if (gx >= 0 && gx < (int)width && gy >= 0 && gy < (int)height) {
-        const size_t idx = ((size_t)gy * width + gx) * 3 + ch;
-        a = dmaps[idx];
-        b = dmaps[npix3 + idx];
-        e = dmaps[2 * npix3 + idx];
+        const size_t pix = (size_t)gy * width + gx, npix = (size_t)width * height;
+        a = dmaps[(size_t)ch * npix + pix];
+        b = dmaps[(size_t)(3 + ch) * npix + pix];
+        e = dmaps[(size_t)(6 + ch) * npix + pix];
       }
       sm01[r][c] = make_float2(a, b);
       sm2[r][c] = e;
