@@ -476,10 +476,11 @@ __device__ __forceinline__ float rcp_fast(float x) {
   return r;
 }
 
-// PPL pixels per thread (1 or 2): a warp owns an 8 x (4 PPL) sub-block, lane L the pixels
-// (L % 8, L / 8 + 4 q) of it for q < PPL. With two, a warp-wide reduction sums the
-// contributions of twice as many pixels. Register budgets: 64 per thread with one pixel
-// (32 warps per SM), 85 with two (24).
+// PPL pixels per thread in scalar arithmetic: a warp owns an 8 x (4 PPL) sub-block, lane L
+// the pixels (L % 8, L / 8 + 4 q) of it for q < PPL. It is launched with one pixel per
+// thread (64 registers, 32 warps per SM); two pixels per thread run as pairs in
+// raster_bwd_x2_kernel below, which replaced this kernel's PPL = 2 form (1.24-1.27 ms
+// against 0.91 ms on the render benchmark).
 template <int TW, int TH, int CH, int PPL>
 __global__ void __launch_bounds__(TW * TH / PPL, (PPL == 1 ? 1024 : 768) / (TW * TH / PPL)) raster_bwd_kernel(
     const float4* __restrict__ rec, const uint32_t* __restrict__ gauss, const uint2* __restrict__ ranges,
